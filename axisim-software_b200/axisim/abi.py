@@ -1,0 +1,354 @@
+"""ctypes binding of libaxisim_b200.so (the C ABI declared in include/axisim_b200.h).
+
+This is the Python mirror of the reference's Solver verbs (set mesh / bcs /
+config, solve, continue, stop, read solutions). The compute path is the CUDA
+library; there is no fallback: loading fails loudly when the library or a GPU
+is missing.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "libaxisim_b200.so")
+
+_i32p = C.POINTER(C.c_int32)
+_f64p = C.POINTER(C.c_double)
+_u8p = C.POINTER(C.c_uint8)
+
+OK, E_ARG, E_CONFIG, E_MESH, E_CUDA, E_DIVERGED, E_STOPPED, E_STATE, E_TIMEOUT = range(9)
+STATUS_NAMES = {0: "OK", 1: "E_ARG", 2: "E_CONFIG", 3: "E_MESH", 4: "E_CUDA", 5: "E_DIVERGED",
+                6: "E_STOPPED", 7: "E_STATE", 8: "E_TIMEOUT"}
+PREC_FP64, PREC_MIXED = 0, 1
+
+# Every entry point include/axisim_b200.h declares.
+EXPORTS = [
+    "axisim_abi_version", "axisim_create", "axisim_destroy", "axisim_last_error", "axisim_set_log",
+    "axisim_set_mesh", "axisim_set_bc", "axisim_set_config", "axisim_set_fluid", "axisim_set_precision",
+    "axisim_solve", "axisim_can_continue", "axisim_request_stop", "axisim_get_field", "axisim_set_field",
+    "axisim_mg_levels", "axisim_mg_level_maps", "axisim_coloring", "axisim_multiblock_build",
+    "axisim_mesh_sizes", "axisim_mesh_view", "axisim_mesh_free", "axisim_resolve_bc",
+]
+
+
+class MeshPacked(C.Structure):
+    _fields_ = [("nCells", C.c_int32), ("nFaces", C.c_int32),
+                ("faceOwner", _i32p), ("faceNeighbor", _i32p),
+                ("faceNormalZ", _f64p), ("faceNormalR", _f64p),
+                ("faceCenterZ", _f64p), ("faceCenterR", _f64p), ("faceArea", _f64p),
+                ("faceBoundaryGroupID", _i32p),
+                ("cellCenterZ", _f64p), ("cellCenterR", _f64p),
+                ("cellArea2D", _f64p), ("cellVolume", _f64p),
+                ("cellFaceStart", _i32p), ("cellFaceIDs", _i32p)]
+
+
+class BCField(C.Structure):
+    _fields_ = [("nGroups", C.c_int32), ("typeByGroup", _u8p), ("boundaryTypeByGroup", _u8p),
+                ("valueByGroup", _f64p), ("lengthByGroup", _f64p), ("pulsatileByGroup", _u8p),
+                ("amplitudeByGroup", _f64p), ("frequencyByGroup", _f64p)]
+
+
+class ConfigSolver(C.Structure):
+    _fields_ = [("velocitySolver", C.c_uint8), ("convectionScheme", C.c_uint8), ("gradientScheme", C.c_uint8),
+                ("type", C.c_uint8), ("timeScheme", C.c_uint8), ("pad_", C.c_uint8 * 3),
+                ("linearMaxIter", C.c_int32), ("useMultigrid", C.c_uint8), ("addConvectionTerm", C.c_uint8),
+                ("transient", C.c_uint8), ("useNonOrthCorrector", C.c_uint8), ("dt", C.c_double),
+                ("tEnd", C.c_double), ("saveKeyFrameIter", C.c_int32), ("pad2_", C.c_int32)]
+
+
+class ConfigSimple(C.Structure):
+    _fields_ = [("maxIter", C.c_int32), ("checkConv", C.c_int32), ("momTol", C.c_double), ("ppTol", C.c_double)]
+
+
+class ConfigMultigrid(C.Structure):
+    _fields_ = [("maxIter", C.c_int32), ("weight", C.c_double), ("linearSweep", C.c_int32),
+                ("linearPreSweep", C.c_int32), ("linearPostSweep", C.c_int32)]
+
+
+class ConfigResidual(C.Structure):
+    _fields_ = [("type", C.c_uint8), ("normType", C.c_uint8), ("scaleType", C.c_uint8), ("enabled", C.c_uint8),
+                ("tol", C.c_double)]
+
+
+class Fluid(C.Structure):
+    _fields_ = [("rho", C.c_double), ("mu", C.c_double), ("cp", C.c_double), ("k", C.c_double), ("D", C.c_double)]
+
+
+class Result(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("totalIterations", C.c_int32), ("converged", C.c_int32),
+                ("timeSteps", C.c_int32), ("residual", C.c_double * 3), ("solveMs", C.c_double)]
+
+
+class BlockSpec(C.Structure):
+    _fields_ = [("z0", C.c_double), ("r0", C.c_double),
+                ("axialLength", C.c_double), ("axialCells", C.c_int32), ("axialGrading", C.c_int32),
+                ("axialCoef", C.c_double),
+                ("radialLength", C.c_double), ("radialCells", C.c_int32), ("radialGrading", C.c_int32),
+                ("radialCoef", C.c_double), ("edgeGroup", C.c_int32 * 4)]
+
+
+RESIDUAL_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int32, _f64p)
+LOG_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_char_p)
+
+
+def build(force=False):
+    """Compile the library in-tree (nvcc for sm_100a); returns its path."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", PKG_DIR], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {PKG_DIR}`")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        sig = {
+            "axisim_abi_version": (C.c_int, []),
+            "axisim_create": (C.c_int, [C.POINTER(Fluid), C.POINTER(vp)]),
+            "axisim_destroy": (C.c_int, [vp]),
+            "axisim_last_error": (C.c_char_p, [vp]),
+            "axisim_set_log": (C.c_int, [vp, LOG_FN, RESIDUAL_FN, vp]),
+            "axisim_set_mesh": (C.c_int, [vp, C.POINTER(MeshPacked)]),
+            "axisim_set_bc": (C.c_int, [vp, C.c_int32, C.POINTER(BCField)]),
+            "axisim_set_config": (C.c_int, [vp, C.POINTER(ConfigSolver), C.POINTER(ConfigSimple),
+                                            C.POINTER(ConfigMultigrid), C.POINTER(ConfigResidual),
+                                            C.c_double, C.c_double]),
+            "axisim_set_fluid": (C.c_int, [vp, C.POINTER(Fluid)]),
+            "axisim_set_precision": (C.c_int, [vp, C.c_int32]),
+            "axisim_solve": (C.c_int, [vp, C.c_int32, C.POINTER(Result)]),
+            "axisim_can_continue": (C.c_int, [vp, C.c_char_p, C.c_size_t]),
+            "axisim_request_stop": (C.c_int, [vp]),
+            "axisim_get_field": (C.c_int64, [vp, C.c_char_p, _f64p, C.c_size_t]),
+            "axisim_set_field": (C.c_int64, [vp, C.c_char_p, _f64p, C.c_size_t]),
+            "axisim_mg_levels": (C.c_int, [vp, _i32p, C.c_int32]),
+            "axisim_mg_level_maps": (C.c_int64, [vp, C.c_int32, vp, vp, vp, vp]),
+            "axisim_coloring": (C.c_int, [vp, _i32p, C.c_size_t]),
+            "axisim_multiblock_build": (C.c_int, [C.c_int32, C.POINTER(BlockSpec), C.c_double, C.c_int32,
+                                                  C.POINTER(vp), _i32p]),
+            "axisim_mesh_sizes": (C.c_int, [vp, _i32p, _i32p, _i32p]),
+            "axisim_mesh_view": (C.c_int, [vp, C.POINTER(MeshPacked)]),
+            "axisim_mesh_free": (C.c_int, [vp]),
+            "axisim_resolve_bc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, _u8p,
+                                            _f64p, _u8p]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class AxisimError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+# ---------------------------------------------------------------- host prep
+MESH_KEYS = ["faceOwner", "faceNeighbor", "faceNormalZ", "faceNormalR", "faceCenterZ", "faceCenterR",
+             "faceArea", "faceBoundaryGroupID", "cellCenterZ", "cellCenterR", "cellArea2D", "cellVolume",
+             "cellFaceStart", "cellFaceIDs"]
+
+
+def multiblock(blocks, tol=1e-9, default_group=-1):
+    """Pack a multiblock mesh with the library's C++ packer (structs/multiblock.h
+    semantics). Returns a dict of numpy arrays (FVMeshHostPacked layout)."""
+    L = lib()
+    arr = (BlockSpec * len(blocks))()
+    for i, b in enumerate(blocks):
+        ax, rd = b["axial"], b["radial"]
+        arr[i] = BlockSpec(b["z0"], b["r0"], ax[0], ax[1], ax[2], ax[3], rd[0], rd[1], rd[2], rd[3],
+                           (C.c_int32 * 4)(*b["edge_group"]))
+    h = C.c_void_p()
+    seam = C.c_int32(0)
+    st = L.axisim_multiblock_build(len(blocks), arr, tol, default_group, C.byref(h), C.byref(seam))
+    if st != OK:
+        raise AxisimError(st, "multiblock build failed")
+    v = MeshPacked()
+    L.axisim_mesh_view(h, C.byref(v))
+    n, f = v.nCells, v.nFaces
+    r = v.cellFaceStart[n]
+    m = {"nCells": n, "nFaces": f, "status": seam.value}
+    sizes = dict(faceOwner=f, faceNeighbor=f, faceNormalZ=f, faceNormalR=f, faceCenterZ=f, faceCenterR=f,
+                 faceArea=f, faceBoundaryGroupID=f, cellCenterZ=n, cellCenterR=n, cellArea2D=n, cellVolume=n,
+                 cellFaceStart=n + 1, cellFaceIDs=r)
+    for k in MESH_KEYS:
+        ptr = getattr(v, k)
+        m[k] = np.ctypeslib.as_array(ptr, shape=(sizes[k],)).copy()
+    L.axisim_mesh_free(h)
+    return m
+
+
+def resolve_bc(boundary_type, variable, user=None):
+    """BoundaryDefaults::getEffectiveBC through the library: returns (type, value, pulsatile)."""
+    t = C.c_uint8()
+    v = C.c_double()
+    p = C.c_uint8()
+    has = 0 if user is None else 1
+    ut, uv = (0, 0.0) if user is None else (user[0], user[1])
+    st = lib().axisim_resolve_bc(boundary_type, variable, has, ut, uv, C.byref(t), C.byref(v), C.byref(p))
+    if st != OK:
+        raise AxisimError(st, "resolve_bc failed")
+    return t.value, v.value, p.value
+
+
+def mesh_struct(m):
+    keep = []
+
+    def P(k, t, dt):
+        a = np.ascontiguousarray(m[k], dtype=dt)
+        keep.append(a)
+        return a.ctypes.data_as(t)
+    s = MeshPacked(m["nCells"], m["nFaces"], P("faceOwner", _i32p, np.int32), P("faceNeighbor", _i32p, np.int32),
+                   P("faceNormalZ", _f64p, np.float64), P("faceNormalR", _f64p, np.float64),
+                   P("faceCenterZ", _f64p, np.float64), P("faceCenterR", _f64p, np.float64),
+                   P("faceArea", _f64p, np.float64), P("faceBoundaryGroupID", _i32p, np.int32),
+                   P("cellCenterZ", _f64p, np.float64), P("cellCenterR", _f64p, np.float64),
+                   P("cellArea2D", _f64p, np.float64), P("cellVolume", _f64p, np.float64),
+                   P("cellFaceStart", _i32p, np.int32), P("cellFaceIDs", _i32p, np.int32))
+    return s, keep
+
+
+def bc_struct(bc):
+    keep = []
+
+    def P(k, t, dt):
+        if k not in bc or bc[k] is None:
+            return None
+        a = np.ascontiguousarray(bc[k], dtype=dt)
+        keep.append(a)
+        return a.ctypes.data_as(t)
+    s = BCField(len(bc["type"]), P("type", _u8p, np.uint8), P("btype", _u8p, np.uint8),
+                P("value", _f64p, np.float64), P("length", _f64p, np.float64), P("puls", _u8p, np.uint8),
+                P("amp", _f64p, np.float64), P("freq", _f64p, np.float64))
+    return s, keep
+
+
+def settings_structs(s):
+    cs = ConfigSolver()
+    cs.velocitySolver = 0
+    cs.convectionScheme = s["convectionScheme"]
+    cs.gradientScheme = s["gradientScheme"]
+    cs.type = s["linearType"]
+    cs.timeScheme = s["timeScheme"]
+    cs.linearMaxIter = s["linearMaxIter"]
+    cs.useMultigrid = s["useMultigrid"]
+    cs.addConvectionTerm = s["addConvectionTerm"]
+    cs.transient = s["transient"]
+    cs.useNonOrthCorrector = s["useNonOrthCorrector"]
+    cs.dt = s["dt"]
+    cs.tEnd = s["tEnd"]
+    cs.saveKeyFrameIter = 2
+    sim = ConfigSimple(s["maxIter"], s["checkConv"], 1e-8, 1e-5)
+    mg = ConfigMultigrid(s["mgMaxIter"], s["mgWeight"], s["mgLinearSweep"], s["mgPreSweep"], s["mgPostSweep"])
+    res = (ConfigResidual * 3)()
+    for i in range(3):
+        res[i] = ConfigResidual(0, s["resNorm"][i], s["resScale"][i], s["resEnabled"][i], s["resTol"][i])
+    fluid = Fluid(s["rho"], s["mu"], 4180.0, 0.6, 3.0277e-9)
+    return cs, sim, mg, res, fluid
+
+
+class Solver:
+    """One solver handle (Solver in the reference): case in, fields out."""
+
+    def __init__(self, mesh, bcs, settings, precision=PREC_FP64):
+        L = lib()
+        cs, sim, mg, res, fluid = settings_structs(settings)
+        self.h = C.c_void_p()
+        st = L.axisim_create(C.byref(fluid), C.byref(self.h))
+        if st != OK:
+            raise AxisimError(st, "axisim_create failed (no CUDA device?)")
+        self.mesh = mesh
+        self.settings = dict(settings)
+        self._residual_log = []
+        ms, keep = mesh_struct(mesh)
+        self._check(L.axisim_set_mesh(self.h, C.byref(ms)))
+        for var, key in enumerate(("u", "v", "p")):
+            b, keep2 = bc_struct(bcs[key])
+            self._check(L.axisim_set_bc(self.h, var, C.byref(b)))
+        self._check(L.axisim_set_config(self.h, C.byref(cs), C.byref(sim), C.byref(mg), res,
+                                        settings["alphaU"], settings["alphaP"]))
+        if precision != PREC_FP64:
+            self._check(L.axisim_set_precision(self.h, precision))
+
+    def _check(self, st):
+        if st != OK:
+            raise AxisimError(st, lib().axisim_last_error(self.h).decode())
+        return st
+
+    def solve(self, cont=False, allow=(OK,)):
+        r = Result()
+        st = lib().axisim_solve(self.h, 1 if cont else 0, C.byref(r))
+        if st not in allow:
+            self._check(st)
+        return dict(status=st, iterations=r.iterations, total=r.totalIterations, converged=bool(r.converged),
+                    steps=r.timeSteps, residual=list(r.residual), ms=r.solveMs)
+
+    def get(self, name):
+        n = max(self.mesh["nCells"], self.mesh["nFaces"], len(self.mesh["cellFaceIDs"]))
+        out = np.zeros(n)
+        k = lib().axisim_get_field(self.h, name.encode(), out.ctypes.data_as(_f64p), n)
+        if k < 0:
+            self._check(int(-k))
+        return out[:k].copy()
+
+    def set(self, name, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        k = lib().axisim_set_field(self.h, name.encode(), a.ctypes.data_as(_f64p), a.size)
+        if k < 0:
+            self._check(int(-k))
+
+    def can_continue(self):
+        buf = C.create_string_buffer(256)
+        r = lib().axisim_can_continue(self.h, buf, 256)
+        return r == 1, buf.value.decode()
+
+    def request_stop(self):
+        return lib().axisim_request_stop(self.h)
+
+    def mg_levels(self):
+        cells = np.zeros(64, np.int32)
+        n = lib().axisim_mg_levels(self.h, cells.ctypes.data_as(_i32p), 64)
+        if n < 0:
+            self._check(-n)
+        return cells[:n].copy()
+
+    def mg_level_maps(self, level):
+        cells = self.mg_levels()
+        S = int(lib().axisim_mg_level_maps(self.h, level - 1, None, None, None, None)) if level > 0 \
+            else len(self.mesh["cellFaceIDs"])
+        Sc = int(lib().axisim_mg_level_maps(self.h, level, None, None, None, None))
+        c2c = np.zeros(cells[level], np.int32)
+        f2c = np.zeros(S, np.int32)
+        cfs = np.zeros(cells[level + 1] + 1, np.int32)
+        cfn = np.zeros(max(Sc, 1), np.int32)
+        lib().axisim_mg_level_maps(self.h, level, c2c.ctypes.data_as(C.c_void_p), f2c.ctypes.data_as(C.c_void_p),
+                                   cfs.ctypes.data_as(C.c_void_p), cfn.ctypes.data_as(C.c_void_p))
+        return c2c, f2c, cfs, cfn[:Sc]
+
+    def coloring(self):
+        out = np.zeros(self.mesh["nCells"], np.int32)
+        nc = lib().axisim_coloring(self.h, out.ctypes.data_as(_i32p), out.size)
+        if nc < 0:
+            self._check(-nc)
+        return out, nc
+
+    def close(self):
+        if self.h:
+            lib().axisim_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

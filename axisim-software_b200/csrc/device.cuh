@@ -1,0 +1,110 @@
+// device.cuh -- device-side data layout of the B200 SIMPLE solver.
+//
+// Layout in HBM (structure of arrays):
+//   * faces:  owner, neighbor, group, normal, centre, area and the precomputed
+//             geometry (invDPN, wP, dPB, length2D, lsqW) as one array each;
+//   * cells:  centre, volume, invA2D, LSQ inverse matrix, fields;
+//   * slots:  a cell's faces in the reference's CSR order, stored as an ELL
+//             block [W][N] (slot j of cell n at j*N + n), so the per-cell face
+//             loops and the smoother sweeps read coalesced columns. W is the
+//             largest face count of any cell (4 on quads, 3 on triangles);
+//             unused slots carry face -1 and neighbour -1.
+// The momentum off-diagonals are identical for u and v in the reference
+// (diffusion -mu A/d plus min(F,0) on the same faces), so one AF block serves
+// both momentum systems.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace axisim {
+
+constexpr int kMaxHist = 128;   // residual history ring (>= largest graph batch)
+
+struct MeshDev {
+    int N = 0, F = 0, W = 0;
+    const int32_t* owner = nullptr;
+    const int32_t* neighbor = nullptr;
+    const int32_t* group = nullptr;
+    const double* nZ = nullptr;
+    const double* nR = nullptr;
+    const double* fcZ = nullptr;
+    const double* fcR = nullptr;
+    const double* area = nullptr;
+    const double* invDPN = nullptr;
+    const double* wP = nullptr;
+    const double* dPB = nullptr;
+    const double* length2D = nullptr;
+    const double* lsqWZ = nullptr;
+    const double* lsqWR = nullptr;
+    const double* ccZ = nullptr;
+    const double* ccR = nullptr;
+    const double* vol = nullptr;
+    const double* invA2D = nullptr;
+    const double* lsqIZZ = nullptr;
+    const double* lsqIZR = nullptr;
+    const double* lsqIRR = nullptr;
+    const int32_t* sface = nullptr;  // [W][N]
+    const int32_t* snb = nullptr;    // [W][N]
+};
+
+struct BCDev {
+    int nGroups = 0;
+    const uint8_t* type = nullptr;
+    const double* value = nullptr;
+    const double* length = nullptr;
+};
+
+// Control block: one per solver, in device memory. Kernels of an iteration
+// return at entry once `done` is set, so a captured iteration graph can be
+// replayed past convergence without changing the result.
+struct Ctl {
+    int done;             // 0 running, 1 converged, 2 stopped, 3 iteration budget, 4 non-finite residual
+    int k;                // SIMPLE iteration within the current time step
+    int currentIteration; // run-global iteration counter (continues across continue runs)
+    int maxIter;
+    int checkConv;
+    int transient;
+    int bdf2;             // BDF2 active in this time step
+    int converged;        // result of the last check
+    int checked;          // a residual check ran this iteration
+    int itersThisCall;
+    int pad0, pad1;
+    double resVal[3];     // U, V, Continuity
+    double scaleVal[3];
+    double tol[3];
+    int resNorm[3];
+    int resScale[3];
+    int resEnabled[3];
+    int histCount;        // entries written since the host last drained
+    double hist[kMaxHist][4];  // iteration, U, V, Continuity
+};
+
+struct MomentumArgs {
+    const double* mDot;
+    const double* u;
+    const double* v;
+    const double* gUZ;
+    const double* gUR;
+    const double* gVZ;
+    const double* gVR;
+    const double* gPZ;
+    const double* gPR;
+    const double* uOld;
+    const double* vOld;
+    const double* uOld2;
+    const double* vOld2;
+    double* AF;     // [W][N] shared by u and v
+    double* ACu;
+    double* ACv;
+    double* bu;
+    double* bv;
+    double* invACu;
+    double* invACv;
+    double* DU;
+    double* DV;
+    double mu, rho, dt, alpha;
+    int conv, scheme, nonOrtho, transient;
+};
+
+}  // namespace axisim

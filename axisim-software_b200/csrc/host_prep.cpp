@@ -1,0 +1,430 @@
+// host_prep.cpp -- multiblock packer, agglomeration hierarchy, colouring and
+// boundary defaults (host side, once per solve). Behaviour follows the
+// reference files cited per routine; the code is this project's own.
+#include "host_prep.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+namespace axisim {
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+struct Node {
+    double z, r;
+};
+
+struct Block {
+    int nr = 0, nz = 0, offset = 0;
+    std::vector<Node> nodes;  // (nr+1)*(nz+1), row I (radial), column J (axial)
+    int edgeGroup[4] = {-1, -1, -1, -1};
+    const Node& at(int I, int J) const { return nodes[(size_t)I * (nz + 1) + J]; }
+    int cell(int i, int j) const { return offset + i * nz + j; }
+};
+
+// Cell-boundary coordinates of one zone (multiblock.h:59-80).
+std::vector<double> zoneFaces(double length, int n, int grading, double coef, double start) {
+    std::vector<double> d((size_t)n, length / n);
+    if (grading == 1 && n > 1 && coef > 0.0 && coef != 1.0) {
+        const double d0 = length * (coef - 1.0) / (std::pow(coef, n) - 1.0);
+        for (int k = 0; k < n; k++) d[(size_t)k] = d0 * std::pow(coef, k);
+    }
+    std::vector<double> f;
+    f.reserve((size_t)n + 1);
+    double x = start;
+    f.push_back(x);
+    for (int k = 0; k < n; k++) {
+        x += d[(size_t)k];
+        f.push_back(x);
+    }
+    return f;
+}
+
+// Edge numbering West, East, South, North (multiblock.h:85).
+void edgeEnds(const Block& b, int e, Node& s, Node& t) {
+    switch (e) {
+        case 0: s = b.at(0, 0); t = b.at(b.nr, 0); break;
+        case 1: s = b.at(0, b.nz); t = b.at(b.nr, b.nz); break;
+        case 2: s = b.at(0, 0); t = b.at(0, b.nz); break;
+        default: s = b.at(b.nr, 0); t = b.at(b.nr, b.nz); break;
+    }
+}
+int edgeLen(const Block& b, int e) { return e <= 1 ? b.nr : b.nz; }
+int edgeLocalCell(const Block& b, int e, int k) {
+    switch (e) {
+        case 0: return k * b.nz;
+        case 1: return k * b.nz + b.nz - 1;
+        case 2: return k;
+        default: return (b.nr - 1) * b.nz + k;
+    }
+}
+void edgeSegment(const Block& b, int e, int k, Node& a, Node& c) {
+    switch (e) {
+        case 0: a = b.at(k, 0); c = b.at(k + 1, 0); break;
+        case 1: a = b.at(k, b.nz); c = b.at(k + 1, b.nz); break;
+        case 2: a = b.at(0, k); c = b.at(0, k + 1); break;
+        default: a = b.at(b.nr, k); c = b.at(b.nr, k + 1); break;
+    }
+}
+
+// Shoelace centroid and area of a quad (multiblock.h:272-295).
+void quadGeometry(const Node (&p)[4], double& cz, double& cr, double& area) {
+    double A = 0.0, Cz = 0.0, Cr = 0.0;
+    for (int k = 0; k < 4; k++) {
+        const Node& a = p[k];
+        const Node& b = p[(k + 1) & 3];
+        const double cross = a.z * b.r - b.z * a.r;
+        A += cross;
+        Cz += (a.z + b.z) * cross;
+        Cr += (a.r + b.r) * cross;
+    }
+    A *= 0.5;
+    if (std::fabs(A) < 1e-30) {
+        cz = 0.25 * (p[0].z + p[1].z + p[2].z + p[3].z);
+        cr = 0.25 * (p[0].r + p[1].r + p[2].r + p[3].r);
+        area = 0.0;
+        return;
+    }
+    cz = Cz / (6.0 * A);
+    cr = Cr / (6.0 * A);
+    area = std::fabs(A);
+}
+
+}  // namespace
+
+PackedMesh buildMultiblock(const std::vector<BlockSpec>& spec, double tol, int defaultGroup, int& seamStatus) {
+    seamStatus = 0;
+    std::vector<Block> blocks(spec.size());
+    int total = 0;
+    for (size_t bi = 0; bi < spec.size(); bi++) {
+        const BlockSpec& s = spec[bi];
+        const std::vector<double> zf = zoneFaces(s.axialLength, s.axialCells, s.axialGrading, s.axialCoef, s.z0);
+        const std::vector<double> rf = zoneFaces(s.radialLength, s.radialCells, s.radialGrading, s.radialCoef, s.r0);
+        Block& b = blocks[bi];
+        b.nz = s.axialCells;
+        b.nr = s.radialCells;
+        b.nodes.resize((size_t)(b.nr + 1) * (b.nz + 1));
+        for (int I = 0; I <= b.nr; I++)
+            for (int J = 0; J <= b.nz; J++) b.nodes[(size_t)I * (b.nz + 1) + J] = Node{zf[(size_t)J], rf[(size_t)I]};
+        for (int e = 0; e < 4; e++) b.edgeGroup[e] = s.edgeGroup[e];
+        b.offset = total;
+        total += b.nr * b.nz;
+    }
+
+    // Conformal interfaces: fully coincident block edges (multiblock.h:220-251).
+    struct Seam {
+        int a, b, ea, eb;
+        bool reversed;
+    };
+    std::vector<Seam> seams;
+    const double tol2 = tol * tol;
+    auto same = [&](const Node& p, const Node& q) {
+        const double dz = p.z - q.z, dr = p.r - q.r;
+        return dz * dz + dr * dr <= tol2;
+    };
+    bool bad = false;
+    for (int a = 0; a < (int)blocks.size() && !bad; a++)
+        for (int b = a + 1; b < (int)blocks.size() && !bad; b++)
+            for (int ea = 0; ea < 4 && !bad; ea++)
+                for (int eb = 0; eb < 4; eb++) {
+                    Node as, ae, bs, be;
+                    edgeEnds(blocks[(size_t)a], ea, as, ae);
+                    edgeEnds(blocks[(size_t)b], eb, bs, be);
+                    const bool aligned = same(as, bs) && same(ae, be);
+                    const bool reversed = same(as, be) && same(ae, bs);
+                    if (!aligned && !reversed) continue;
+                    if (edgeLen(blocks[(size_t)a], ea) != edgeLen(blocks[(size_t)b], eb)) {
+                        bad = true;
+                        break;
+                    }
+                    seams.push_back(Seam{a, b, ea, eb, reversed});
+                }
+    if (bad) {
+        seamStatus = 1;
+        seams.clear();
+    }
+
+    PackedMesh m;
+    m.nCells = total;
+    m.cellCenterZ.assign((size_t)total, 0.0);
+    m.cellCenterR.assign((size_t)total, 0.0);
+    m.cellArea2D.assign((size_t)total, 0.0);
+    m.cellVolume.assign((size_t)total, 0.0);
+    for (const Block& b : blocks)
+        for (int i = 0; i < b.nr; i++)
+            for (int j = 0; j < b.nz; j++) {
+                const Node q[4] = {b.at(i, j), b.at(i, j + 1), b.at(i + 1, j + 1), b.at(i + 1, j)};
+                double cz, cr, area;
+                quadGeometry(q, cz, cr, area);
+                const size_t g = (size_t)b.cell(i, j);
+                m.cellCenterZ[g] = cz;
+                m.cellCenterR[g] = cr;
+                m.cellArea2D[g] = area;
+                m.cellVolume[g] = 2.0 * kPi * std::fabs(cr) * area;
+            }
+
+    std::vector<std::vector<int32_t>> cellFaces((size_t)total);
+    auto emit = [&](int owner, int nb, const Node& a, const Node& c, int gid) {
+        const int fid = (int)m.faceOwner.size();
+        const double dz = c.z - a.z, dr = c.r - a.r;
+        const double L = std::sqrt(dz * dz + dr * dr);
+        const double fz = 0.5 * (a.z + c.z), fr = 0.5 * (a.r + c.r);
+        double nz = (L > 0.0) ? dr / L : 0.0;
+        double nr = (L > 0.0) ? -dz / L : 0.0;
+        double tz, tr;
+        if (nb >= 0) {
+            tz = m.cellCenterZ[(size_t)nb] - m.cellCenterZ[(size_t)owner];
+            tr = m.cellCenterR[(size_t)nb] - m.cellCenterR[(size_t)owner];
+        } else {
+            tz = fz - m.cellCenterZ[(size_t)owner];
+            tr = fr - m.cellCenterR[(size_t)owner];
+        }
+        if (nz * tz + nr * tr < 0.0) {
+            nz = -nz;
+            nr = -nr;
+        }
+        m.faceOwner.push_back(owner);
+        m.faceNeighbor.push_back(nb);
+        m.faceNormalZ.push_back(nz);
+        m.faceNormalR.push_back(nr);
+        m.faceCenterZ.push_back(fz);
+        m.faceCenterR.push_back(fr);
+        m.faceArea.push_back(2.0 * kPi * std::fabs(fr) * L);
+        m.faceBoundaryGroupID.push_back(gid);
+        cellFaces[(size_t)owner].push_back(fid);
+        if (nb >= 0) cellFaces[(size_t)nb].push_back(fid);
+    };
+    // Faces inside blocks: east then north of each cell (multiblock.h:382-394).
+    for (const Block& b : blocks)
+        for (int i = 0; i < b.nr; i++)
+            for (int j = 0; j < b.nz; j++) {
+                const int owner = b.cell(i, j);
+                if (j + 1 < b.nz) emit(owner, b.cell(i, j + 1), b.at(i, j + 1), b.at(i + 1, j + 1), -1);
+                if (i + 1 < b.nr) emit(owner, b.cell(i + 1, j), b.at(i + 1, j), b.at(i + 1, j + 1), -1);
+            }
+    // Interface faces (multiblock.h:397-414).
+    std::vector<char> claimed(blocks.size() * 4, 0);
+    for (const Seam& s : seams) {
+        claimed[(size_t)s.a * 4 + s.ea] = 1;
+        claimed[(size_t)s.b * 4 + s.eb] = 1;
+        const Block& A = blocks[(size_t)s.a];
+        const Block& B = blocks[(size_t)s.b];
+        const int count = edgeLen(A, s.ea);
+        for (int k = 0; k < count; k++) {
+            Node n0, n1;
+            edgeSegment(A, s.ea, k, n0, n1);
+            const int kb = s.reversed ? (count - 1 - k) : k;
+            emit(A.offset + edgeLocalCell(A, s.ea, k), B.offset + edgeLocalCell(B, s.eb, kb), n0, n1, -1);
+        }
+    }
+    // External faces (multiblock.h:417-432).
+    for (size_t bi = 0; bi < blocks.size(); bi++) {
+        const Block& b = blocks[bi];
+        for (int e = 0; e < 4; e++) {
+            if (claimed[bi * 4 + (size_t)e]) continue;
+            const int gid = b.edgeGroup[e] >= 0 ? b.edgeGroup[e] : defaultGroup;
+            const int count = edgeLen(b, e);
+            for (int k = 0; k < count; k++) {
+                Node n0, n1;
+                edgeSegment(b, e, k, n0, n1);
+                emit(b.offset + edgeLocalCell(b, e, k), -1, n0, n1, gid);
+            }
+        }
+    }
+    m.nFaces = (int)m.faceOwner.size();
+    m.cellFaceStart.assign((size_t)total + 1, 0);
+    for (int c = 0; c < total; c++) m.cellFaceStart[(size_t)c + 1] = m.cellFaceStart[(size_t)c] + (int)cellFaces[(size_t)c].size();
+    m.cellFaceIDs.reserve((size_t)m.cellFaceStart[(size_t)total]);
+    for (int c = 0; c < total; c++)
+        m.cellFaceIDs.insert(m.cellFaceIDs.end(), cellFaces[(size_t)c].begin(), cellFaces[(size_t)c].end());
+    return m;
+}
+
+GridLevel finestLevel(int nCells, int nFaces, const int32_t* cfs, const int32_t* cfi, const int32_t* owner,
+                      const int32_t* neighbor) {
+    GridLevel g;
+    g.nCells = nCells;
+    g.faceStart.assign(cfs, cfs + nCells + 1);
+    g.faceNeighbor.resize((size_t)cfs[nCells]);
+    for (int c = 0; c < nCells; c++)
+        for (int k = cfs[c]; k < cfs[c + 1]; k++) {
+            const int f = cfi[k];
+            int nb = -1;
+            if (f >= 0 && f < nFaces) {
+                if (owner[f] == c) nb = neighbor[f];
+                else if (neighbor[f] == c) nb = owner[f];
+            }
+            g.faceNeighbor[(size_t)k] = nb;
+        }
+    return g;
+}
+
+namespace {
+
+// Greedy breadth-first aggregates of up to four cells, singletons merged into
+// their smallest neighbouring aggregate, ids compacted by first appearance
+// (multigrid.cu:79-194).
+int aggregate(const GridLevel& fine, std::vector<int32_t>& c2c) {
+    constexpr int target = 4;
+    const int N = fine.nCells;
+    c2c.assign((size_t)N, -1);
+    int nAgg = 0;
+    int members[target];
+    for (int n = 0; n < N; n++) {
+        if (c2c[(size_t)n] >= 0) continue;
+        const int c = nAgg++;
+        c2c[(size_t)n] = c;
+        int count = 0;
+        members[count++] = n;
+        for (int m = 0; m < count && count < target; m++) {
+            const int cell = members[m];
+            for (int k = fine.faceStart[(size_t)cell]; k < fine.faceStart[(size_t)cell + 1] && count < target; k++) {
+                const int nb = fine.faceNeighbor[(size_t)k];
+                if (nb < 0 || c2c[(size_t)nb] >= 0) continue;
+                c2c[(size_t)nb] = c;
+                members[count++] = nb;
+            }
+        }
+    }
+    std::vector<int> size((size_t)nAgg, 0);
+    for (int n = 0; n < N; n++) size[(size_t)c2c[(size_t)n]]++;
+    for (int n = 0; n < N; n++) {
+        const int c = c2c[(size_t)n];
+        if (size[(size_t)c] != 1) continue;
+        int best = -1, bestSize = 0;
+        for (int k = fine.faceStart[(size_t)n]; k < fine.faceStart[(size_t)n + 1]; k++) {
+            const int nb = fine.faceNeighbor[(size_t)k];
+            if (nb < 0) continue;
+            const int cn = c2c[(size_t)nb];
+            if (cn == c) continue;
+            if (best < 0 || size[(size_t)cn] < bestSize) {
+                best = cn;
+                bestSize = size[(size_t)cn];
+            }
+        }
+        if (best < 0) continue;
+        c2c[(size_t)n] = best;
+        size[(size_t)best]++;
+        size[(size_t)c] = 0;
+    }
+    std::vector<int> remap((size_t)nAgg, -1);
+    int next = 0;
+    for (int n = 0; n < N; n++) {
+        int& r = remap[(size_t)c2c[(size_t)n]];
+        if (r < 0) r = next++;
+        c2c[(size_t)n] = r;
+    }
+    return next;
+}
+
+// Coarse CSR + fine slot -> coarse slot map (multigrid.cu:196-287).
+GridLevel coarsen(GridLevel& fine) {
+    GridLevel coarse;
+    const int nC = aggregate(fine, fine.cellToCoarse);
+    coarse.nCells = nC;
+    struct Ref {
+        int cc, cn, slot;
+    };
+    std::vector<Ref> refs;
+    refs.reserve((size_t)fine.nFaceRefs());
+    for (int n = 0; n < fine.nCells; n++) {
+        const int cn = fine.cellToCoarse[(size_t)n];
+        for (int k = fine.faceStart[(size_t)n]; k < fine.faceStart[(size_t)n + 1]; k++) {
+            const int nb = fine.faceNeighbor[(size_t)k];
+            if (nb < 0) continue;
+            const int cb = fine.cellToCoarse[(size_t)nb];
+            if (cb != cn) refs.push_back(Ref{cn, cb, k});
+        }
+    }
+    std::sort(refs.begin(), refs.end(), [](const Ref& a, const Ref& b) {
+        return a.cc != b.cc ? a.cc < b.cc : a.cn < b.cn;
+    });
+    fine.fineSlotToCoarseSlot.assign((size_t)fine.nFaceRefs(), -1);
+    coarse.faceStart.assign((size_t)nC + 1, 0);
+    coarse.faceNeighbor.reserve(refs.size());
+    for (size_t i = 0; i < refs.size(); i++) {
+        const bool fresh = i == 0 || refs[i].cc != refs[i - 1].cc || refs[i].cn != refs[i - 1].cn;
+        if (fresh) {
+            coarse.faceNeighbor.push_back(refs[i].cn);
+            coarse.faceStart[(size_t)refs[i].cc + 1]++;
+        }
+        fine.fineSlotToCoarseSlot[(size_t)refs[i].slot] = (int)coarse.faceNeighbor.size() - 1;
+    }
+    for (int c = 0; c < nC; c++) coarse.faceStart[(size_t)c + 1] += coarse.faceStart[(size_t)c];
+    return coarse;
+}
+
+}  // namespace
+
+std::vector<GridLevel> buildHierarchy(GridLevel fine) {
+    constexpr int minCoarseCells = 64;
+    constexpr double maxShrinkRatio = 0.8;
+    std::vector<GridLevel> levels;
+    while (fine.nCells > minCoarseCells) {
+        GridLevel coarse = coarsen(fine);
+        if (coarse.nCells >= (int)(fine.nCells * maxShrinkRatio)) {
+            fine.cellToCoarse.clear();
+            fine.fineSlotToCoarseSlot.clear();
+            break;
+        }
+        levels.push_back(std::move(fine));
+        fine = std::move(coarse);
+    }
+    levels.push_back(std::move(fine));
+    return levels;
+}
+
+int greedyColoring(const GridLevel& g, std::vector<int32_t>& color) {
+    const int N = g.nCells;
+    color.assign((size_t)N, -1);
+    std::vector<int> stamp;
+    int nColors = 0;
+    for (int c = 0; c < N; c++) {
+        for (int k = g.faceStart[(size_t)c]; k < g.faceStart[(size_t)c + 1]; k++) {
+            const int nb = g.faceNeighbor[(size_t)k];
+            if (nb < 0 || color[(size_t)nb] < 0) continue;
+            const int cl = color[(size_t)nb];
+            if (cl >= (int)stamp.size()) stamp.resize((size_t)cl + 1, -1);
+            stamp[(size_t)cl] = c;
+        }
+        int pick = 0;
+        while (pick < (int)stamp.size() && stamp[(size_t)pick] == c) pick++;
+        color[(size_t)c] = pick;
+        nColors = std::max(nColors, pick + 1);
+    }
+    return nColors;
+}
+
+uint8_t defaultBCType(int boundaryType, int variable) {
+    // BCType: 0 DIRICHLET 1 NEUMANN 5 NONE; variables 0 u 1 v 2 p.
+    switch (boundaryType) {
+        case 1:  // VELOCITY_INLET
+            return variable == 2 ? 1 : 0;
+        case 2:  // PRESSURE_OUTLET
+            return variable == 2 ? 0 : 1;
+        case 0:  // WALL
+            return variable == 2 ? 1 : 0;
+        case 3:  // SYMMETRY: v Dirichlet 0, u and p zero-gradient
+            return variable == 1 ? 0 : 1;
+        case 4:  // FAR_FIELD
+            return variable == 2 ? 1 : 0;
+        default:
+            return 5;
+    }
+}
+
+bool variableEditable(int variable, int boundaryType) {
+    switch (boundaryType) {
+        case 0: return variable == 0 || variable == 1;
+        case 3: return false;
+        case 4: return variable == 0 || variable == 1;
+        case 1: return variable == 0 || variable == 1;
+        case 2: return variable == 2;
+        default: return false;
+    }
+}
+
+}  // namespace axisim

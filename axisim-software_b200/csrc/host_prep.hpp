@@ -1,0 +1,64 @@
+// host_prep.hpp -- host-side case preparation for the B200 SIMPLE solver.
+//
+// Pieces of the reference that run once per solve on the CPU: the multiblock
+// packer (structs/multiblock.h), the agglomeration hierarchy
+// (solver/source/multigrid.cu:79-325), the greedy colouring
+// (manager/source/memory_manger.cpp:325-409) and the boundary defaults
+// (manager/source/boundary_func.cpp:104-201, 333-378).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace axisim {
+
+// Packed face-based mesh (FVMeshHostPacked, structs/solver_struct.h:400-429).
+struct PackedMesh {
+    int nCells = 0;
+    int nFaces = 0;
+    std::vector<int32_t> faceOwner, faceNeighbor, faceBoundaryGroupID;
+    std::vector<double> faceNormalZ, faceNormalR, faceCenterZ, faceCenterR, faceArea;
+    std::vector<double> cellCenterZ, cellCenterR, cellArea2D, cellVolume;
+    std::vector<int32_t> cellFaceStart, cellFaceIDs;
+};
+
+struct BlockSpec {
+    double z0 = 0, r0 = 0;
+    double axialLength = 0;  int axialCells = 0;  int axialGrading = 0;  double axialCoef = 1;
+    double radialLength = 0; int radialCells = 0; int radialGrading = 0; double radialCoef = 1;
+    int edgeGroup[4] = {-1, -1, -1, -1};
+};
+
+// makeRectBlock + autoDetectInterfaces + assignGlobalNumbering + toPackedMesh.
+// seamStatus = 1 when a non-conformal seam made every interface drop.
+PackedMesh buildMultiblock(const std::vector<BlockSpec>& blocks, double tol, int defaultGroup,
+                           int& seamStatus);
+
+// One multigrid level's graph, CSR exactly as GridLevel (multigrid.cuh:29-68).
+struct GridLevel {
+    int nCells = 0;
+    std::vector<int32_t> faceStart;
+    std::vector<int32_t> faceNeighbor;
+    std::vector<int32_t> cellToCoarse;          // empty on the coarsest level
+    std::vector<int32_t> fineSlotToCoarseSlot;  // empty on the coarsest level
+    int nFaceRefs() const { return (int)faceNeighbor.size(); }
+    bool isCoarsest() const { return cellToCoarse.empty(); }
+};
+
+// buildCellFaceCSR (memory_manger.cpp:287-323) from a packed mesh.
+GridLevel finestLevel(int nCells, int nFaces, const int32_t* cellFaceStart, const int32_t* cellFaceIDs,
+                      const int32_t* faceOwner, const int32_t* faceNeighbor);
+
+// buildLevels (multigrid.cu:298-325): coarsen until <= 64 cells or a pass
+// shrinks by less than 0.8.
+std::vector<GridLevel> buildHierarchy(GridLevel finest);
+
+// buildMeshColoring (memory_manger.cpp:334-409): greedy colour per cell.
+int greedyColoring(const GridLevel& g, std::vector<int32_t>& color);
+
+// Boundary defaults: effective BC for a group type and variable.
+uint8_t defaultBCType(int boundaryType, int variable);
+bool variableEditable(int variable, int boundaryType);
+
+}  // namespace axisim

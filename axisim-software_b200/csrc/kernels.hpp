@@ -1,0 +1,85 @@
+// kernels.hpp -- host launchers for the sm_100a kernels of the SIMPLE path.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace axisim {
+
+// One multigrid level on the device. Level 0 aliases the p' system.
+struct LevelDev {
+    int N = 0, W = 0;
+    int32_t* nb = nullptr;     // [W][N], -1 = no neighbour
+    double* AF = nullptr;      // [W][N]
+    double* AC = nullptr;
+    double* b = nullptr;
+    double* x = nullptr;
+    double* xNew = nullptr;
+    double* xF = nullptr;      // single precision copy used by the mixed smoother
+    int32_t* c2c = nullptr;    // fine -> coarse (null on the coarsest level)
+    // Galerkin / restriction gathers, stored on the COARSE level (built from level-1):
+    int32_t* mStart = nullptr;  // [N+1] members of each coarse cell
+    int32_t* mList = nullptr;   // fine cell ids, ascending
+    int32_t* gStart = nullptr;  // [W*N+1] fine slots feeding each coarse ELL slot
+    int32_t* gList = nullptr;   // fine ELL slot indices, ascending fine cell then slot
+    uint32_t* internalMask = nullptr;  // on the FINE level: slots folding into the coarse diagonal
+    // single precision copies for the mixed-precision cycle
+    float* AFf = nullptr;
+    float* ACf = nullptr;
+    float* invACf = nullptr;
+    float* bf = nullptr;
+    float* xf = nullptr;
+    float* xNewf = nullptr;
+};
+
+// ---- setup ----
+void launchPrecompute(const MeshDev& m, const int32_t* cfs, const int32_t* cfi, double* lsqDZ, double* lsqDR,
+                      cudaStream_t s);
+void launchBuildEll(int N, int W, const int32_t* cfs, const int32_t* cfi, const int32_t* owner,
+                    const int32_t* neighbor, int32_t* sface, int32_t* snb, cudaStream_t s);
+
+// ---- one SIMPLE iteration ----
+void launchIterBegin(Ctl* ctl, const volatile int* hostStop, cudaStream_t s);
+// gradients of up to three fields (u, v, p) with their boundary fields
+void launchGradient(const MeshDev& m, const Ctl* ctl, int nFields, const double* const* phi, const BCDev* bc,
+                    double* const* gZ, double* const* gR, int scheme, cudaStream_t s);
+void launchMomentum(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, const BCDev& bcV,
+                    const MomentumArgs& a, cudaStream_t s);
+void launchJacobiUV(const MeshDev& m, const Ctl* ctl, const double* AF, const double* bu, const double* bv,
+                    const double* invu, const double* invv, const double* xu, const double* xv, double* yu,
+                    double* yv, cudaStream_t s);
+void launchGaussSeidelUV(const MeshDev& m, const Ctl* ctl, const double* AF, const double* bu, const double* bv,
+                         const double* invu, const double* invv, double* xu, double* xv, const int32_t* order,
+                         int begin, int count, cudaStream_t s);
+// p' system + inverse diagonal + Rhie-Chow face mass flux (owner writes each face)
+void launchPressureSystem(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, const BCDev& bcV,
+                          const BCDev& bcP, double rho, const double* u, const double* v, const double* p,
+                          const double* gPZ, const double* gPR, const double* DU, const double* DV,
+                          double* AFpp, double* ACpp, double* invACpp, double* mDot, cudaStream_t s);
+void launchPressureRhs(const MeshDev& m, const Ctl* ctl, double rho, const double* mDot, const double* DU,
+                       const double* DV, const double* gZ, const double* gR, int cross, int zeroPP, double* bpp,
+                       double* pp, cudaStream_t s);
+// p' linear solve without multigrid (Jacobi ping-pong or colour sweep on one field)
+void launchJacobi1(const MeshDev& m, const Ctl* ctl, const double* AF, const double* b, const double* inv,
+                   const double* x, double* y, cudaStream_t s);
+void launchGaussSeidel1(const MeshDev& m, const Ctl* ctl, const double* AF, const double* b, const double* inv,
+                        double* x, const int32_t* order, int begin, int count, cudaStream_t s);
+void launchCorrect(const MeshDev& m, const Ctl* ctl, const BCDev& bcP, double rho, double alphaP, int nonOrtho,
+                   const double* pp, const double* gZ, const double* gR, const double* DU, const double* DV,
+                   double* u, double* v, double* p, double* mDot, cudaStream_t s);
+void launchResiduals(const MeshDev& m, const Ctl* ctl, const double* AF, const double* ACu, const double* ACv,
+                     const double* bu, const double* bv, const double* u, const double* v, const double* mDot,
+                     double* resU, double* resV, double* resC, double* scaleU, double* scaleV, double* partial,
+                     int* nBlocksOut, cudaStream_t s);
+void launchIterEnd(Ctl* ctl, const double* partial, int nBlocks, int N, cudaStream_t s);
+void launchCopy(const Ctl* ctl, double* dst, const double* src, int n, cudaStream_t s);
+
+// ---- multigrid (FP64) ----
+void launchGalerkin(const Ctl* ctl, const LevelDev& fine, const LevelDev& coarse, cudaStream_t s);
+void launchMGSmooth(const Ctl* ctl, const LevelDev& L, const double* x, double* y, double w, cudaStream_t s);
+void launchMGSmoothBlock(const Ctl* ctl, const LevelDev& L, double* x, double w, int sweeps, cudaStream_t s);
+void launchMGRestrict(const Ctl* ctl, const LevelDev& fine, const double* xFine, LevelDev& coarse, cudaStream_t s);
+void launchMGProlong(const Ctl* ctl, const LevelDev& fine, double* xFine, const double* xCoarse, cudaStream_t s);
+
+}  // namespace axisim

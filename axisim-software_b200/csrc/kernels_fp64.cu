@@ -1,0 +1,1090 @@
+// kernels_fp64.cu -- FP64 kernels of the SIMPLE iteration for sm_100a.
+//
+// Compiled with --fmad=false: every a*b+c is two rounded operations, in the
+// order the reference kernels write them, so this path reproduces the CPU
+// oracle bit for bit. The kernels are HBM-bound (stencil / CSR work well under
+// 1 flop/byte); the layout they read is described in device.cuh.
+//
+// Fusions relative to the reference launch sequence (solver.cpp:1116-1266):
+//   k_momentum   clearAllCoefficients + addTransportCoefficients(u) and (v)
+//                + addRadialMomentumCylindricalSource + addTransientCoefficient
+//                + createMomentumPressureRhs + underRelaxEquation + buildInverseDiagonal
+//                + getCorrectionCoefficients (per-cell arithmetic order unchanged)
+//   k_jacobi_uv  the u and v Jacobi sweeps in one pass over the shared AF
+//   k_pressure   createPPCoeff + buildInverseDiagonal(pp) + computeFaceMassFluxRhieChow
+//   k_pp_rhs     createPPRhs + the p' reset
+//   k_correct    updateMomentumPressure + updateMassFlux
+//   k_residual   residualAll + continuityResidual + first reduction pass
+// Multigrid: the Galerkin build and the restriction are deterministic gathers
+// (ascending fine-cell order) in place of the reference's atomicAdd scatters
+// (multigrid.cu:350-410); the residual is fused into the restriction.
+#include <cmath>
+#include <cstdio>
+
+#include "kernels.hpp"
+
+namespace axisim {
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr int kThreads = 256;
+constexpr uint8_t BC_DIRICHLET = 0, BC_NEUMANN = 1, BC_FULLY_DEVELOPED = 2;
+constexpr int CONV_UPWIND = 0, CONV_CENTRAL = 1, CONV_SOU = 2;
+
+inline int blocksFor(int n, int t = kThreads) { return (n + t - 1) / t; }
+
+// ---------------- face helpers (solver_util.cuh:56-297) ----------------
+
+__device__ __forceinline__ double normalCorr(const double* DU, const double* DV, double nz, double nr, int c) {
+    return DU[c] * nz * nz + DV[c] * nr * nr;
+}
+
+// interpolateNormalCorrectionCoeffToFace (solver_util.cuh:126-161)
+__device__ __forceinline__ double interpCorr(const MeshDev& m, const double* DU, const double* DV, int c, int f,
+                                             int own, int nb) {
+    const double nz = m.nZ[f], nr = m.nR[f];
+    const double DP = normalCorr(DU, DV, nz, nr, c);
+    if (nb < 0) return DP;
+    const int o = (own == c) ? nb : own;
+    const double DN = normalCorr(DU, DV, nz, nr, o);
+    const double w = (own == c) ? m.wP[f] : 1.0 - m.wP[f];
+    return w * DP + (1.0 - w) * DN;
+}
+
+// prescribedBoundaryFaceValue (solver_util.cuh:223-238)
+__device__ __forceinline__ double prescribed(const MeshDev& m, int f, uint8_t type, double value, double len) {
+    if (type != BC_FULLY_DEVELOPED) return value;
+    const double nz = m.nZ[f], nr = m.nR[f];
+    const double along = m.fcR[f] * nz * nz + m.fcZ[f] * nr * nr;
+    const double x = along / len;
+    return value * (1.0 - x * x);
+}
+
+// interpolateFieldToFace, boundary branch (solver_util.cuh:264-296)
+__device__ __forceinline__ double boundaryFaceValue(const MeshDev& m, int f, const BCDev& bc, double phiP) {
+    const int g = m.group[f];
+    if (g < 0 || g >= bc.nGroups) return phiP;
+    const uint8_t t = bc.type[g];
+    const double val = bc.value[g];
+    if (t == BC_DIRICHLET || t == BC_FULLY_DEVELOPED) return prescribed(m, f, t, val, bc.length[g]);
+    if (t == BC_NEUMANN) return phiP + val * m.dPB[f];
+    return phiP;
+}
+
+// nonOrthoScalarDiffusionFlux (solver_util.cuh:383-430)
+__device__ __forceinline__ double nonOrthoFlux(const MeshDev& m, int c, int f, int own, int nb, const double* gZ,
+                                               const double* gR, double gamma) {
+    if (nb < 0) return 0.0;
+    const int o = (own == c) ? nb : own;
+    double nz = m.nZ[f], nr = m.nR[f];
+    if (nb == c) {
+        nz = -nz;
+        nr = -nr;
+    }
+    const double a = m.area[f];
+    const double dz = m.ccZ[o] - m.ccZ[c];
+    const double dr = m.ccR[o] - m.ccR[c];
+    const double aOverNd = a * m.invDPN[f];
+    const double Tz = a * nz - aOverNd * dz;
+    const double Tr = a * nr - aOverNd * dr;
+    const double w = (own == c) ? m.wP[f] : 1.0 - m.wP[f];
+    const double gfz = w * gZ[c] + (1.0 - w) * gZ[o];
+    const double gfr = w * gR[c] + (1.0 - w) * gR[o];
+    return gamma * (Tz * gfz + Tr * gfr);
+}
+
+// ---------------- set-up kernels ----------------
+// preComputeVariables, face part (memory_manger.cpp:528-591)
+__global__ void k_precompute_faces(MeshDev m, double* invDPN, double* wP, double* dPB, double* length2D,
+                                   double* lsqWZ, double* lsqWR, double* lsqDZ, double* lsqDR) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.F) return;
+    length2D[f] = m.area[f] / (2 * kPi * m.fcR[f]);
+    const int nb = m.neighbor[f], o = m.owner[f];
+    const double dzPF = m.fcZ[f] - m.ccZ[o];
+    const double drPF = m.fcR[f] - m.ccR[o];
+    if (nb < 0) {
+        dPB[f] = fabs(dzPF * m.nZ[f] + drPF * m.nR[f]);
+        invDPN[f] = 0.0;
+        wP[f] = 0.0;
+    } else {
+        const double dzNF = m.fcZ[f] - m.ccZ[nb];
+        const double drNF = m.fcR[f] - m.ccR[nb];
+        const double dzPN = m.ccZ[nb] - m.ccZ[o];
+        const double drPN = m.ccR[nb] - m.ccR[o];
+        const double dPF = fabs(dzPF * m.nZ[f] + drPF * m.nR[f]);
+        const double dNF = fabs(dzNF * m.nZ[f] + drNF * m.nR[f]);
+        const double dPN = sqrt(dzPN * dzPN + drPN * drPN);
+        const double denom = dPF + dNF;
+        invDPN[f] = 1.0 / dPN;
+        wP[f] = dNF / denom;
+        dPB[f] = 0.0;
+    }
+    const double dz = (nb >= 0 ? m.ccZ[nb] : m.fcZ[f]) - m.ccZ[o];
+    const double dr = (nb >= 0 ? m.ccR[nb] : m.fcR[f]) - m.ccR[o];
+    const double w = 1.0 / (dz * dz + dr * dr);
+    lsqDZ[f] = dz;
+    lsqDR[f] = dr;
+    lsqWZ[f] = w * dz;
+    lsqWR[f] = w * dr;
+}
+
+// preComputeVariables, cell part (memory_manger.cpp:524-526, 593-613)
+__global__ void k_precompute_cells(MeshDev m, const int32_t* cfs, const int32_t* cfi, const double* lsqDZ,
+                                   const double* lsqDR, double* invA2D, double* IZZ, double* IZR, double* IRR) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.N) return;
+    invA2D[c] = 2.0 * kPi * m.ccR[c] / m.vol[c];
+    double Szz = 0.0, Szr = 0.0, Srr = 0.0;
+    for (int k = cfs[c]; k < cfs[c + 1]; k++) {
+        const int f = cfi[k];
+        Szz += m.lsqWZ[f] * lsqDZ[f];
+        Szr += m.lsqWZ[f] * lsqDR[f];
+        Srr += m.lsqWR[f] * lsqDR[f];
+    }
+    const double det = Szz * Srr - Szr * Szr;
+    if (fabs(det) <= 1.0e-30) {
+        IZZ[c] = 0.0;
+        IZR[c] = 0.0;
+        IRR[c] = 0.0;
+        return;
+    }
+    IZZ[c] = Srr / det;
+    IZR[c] = -Szr / det;
+    IRR[c] = Szz / det;
+}
+
+// buildCellFaceCSR (memory_manger.cpp:287-323) into the [W][N] slot block
+__global__ void k_build_ell(int N, int W, const int32_t* cfs, const int32_t* cfi, const int32_t* owner,
+                            const int32_t* neighbor, int32_t* sface, int32_t* snb) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int k0 = cfs[n], deg = cfs[n + 1] - k0;
+    for (int j = 0; j < W; j++) {
+        int f = -1, nb = -1;
+        if (j < deg) {
+            f = cfi[k0 + j];
+            if (owner[f] == n) nb = neighbor[f];
+            else if (neighbor[f] == n) nb = owner[f];
+        }
+        sface[(size_t)j * N + n] = f;
+        snb[(size_t)j * N + n] = nb;
+    }
+}
+
+// ---------------- iteration control ----------------
+__global__ void k_iter_begin(Ctl* ctl, const volatile int* hostStop) {
+    if (ctl->done) return;
+    if (hostStop && *hostStop) {
+        ctl->done = 2;
+        return;
+    }
+    if (ctl->k >= ctl->maxIter) {
+        ctl->done = 3;
+        return;
+    }
+    ctl->checked = (ctl->k % ctl->checkConv) == 0;
+}
+
+// ---------------- gradients (solver_util.cu:146-169, cuh:458-588) ----------------
+struct GradArgs {
+    const double* phi[3];
+    BCDev bc[3];
+    double* gZ[3];
+    double* gR[3];
+};
+
+template <int NF>
+__global__ void k_gradient(MeshDev m, const Ctl* ctl, GradArgs a, int scheme) {
+    if (ctl && ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= m.N) return;
+    const int N = m.N;
+    if (scheme == 0) {
+        double gz[NF], gr[NF], axisPhi[NF];
+        double clZ = 0.0, clR = 0.0;
+        bool hasAxis = false;
+        for (int q = 0; q < NF; q++) gz[q] = gr[q] = axisPhi[q] = 0.0;
+        for (int j = 0; j < m.W; j++) {
+            const int f = m.sface[(size_t)j * N + n];
+            if (f < 0) break;
+            const int own = m.owner[f], nb = m.neighbor[f];
+            double nz = m.nZ[f], nr = m.nR[f];
+            if (nb == n) {
+                nz = -nz;
+                nr = -nr;
+            }
+            double phiF[NF];
+            if (nb >= 0) {
+                const int o = (own == n) ? nb : own;
+                const double w = (own == n) ? m.wP[f] : 1.0 - m.wP[f];
+                for (int q = 0; q < NF; q++) phiF[q] = w * a.phi[q][n] + (1.0 - w) * a.phi[q][o];
+            } else {
+                for (int q = 0; q < NF; q++) phiF[q] = boundaryFaceValue(m, f, a.bc[q], a.phi[q][n]);
+            }
+            const double rf = m.fcR[f];
+            if (rf > 1.0e-30) {
+                const double L = m.length2D[f];
+                for (int q = 0; q < NF; q++) {
+                    gz[q] += phiF[q] * nz * L;
+                    gr[q] += phiF[q] * nr * L;
+                }
+                clZ += nz * L;
+                clR += nr * L;
+            } else {
+                hasAxis = true;
+                for (int q = 0; q < NF; q++) axisPhi[q] = phiF[q];
+            }
+        }
+        const double inv = m.invA2D[n];
+        for (int q = 0; q < NF; q++) {
+            if (hasAxis) {
+                gz[q] += axisPhi[q] * (-clZ);
+                gr[q] += axisPhi[q] * (-clR);
+            }
+            a.gZ[q][n] = gz[q] * inv;
+            a.gR[q][n] = gr[q] * inv;
+        }
+    } else if (scheme == 1) {
+        double bz[NF], br[NF], phiP[NF];
+        for (int q = 0; q < NF; q++) {
+            bz[q] = br[q] = 0.0;
+            phiP[q] = a.phi[q][n];
+        }
+        for (int j = 0; j < m.W; j++) {
+            const int f = m.sface[(size_t)j * N + n];
+            if (f < 0) break;
+            const int own = m.owner[f], nb = m.neighbor[f];
+            const double wz = m.lsqWZ[f], wr = m.lsqWR[f];
+            for (int q = 0; q < NF; q++) {
+                double dphi;
+                if (nb >= 0) {
+                    const bool isOwner = (own == n);
+                    const double phiNb = a.phi[q][isOwner ? nb : own];
+                    dphi = isOwner ? (phiNb - phiP[q]) : (phiP[q] - phiNb);
+                } else {
+                    dphi = boundaryFaceValue(m, f, a.bc[q], phiP[q]) - phiP[q];
+                }
+                bz[q] += wz * dphi;
+                br[q] += wr * dphi;
+            }
+        }
+        const double izz = m.lsqIZZ[n], izr = m.lsqIZR[n], irr = m.lsqIRR[n];
+        for (int q = 0; q < NF; q++) {
+            a.gZ[q][n] = izz * bz[q] + izr * br[q];
+            a.gR[q][n] = izr * bz[q] + irr * br[q];
+        }
+    } else {
+        for (int q = 0; q < NF; q++) {
+            a.gZ[q][n] = 0.0;
+            a.gR[q][n] = 0.0;
+        }
+    }
+}
+
+// ---------------- momentum assembly ----------------
+// Higher-order face value of the deferred correction (solver_util.cuh:724-768)
+__device__ __forceinline__ double higherOrder(const MeshDev& m, int n, int o, int f, int scheme, double F, double phiUD,
+                                              const double* phi, const double* gZ, const double* gR) {
+    if (scheme == CONV_CENTRAL) {
+        const double w = (m.owner[f] == n) ? m.wP[f] : 1.0 - m.wP[f];
+        return w * phi[n] + (1.0 - w) * phi[o];
+    }
+    if (scheme == CONV_SOU) {
+        const int up = (F > 0.0) ? n : o;
+        const double dz = m.fcZ[f] - m.ccZ[up];
+        const double dr = m.fcR[f] - m.ccR[up];
+        const double ho = phi[up] + gZ[up] * dz + gR[up] * dr;
+        const double lo = fmin(phi[n], phi[o]);
+        const double hi = fmax(phi[n], phi[o]);
+        return fmin(fmax(ho, lo), hi);
+    }
+    return phiUD;
+}
+
+// Boundary face of one momentum component: diffusion BC (solver_util.cu:355-413)
+// and first-order convection (solver_util.cuh:817-864).
+__device__ __forceinline__ void momentumBoundary(const MeshDev& m, int n, int f, double area, double F, double mu,
+                                                 const BCDev& bc, double& AC, double& b) {
+    const int g = m.group[f];
+    const bool valid = g >= 0 && g < bc.nGroups;
+    if (valid) {
+        const uint8_t t = bc.type[g];
+        const double val = bc.value[g];
+        const double nz = m.nZ[f], nr = m.nR[f];
+        const double dPF = fabs((m.fcZ[f] - m.ccZ[n]) * nz + (m.fcR[f] - m.ccR[n]) * nr);
+        const double K = mu * area / dPF;
+        if (t == BC_DIRICHLET) {
+            AC += K;
+            b += K * val;
+        } else if (t == BC_NEUMANN) {
+            b += mu * area * val;
+        } else if (t == BC_FULLY_DEVELOPED) {
+            AC += K;
+            b += K * prescribed(m, f, t, val, bc.length[g]);
+        }
+    }
+    if (F != 0.0) {
+        if (!valid) {
+            AC += F;
+            return;
+        }
+        const uint8_t t = bc.type[g];
+        const double val = bc.value[g];
+        if (t == BC_DIRICHLET) {
+            if (F < 0.0) b += -F * val;
+            else AC += F;
+        } else if (t == BC_NEUMANN) {
+            AC += F;
+        } else if (t == BC_FULLY_DEVELOPED) {
+            if (F < 0.0) b += -F * prescribed(m, f, t, val, bc.length[g]);
+            else AC += F;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_momentum(MeshDev m, const Ctl* ctl, BCDev bcU, BCDev bcV,
+                                                       MomentumArgs a) {
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= m.N) return;
+    const int N = m.N;
+    double ACu = 0.0, ACv = 0.0, bu = 0.0, bv = 0.0, netF = 0.0;
+    for (int j = 0; j < m.W; j++) {
+        const size_t s = (size_t)j * N + n;
+        const int f = m.sface[s];
+        if (f < 0) break;
+        const int own = m.owner[f], nb = m.neighbor[f];
+        const double area = m.area[f];
+        double F = 0.0;
+        if (a.conv) {
+            const double Fo = a.mDot[f] * 1.0;
+            if (own == n) F = Fo;
+            else if (nb == n) F = -Fo;
+            if (fabs(F) <= 1.0e-30) F = 0.0;
+            netF += F;
+        }
+        if (nb >= 0) {
+            const int o = (own == n) ? nb : own;
+            const double K = a.mu * area * m.invDPN[f];
+            ACu += K;
+            ACv += K;
+            double af = 0.0 - K;
+            if (a.nonOrtho) {
+                bu += nonOrthoFlux(m, n, f, own, nb, a.gUZ, a.gUR, a.mu);
+                bv += nonOrthoFlux(m, n, f, own, nb, a.gVZ, a.gVR, a.mu);
+            }
+            if (F != 0.0) {
+                ACu += fmax(F, 0.0);
+                ACv += fmax(F, 0.0);
+                af += fmin(F, 0.0);
+                if (a.scheme != CONV_UPWIND) {
+                    const double udU = (F > 0.0) ? a.u[n] : a.u[o];
+                    const double hoU = higherOrder(m, n, o, f, a.scheme, F, udU, a.u, a.gUZ, a.gUR);
+                    bu -= F * (hoU - udU);
+                    const double udV = (F > 0.0) ? a.v[n] : a.v[o];
+                    const double hoV = higherOrder(m, n, o, f, a.scheme, F, udV, a.v, a.gVZ, a.gVR);
+                    bv -= F * (hoV - udV);
+                }
+            }
+            a.AF[s] = af;
+        } else {
+            a.AF[s] = 0.0;
+            momentumBoundary(m, n, f, area, F, a.mu, bcU, ACu, bu);
+            momentumBoundary(m, n, f, area, F, a.mu, bcV, ACv, bv);
+        }
+    }
+    if (a.conv) {
+        ACu -= netF;
+        ACv -= netF;
+    }
+    const double V = m.vol[n];
+    const double r = m.ccR[n];
+    ACv += a.mu * V / (r * r);  // hoop term, solver_util.cu:454-470
+    if (a.transient && a.dt > 0.0) {  // solver_util.cu:536-578
+        const double cV = a.rho * V;
+        if (ctl->bdf2) {
+            const double c2 = cV / (2.0 * a.dt);
+            ACu += 3.0 * c2;
+            bu += c2 * (4.0 * a.uOld[n] - a.uOld2[n]);
+            ACv += 3.0 * c2;
+            bv += c2 * (4.0 * a.vOld[n] - a.vOld2[n]);
+        } else {
+            const double c1 = cV / a.dt;
+            ACu += c1;
+            bu += c1 * a.uOld[n];
+            ACv += c1;
+            bv += c1 * a.vOld[n];
+        }
+    }
+    bu += -V * a.gPZ[n];  // simple.cu:144-164
+    bv += -V * a.gPR[n];
+    const double al = a.alpha;  // solver_util.cu:582-600
+    if (!(fabs(ACu) < 1.0e-30)) {
+        const double ACo = ACu;
+        ACu = ACo / al;
+        bu += ((1.0 - al) / al) * ACo * a.u[n];
+    }
+    if (!(fabs(ACv) < 1.0e-30)) {
+        const double ACo = ACv;
+        ACv = ACo / al;
+        bv += ((1.0 - al) / al) * ACo * a.v[n];
+    }
+    const double iu = (fabs(ACu) < 1.0e-30) ? 0.0 : 1.0 / ACu;  // solver_util.cu:602-612
+    const double iv = (fabs(ACv) < 1.0e-30) ? 0.0 : 1.0 / ACv;
+    a.ACu[n] = ACu;
+    a.ACv[n] = ACv;
+    a.bu[n] = bu;
+    a.bv[n] = bv;
+    a.invACu[n] = iu;
+    a.invACv[n] = iv;
+    a.DU[n] = V * iu;  // solver_util.cu:127-144
+    a.DV[n] = V * iv;
+}
+
+// ---------------- momentum sweeps (linear_solver.cu:9-72) ----------------
+__global__ void __launch_bounds__(kThreads) k_jacobi_uv(int N, int W, const int32_t* __restrict__ snb,
+                                                        const Ctl* ctl, const double* __restrict__ AF,
+                                                        const double* __restrict__ bu, const double* __restrict__ bv,
+                                                        const double* __restrict__ iu, const double* __restrict__ iv,
+                                                        const double* __restrict__ xu, const double* __restrict__ xv,
+                                                        double* __restrict__ yu, double* __restrict__ yv) {
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    double vu = bu[n], vv = bv[n];
+    for (int j = 0; j < W; j++) {
+        const size_t s = (size_t)j * N + n;
+        const int nb = snb[s];
+        if (nb >= 0) {
+            const double a = AF[s];
+            vu -= a * xu[nb];
+            vv -= a * xv[nb];
+        }
+    }
+    const double au = iu[n], av = iv[n];
+    yu[n] = (au != 0.0) ? vu * au : xu[n];
+    yv[n] = (av != 0.0) ? vv * av : xv[n];
+}
+
+__global__ void __launch_bounds__(kThreads) k_gs_uv(int N, int W, const int32_t* __restrict__ snb, const Ctl* ctl,
+                                                    const double* __restrict__ AF, const double* __restrict__ bu,
+                                                    const double* __restrict__ bv, const double* __restrict__ iu,
+                                                    const double* __restrict__ iv, double* xu, double* xv,
+                                                    const int32_t* __restrict__ order, int begin, int count) {
+    if (ctl->done) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const int n = order[begin + t];
+    double vu = bu[n], vv = bv[n];
+    for (int j = 0; j < W; j++) {
+        const size_t s = (size_t)j * N + n;
+        const int nb = snb[s];
+        if (nb >= 0) {
+            const double a = AF[s];
+            vu -= a * xu[nb];
+            vv -= a * xv[nb];
+        }
+    }
+    const double au = iu[n], av = iv[n];
+    xu[n] = (au != 0.0) ? vu * au : xu[n];
+    xv[n] = (av != 0.0) ? vv * av : xv[n];
+}
+
+__global__ void __launch_bounds__(kThreads) k_jacobi1(int N, int W, const int32_t* __restrict__ snb, const Ctl* ctl,
+                                                      const double* __restrict__ AF, const double* __restrict__ b,
+                                                      const double* __restrict__ inv, const double* __restrict__ x,
+                                                      double* __restrict__ y) {
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    double v = b[n];
+    for (int j = 0; j < W; j++) {
+        const size_t s = (size_t)j * N + n;
+        const int nb = snb[s];
+        if (nb >= 0) v -= AF[s] * x[nb];
+    }
+    const double a = inv[n];
+    y[n] = (a != 0.0) ? v * a : x[n];
+}
+
+__global__ void __launch_bounds__(kThreads) k_gs1(int N, int W, const int32_t* __restrict__ snb, const Ctl* ctl,
+                                                  const double* __restrict__ AF, const double* __restrict__ b,
+                                                  const double* __restrict__ inv, double* x,
+                                                  const int32_t* __restrict__ order, int begin, int count) {
+    if (ctl->done) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const int n = order[begin + t];
+    double v = b[n];
+    for (int j = 0; j < W; j++) {
+        const size_t s = (size_t)j * N + n;
+        const int nb = snb[s];
+        if (nb >= 0) v -= AF[s] * x[nb];
+    }
+    const double a = inv[n];
+    x[n] = (a != 0.0) ? v * a : x[n];
+}
+
+// ---------------- pressure correction system + Rhie-Chow ----------------
+struct PressureArgs {
+    double rho;
+    const double* u;
+    const double* v;
+    const double* p;
+    const double* gPZ;
+    const double* gPR;
+    const double* DU;
+    const double* DV;
+    double* AFpp;
+    double* ACpp;
+    double* invACpp;
+    double* mDot;
+};
+
+__global__ void __launch_bounds__(kThreads) k_pressure(MeshDev m, const Ctl* ctl, BCDev bcU, BCDev bcV, BCDev bcP,
+                                                       PressureArgs a) {
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= m.N) return;
+    const int N = m.N;
+    const double rho = a.rho;
+    double AC = 0.0;
+    for (int j = 0; j < m.W; j++) {
+        const size_t s = (size_t)j * N + n;
+        const int f = m.sface[s];
+        if (f < 0) break;
+        const int own = m.owner[f], nb = m.neighbor[f];
+        const double area = m.area[f];
+        const double nz = m.nZ[f], nr = m.nR[f];
+        const double Df = interpCorr(m, a.DU, a.DV, n, f, own, nb);
+        // createPPCoeff (simple.cu:7-88)
+        if (nb >= 0) {
+            const double K = rho * area * Df * m.invDPN[f];
+            AC += K;
+            a.AFpp[s] = 0.0 - K;
+        } else {
+            a.AFpp[s] = 0.0;
+            const int g = m.group[f];
+            if (g >= 0 && g < bcP.nGroups && bcP.type[g] == BC_DIRICHLET) {
+                const double K = rho * area * Df / m.dPB[f];
+                AC += K;
+            }
+        }
+        // Rhie-Chow face mass flux, computed once per face by its owner
+        // (solver_util.cu:171-203, solver_util.cuh:590-713)
+        if (own != n) continue;
+        if (area <= 1.0e-30) {
+            a.mDot[f] = 0.0;
+            continue;
+        }
+        double uF, vF;
+        if (nb >= 0) {
+            const double w = m.wP[f];
+            uF = w * a.u[n] + (1.0 - w) * a.u[nb];
+            vF = w * a.v[n] + (1.0 - w) * a.v[nb];
+        } else {
+            uF = boundaryFaceValue(m, f, bcU, a.u[n]);
+            vF = boundaryFaceValue(m, f, bcV, a.v[n]);
+        }
+        const double unLin = uF * nz + vF * nr;
+        double un;
+        if (nb < 0) {
+            const int g = m.group[f];
+            if (g < 0 || g >= bcP.nGroups || bcP.type[g] != BC_DIRICHLET) {
+                un = unLin;
+            } else {
+                const double gc = (bcP.value[g] - a.p[n]) / m.dPB[f];
+                const double gn = a.gPZ[n] * nz + a.gPR[n] * nr;
+                un = unLin - Df * (gc - gn);
+            }
+        } else {
+            const double gpn = (a.p[nb] - a.p[n]) * m.invDPN[f];
+            const double w = m.wP[f];
+            const double gzf = w * a.gPZ[n] + (1.0 - w) * a.gPZ[nb];
+            const double grf = w * a.gPR[n] + (1.0 - w) * a.gPR[nb];
+            const double gfn = gzf * nz + grf * nr;
+            un = unLin - Df * (gpn - gfn);
+        }
+        a.mDot[f] = rho * un * area;
+    }
+    a.ACpp[n] = AC;
+    a.invACpp[n] = (fabs(AC) < 1.0e-30) ? 0.0 : 1.0 / AC;
+}
+
+// createPPRhs (simple.cu:90-142) + the p' reset before the corrector loop
+__global__ void __launch_bounds__(kThreads) k_pp_rhs(MeshDev m, const Ctl* ctl, double rho, const double* mDot,
+                                                     const double* DU, const double* DV, const double* gZ,
+                                                     const double* gR, int cross, int zeroPP, double* bpp,
+                                                     double* pp) {
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= m.N) return;
+    const int N = m.N;
+    double imb = 0.0, crossSum = 0.0;
+    for (int j = 0; j < m.W; j++) {
+        const int f = m.sface[(size_t)j * N + n];
+        if (f < 0) break;
+        const int own = m.owner[f], nb = m.neighbor[f];
+        const double md = mDot[f];
+        if (own == n) imb += md;
+        else if (nb == n) imb -= md;
+        if (cross) {
+            const double Df = interpCorr(m, DU, DV, n, f, own, nb);
+            crossSum += nonOrthoFlux(m, n, f, own, nb, gZ, gR, rho * Df);
+        }
+    }
+    bpp[n] = -imb + crossSum;
+    if (zeroPP) pp[n] = 0.0;
+}
+
+// updateMomentumPressure + updateMassFlux (simple.cu:166-258); the owner of
+// each face updates its mass flux.
+struct CorrectArgs {
+    double rho, alphaP;
+    int nonOrtho;
+    const double* pp;
+    const double* gZ;
+    const double* gR;
+    const double* DU;
+    const double* DV;
+    double* u;
+    double* v;
+    double* p;
+    double* mDot;
+};
+
+__global__ void __launch_bounds__(kThreads) k_correct(MeshDev m, const Ctl* ctl, BCDev bcP, CorrectArgs a) {
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= m.N) return;
+    const int N = m.N;
+    a.u[n] -= a.DU[n] * a.gZ[n];
+    a.v[n] -= a.DV[n] * a.gR[n];
+    a.p[n] += a.alphaP * a.pp[n];
+    const double rho = a.rho;
+    for (int j = 0; j < m.W; j++) {
+        const int f = m.sface[(size_t)j * N + n];
+        if (f < 0) break;
+        const int own = m.owner[f];
+        if (own != n) continue;
+        const int nb = m.neighbor[f];
+        const double area = m.area[f];
+        if (area <= 1.0e-30) {
+            a.mDot[f] = 0.0;
+            continue;
+        }
+        const double Df = interpCorr(m, a.DU, a.DV, n, f, own, nb);
+        if (nb >= 0) {
+            double md = a.mDot[f];
+            md -= rho * area * Df * (a.pp[nb] - a.pp[n]) * m.invDPN[f];
+            if (a.nonOrtho) md -= nonOrthoFlux(m, n, f, own, nb, a.gZ, a.gR, rho * Df);
+            a.mDot[f] = md;
+            continue;
+        }
+        const int g = m.group[f];
+        if (g < 0 || g >= bcP.nGroups) continue;
+        if (bcP.type[g] == BC_DIRICHLET) {
+            const double nz = m.nZ[f], nr = m.nR[f];
+            const double dPB = fabs((m.fcZ[f] - m.ccZ[n]) * nz + (m.fcR[f] - m.ccR[n]) * nr);
+            const double ppB = 0.0;
+            a.mDot[f] -= rho * area * Df * (ppB - a.pp[n]) / dPB;
+        }
+    }
+}
+
+// ---------------- residuals (residuals.cuh:17-60, residuals.cu:5-100) ----------------
+constexpr int kResQ = 5;  // |r_u| stat, scale_u, |r_v| stat, scale_v, continuity
+
+__device__ __forceinline__ double normStat(double r, int norm) {
+    return norm == 1 ? r * r : r;  // r is already |r|
+}
+
+__device__ __forceinline__ double combine(double a, double b, int isMax) { return isMax ? fmax(a, b) : a + b; }
+
+template <int NT>
+__device__ __forceinline__ void blockReduce(double (&v)[kResQ], const int (&isMax)[kResQ], double* out) {
+    __shared__ double sh[NT / 32][kResQ];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int q = 0; q < kResQ; q++) {
+        double x = v[q];
+        for (int o = 16; o > 0; o >>= 1) x = combine(x, __shfl_down_sync(0xffffffffu, x, o), isMax[q]);
+        if (lane == 0) sh[warp][q] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < kResQ; q++) {
+            double x = sh[0][q];
+            for (int w = 1; w < NT / 32; w++) x = combine(x, sh[w][q], isMax[q]);
+            out[q] = x;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_residual(MeshDev m, const Ctl* ctl, const double* AF, const double* ACu,
+                                                       const double* ACv, const double* bu, const double* bv,
+                                                       const double* u, const double* v, const double* mDot,
+                                                       double* resU, double* resV, double* resC, double* scaleU,
+                                                       double* scaleV, double* partial) {
+    if (ctl->done || !ctl->checked) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int N = m.N;
+    const int normU = ctl->resNorm[0], normV = ctl->resNorm[1];
+    const int isMax[kResQ] = {normU == 2, 0, normV == 2, 0, 0};
+    double acc[kResQ];
+    for (int q = 0; q < kResQ; q++) acc[q] = isMax[q] ? -INFINITY : 0.0;
+    if (n < N) {
+        double Axu = ACu[n] * u[n];
+        double Axv = ACv[n] * v[n];
+        const double su = Axu, sv = Axv;
+        double imb = 0.0;
+        for (int j = 0; j < m.W; j++) {
+            const size_t s = (size_t)j * N + n;
+            const int nb = m.snb[s];
+            if (nb >= 0) {
+                const double a = AF[s];
+                Axu += a * u[nb];
+                Axv += a * v[nb];
+            }
+            const int f = m.sface[s];
+            if (f >= 0) {
+                const double md = mDot[f];
+                if (m.owner[f] == n) imb += md;
+                else if (m.neighbor[f] == n) imb -= md;
+            }
+        }
+        const double ru = fabs(bu[n] - Axu);
+        const double rv = fabs(bv[n] - Axv);
+        resU[n] = ru;
+        resV[n] = rv;
+        resC[n] = imb;
+        scaleU[n] = su;
+        scaleV[n] = sv;
+        acc[0] = normStat(ru, normU);
+        acc[1] = fabs(su);
+        acc[2] = normStat(rv, normV);
+        acc[3] = fabs(sv);
+        acc[4] = fabs(imb);
+    }
+    blockReduce<kThreads>(acc, isMax, partial + (size_t)blockIdx.x * kResQ);
+}
+
+// Second reduction pass + residualAllHost's host arithmetic + convergence test
+// + iteration counters, all on the device (no host synchronisation).
+__global__ void __launch_bounds__(kThreads) k_iter_end(Ctl* ctl, const double* partial, int nBlocks, int N) {
+    if (ctl->done) return;
+    __shared__ double sh[kThreads][kResQ];
+    if (ctl->checked) {
+        const int isMax[kResQ] = {ctl->resNorm[0] == 2, 0, ctl->resNorm[1] == 2, 0, 0};
+        double acc[kResQ];
+        for (int q = 0; q < kResQ; q++) acc[q] = isMax[q] ? -INFINITY : 0.0;
+        for (int i = threadIdx.x; i < nBlocks; i += blockDim.x)
+            for (int q = 0; q < kResQ; q++) acc[q] = combine(acc[q], partial[(size_t)i * kResQ + q], isMax[q]);
+        for (int q = 0; q < kResQ; q++) sh[threadIdx.x][q] = acc[q];
+        __syncthreads();
+        for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+            if ((int)threadIdx.x < st)
+                for (int q = 0; q < kResQ; q++)
+                    sh[threadIdx.x][q] = combine(sh[threadIdx.x][q], sh[threadIdx.x + st][q], isMax[q]);
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x != 0) return;
+    if (ctl->checked) {
+        const double raw[3] = {sh[0][0], sh[0][2], sh[0][4]};
+        const double diag[2] = {sh[0][1], sh[0][3]};
+        const int scaleIteration = ctl->transient ? ctl->k : ctl->currentIteration;
+        for (int i = 0; i < 3; i++) {
+            if (!ctl->resEnabled[i]) continue;
+            ctl->resVal[i] = raw[i];
+            if (i < 2) {
+                switch (ctl->resScale[i]) {
+                    case 0: ctl->scaleVal[i] = 1.0; break;
+                    case 1: ctl->scaleVal[i] = (double)N; break;
+                    case 2: ctl->scaleVal[i] = sqrt((double)N); break;
+                    case 3: ctl->scaleVal[i] = diag[i]; break;
+                    default: break;
+                }
+            }
+        }
+        bool finite = true;
+        for (int i = 0; i < 3; i++) {
+            if (!ctl->resEnabled[i]) continue;
+            if (i == 2 && scaleIteration < 5) ctl->scaleVal[i] = fmax(ctl->resVal[i], 0.0);
+            if (ctl->scaleVal[i] == 0.0) continue;
+            if (ctl->resNorm[i] == 1) ctl->resVal[i] = sqrt(ctl->resVal[i]);
+            ctl->resVal[i] /= ctl->scaleVal[i];
+        }
+        bool any = false, conv = true;
+        for (int i = 0; i < 3; i++) {
+            if (!ctl->resEnabled[i]) continue;
+            any = true;
+            if (!(ctl->resVal[i] <= ctl->tol[i])) conv = false;
+            if (!isfinite(ctl->resVal[i])) finite = false;
+        }
+        ctl->converged = any && conv;
+        const int h = ctl->histCount % kMaxHist;
+        ctl->hist[h][0] = (double)ctl->currentIteration;
+        ctl->hist[h][1] = ctl->resVal[0];
+        ctl->hist[h][2] = ctl->resVal[1];
+        ctl->hist[h][3] = ctl->resVal[2];
+        ctl->histCount++;
+        if (ctl->converged) ctl->done = 1;
+        else if (!finite) ctl->done = 4;
+    }
+    ctl->k++;
+    ctl->currentIteration++;
+    ctl->itersThisCall++;
+}
+
+__global__ void k_copy(const Ctl* ctl, double* dst, const double* src, int n) {
+    if (ctl && ctl->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[i];
+}
+
+// ---------------- multigrid (multigrid.cu:350-541) ----------------
+// Galerkin A_H = P^T A P as a gather per coarse cell: the coarse diagonal sums
+// each member's AC plus its agglomerate-internal off-diagonals, the coarse
+// off-diagonals sum their feeding fine slots; both in ascending fine order.
+__global__ void __launch_bounds__(kThreads) k_galerkin(const Ctl* ctl, LevelDev F, LevelDev C) {
+    if (ctl->done) return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C.N) return;
+    double ac = 0.0;
+    for (int q = C.mStart[c]; q < C.mStart[c + 1]; q++) {
+        const int n = C.mList[q];
+        double diag = F.AC[n];
+        uint32_t mask = F.internalMask[n];
+        while (mask) {
+            const int j = __ffs(mask) - 1;
+            mask &= mask - 1;
+            diag += F.AF[(size_t)j * F.N + n];
+        }
+        ac += diag;
+    }
+    C.AC[c] = ac;
+    for (int j = 0; j < C.W; j++) {
+        const size_t s = (size_t)j * C.N + c;
+        double af = 0.0;
+        for (int q = C.gStart[s]; q < C.gStart[s + 1]; q++) af += F.AF[C.gList[q]];
+        C.AF[s] = af;
+    }
+}
+
+// weighted Jacobi, jacobiRow (multigrid.cu:447-484)
+__global__ void __launch_bounds__(kThreads) k_mg_smooth(const Ctl* ctl, int N, int W, const int32_t* __restrict__ nb,
+                                                        const double* __restrict__ AF, const double* __restrict__ AC,
+                                                        const double* __restrict__ b, const double* __restrict__ x,
+                                                        double* __restrict__ y, double w) {
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const double ac = AC[n];
+    if (fabs(ac) < 1.0e-30) {
+        y[n] = x[n];
+        return;
+    }
+    double Ax = ac * x[n];
+    for (int j = 0; j < W; j++) {
+        const size_t s = (size_t)j * N + n;
+        const int k = nb[s];
+        if (k != -1) Ax += AF[s] * x[k];
+    }
+    y[n] = x[n] + w * (b[n] - Ax) / ac;
+}
+
+// Whole-level weighted Jacobi inside one CTA with a shared-memory ping-pong
+// (jacobiSingleBlock, multigrid.cu:501-541). N <= blockDim.x.
+__global__ void k_mg_smooth_block(const Ctl* ctl, int N, int W, const int32_t* __restrict__ nb,
+                                  const double* __restrict__ AF, const double* __restrict__ AC,
+                                  const double* __restrict__ b, double* x, double w, int sweeps) {
+    if (ctl->done) return;
+    extern __shared__ double sx[];
+    double* xo = sx;
+    double* xn = sx + N;
+    const int n = threadIdx.x;
+    if (n < N) xo[n] = x[n];
+    __syncthreads();
+    for (int it = 0; it < sweeps; it++) {
+        if (n < N) {
+            const double ac = AC[n];
+            if (fabs(ac) < 1.0e-30) {
+                xn[n] = xo[n];
+            } else {
+                double Ax = ac * xo[n];
+                for (int j = 0; j < W; j++) {
+                    const size_t s = (size_t)j * N + n;
+                    const int k = nb[s];
+                    if (k != -1) Ax += AF[s] * xo[k];
+                }
+                xn[n] = xo[n] + w * (b[n] - Ax) / ac;
+            }
+        }
+        __syncthreads();
+        double* t = xo;
+        xo = xn;
+        xn = t;
+    }
+    if (n < N) x[n] = xo[n];
+}
+
+// residual (residualAll with sign) fused into the restriction: each coarse cell
+// sums its members' b - Ax in ascending order, and zeroes its correction.
+__global__ void __launch_bounds__(kThreads) k_mg_restrict(const Ctl* ctl, LevelDev F, const double* __restrict__ x,
+                                                          LevelDev C) {
+    if (ctl->done) return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C.N) return;
+    double sum = 0.0;
+    for (int q = C.mStart[c]; q < C.mStart[c + 1]; q++) {
+        const int n = C.mList[q];
+        double Ax = F.AC[n] * x[n];
+        for (int j = 0; j < F.W; j++) {
+            const size_t s = (size_t)j * F.N + n;
+            const int k = F.nb[s];
+            if (k >= 0) Ax += F.AF[s] * x[k];
+        }
+        sum += F.b[n] - Ax;
+    }
+    C.b[c] = sum;
+    C.x[c] = 0.0;
+}
+
+__global__ void __launch_bounds__(kThreads) k_mg_prolong(const Ctl* ctl, int N, const int32_t* __restrict__ c2c,
+                                                         double* x, const double* __restrict__ xc) {
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    x[n] += xc[c2c[n]];
+}
+
+}  // namespace
+
+// ---------------- launchers ----------------
+void launchPrecompute(const MeshDev& m, const int32_t* cfs, const int32_t* cfi, double* lsqDZ, double* lsqDR,
+                      cudaStream_t s) {
+    k_precompute_faces<<<blocksFor(m.F), kThreads, 0, s>>>(m, const_cast<double*>(m.invDPN), const_cast<double*>(m.wP),
+                                                            const_cast<double*>(m.dPB), const_cast<double*>(m.length2D),
+                                                            const_cast<double*>(m.lsqWZ), const_cast<double*>(m.lsqWR),
+                                                            lsqDZ, lsqDR);
+    k_precompute_cells<<<blocksFor(m.N), kThreads, 0, s>>>(m, cfs, cfi, lsqDZ, lsqDR, const_cast<double*>(m.invA2D),
+                                                            const_cast<double*>(m.lsqIZZ), const_cast<double*>(m.lsqIZR),
+                                                            const_cast<double*>(m.lsqIRR));
+}
+
+void launchBuildEll(int N, int W, const int32_t* cfs, const int32_t* cfi, const int32_t* owner,
+                    const int32_t* neighbor, int32_t* sface, int32_t* snb, cudaStream_t s) {
+    k_build_ell<<<blocksFor(N), kThreads, 0, s>>>(N, W, cfs, cfi, owner, neighbor, sface, snb);
+}
+
+void launchIterBegin(Ctl* ctl, const volatile int* hostStop, cudaStream_t s) {
+    k_iter_begin<<<1, 1, 0, s>>>(ctl, hostStop);
+}
+
+void launchGradient(const MeshDev& m, const Ctl* ctl, int nFields, const double* const* phi, const BCDev* bc,
+                    double* const* gZ, double* const* gR, int scheme, cudaStream_t s) {
+    GradArgs a{};
+    for (int q = 0; q < nFields; q++) {
+        a.phi[q] = phi[q];
+        a.bc[q] = bc[q];
+        a.gZ[q] = gZ[q];
+        a.gR[q] = gR[q];
+    }
+    const int b = blocksFor(m.N);
+    if (nFields == 1) k_gradient<1><<<b, kThreads, 0, s>>>(m, ctl, a, scheme);
+    else if (nFields == 2) k_gradient<2><<<b, kThreads, 0, s>>>(m, ctl, a, scheme);
+    else k_gradient<3><<<b, kThreads, 0, s>>>(m, ctl, a, scheme);
+}
+
+void launchMomentum(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, const BCDev& bcV, const MomentumArgs& a,
+                    cudaStream_t s) {
+    k_momentum<<<blocksFor(m.N), kThreads, 0, s>>>(m, ctl, bcU, bcV, a);
+}
+
+void launchJacobiUV(const MeshDev& m, const Ctl* ctl, const double* AF, const double* bu, const double* bv,
+                    const double* iu, const double* iv, const double* xu, const double* xv, double* yu, double* yv,
+                    cudaStream_t s) {
+    k_jacobi_uv<<<blocksFor(m.N), kThreads, 0, s>>>(m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
+}
+
+void launchGaussSeidelUV(const MeshDev& m, const Ctl* ctl, const double* AF, const double* bu, const double* bv,
+                         const double* iu, const double* iv, double* xu, double* xv, const int32_t* order, int begin,
+                         int count, cudaStream_t s) {
+    k_gs_uv<<<blocksFor(count), kThreads, 0, s>>>(m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, order, begin,
+                                                  count);
+}
+
+void launchPressureSystem(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, const BCDev& bcV, const BCDev& bcP,
+                          double rho, const double* u, const double* v, const double* p, const double* gPZ,
+                          const double* gPR, const double* DU, const double* DV, double* AFpp, double* ACpp,
+                          double* invACpp, double* mDot, cudaStream_t s) {
+    PressureArgs a{rho, u, v, p, gPZ, gPR, DU, DV, AFpp, ACpp, invACpp, mDot};
+    k_pressure<<<blocksFor(m.N), kThreads, 0, s>>>(m, ctl, bcU, bcV, bcP, a);
+}
+
+void launchPressureRhs(const MeshDev& m, const Ctl* ctl, double rho, const double* mDot, const double* DU,
+                       const double* DV, const double* gZ, const double* gR, int cross, int zeroPP, double* bpp,
+                       double* pp, cudaStream_t s) {
+    k_pp_rhs<<<blocksFor(m.N), kThreads, 0, s>>>(m, ctl, rho, mDot, DU, DV, gZ, gR, cross, zeroPP, bpp, pp);
+}
+
+void launchJacobi1(const MeshDev& m, const Ctl* ctl, const double* AF, const double* b, const double* inv,
+                   const double* x, double* y, cudaStream_t s) {
+    k_jacobi1<<<blocksFor(m.N), kThreads, 0, s>>>(m.N, m.W, m.snb, ctl, AF, b, inv, x, y);
+}
+
+void launchGaussSeidel1(const MeshDev& m, const Ctl* ctl, const double* AF, const double* b, const double* inv,
+                        double* x, const int32_t* order, int begin, int count, cudaStream_t s) {
+    k_gs1<<<blocksFor(count), kThreads, 0, s>>>(m.N, m.W, m.snb, ctl, AF, b, inv, x, order, begin, count);
+}
+
+void launchCorrect(const MeshDev& m, const Ctl* ctl, const BCDev& bcP, double rho, double alphaP, int nonOrtho,
+                   const double* pp, const double* gZ, const double* gR, const double* DU, const double* DV, double* u,
+                   double* v, double* p, double* mDot, cudaStream_t s) {
+    CorrectArgs a{rho, alphaP, nonOrtho, pp, gZ, gR, DU, DV, u, v, p, mDot};
+    k_correct<<<blocksFor(m.N), kThreads, 0, s>>>(m, ctl, bcP, a);
+}
+
+void launchResiduals(const MeshDev& m, const Ctl* ctl, const double* AF, const double* ACu, const double* ACv,
+                     const double* bu, const double* bv, const double* u, const double* v, const double* mDot,
+                     double* resU, double* resV, double* resC, double* scaleU, double* scaleV, double* partial,
+                     int* nBlocksOut, cudaStream_t s) {
+    const int b = blocksFor(m.N);
+    *nBlocksOut = b;
+    k_residual<<<b, kThreads, 0, s>>>(m, ctl, AF, ACu, ACv, bu, bv, u, v, mDot, resU, resV, resC, scaleU, scaleV,
+                                      partial);
+}
+
+void launchIterEnd(Ctl* ctl, const double* partial, int nBlocks, int N, cudaStream_t s) {
+    k_iter_end<<<1, kThreads, 0, s>>>(ctl, partial, nBlocks, N);
+}
+
+void launchCopy(const Ctl* ctl, double* dst, const double* src, int n, cudaStream_t s) {
+    k_copy<<<blocksFor(n), kThreads, 0, s>>>(ctl, dst, src, n);
+}
+
+void launchGalerkin(const Ctl* ctl, const LevelDev& fine, const LevelDev& coarse, cudaStream_t s) {
+    k_galerkin<<<blocksFor(coarse.N), kThreads, 0, s>>>(ctl, fine, coarse);
+}
+
+void launchMGSmooth(const Ctl* ctl, const LevelDev& L, const double* x, double* y, double w, cudaStream_t s) {
+    k_mg_smooth<<<blocksFor(L.N), kThreads, 0, s>>>(ctl, L.N, L.W, L.nb, L.AF, L.AC, L.b, x, y, w);
+}
+
+void launchMGSmoothBlock(const Ctl* ctl, const LevelDev& L, double* x, double w, int sweeps, cudaStream_t s) {
+    const int threads = ((L.N + 31) / 32) * 32;
+    k_mg_smooth_block<<<1, threads, 2 * (size_t)L.N * sizeof(double), s>>>(ctl, L.N, L.W, L.nb, L.AF, L.AC, L.b, x,
+                                                                          w, sweeps);
+}
+
+void launchMGRestrict(const Ctl* ctl, const LevelDev& fine, const double* xFine, LevelDev& coarse, cudaStream_t s) {
+    k_mg_restrict<<<blocksFor(coarse.N), kThreads, 0, s>>>(ctl, fine, xFine, coarse);
+}
+
+void launchMGProlong(const Ctl* ctl, const LevelDev& fine, double* xFine, const double* xCoarse, cudaStream_t s) {
+    k_mg_prolong<<<blocksFor(fine.N), kThreads, 0, s>>>(ctl, fine.N, fine.c2c, xFine, xCoarse);
+}
+
+}  // namespace axisim

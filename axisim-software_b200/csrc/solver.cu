@@ -1,0 +1,1188 @@
+// solver.cu -- host orchestration of the B200 SIMPLE solver and its C ABI.
+//
+// Follows Solver::runSimple (solver/source/solver.cpp:753-1396): same set-up,
+// time loop, SIMPLE iteration and convergence rules. Differences by design:
+//   * one SIMPLE iteration is captured ONCE as a CUDA graph (the reference
+//     captures only the linear solves) and replayed in batches; convergence is
+//     decided on the device, so there is no host synchronisation per iteration
+//     (the reference syncs in residualAllHost, residuals.cu:79);
+//   * the multigrid hierarchy operators live in the same graph;
+//   * errors come back as status codes, never abort().
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/axisim_b200.h"
+#include "host_prep.hpp"
+#include "kernels.hpp"
+
+namespace axisim {
+
+namespace {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(x) check((x), #x)
+
+struct StatusError : std::runtime_error {
+    int status;
+    StatusError(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+}  // namespace
+
+// Every device allocation of a solver; freed together.
+class Arena {
+public:
+    ~Arena() { release(); }
+    template <class T>
+    T* alloc(size_t n) {
+        void* p = nullptr;
+        CK(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+        ptrs_.push_back(p);
+        CK(cudaMemset(p, 0, std::max<size_t>(n, 1) * sizeof(T)));
+        return static_cast<T*>(p);
+    }
+    template <class T>
+    T* upload(const T* h, size_t n) {
+        T* d = alloc<T>(n);
+        if (n) CK(cudaMemcpy(d, h, n * sizeof(T), cudaMemcpyHostToDevice));
+        return d;
+    }
+    void release() {
+        for (void* p : ptrs_) cudaFree(p);
+        ptrs_.clear();
+    }
+
+private:
+    std::vector<void*> ptrs_;
+};
+
+struct HostBC {
+    int nGroups = 0;
+    std::vector<uint8_t> type, btype, puls;
+    std::vector<double> value, length, amp, freq;
+};
+
+class Solver {
+public:
+    explicit Solver(const axisim_fluid& f) : fluid_(f) {
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        CK(cudaHostAlloc(&hostStop_, sizeof(int), cudaHostAllocMapped));
+        *hostStop_ = 0;
+        CK(cudaHostGetDevicePointer((void**)&hostStopDev_, (void*)hostStop_, 0));
+        CK(cudaEventCreate(&ev0_));
+        CK(cudaEventCreate(&ev1_));
+        defaults();
+    }
+    ~Solver() {
+        destroyGraph();
+        if (stream_) cudaStreamSynchronize(stream_);
+        meshArena_.release();
+        mgArena_.release();
+        bcArena_.release();
+        if (hostStop_) cudaFreeHost((void*)hostStop_);
+        if (hostBCStage_) cudaFreeHost(hostBCStage_);
+        if (ev0_) cudaEventDestroy(ev0_);
+        if (ev1_) cudaEventDestroy(ev1_);
+        if (stream_) cudaStreamDestroy(stream_);
+    }
+
+    std::string lastError;
+    axisim_log_fn logFn = nullptr;
+    axisim_residual_fn resFn = nullptr;
+    void* cbCtx = nullptr;
+
+    void defaults() {
+        std::memset(&cs_, 0, sizeof(cs_));
+        cs_.convectionScheme = 0;
+        cs_.gradientScheme = 1;
+        cs_.type = 0;
+        cs_.linearMaxIter = 20;
+        cs_.useMultigrid = 1;
+        cs_.addConvectionTerm = 1;
+        cs_.dt = 0.1;
+        cs_.tEnd = 2.0;
+        cs_.saveKeyFrameIter = 2;
+        csim_ = axisim_config_simple{50, 1, 1e-8, 1e-5};
+        cmg_ = axisim_config_multigrid{3, 0.6, 30, 1, 1};
+        for (int i = 0; i < 3; i++) cres_[i] = axisim_config_residual{0, 0, 3, 1, 1e-3};
+        alphaU_ = 0.7;
+        alphaP_ = 0.3;
+    }
+
+    void setFluid(const axisim_fluid& f) {
+        fluid_ = f;
+        destroyGraph();
+    }
+
+    void setPrecision(int mode) {
+        if (mode != AXISIM_PREC_FP64 && mode != AXISIM_PREC_MIXED) throw StatusError(AXISIM_E_ARG, "unknown precision mode");
+        if (mode == AXISIM_PREC_MIXED) throw StatusError(AXISIM_E_CONFIG, "mixed precision is not built in this library");
+        precision_ = mode;
+        destroyGraph();
+    }
+
+    // ---------------- mesh ----------------
+    void setMesh(const axisim_mesh_packed& pm) {
+        const int N = pm.nCells, F = pm.nFaces;
+        if (N <= 0 || F <= 0) throw StatusError(AXISIM_E_MESH, "mesh needs cells and faces");
+        const void* req[] = {pm.faceOwner, pm.faceNeighbor, pm.faceNormalZ, pm.faceNormalR, pm.faceCenterZ,
+                             pm.faceCenterR, pm.faceArea, pm.faceBoundaryGroupID, pm.cellCenterZ, pm.cellCenterR,
+                             pm.cellVolume, pm.cellFaceStart, pm.cellFaceIDs};
+        for (const void* p : req)
+            if (!p) throw StatusError(AXISIM_E_ARG, "mesh array is null");
+        if (pm.cellFaceStart[0] != 0) throw StatusError(AXISIM_E_MESH, "cellFaceStart[0] must be 0");
+        int W = 0;
+        for (int c = 0; c < N; c++) {
+            const int d = pm.cellFaceStart[c + 1] - pm.cellFaceStart[c];
+            if (d < 0) throw StatusError(AXISIM_E_MESH, "cellFaceStart is not monotone");
+            W = std::max(W, d);
+        }
+        if (W > 32) throw StatusError(AXISIM_E_MESH, "a cell has more than 32 faces");
+        const int S = pm.cellFaceStart[N];
+        for (int k = 0; k < S; k++)
+            if (pm.cellFaceIDs[k] < 0 || pm.cellFaceIDs[k] >= F) throw StatusError(AXISIM_E_MESH, "cellFaceIDs out of range");
+        for (int f = 0; f < F; f++) {
+            if (pm.faceOwner[f] < 0 || pm.faceOwner[f] >= N) throw StatusError(AXISIM_E_MESH, "faceOwner out of range");
+            if (pm.faceNeighbor[f] >= N) throw StatusError(AXISIM_E_MESH, "faceNeighbor out of range");
+        }
+        destroyGraph();
+        mgArena_.release();
+        levels_.clear();
+        hier_.clear();
+        haveHierarchy_ = false;
+        colorN_ = 0;
+        meshArena_.release();
+        N_ = N;
+        F_ = F;
+        S_ = S;
+        W_ = W;
+        hCfs_.assign(pm.cellFaceStart, pm.cellFaceStart + N + 1);
+        hCfi_.assign(pm.cellFaceIDs, pm.cellFaceIDs + S);
+        hOwner_.assign(pm.faceOwner, pm.faceOwner + F);
+        hNeighbor_.assign(pm.faceNeighbor, pm.faceNeighbor + F);
+        Arena& A = meshArena_;
+        MeshDev& m = mesh_;
+        m.N = N;
+        m.F = F;
+        m.W = W;
+        m.owner = A.upload(pm.faceOwner, F);
+        m.neighbor = A.upload(pm.faceNeighbor, F);
+        m.group = A.upload(pm.faceBoundaryGroupID, F);
+        m.nZ = A.upload(pm.faceNormalZ, F);
+        m.nR = A.upload(pm.faceNormalR, F);
+        m.fcZ = A.upload(pm.faceCenterZ, F);
+        m.fcR = A.upload(pm.faceCenterR, F);
+        m.area = A.upload(pm.faceArea, F);
+        m.ccZ = A.upload(pm.cellCenterZ, N);
+        m.ccR = A.upload(pm.cellCenterR, N);
+        m.vol = A.upload(pm.cellVolume, N);
+        m.invDPN = A.alloc<double>(F);
+        m.wP = A.alloc<double>(F);
+        m.dPB = A.alloc<double>(F);
+        m.length2D = A.alloc<double>(F);
+        m.lsqWZ = A.alloc<double>(F);
+        m.lsqWR = A.alloc<double>(F);
+        m.invA2D = A.alloc<double>(N);
+        m.lsqIZZ = A.alloc<double>(N);
+        m.lsqIZR = A.alloc<double>(N);
+        m.lsqIRR = A.alloc<double>(N);
+        int32_t* dCfs = A.upload(pm.cellFaceStart, (size_t)N + 1);
+        int32_t* dCfi = A.upload(pm.cellFaceIDs, (size_t)S);
+        int32_t* sface = A.alloc<int32_t>((size_t)W * N);
+        int32_t* snb = A.alloc<int32_t>((size_t)W * N);
+        m.sface = sface;
+        m.snb = snb;
+        double* tz = A.alloc<double>(F);
+        double* tr = A.alloc<double>(F);
+        launchPrecompute(m, dCfs, dCfi, tz, tr, stream_);
+        launchBuildEll(N, W, dCfs, dCfi, m.owner, m.neighbor, sface, snb, stream_);
+        CK(cudaGetLastError());
+        // fields and coefficient systems (allocateSimple / allocateCoefficients)
+        const size_t WN = (size_t)W * N;
+        u_ = A.alloc<double>(N); v_ = A.alloc<double>(N); p_ = A.alloc<double>(N); pp_ = A.alloc<double>(N);
+        uT_ = A.alloc<double>(N); vT_ = A.alloc<double>(N); ppT_ = A.alloc<double>(N);
+        DU_ = A.alloc<double>(N); DV_ = A.alloc<double>(N);
+        gPZ_ = A.alloc<double>(N); gPR_ = A.alloc<double>(N);
+        gUZ_ = A.alloc<double>(N); gUR_ = A.alloc<double>(N); gVZ_ = A.alloc<double>(N); gVR_ = A.alloc<double>(N);
+        uOld_ = A.alloc<double>(N); vOld_ = A.alloc<double>(N); uOld2_ = A.alloc<double>(N); vOld2_ = A.alloc<double>(N);
+        mDot_ = A.alloc<double>(F);
+        AFm_ = A.alloc<double>(WN);
+        ACu_ = A.alloc<double>(N); ACv_ = A.alloc<double>(N); bu_ = A.alloc<double>(N); bv_ = A.alloc<double>(N);
+        iu_ = A.alloc<double>(N); iv_ = A.alloc<double>(N);
+        AFpp_ = A.alloc<double>(WN); ACpp_ = A.alloc<double>(N); bpp_ = A.alloc<double>(N); ipp_ = A.alloc<double>(N);
+        resU_ = A.alloc<double>(N); resV_ = A.alloc<double>(N); resC_ = A.alloc<double>(N);
+        scU_ = A.alloc<double>(N); scV_ = A.alloc<double>(N);
+        partial_ = A.alloc<double>((size_t)((N + 255) / 256) * 5 + 5);
+        ctl_ = A.alloc<Ctl>(1);
+        CK(cudaStreamSynchronize(stream_));
+        haveMesh_ = true;
+        isReady_ = false;
+    }
+
+    void setBC(int var, const axisim_bc_field& b) {
+        if (var < 0 || var > 2) throw StatusError(AXISIM_E_ARG, "variable must be 0 (u), 1 (v) or 2 (p)");
+        if (b.nGroups < 0 || (b.nGroups > 0 && (!b.typeByGroup || !b.valueByGroup)))
+            throw StatusError(AXISIM_E_ARG, "bc arrays are null");
+        HostBC h;
+        const int G = b.nGroups;
+        h.nGroups = G;
+        h.type.assign(b.typeByGroup, b.typeByGroup + G);
+        h.btype = b.boundaryTypeByGroup ? std::vector<uint8_t>(b.boundaryTypeByGroup, b.boundaryTypeByGroup + G)
+                                        : std::vector<uint8_t>((size_t)G, 0);
+        h.value.assign(b.valueByGroup, b.valueByGroup + G);
+        h.length = b.lengthByGroup ? std::vector<double>(b.lengthByGroup, b.lengthByGroup + G)
+                                   : std::vector<double>((size_t)G, 0.0);
+        h.puls.assign((size_t)G, 0);
+        h.amp.assign((size_t)G, 0.0);
+        h.freq.assign((size_t)G, 0.0);
+        for (int g = 0; g < G; g++) {
+            if (h.type[(size_t)g] == AXISIM_BC_PULSATILE) h.type[(size_t)g] = AXISIM_BC_DIRICHLET;
+            if (b.pulsatileByGroup && b.pulsatileByGroup[g]) {
+                h.puls[(size_t)g] = 1;
+                h.amp[(size_t)g] = b.amplitudeByGroup ? b.amplitudeByGroup[g] : 0.0;
+                h.freq[(size_t)g] = b.frequencyByGroup ? b.frequencyByGroup[g] : 0.0;
+            }
+        }
+        hbc_[var] = h;
+        haveBC_[var] = true;
+        bcDirty_ = true;
+    }
+
+    void setConfig(const axisim_config_solver* s, const axisim_config_simple* sim, const axisim_config_multigrid* mg,
+                   const axisim_config_residual* r3, double aU, double aP) {
+        if (s) cs_ = *s;
+        if (sim) csim_ = *sim;
+        if (mg) cmg_ = *mg;
+        if (r3)
+            for (int i = 0; i < 3; i++) cres_[i] = r3[i];
+        alphaU_ = aU;
+        alphaP_ = aP;
+        destroyGraph();
+    }
+
+    bool canContinue(std::string* reason) const {
+        auto why = [&](const char* t) {
+            if (reason) *reason = t;
+            return false;
+        };
+        if (running_) return why("Solver is already running.");
+        if (!isReady_) return why("Run the solver once before continuing.");
+        if (!haveMesh_) return why("Generate a valid mesh first.");
+        return true;
+    }
+
+    void requestStop() {
+        if (running_) __atomic_store_n(hostStop_, 1, __ATOMIC_SEQ_CST);
+    }
+
+    int solve(int continueRun, axisim_result* res);
+
+    int64_t getField(const std::string& name, double* out, size_t n) const;
+    int64_t setField(const std::string& name, const double* in, size_t n);
+
+    int mgLevels(int32_t* cells, int maxL) {
+        ensureHierarchy();
+        for (int l = 0; l < (int)hier_.size() && l < maxL; l++) cells[l] = hier_[(size_t)l].nCells;
+        return (int)hier_.size();
+    }
+    int64_t mgLevelMaps(int level, int32_t* c2c, int32_t* f2c, int32_t* cfs, int32_t* cfn) {
+        ensureHierarchy();
+        if (level < 0 || level + 1 >= (int)hier_.size()) throw StatusError(AXISIM_E_ARG, "level out of range");
+        const GridLevel& f = hier_[(size_t)level];
+        const GridLevel& c = hier_[(size_t)level + 1];
+        if (c2c) std::copy(f.cellToCoarse.begin(), f.cellToCoarse.end(), c2c);
+        if (f2c) std::copy(f.fineSlotToCoarseSlot.begin(), f.fineSlotToCoarseSlot.end(), f2c);
+        if (cfs) std::copy(c.faceStart.begin(), c.faceStart.end(), cfs);
+        if (cfn) std::copy(c.faceNeighbor.begin(), c.faceNeighbor.end(), cfn);
+        return c.nFaceRefs();
+    }
+    int coloring(int32_t* out, size_t n) {
+        ensureColoring();
+        if (n < (size_t)N_) throw StatusError(AXISIM_E_ARG, "buffer too small");
+        std::copy(hColor_.begin(), hColor_.end(), out);
+        return colorN_;
+    }
+
+private:
+    axisim_fluid fluid_;
+    axisim_config_solver cs_;
+    axisim_config_simple csim_;
+    axisim_config_multigrid cmg_;
+    axisim_config_residual cres_[3];
+    double alphaU_ = 0.7, alphaP_ = 0.3;
+    int precision_ = AXISIM_PREC_FP64;
+
+    cudaStream_t stream_ = nullptr;
+    volatile int* hostStop_ = nullptr;
+    int* hostStopDev_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    std::atomic<bool> running_{false};
+    bool isReady_ = false;
+    double simTime_ = 0.0;
+
+    // mesh
+    bool haveMesh_ = false;
+    int N_ = 0, F_ = 0, S_ = 0, W_ = 0;
+    std::vector<int32_t> hCfs_, hCfi_, hOwner_, hNeighbor_;
+    Arena meshArena_, mgArena_, bcArena_;
+    MeshDev mesh_;
+    double *u_ = nullptr, *v_ = nullptr, *p_ = nullptr, *pp_ = nullptr, *uT_ = nullptr, *vT_ = nullptr, *ppT_ = nullptr;
+    double *DU_ = nullptr, *DV_ = nullptr, *gPZ_ = nullptr, *gPR_ = nullptr, *gUZ_ = nullptr, *gUR_ = nullptr;
+    double *gVZ_ = nullptr, *gVR_ = nullptr, *uOld_ = nullptr, *vOld_ = nullptr, *uOld2_ = nullptr, *vOld2_ = nullptr;
+    double *mDot_ = nullptr, *AFm_ = nullptr, *ACu_ = nullptr, *ACv_ = nullptr, *bu_ = nullptr, *bv_ = nullptr;
+    double *iu_ = nullptr, *iv_ = nullptr, *AFpp_ = nullptr, *ACpp_ = nullptr, *bpp_ = nullptr, *ipp_ = nullptr;
+    double *resU_ = nullptr, *resV_ = nullptr, *resC_ = nullptr, *scU_ = nullptr, *scV_ = nullptr, *partial_ = nullptr;
+    Ctl* ctl_ = nullptr;
+
+    // boundary conditions
+    HostBC hbc_[3];
+    bool haveBC_[3] = {false, false, false};
+    bool bcDirty_ = true;
+    BCDev bc_[4];  // u, v, p, p'
+    double* bcValueDev_[2] = {nullptr, nullptr};
+    double* hostBCStage_ = nullptr;
+
+    // multigrid / colouring
+    std::vector<GridLevel> hier_;
+    bool haveHierarchy_ = false;
+    std::vector<LevelDev> levels_;
+    std::vector<int32_t> hColor_, hColorStart_;
+    int colorN_ = 0;
+    int32_t* dCellOrder_ = nullptr;
+
+    // graph
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t exec_ = nullptr;
+    int residualBlocks_ = 0;
+
+    void destroyGraph() {
+        if (exec_) cudaGraphExecDestroy(exec_);
+        if (graph_) cudaGraphDestroy(graph_);
+        exec_ = nullptr;
+        graph_ = nullptr;
+    }
+
+    void log(const std::string& s) {
+        if (logFn) logFn(cbCtx, s.c_str());
+    }
+
+    void uploadBC() {
+        if (!bcDirty_) return;
+        bcArena_.release();
+        for (int var = 0; var < 3; var++) {
+            const HostBC& h = hbc_[var];
+            BCDev d;
+            d.nGroups = h.nGroups;
+            d.type = bcArena_.upload(h.type.data(), h.type.size());
+            d.value = bcArena_.upload(h.value.data(), h.value.size());
+            d.length = bcArena_.upload(h.length.data(), h.length.size());
+            bc_[var] = d;
+            if (var < 2) bcValueDev_[var] = const_cast<double*>(d.value);
+        }
+        // p' boundary field: p's types with every value zero (solver.cpp:788-795)
+        BCDev pp = bc_[2];
+        std::vector<double> zeros((size_t)std::max(hbc_[2].nGroups, 1), 0.0);
+        pp.value = bcArena_.upload(zeros.data(), zeros.size());
+        bc_[3] = pp;
+        int maxG = std::max(hbc_[0].nGroups, hbc_[1].nGroups);
+        if (hostBCStage_) cudaFreeHost(hostBCStage_);
+        hostBCStage_ = nullptr;
+        CK(cudaHostAlloc((void**)&hostBCStage_, sizeof(double) * 2 * (size_t)std::max(maxG, 1), cudaHostAllocDefault));
+        bcDirty_ = false;
+        destroyGraph();
+    }
+
+    void ensureHierarchy() {
+        if (haveHierarchy_) return;
+        if (!haveMesh_) throw StatusError(AXISIM_E_STATE, "no mesh");
+        hier_ = buildHierarchy(finestLevel(N_, F_, hCfs_.data(), hCfi_.data(), hOwner_.data(), hNeighbor_.data()));
+        haveHierarchy_ = true;
+        levels_.clear();
+        mgArena_.release();
+    }
+
+    void ensureColoring() {
+        if (colorN_ > 0) return;
+        GridLevel g = finestLevel(N_, F_, hCfs_.data(), hCfi_.data(), hOwner_.data(), hNeighbor_.data());
+        colorN_ = greedyColoring(g, hColor_);
+        hColorStart_.assign((size_t)colorN_ + 1, 0);
+        for (int c = 0; c < N_; c++) hColorStart_[(size_t)hColor_[(size_t)c] + 1]++;
+        for (int k = 0; k < colorN_; k++) hColorStart_[(size_t)k + 1] += hColorStart_[(size_t)k];
+        std::vector<int32_t> order((size_t)N_);
+        std::vector<int32_t> fill(hColorStart_);
+        for (int c = 0; c < N_; c++) order[(size_t)fill[(size_t)hColor_[(size_t)c]]++] = c;
+        dCellOrder_ = meshArena_.upload(order.data(), order.size());
+    }
+
+    // Device copies of the hierarchy: ELL topology, Galerkin/restriction gathers.
+    void ensureDeviceLevels() {
+        ensureHierarchy();
+        if (!levels_.empty()) return;
+        const int L = (int)hier_.size();
+        levels_.resize((size_t)L);
+        for (int l = 0; l < L; l++) {
+            const GridLevel& g = hier_[(size_t)l];
+            LevelDev& d = levels_[(size_t)l];
+            d.N = g.nCells;
+            if (l == 0) {
+                d.W = W_;
+                d.nb = const_cast<int32_t*>(mesh_.snb);
+                d.AF = AFpp_;
+                d.AC = ACpp_;
+                d.b = bpp_;
+                d.x = pp_;
+                d.xNew = ppT_;
+            } else {
+                int W = 0;
+                for (int c = 0; c < g.nCells; c++) W = std::max(W, g.faceStart[(size_t)c + 1] - g.faceStart[(size_t)c]);
+                d.W = W;
+                std::vector<int32_t> nb((size_t)W * g.nCells, -1);
+                for (int c = 0; c < g.nCells; c++)
+                    for (int k = g.faceStart[(size_t)c], j = 0; k < g.faceStart[(size_t)c + 1]; k++, j++)
+                        nb[(size_t)j * g.nCells + c] = g.faceNeighbor[(size_t)k];
+                d.nb = mgArena_.upload(nb.data(), nb.size());
+                d.AF = mgArena_.alloc<double>(nb.size());
+                d.AC = mgArena_.alloc<double>((size_t)g.nCells);
+                d.b = mgArena_.alloc<double>((size_t)g.nCells);
+                d.x = mgArena_.alloc<double>((size_t)g.nCells);
+                d.xNew = mgArena_.alloc<double>((size_t)g.nCells);
+            }
+            if (!g.isCoarsest()) d.c2c = mgArena_.upload(g.cellToCoarse.data(), g.cellToCoarse.size());
+        }
+        // gathers for coarse level l from fine level l-1
+        for (int l = 1; l < L; l++) {
+            const GridLevel& f = hier_[(size_t)l - 1];
+            const GridLevel& c = hier_[(size_t)l];
+            LevelDev& fd = levels_[(size_t)l - 1];
+            LevelDev& cd = levels_[(size_t)l];
+            // members of each coarse cell, ascending fine id
+            std::vector<int32_t> mStart((size_t)c.nCells + 1, 0), mList((size_t)f.nCells);
+            for (int n = 0; n < f.nCells; n++) mStart[(size_t)f.cellToCoarse[(size_t)n] + 1]++;
+            for (int k = 0; k < c.nCells; k++) mStart[(size_t)k + 1] += mStart[(size_t)k];
+            {
+                std::vector<int32_t> fill(mStart);
+                for (int n = 0; n < f.nCells; n++) mList[(size_t)fill[(size_t)f.cellToCoarse[(size_t)n]]++] = n;
+            }
+            // fine ELL slots feeding each coarse ELL slot; mask of diagonal-folding slots
+            const int Wc = cd.W;
+            std::vector<int32_t> coarseSlotOfCsr((size_t)c.nFaceRefs());
+            for (int cc = 0; cc < c.nCells; cc++)
+                for (int k = c.faceStart[(size_t)cc], j = 0; k < c.faceStart[(size_t)cc + 1]; k++, j++)
+                    coarseSlotOfCsr[(size_t)k] = j * c.nCells + cc;
+            std::vector<int32_t> gCount((size_t)Wc * c.nCells + 1, 0);
+            std::vector<uint32_t> mask((size_t)f.nCells, 0u);
+            for (int n = 0; n < f.nCells; n++)
+                for (int k = f.faceStart[(size_t)n], j = 0; k < f.faceStart[(size_t)n + 1]; k++, j++) {
+                    if (f.faceNeighbor[(size_t)k] < 0) continue;
+                    const int s = f.fineSlotToCoarseSlot[(size_t)k];
+                    if (s >= 0) gCount[(size_t)coarseSlotOfCsr[(size_t)s] + 1]++;
+                    else mask[(size_t)n] |= (1u << j);
+                }
+            std::vector<int32_t> gStart(gCount.size(), 0);
+            for (size_t i = 1; i < gCount.size(); i++) gStart[i] = gStart[i - 1] + gCount[i];
+            std::vector<int32_t> gList((size_t)gStart.back());
+            {
+                std::vector<int32_t> fill(gStart);
+                for (int n = 0; n < f.nCells; n++)
+                    for (int k = f.faceStart[(size_t)n], j = 0; k < f.faceStart[(size_t)n + 1]; k++, j++) {
+                        if (f.faceNeighbor[(size_t)k] < 0) continue;
+                        const int s = f.fineSlotToCoarseSlot[(size_t)k];
+                        if (s >= 0) gList[(size_t)fill[(size_t)coarseSlotOfCsr[(size_t)s]]++] = j * f.nCells + n;
+                    }
+            }
+            cd.mStart = mgArena_.upload(mStart.data(), mStart.size());
+            cd.mList = mgArena_.upload(mList.data(), mList.size());
+            cd.gStart = mgArena_.upload(gStart.data(), gStart.size());
+            cd.gList = mgArena_.upload(gList.data(), std::max<size_t>(gList.size(), 1));
+            fd.internalMask = mgArena_.upload(mask.data(), mask.size());
+        }
+    }
+
+    // ---------- capture of one SIMPLE iteration (solver.cpp:1109-1284) ----------
+    void smooth(int l, int sweeps, std::vector<double*>& cur, std::vector<double*>& alt) {
+        LevelDev& L = levels_[(size_t)l];
+        if (L.N <= 0 || sweeps <= 0) return;
+        if (sweeps > 1 && L.N <= 1024) {
+            launchMGSmoothBlock(ctl_, L, cur[(size_t)l], cmg_.weight, sweeps, stream_);
+            return;
+        }
+        for (int i = 0; i < sweeps; i++) {
+            launchMGSmooth(ctl_, L, cur[(size_t)l], alt[(size_t)l], cmg_.weight, stream_);
+            std::swap(cur[(size_t)l], alt[(size_t)l]);
+        }
+    }
+
+    void vcycle(int l, std::vector<double*>& cur, std::vector<double*>& alt) {
+        const int L = (int)levels_.size();
+        if (l < 0 || l >= L) return;
+        if (hier_[(size_t)l].isCoarsest()) {
+            smooth(l, cmg_.linearSweep, cur, alt);
+            return;
+        }
+        smooth(l, cmg_.linearPreSweep, cur, alt);
+        LevelDev coarse = levels_[(size_t)l + 1];
+        coarse.x = cur[(size_t)l + 1];
+        launchMGRestrict(ctl_, levels_[(size_t)l], cur[(size_t)l], coarse, stream_);
+        vcycle(l + 1, cur, alt);
+        launchMGProlong(ctl_, levels_[(size_t)l], cur[(size_t)l], cur[(size_t)l + 1], stream_);
+        smooth(l, cmg_.linearPostSweep, cur, alt);
+    }
+
+    void enqueueMultigrid() {
+        const int L = (int)levels_.size();
+        for (int l = 1; l < L; l++) launchGalerkin(ctl_, levels_[(size_t)l - 1], levels_[(size_t)l], stream_);
+        std::vector<double*> cur((size_t)L), alt((size_t)L);
+        for (int l = 0; l < L; l++) {
+            cur[(size_t)l] = levels_[(size_t)l].x;
+            alt[(size_t)l] = levels_[(size_t)l].xNew;
+        }
+        const int cycles = cmg_.maxIter > 1 ? cmg_.maxIter : 1;
+        for (int c = 0; c < cycles; c++) vcycle(0, cur, alt);
+        if (cur[0] != pp_) launchCopy(ctl_, pp_, cur[0], N_, stream_);
+    }
+
+    void enqueueLinear(double* x, double* xT, const double* AF, const double* b, const double* inv) {
+        const int iters = cs_.linearMaxIter;
+        if (cs_.type == 1 && colorN_ > 0) {
+            for (int k = 0; k < iters; k++)
+                for (int c = 0; c < colorN_; c++) {
+                    const int b0 = hColorStart_[(size_t)c], cnt = hColorStart_[(size_t)c + 1] - b0;
+                    if (cnt > 0) launchGaussSeidel1(mesh_, ctl_, AF, b, inv, x, dCellOrder_, b0, cnt, stream_);
+                }
+            return;
+        }
+        double *live = x, *spare = xT;
+        for (int k = 0; k < iters; k++) {
+            launchJacobi1(mesh_, ctl_, AF, b, inv, live, spare, stream_);
+            std::swap(live, spare);
+        }
+        if (live != x) launchCopy(ctl_, x, live, N_, stream_);
+    }
+
+    void enqueueIteration() {
+        const int scheme = cs_.convectionScheme;
+        const int conv = cs_.addConvectionTerm ? 1 : 0;
+        const int nonOrtho = cs_.useNonOrthCorrector ? 1 : 0;
+        const bool convNeedsGrad = conv && (scheme == 2 || scheme == 3);
+        const int grad = cs_.gradientScheme;
+        launchIterBegin(ctl_, hostStopDev_, stream_);
+        // gradients of u, v (when SOU / non-orthogonal) and p in one pass
+        {
+            const double* phi[3];
+            BCDev bc[3];
+            double* gz[3];
+            double* gr[3];
+            int nf = 0;
+            if (nonOrtho || convNeedsGrad) {
+                phi[nf] = u_; bc[nf] = bc_[0]; gz[nf] = gUZ_; gr[nf] = gUR_; nf++;
+                phi[nf] = v_; bc[nf] = bc_[1]; gz[nf] = gVZ_; gr[nf] = gVR_; nf++;
+            }
+            phi[nf] = p_; bc[nf] = bc_[2]; gz[nf] = gPZ_; gr[nf] = gPR_; nf++;
+            launchGradient(mesh_, ctl_, nf, phi, bc, gz, gr, grad, stream_);
+        }
+        MomentumArgs a{};
+        a.mDot = mDot_; a.u = u_; a.v = v_; a.gUZ = gUZ_; a.gUR = gUR_; a.gVZ = gVZ_; a.gVR = gVR_;
+        a.gPZ = gPZ_; a.gPR = gPR_; a.uOld = uOld_; a.vOld = vOld_; a.uOld2 = uOld2_; a.vOld2 = vOld2_;
+        a.AF = AFm_; a.ACu = ACu_; a.ACv = ACv_; a.bu = bu_; a.bv = bv_; a.invACu = iu_; a.invACv = iv_;
+        a.DU = DU_; a.DV = DV_; a.mu = fluid_.mu; a.rho = fluid_.rho; a.dt = cs_.dt; a.alpha = alphaU_;
+        a.conv = conv; a.scheme = (scheme == 3) ? 0 : scheme; a.nonOrtho = nonOrtho; a.transient = cs_.transient ? 1 : 0;
+        launchMomentum(mesh_, ctl_, bc_[0], bc_[1], a, stream_);
+        // momentum solves (LinearSolver::run for u then v; fused, identical arithmetic)
+        const int iters = cs_.linearMaxIter;
+        if (cs_.type == 1 && colorN_ > 0) {
+            for (int k = 0; k < iters; k++)
+                for (int c = 0; c < colorN_; c++) {
+                    const int b0 = hColorStart_[(size_t)c], cnt = hColorStart_[(size_t)c + 1] - b0;
+                    if (cnt > 0)
+                        launchGaussSeidelUV(mesh_, ctl_, AFm_, bu_, bv_, iu_, iv_, u_, v_, dCellOrder_, b0, cnt, stream_);
+                }
+        } else {
+            double *lu = u_, *su = uT_, *lv = v_, *sv = vT_;
+            for (int k = 0; k < iters; k++) {
+                launchJacobiUV(mesh_, ctl_, AFm_, bu_, bv_, iu_, iv_, lu, lv, su, sv, stream_);
+                std::swap(lu, su);
+                std::swap(lv, sv);
+            }
+            if (lu != u_) {
+                launchCopy(ctl_, u_, lu, N_, stream_);
+                launchCopy(ctl_, v_, lv, N_, stream_);
+            }
+        }
+        launchPressureSystem(mesh_, ctl_, bc_[0], bc_[1], bc_[2], fluid_.rho, u_, v_, p_, gPZ_, gPR_, DU_, DV_, AFpp_,
+                             ACpp_, ipp_, mDot_, stream_);
+        for (int corr = 0; corr <= nonOrtho; corr++) {
+            const int cross = corr > 0;
+            if (cross) {
+                const double* phi[1] = {pp_};
+                double* gz[1] = {gPZ_};
+                double* gr[1] = {gPR_};
+                launchGradient(mesh_, ctl_, 1, phi, &bc_[3], gz, gr, grad, stream_);
+            }
+            launchPressureRhs(mesh_, ctl_, fluid_.rho, mDot_, DU_, DV_, gPZ_, gPR_, cross, corr == 0, bpp_, pp_, stream_);
+            if (cs_.useMultigrid) enqueueMultigrid();
+            else enqueueLinear(pp_, ppT_, AFpp_, bpp_, ipp_);
+        }
+        {
+            const double* phi[1] = {pp_};
+            double* gz[1] = {gPZ_};
+            double* gr[1] = {gPR_};
+            launchGradient(mesh_, ctl_, 1, phi, &bc_[3], gz, gr, grad, stream_);
+        }
+        launchCorrect(mesh_, ctl_, bc_[2], fluid_.rho, alphaP_, nonOrtho, pp_, gPZ_, gPR_, DU_, DV_, u_, v_, p_, mDot_,
+                      stream_);
+        launchResiduals(mesh_, ctl_, AFm_, ACu_, ACv_, bu_, bv_, u_, v_, mDot_, resU_, resV_, resC_, scU_, scV_,
+                        partial_, &residualBlocks_, stream_);
+        launchIterEnd(ctl_, partial_, residualBlocks_, N_, stream_);
+    }
+
+    void buildGraph() {
+        if (exec_) return;
+        if (cs_.useMultigrid) {
+            ensureDeviceLevels();
+        }
+        if (cs_.type == 1) ensureColoring();
+        CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        try {
+            enqueueIteration();
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(stream_, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        CK(cudaStreamEndCapture(stream_, &graph_));
+        CK(cudaGraphInstantiate(&exec_, graph_, 0));
+        CK(cudaGraphUpload(exec_, stream_));
+    }
+
+    void zeroState() {
+        const size_t N = (size_t)N_;
+        double* fields[] = {u_, v_, p_, pp_, uT_, vT_, ppT_, DU_, DV_, gPZ_, gPR_, gUZ_, gUR_, gVZ_, gVR_,
+                            uOld_, vOld_, uOld2_, vOld2_};
+        for (double* f : fields) CK(cudaMemsetAsync(f, 0, N * sizeof(double), stream_));
+        CK(cudaMemsetAsync(mDot_, 0, (size_t)F_ * sizeof(double), stream_));
+        CK(cudaMemsetAsync(ctl_, 0, sizeof(Ctl), stream_));
+    }
+
+    friend int64_t getFieldImpl(const Solver&, const std::string&, double*, size_t);
+};
+
+int Solver::solve(int continueRun, axisim_result* res) {
+    if (!haveMesh_) throw StatusError(AXISIM_E_STATE, "set a mesh before solving");
+    for (int v = 0; v < 3; v++)
+        if (!haveBC_[v]) throw StatusError(AXISIM_E_STATE, "set boundary conditions for u, v and p before solving");
+    // Solver::runCheck (solver.cpp:530-661)
+    if (running_) throw StatusError(AXISIM_E_STATE, "Solver still running");
+    if (csim_.maxIter < 1) csim_.maxIter = 50;
+    if (csim_.checkConv < 1) csim_.checkConv = 1;
+    if (cs_.linearMaxIter < 1) cs_.linearMaxIter = 20;
+    if (cs_.saveKeyFrameIter < 1) cs_.saveKeyFrameIter = 1;
+    const bool transient = cs_.transient != 0;
+    if (transient) {
+        if (!std::isfinite(cs_.dt) || cs_.dt <= 0.0) throw StatusError(AXISIM_E_CONFIG, "Transient run needs a positive time step.");
+        if (!std::isfinite(cs_.tEnd) || cs_.tEnd <= 0.0) throw StatusError(AXISIM_E_CONFIG, "Transient run needs a positive end time.");
+    }
+    bool anyPuls = false;
+    for (int var = 0; var < 2; var++) {
+        const HostBC& h = hbc_[var];
+        for (int g = 0; g < h.nGroups; g++) {
+            if (!h.puls[(size_t)g]) continue;
+            anyPuls = true;
+            if (!std::isfinite(h.value[(size_t)g]) || !std::isfinite(h.amp[(size_t)g]) || h.amp[(size_t)g] < 0.0 ||
+                !std::isfinite(h.freq[(size_t)g]) || h.freq[(size_t)g] <= 0.0)
+                throw StatusError(AXISIM_E_CONFIG, "Pulsatile inlet needs a finite mean velocity, A >= 0, and f > 0 Hz.");
+        }
+    }
+    if (anyPuls && !transient) throw StatusError(AXISIM_E_CONFIG, "Pulsatile inlet requires Transient Solver to be enabled.");
+    if (!std::isfinite(fluid_.rho) || !std::isfinite(fluid_.mu) || fluid_.rho <= 0.0 || fluid_.mu <= 0.0)
+        throw StatusError(AXISIM_E_CONFIG, "Solver needs positive density and viscosity.");
+    bool cont = continueRun != 0;
+    if (cont) {
+        std::string why;
+        if (!canContinue(&why)) {
+            log("Continue Solver disabled: " + why + " Starting from a fresh solve.\n");
+            cont = false;
+        }
+    }
+    uploadBC();
+    running_ = true;
+    struct Guard {
+        std::atomic<bool>& r;
+        ~Guard() { r = false; }
+    } guard{running_};
+    *hostStop_ = 0;
+    if (!cont) {
+        zeroState();
+        simTime_ = 0.0;
+    }
+    buildGraph();
+    // control block: settings for this run
+    Ctl h;
+    CK(cudaMemcpyAsync(&h, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    h.maxIter = csim_.maxIter;
+    h.checkConv = csim_.checkConv;
+    h.transient = transient ? 1 : 0;
+    h.itersThisCall = 0;
+    for (int i = 0; i < 3; i++) {
+        h.tol[i] = cres_[i].tol;
+        h.resNorm[i] = cres_[i].normType;
+        h.resScale[i] = cres_[i].scaleType;
+        h.resEnabled[i] = cres_[i].enabled;
+    }
+    const double timeOffset = (transient && cont) ? simTime_ : 0.0;
+    const int numSteps = transient ? (int)std::ceil(cs_.tEnd / cs_.dt) : 1;
+    const bool bdf2 = transient && cs_.timeScheme == 1;
+    CK(cudaEventRecord(ev0_, stream_));
+    int stepsDone = 0;
+    int status = AXISIM_OK;
+    int totalIters = 0;
+    bool converged = false;
+    for (int t = 0; t < numSteps; t++) {
+        if (transient) {
+            const double stepTime = timeOffset + (double)(t + 1) * cs_.dt;
+            for (int var = 0; var < 2; var++) {
+                const HostBC& hb = hbc_[var];
+                bool any = false;
+                for (int g = 0; g < hb.nGroups; g++) {
+                    double val = hb.value[(size_t)g];
+                    if (hb.puls[(size_t)g]) {
+                        any = true;
+                        const double twoPi = 2.0 * 3.14159265358979323846;
+                        val = hb.value[(size_t)g] * (1.0 + hb.amp[(size_t)g] * std::sin(twoPi * hb.freq[(size_t)g] * stepTime));
+                    }
+                    hostBCStage_[(size_t)var * std::max(std::max(hbc_[0].nGroups, hbc_[1].nGroups), 1) + (size_t)g] = val;
+                }
+                if (any) {
+                    // the previous step's kernels have finished (we synchronised below)
+                    CK(cudaMemcpy(bcValueDev_[var],
+                                  hostBCStage_ + (size_t)var * std::max(std::max(hbc_[0].nGroups, hbc_[1].nGroups), 1),
+                                  sizeof(double) * (size_t)hb.nGroups, cudaMemcpyHostToDevice));
+                }
+            }
+            if (bdf2) {
+                CK(cudaMemcpyAsync(uOld2_, uOld_, (size_t)N_ * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+                CK(cudaMemcpyAsync(vOld2_, vOld_, (size_t)N_ * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+            }
+            CK(cudaMemcpyAsync(uOld_, u_, (size_t)N_ * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+            CK(cudaMemcpyAsync(vOld_, v_, (size_t)N_ * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+        }
+        h.done = 0;
+        h.k = 0;
+        h.bdf2 = (bdf2 && t > 0) ? 1 : 0;
+        h.converged = 0;
+        h.histCount = 0;
+        const int startIters = h.itersThisCall;
+        CK(cudaMemcpyAsync(ctl_, &h, sizeof(Ctl), cudaMemcpyHostToDevice, stream_));
+        int batch = 4;
+        int launched = 0;
+        int drained = 0;
+        for (;;) {
+            const int nb = std::min(batch, std::max(1, csim_.maxIter - launched + 1));
+            for (int i = 0; i < nb; i++) CK(cudaGraphLaunch(exec_, stream_));
+            launched += nb;
+            CK(cudaMemcpyAsync(&h, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost, stream_));
+            CK(cudaStreamSynchronize(stream_));
+            if (resFn) {
+                for (int q = drained; q < h.histCount; q++) {
+                    const double* e = h.hist[q % kMaxHist];
+                    resFn(cbCtx, (int32_t)e[0], e + 1);
+                }
+            }
+            drained = h.histCount;
+            if (h.done) break;
+            batch = std::min(batch * 2, 64);
+        }
+        totalIters += h.itersThisCall - startIters;
+        converged = h.converged != 0;
+        stepsDone++;
+        if (transient) simTime_ = timeOffset + (double)(t + 1) * cs_.dt;
+        if (h.done == 2) {
+            status = AXISIM_E_STOPPED;
+            break;
+        }
+        if (h.done == 4) {
+            status = AXISIM_E_DIVERGED;
+            break;
+        }
+    }
+    CK(cudaEventRecord(ev1_, stream_));
+    // final gradients of u, v, p for the solution fields (solver.cpp:1330-1332)
+    {
+        const double* phi[3] = {u_, v_, p_};
+        double* gz[3] = {gUZ_, gVZ_, gPZ_};
+        double* gr[3] = {gUR_, gVR_, gPR_};
+        BCDev bc[3] = {bc_[0], bc_[1], bc_[2]};
+        launchGradient(mesh_, nullptr, 3, phi, bc, gz, gr, cs_.gradientScheme, stream_);
+    }
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaGetLastError());
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    isReady_ = true;
+    if (res) {
+        res->iterations = totalIters;
+        res->totalIterations = h.currentIteration;
+        res->converged = converged ? 1 : 0;
+        res->timeSteps = stepsDone;
+        for (int i = 0; i < 3; i++) res->residual[i] = h.resVal[i];
+        res->solveMs = ms;
+    }
+    if (status == AXISIM_E_STOPPED) lastError = "Solver stopped by user";
+    if (status == AXISIM_E_DIVERGED) lastError = "non-finite residual: the solve diverged";
+    return status;
+}
+
+// Field access (Solver::createSolutions, solver.cpp:186-219, plus internals).
+int64_t Solver::getField(const std::string& name, double* out, size_t n) const {
+    if (!haveMesh_) throw StatusError(AXISIM_E_STATE, "no mesh");
+    const size_t N = (size_t)N_, F = (size_t)F_, S = (size_t)S_;
+    struct E {
+        const char* n;
+        const double* p;
+        size_t len;
+        int ell;
+    };
+    const E tab[] = {
+        {"u", u_, N, 0}, {"v", v_, N, 0}, {"p", p_, N, 0}, {"pp", pp_, N, 0}, {"mDot", mDot_, F, 0},
+        {"DU", DU_, N, 0}, {"DV", DV_, N, 0}, {"gradPZ", gPZ_, N, 0}, {"gradPR", gPR_, N, 0},
+        {"gradUZ", gUZ_, N, 0}, {"gradUR", gUR_, N, 0}, {"gradVZ", gVZ_, N, 0}, {"gradVR", gVR_, N, 0},
+        {"AC_u", ACu_, N, 0}, {"b_u", bu_, N, 0}, {"AF_u", AFm_, S, 1}, {"invAC_u", iu_, N, 0},
+        {"AC_v", ACv_, N, 0}, {"b_v", bv_, N, 0}, {"AF_v", AFm_, S, 1}, {"invAC_v", iv_, N, 0},
+        {"AC_pp", ACpp_, N, 0}, {"b_pp", bpp_, N, 0}, {"AF_pp", AFpp_, S, 1}, {"invAC_pp", ipp_, N, 0},
+        {"res_U", resU_, N, 0}, {"res_V", resV_, N, 0}, {"res_Continuity", resC_, N, 0},
+        {"continuity", resC_, N, 0},
+        {"uOld", uOld_, N, 0}, {"vOld", vOld_, N, 0}, {"uOld2", uOld2_, N, 0}, {"vOld2", vOld2_, N, 0},
+        {"invDPN", mesh_.invDPN, F, 0}, {"wP", mesh_.wP, F, 0}, {"dPB", mesh_.dPB, F, 0},
+        {"length2D", mesh_.length2D, F, 0}, {"lsqWZ", mesh_.lsqWZ, F, 0}, {"lsqWR", mesh_.lsqWR, F, 0},
+        {"invA2D", mesh_.invA2D, N, 0}, {"lsqInvZZ", mesh_.lsqIZZ, N, 0}, {"lsqInvZR", mesh_.lsqIZR, N, 0},
+        {"lsqInvRR", mesh_.lsqIRR, N, 0},
+    };
+    for (const E& e : tab) {
+        if (name != e.n) continue;
+        if (!out || n < e.len) throw StatusError(AXISIM_E_ARG, "output buffer too small for " + name);
+        CK(cudaStreamSynchronize(stream_));
+        if (!e.ell) {
+            CK(cudaMemcpy(out, e.p, e.len * sizeof(double), cudaMemcpyDeviceToHost));
+        } else {
+            std::vector<double> ell((size_t)W_ * N);
+            CK(cudaMemcpy(ell.data(), e.p, ell.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            for (int c = 0; c < N_; c++)
+                for (int k = hCfs_[(size_t)c], j = 0; k < hCfs_[(size_t)c + 1]; k++, j++)
+                    out[k] = ell[(size_t)j * N + (size_t)c];
+        }
+        return (int64_t)e.len;
+    }
+    throw StatusError(AXISIM_E_ARG, "unknown field " + name);
+}
+
+int64_t Solver::setField(const std::string& name, const double* in, size_t n) {
+    if (!haveMesh_) throw StatusError(AXISIM_E_STATE, "no mesh");
+    const size_t N = (size_t)N_, F = (size_t)F_;
+    struct E {
+        const char* n;
+        double* p;
+        size_t len;
+    };
+    const E tab[] = {{"u", u_, N}, {"v", v_, N}, {"p", p_, N}, {"mDot", mDot_, F}, {"uOld", uOld_, N},
+                     {"vOld", vOld_, N}, {"uOld2", uOld2_, N}, {"vOld2", vOld2_, N}};
+    for (const E& e : tab) {
+        if (name != e.n) continue;
+        if (!in || n < e.len) throw StatusError(AXISIM_E_ARG, "input buffer too small for " + name);
+        CK(cudaStreamSynchronize(stream_));
+        CK(cudaMemcpy(e.p, in, e.len * sizeof(double), cudaMemcpyHostToDevice));
+        isReady_ = true;  // a seeded state can be continued from
+        return (int64_t)e.len;
+    }
+    throw StatusError(AXISIM_E_ARG, "field is not settable: " + name);
+}
+
+}  // namespace axisim
+
+// ====================================================================== C ABI
+using axisim::Solver;
+using axisim::StatusError;
+
+struct axisim_handle {
+    std::unique_ptr<Solver> s;
+    std::string err;
+    std::mutex mu;
+};
+
+struct axisim_mesh {
+    axisim::PackedMesh m;
+};
+
+namespace {
+
+template <class Fn>
+int guarded(axisim_handle* h, Fn&& fn) {
+    if (!h) return AXISIM_E_ARG;
+    try {
+        return fn();
+    } catch (const StatusError& e) {
+        h->err = e.what();
+        return e.status;
+    } catch (const std::exception& e) {
+        h->err = e.what();
+        return AXISIM_E_CUDA;
+    } catch (...) {
+        h->err = "unknown error";
+        return AXISIM_E_CUDA;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int axisim_abi_version(void) { return AXISIM_ABI_VERSION; }
+
+int axisim_create(const axisim_fluid* fluid, axisim_handle** out) {
+    if (!out) return AXISIM_E_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        return AXISIM_E_CUDA;
+    }
+    try {
+        axisim_fluid f{998.0, 0.0010518, 4180.0, 0.6, 3.0277e-9};
+        if (fluid) f = *fluid;
+        auto* h = new axisim_handle;
+        h->s.reset(new Solver(f));
+        *out = h;
+        return AXISIM_OK;
+    } catch (...) {
+        return AXISIM_E_CUDA;
+    }
+}
+
+int axisim_destroy(axisim_handle* h) {
+    if (!h) return AXISIM_E_ARG;
+    delete h;
+    return AXISIM_OK;
+}
+
+const char* axisim_last_error(const axisim_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int axisim_set_log(axisim_handle* h, axisim_log_fn log, axisim_residual_fn residual, void* ctx) {
+    return guarded(h, [&] {
+        h->s->logFn = log;
+        h->s->resFn = residual;
+        h->s->cbCtx = ctx;
+        return AXISIM_OK;
+    });
+}
+
+int axisim_set_mesh(axisim_handle* h, const axisim_mesh_packed* mesh) {
+    return guarded(h, [&] {
+        if (!mesh) throw StatusError(AXISIM_E_ARG, "mesh is null");
+        h->s->setMesh(*mesh);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_set_bc(axisim_handle* h, int32_t variable, const axisim_bc_field* bc) {
+    return guarded(h, [&] {
+        if (!bc) throw StatusError(AXISIM_E_ARG, "bc is null");
+        h->s->setBC(variable, *bc);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_set_config(axisim_handle* h, const axisim_config_solver* solver, const axisim_config_simple* simple,
+                      const axisim_config_multigrid* mg, const axisim_config_residual* res3, double alphaU,
+                      double alphaP) {
+    return guarded(h, [&] {
+        h->s->setConfig(solver, simple, mg, res3, alphaU, alphaP);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_set_fluid(axisim_handle* h, const axisim_fluid* fluid) {
+    return guarded(h, [&] {
+        if (!fluid) throw StatusError(AXISIM_E_ARG, "fluid is null");
+        h->s->setFluid(*fluid);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_set_precision(axisim_handle* h, int32_t mode) {
+    return guarded(h, [&] {
+        h->s->setPrecision(mode);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_solve(axisim_handle* h, int32_t continueRun, axisim_result* result) {
+    if (!h) return AXISIM_E_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    return guarded(h, [&] { return h->s->solve(continueRun, result); });
+}
+
+int axisim_can_continue(const axisim_handle* h, char* reason, size_t reasonLen) {
+    if (!h) return -AXISIM_E_ARG;
+    std::string why;
+    const bool ok = h->s->canContinue(&why);
+    if (!ok && reason && reasonLen) {
+        std::snprintf(reason, reasonLen, "%s", why.c_str());
+    }
+    return ok ? 1 : 0;
+}
+
+int axisim_request_stop(axisim_handle* h) {
+    if (!h) return AXISIM_E_ARG;
+    h->s->requestStop();
+    return AXISIM_OK;
+}
+
+int64_t axisim_get_field(const axisim_handle* h, const char* name, double* out, size_t n) {
+    auto* hh = const_cast<axisim_handle*>(h);
+    int64_t r = 0;
+    const int st = guarded(hh, [&] {
+        if (!name) throw StatusError(AXISIM_E_ARG, "name is null");
+        r = h->s->getField(name, out, n);
+        return AXISIM_OK;
+    });
+    return st == AXISIM_OK ? r : -st;
+}
+
+int64_t axisim_set_field(axisim_handle* h, const char* name, const double* in, size_t n) {
+    int64_t r = 0;
+    const int st = guarded(h, [&] {
+        if (!name) throw StatusError(AXISIM_E_ARG, "name is null");
+        r = h->s->setField(name, in, n);
+        return AXISIM_OK;
+    });
+    return st == AXISIM_OK ? r : -st;
+}
+
+int axisim_mg_levels(const axisim_handle* h, int32_t* cellsPerLevel, int32_t maxLevels) {
+    auto* hh = const_cast<axisim_handle*>(h);
+    int r = 0;
+    const int st = guarded(hh, [&] {
+        r = hh->s->mgLevels(cellsPerLevel, maxLevels);
+        return AXISIM_OK;
+    });
+    return st == AXISIM_OK ? r : -st;
+}
+
+int64_t axisim_mg_level_maps(const axisim_handle* h, int32_t level, int32_t* cellToCoarse,
+                             int32_t* fineSlotToCoarseSlot, int32_t* coarseFaceStart, int32_t* coarseFaceNeighbor) {
+    auto* hh = const_cast<axisim_handle*>(h);
+    int64_t r = 0;
+    const int st = guarded(hh, [&] {
+        r = hh->s->mgLevelMaps(level, cellToCoarse, fineSlotToCoarseSlot, coarseFaceStart, coarseFaceNeighbor);
+        return AXISIM_OK;
+    });
+    return st == AXISIM_OK ? r : -st;
+}
+
+int axisim_coloring(const axisim_handle* h, int32_t* colorOut, size_t n) {
+    auto* hh = const_cast<axisim_handle*>(h);
+    int r = 0;
+    const int st = guarded(hh, [&] {
+        r = hh->s->coloring(colorOut, n);
+        return AXISIM_OK;
+    });
+    return st == AXISIM_OK ? r : -st;
+}
+
+int axisim_multiblock_build(int32_t nBlocks, const axisim_block_spec* blocks, double tol, int32_t defaultGroup,
+                            axisim_mesh** out, int32_t* seamStatus) {
+    if (!out || nBlocks <= 0 || !blocks) return AXISIM_E_ARG;
+    try {
+        std::vector<axisim::BlockSpec> spec((size_t)nBlocks);
+        for (int i = 0; i < nBlocks; i++) {
+            const axisim_block_spec& b = blocks[i];
+            if (b.axialCells <= 0 || b.radialCells <= 0) return AXISIM_E_ARG;
+            axisim::BlockSpec& s = spec[(size_t)i];
+            s.z0 = b.z0; s.r0 = b.r0;
+            s.axialLength = b.axialLength; s.axialCells = b.axialCells; s.axialGrading = b.axialGrading; s.axialCoef = b.axialCoef;
+            s.radialLength = b.radialLength; s.radialCells = b.radialCells; s.radialGrading = b.radialGrading; s.radialCoef = b.radialCoef;
+            for (int e = 0; e < 4; e++) s.edgeGroup[e] = b.edgeGroup[e];
+        }
+        int seam = 0;
+        auto* m = new axisim_mesh;
+        m->m = axisim::buildMultiblock(spec, tol, defaultGroup, seam);
+        if (seamStatus) *seamStatus = seam;
+        *out = m;
+        return AXISIM_OK;
+    } catch (...) {
+        return AXISIM_E_MESH;
+    }
+}
+
+int axisim_mesh_sizes(const axisim_mesh* m, int32_t* nCells, int32_t* nFaces, int32_t* nRefs) {
+    if (!m) return AXISIM_E_ARG;
+    if (nCells) *nCells = m->m.nCells;
+    if (nFaces) *nFaces = m->m.nFaces;
+    if (nRefs) *nRefs = (int32_t)m->m.cellFaceIDs.size();
+    return AXISIM_OK;
+}
+
+int axisim_mesh_view(const axisim_mesh* m, axisim_mesh_packed* v) {
+    if (!m || !v) return AXISIM_E_ARG;
+    const axisim::PackedMesh& p = m->m;
+    v->nCells = p.nCells;
+    v->nFaces = p.nFaces;
+    v->faceOwner = p.faceOwner.data();
+    v->faceNeighbor = p.faceNeighbor.data();
+    v->faceNormalZ = p.faceNormalZ.data();
+    v->faceNormalR = p.faceNormalR.data();
+    v->faceCenterZ = p.faceCenterZ.data();
+    v->faceCenterR = p.faceCenterR.data();
+    v->faceArea = p.faceArea.data();
+    v->faceBoundaryGroupID = p.faceBoundaryGroupID.data();
+    v->cellCenterZ = p.cellCenterZ.data();
+    v->cellCenterR = p.cellCenterR.data();
+    v->cellArea2D = p.cellArea2D.data();
+    v->cellVolume = p.cellVolume.data();
+    v->cellFaceStart = p.cellFaceStart.data();
+    v->cellFaceIDs = p.cellFaceIDs.data();
+    return AXISIM_OK;
+}
+
+int axisim_mesh_free(axisim_mesh* m) {
+    delete m;
+    return AXISIM_OK;
+}
+
+int axisim_resolve_bc(int32_t boundaryType, int32_t variable, int32_t hasUser, int32_t userType, double userValue,
+                      uint8_t* typeOut, double* valueOut, uint8_t* pulsatileOut) {
+    if (!typeOut || !valueOut || variable < 0 || variable > 2) return AXISIM_E_ARG;
+    int t;
+    double v;
+    if (hasUser && axisim::variableEditable(variable, boundaryType)) {
+        t = userType;
+        v = userValue;
+    } else {
+        t = axisim::defaultBCType(boundaryType, variable);
+        v = 0.0;
+    }
+    if (pulsatileOut) *pulsatileOut = (t == AXISIM_BC_PULSATILE) ? 1 : 0;
+    *typeOut = (uint8_t)(t == AXISIM_BC_PULSATILE ? AXISIM_BC_DIRICHLET : t);
+    *valueOut = v;
+    return AXISIM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,248 @@
+/*
+ * axisim_b200.h -- C ABI of the B200-native SIMPLE pressure-velocity solver.
+ *
+ * A drop-in for AxiSim's solver path (Luippe/AxiSim-Software): the structs below
+ * are plain-old-data mirrors of the reference's case, mesh and boundary types,
+ * and the verbs mirror Solver's solve / continue / stop entry points. Every entry
+ * point takes plain pointers and sizes, returns an int status (never aborts),
+ * and leaves a message for axisim_last_error().
+ *
+ * Reference interface each declaration replaces is cited beside it
+ * (path:line inside the reference project).
+ */
+#ifndef AXISIM_B200_H
+#define AXISIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AXISIM_ABI_VERSION 1
+
+/* ---- status codes (the reference aborts in CUDA_CHECK, gpu_utils.h:5-11) ---- */
+enum axisim_status {
+    AXISIM_OK = 0,
+    AXISIM_E_ARG = 1,       /* null pointer, bad size, unknown name */
+    AXISIM_E_CONFIG = 2,    /* Solver::runCheck rejections (solver.cpp:530-661) */
+    AXISIM_E_MESH = 3,      /* inconsistent packed mesh */
+    AXISIM_E_CUDA = 4,      /* CUDA runtime error or no usable device */
+    AXISIM_E_DIVERGED = 5,  /* NaN/Inf residual */
+    AXISIM_E_STOPPED = 6,   /* axisim_request_stop() ended the run */
+    AXISIM_E_STATE = 7,     /* verb called in the wrong state (e.g. solve before set_mesh) */
+    AXISIM_E_TIMEOUT = 8    /* a device wait ran out of its iteration budget */
+};
+
+/* ---- enums: same numbering as the reference's uint8_t enums ---- */
+/* BCType (structs/boundary_struct.h:90-99) */
+enum { AXISIM_BC_DIRICHLET = 0, AXISIM_BC_NEUMANN = 1, AXISIM_BC_FULLY_DEVELOPED = 2,
+       AXISIM_BC_MICHAELIS_MENTEN = 3, AXISIM_BC_HILL = 4, AXISIM_BC_NONE = 5, AXISIM_BC_PULSATILE = 6 };
+/* BoundaryType (structs/boundary_struct.h:342-348) */
+enum { AXISIM_WALL = 0, AXISIM_VELOCITY_INLET = 1, AXISIM_PRESSURE_OUTLET = 2, AXISIM_SYMMETRY = 3,
+       AXISIM_FAR_FIELD = 4 };
+/* BoundaryVariable (structs/boundary_struct.h:48-57) */
+enum { AXISIM_VAR_U = 0, AXISIM_VAR_V = 1, AXISIM_VAR_P = 2 };
+/* Precision of the pressure-correction multigrid (new; no reference counterpart) */
+enum { AXISIM_PREC_FP64 = 0, AXISIM_PREC_MIXED = 1 };
+
+/* Mirror of FVMeshHostPacked (structs/solver_struct.h:400-429). */
+typedef struct axisim_mesh_packed {
+    int32_t nCells;
+    int32_t nFaces;
+    const int32_t* faceOwner;
+    const int32_t* faceNeighbor;          /* -1 on a boundary face */
+    const double* faceNormalZ;            /* unit, owner -> neighbour / outward */
+    const double* faceNormalR;
+    const double* faceCenterZ;
+    const double* faceCenterR;
+    const double* faceArea;               /* revolved area 2 pi r_f L */
+    const int32_t* faceBoundaryGroupID;   /* -1 = unassigned */
+    const double* cellCenterZ;
+    const double* cellCenterR;
+    const double* cellArea2D;
+    const double* cellVolume;             /* revolved volume 2 pi r_c A */
+    const int32_t* cellFaceStart;         /* nCells + 1 */
+    const int32_t* cellFaceIDs;           /* cellFaceStart[nCells] */
+} axisim_mesh_packed;
+
+/* Mirror of BoundaryFieldHost (structs/solver_struct.h:464-476) for one
+ * variable. lengthByGroup holds the group's float totalLength widened to
+ * double (structs/boundary_struct.h:515). The three pulsatile arrays are new:
+ * the reference re-derives them from BoundarySegmentGroup each time step
+ * (solver.cpp:375-424); here a group flagged pulsatile is a Dirichlet value
+ * valueByGroup * (1 + amplitude sin(2 pi frequency t)). Any may be NULL. */
+typedef struct axisim_bc_field {
+    int32_t nGroups;
+    const uint8_t* typeByGroup;
+    const uint8_t* boundaryTypeByGroup;
+    const double* valueByGroup;
+    const double* lengthByGroup;
+    const uint8_t* pulsatileByGroup;
+    const double* amplitudeByGroup;
+    const double* frequencyByGroup;
+} axisim_bc_field;
+
+/* Mirror of ConfigSolver (structs/solver_struct.h:203-238), byte-compatible:
+ * sizeof == 40 like the reference's static_assert. */
+typedef struct axisim_config_solver {
+    uint8_t velocitySolver;     /* 0 SIMPLE */
+    uint8_t convectionScheme;   /* 0 UPWIND 1 CENTRAL 2 SECOND_ORDER_UPWIND 3 QUICK (-> upwind) */
+    uint8_t gradientScheme;     /* 0 GREEN_GAUSS 1 LSQ */
+    uint8_t type;               /* linear solver: 0 JACOBI 1 GS_RB (multicolour) */
+    uint8_t timeScheme;         /* 0 first order 1 BDF2 */
+    uint8_t pad_[3];
+    int32_t linearMaxIter;
+    uint8_t useMultigrid;
+    uint8_t addConvectionTerm;
+    uint8_t transient;
+    uint8_t useNonOrthCorrector;
+    double dt;
+    double tEnd;
+    int32_t saveKeyFrameIter;
+    int32_t pad2_;
+} axisim_config_solver;
+
+/* Mirror of ConfigSimple (structs/solver_struct.h:158-165), sizeof == 24. */
+typedef struct axisim_config_simple {
+    int32_t maxIter;
+    int32_t checkConv;
+    double momTol;   /* carried, unread (as in the reference) */
+    double ppTol;    /* carried, unread (as in the reference) */
+} axisim_config_simple;
+
+/* Mirror of ConfigMultigrid (structs/solver_struct.h:167-190). */
+typedef struct axisim_config_multigrid {
+    int32_t maxIter;
+    double weight;
+    int32_t linearSweep;
+    int32_t linearPreSweep;
+    int32_t linearPostSweep;
+} axisim_config_multigrid;
+
+/* ConfigResidual without its device pointers (structs/solver_struct.h:240-258). */
+typedef struct axisim_config_residual {
+    uint8_t type;        /* 0 SCALED 1 RAW 2 RMS (informational, as in the reference) */
+    uint8_t normType;    /* 0 L1 1 L2 2 LINF */
+    uint8_t scaleType;   /* 0 NONE 1 N 2 SQRT_N 3 DIAGONAL 4 CONTINUITY(unused) */
+    uint8_t enabled;
+    double tol;
+} axisim_config_residual;
+
+/* Mirror of FluidPropertyConfig (src/header/setting.cuh:60-71). */
+typedef struct axisim_fluid {
+    double rho;
+    double mu;
+    double cp;
+    double k;
+    double D;
+} axisim_fluid;
+
+/* Result of a solve (Console::addCompletionTime + residual line, solver.cpp:1266-1323). */
+typedef struct axisim_result {
+    int32_t iterations;        /* SIMPLE iterations executed in this call */
+    int32_t totalIterations;   /* currentIteration after the call */
+    int32_t converged;
+    int32_t timeSteps;
+    double residual[3];        /* last U, V, Continuity residual */
+    double solveMs;            /* CUDA-event time of the time + SIMPLE loops */
+} axisim_result;
+
+typedef struct axisim_handle axisim_handle;
+
+/* Per-iteration residual callback, replacing ResidualPlot::add / Console line
+ * (solver.cpp:1267-1268). Called after each check with U, V, Continuity. */
+typedef void (*axisim_residual_fn)(void* ctx, int32_t iteration, const double* residuals3);
+typedef void (*axisim_log_fn)(void* ctx, const char* line);
+
+/* ---- lifetime ---- */
+int axisim_abi_version(void);
+/* Solver::Solver(Config&) (solver.cpp:104-114). */
+int axisim_create(const axisim_fluid* fluid, axisim_handle** out);
+/* Solver::reset + free (solver.cpp:118-144); frees every device allocation. */
+int axisim_destroy(axisim_handle* h);
+const char* axisim_last_error(const axisim_handle* h);
+int axisim_set_log(axisim_handle* h, axisim_log_fn log, axisim_residual_fn residual, void* ctx);
+
+/* ---- case ---- */
+/* Mesh::getFVMesh + createFVMeshDevice (solver.cpp:774-785, memory_manger.cpp:679-689):
+ * copies the packed mesh to the device and precomputes the geometry on the GPU. */
+int axisim_set_mesh(axisim_handle* h, const axisim_mesh_packed* mesh);
+/* createBoundarySolverDevice (memory_manger.cpp:191-237) for one variable. */
+int axisim_set_bc(axisim_handle* h, int32_t variable, const axisim_bc_field* bc);
+/* Solver's public config members configSolver / configSimple / configMultigrid /
+ * cfg / simple.{momentum,pressure}Relaxation (solver.h:83-133). res[3] = U, V,
+ * Continuity. */
+int axisim_set_config(axisim_handle* h, const axisim_config_solver* solver,
+                      const axisim_config_simple* simple, const axisim_config_multigrid* mg,
+                      const axisim_config_residual* res3, double alphaU, double alphaP);
+int axisim_set_fluid(axisim_handle* h, const axisim_fluid* fluid);
+/* New: precision of the pressure-correction solve (AXISIM_PREC_*). */
+int axisim_set_precision(axisim_handle* h, int32_t mode);
+
+/* ---- solve / continue / stop ---- */
+/* Solver::run + runSimple (solver.cpp:146-173, 753-1396), synchronous on the
+ * caller's thread. continueRun mirrors Solver::continueSolver: the device fields
+ * are reused as the initial guess when axisim_can_continue() holds. */
+int axisim_solve(axisim_handle* h, int32_t continueRun, axisim_result* result);
+/* Solver::canContinue (solver.cpp:469-528). Returns 1 if a continue is possible,
+ * 0 otherwise (reason written to `reason`), or a negative status. */
+int axisim_can_continue(const axisim_handle* h, char* reason, size_t reasonLen);
+/* Solver::requestStop (solver.cpp:175-184): thread-safe; the running solve stops
+ * at the top of its next SIMPLE iteration with the fields consistent. */
+int axisim_request_stop(axisim_handle* h);
+
+/* ---- fields ---- */
+/* Solver::solutions (solver.cpp:186-219) plus solver internals for checking:
+ * "u" "v" "p" "pp" "mDot" "DU" "DV" "gradPZ" "gradPR" "gradUZ" "gradUR"
+ * "gradVZ" "gradVR" "AC_u" "b_u" "AF_u" "invAC_u" (and _v, _pp; AF in the
+ * reference's CSR slot order) "res_U" "res_V" "res_Continuity" "continuity"
+ * (per-cell mass imbalance, Solver::getMassImbalance) and the geometry
+ * "invDPN" "wP" "dPB" "length2D" "lsqWZ" "lsqWR" "invA2D" "lsqInvZZ"
+ * "lsqInvZR" "lsqInvRR". Returns the element count written, or -status. */
+int64_t axisim_get_field(const axisim_handle* h, const char* name, double* out, size_t n);
+/* Initial state for u v p mDot (and uOld vOld for a transient restart). */
+int64_t axisim_set_field(axisim_handle* h, const char* name, const double* in, size_t n);
+
+/* ---- multigrid hierarchy (MultigridSolver::describeHierarchy, multigrid.cu:727-764) ---- */
+int axisim_mg_levels(const axisim_handle* h, int32_t* cellsPerLevel, int32_t maxLevels);
+/* fine->coarse maps of level `level` (GridLevel::cellToCoarse / fineSlotToCoarseSlot,
+ * multigrid.cuh:29-68) and the coarse CSR; returns the coarse slot count. */
+int64_t axisim_mg_level_maps(const axisim_handle* h, int32_t level, int32_t* cellToCoarse,
+                             int32_t* fineSlotToCoarseSlot, int32_t* coarseFaceStart,
+                             int32_t* coarseFaceNeighbor);
+/* MeshColoring (solver_struct.h:122-154): colour per cell; returns nColors. */
+int axisim_coloring(const axisim_handle* h, int32_t* colorOut, size_t n);
+
+/* ---- host case preparation ---- */
+/* Multiblock structured mesh (structs/multiblock.h): makeRectBlock +
+ * autoDetectInterfaces + assignGlobalNumbering + toPackedMesh. */
+typedef struct axisim_block_spec {
+    double z0, r0;
+    double axialLength;  int32_t axialCells;  int32_t axialGrading;  double axialCoef;
+    double radialLength; int32_t radialCells; int32_t radialGrading; double radialCoef;
+    int32_t edgeGroup[4];  /* West, East, South, North; -1 = default group */
+} axisim_block_spec;
+
+typedef struct axisim_mesh axisim_mesh;
+/* status_out: 0 ok, 1 non-conformal seam (interfaces dropped, as mesh.cpp:2742-2745) */
+int axisim_multiblock_build(int32_t nBlocks, const axisim_block_spec* blocks, double tol,
+                            int32_t defaultGroup, axisim_mesh** out, int32_t* seamStatus);
+int axisim_mesh_sizes(const axisim_mesh* m, int32_t* nCells, int32_t* nFaces, int32_t* nRefs);
+/* fills `view` with pointers into the mesh object (valid until axisim_mesh_free) */
+int axisim_mesh_view(const axisim_mesh* m, axisim_mesh_packed* view);
+int axisim_mesh_free(axisim_mesh* m);
+
+/* BoundaryDefaults::getEffectiveBC + createBoundaryFieldHost for one group and
+ * one variable (boundary_func.cpp:104-201, 333-378; memory_manger.cpp:96-109):
+ * given the group's BoundaryType and the user's BC (hasUser = 0 for none),
+ * writes the effective BCType (PULSATILE mapped to DIRICHLET) and value. */
+int axisim_resolve_bc(int32_t boundaryType, int32_t variable, int32_t hasUser,
+                      int32_t userType, double userValue, uint8_t* typeOut, double* valueOut,
+                      uint8_t* pulsatileOut);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
