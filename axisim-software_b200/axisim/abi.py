@@ -30,6 +30,7 @@ EXPORTS = [
     "axisim_solve", "axisim_can_continue", "axisim_request_stop", "axisim_get_field", "axisim_set_field",
     "axisim_mg_levels", "axisim_mg_level_maps", "axisim_coloring", "axisim_multiblock_build",
     "axisim_mesh_sizes", "axisim_mesh_view", "axisim_mesh_free", "axisim_resolve_bc",
+    "axisim_profile_iteration", "axisim_create_on",
 ]
 
 
@@ -89,6 +90,10 @@ class BlockSpec(C.Structure):
                 ("radialCoef", C.c_double), ("edgeGroup", C.c_int32 * 4)]
 
 
+class KernelStat(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_int32), ("ms", C.c_double), ("bytes", C.c_double)]
+
+
 RESIDUAL_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int32, _f64p)
 LOG_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_char_p)
 
@@ -113,6 +118,7 @@ def lib():
         sig = {
             "axisim_abi_version": (C.c_int, []),
             "axisim_create": (C.c_int, [C.POINTER(Fluid), C.POINTER(vp)]),
+            "axisim_create_on": (C.c_int, [C.c_int32, C.POINTER(Fluid), C.POINTER(vp)]),
             "axisim_destroy": (C.c_int, [vp]),
             "axisim_last_error": (C.c_char_p, [vp]),
             "axisim_set_log": (C.c_int, [vp, LOG_FN, RESIDUAL_FN, vp]),
@@ -138,6 +144,7 @@ def lib():
             "axisim_mesh_free": (C.c_int, [vp]),
             "axisim_resolve_bc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, _u8p,
                                             _f64p, _u8p]),
+            "axisim_profile_iteration": (C.c_int, [vp, C.c_int32, C.POINTER(KernelStat), C.c_int32, _i32p]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -260,11 +267,11 @@ def settings_structs(s):
 class Solver:
     """One solver handle (Solver in the reference): case in, fields out."""
 
-    def __init__(self, mesh, bcs, settings, precision=PREC_FP64):
+    def __init__(self, mesh, bcs, settings, precision=PREC_FP64, device=0):
         L = lib()
         cs, sim, mg, res, fluid = settings_structs(settings)
         self.h = C.c_void_p()
-        st = L.axisim_create(C.byref(fluid), C.byref(self.h))
+        st = L.axisim_create_on(device, C.byref(fluid), C.byref(self.h))
         if st != OK:
             raise AxisimError(st, "axisim_create failed (no CUDA device?)")
         self.mesh = mesh
@@ -306,6 +313,25 @@ class Solver:
         k = lib().axisim_set_field(self.h, name.encode(), a.ctypes.data_as(_f64p), a.size)
         if k < 0:
             self._check(int(-k))
+
+    def set_max_iter(self, max_iter, tol=None):
+        """Change ConfigSimple.maxIter (and optionally every residual tolerance)
+        without touching the settings baked into the captured iteration."""
+        self.settings["maxIter"] = int(max_iter)
+        if tol is not None:
+            self.settings["resTol"] = [tol, tol, tol]
+        cs, sim, mg, res, fluid = settings_structs(self.settings)
+        self._check(lib().axisim_set_config(self.h, C.byref(cs), C.byref(sim), C.byref(mg), res,
+                                            self.settings["alphaU"], self.settings["alphaP"]))
+
+    def profile(self, iterations=1):
+        """Per-kernel launches / CUDA-event ms / algorithmic bytes over `iterations`
+        eagerly replayed SIMPLE iterations (advances the solution)."""
+        out = (KernelStat * 64)()
+        n = C.c_int32(0)
+        self._check(lib().axisim_profile_iteration(self.h, iterations, out, 64, C.byref(n)))
+        return [dict(name=out[i].name.decode(), launches=out[i].launches, ms=out[i].ms, bytes=out[i].bytes)
+                for i in range(min(n.value, 64))]
 
     def can_continue(self):
         buf = C.create_string_buffer(256)

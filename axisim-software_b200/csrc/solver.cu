@@ -80,9 +80,8 @@ struct HostBC {
 
 class Solver {
 public:
-    explicit Solver(const axisim_fluid& f) : fluid_(f) {
-        int dev = 0;
-        CK(cudaGetDevice(&dev));
+    Solver(int device, const axisim_fluid& f) : fluid_(f), device_(device) {
+        CK(cudaSetDevice(device_));
         CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         CK(cudaHostAlloc(&hostStop_, sizeof(int), cudaHostAllocMapped));
         *hostStop_ = 0;
@@ -103,6 +102,9 @@ public:
         if (ev1_) cudaEventDestroy(ev1_);
         if (stream_) cudaStreamDestroy(stream_);
     }
+
+    // Every entry point makes the handle's device current on the calling thread.
+    void activate() const { CK(cudaSetDevice(device_)); }
 
     std::string lastError;
     axisim_log_fn logFn = nullptr;
@@ -268,14 +270,25 @@ public:
 
     void setConfig(const axisim_config_solver* s, const axisim_config_simple* sim, const axisim_config_multigrid* mg,
                    const axisim_config_residual* r3, double aU, double aP) {
-        if (s) cs_ = *s;
+        // maxIter, checkConv and the residual settings are read from the device
+        // control block at run time; only settings baked into the captured
+        // iteration graph force a recapture.
+        bool baked = false;
+        if (s) {
+            baked |= std::memcmp(&cs_, s, sizeof(cs_)) != 0;
+            cs_ = *s;
+        }
         if (sim) csim_ = *sim;
-        if (mg) cmg_ = *mg;
+        if (mg) {
+            baked |= std::memcmp(&cmg_, mg, sizeof(cmg_)) != 0;
+            cmg_ = *mg;
+        }
         if (r3)
             for (int i = 0; i < 3; i++) cres_[i] = r3[i];
+        baked |= alphaU_ != aU || alphaP_ != aP;
         alphaU_ = aU;
         alphaP_ = aP;
-        destroyGraph();
+        if (baked) destroyGraph();
     }
 
     bool canContinue(std::string* reason) const {
@@ -323,6 +336,7 @@ public:
 
 private:
     axisim_fluid fluid_;
+    int device_ = 0;
     axisim_config_solver cs_;
     axisim_config_simple csim_;
     axisim_config_multigrid cmg_;
@@ -367,6 +381,22 @@ private:
     std::vector<int32_t> hColor_, hColorStart_;
     int colorN_ = 0;
     int32_t* dCellOrder_ = nullptr;
+
+    // per-kernel profiling (eager replay of one iteration with an event after each launch)
+    struct Mark {
+        std::string name;
+        cudaEvent_t ev;
+        double bytes;
+    };
+    bool profiling_ = false;
+    std::vector<Mark> marks_;
+    void mark(const char* name, double bytes) {
+        if (!profiling_) return;
+        Mark m{name, nullptr, bytes};
+        CK(cudaEventCreate(&m.ev));
+        CK(cudaEventRecord(m.ev, stream_));
+        marks_.push_back(m);
+    }
 
     // graph
     cudaGraph_t graph_ = nullptr;
@@ -522,10 +552,12 @@ private:
         if (L.N <= 0 || sweeps <= 0) return;
         if (sweeps > 1 && L.N <= 1024) {
             launchMGSmoothBlock(ctl_, L, cur[(size_t)l], cmg_.weight, sweeps, stream_);
+            mark("mg_smooth_block", (double)L.N * (12.0 * L.W + 32.0));
             return;
         }
         for (int i = 0; i < sweeps; i++) {
             launchMGSmooth(ctl_, L, cur[(size_t)l], alt[(size_t)l], cmg_.weight, stream_);
+            mark(l == 0 ? "mg_smooth_l0" : "mg_smooth", (double)L.N * (12.0 * L.W + 32.0));
             std::swap(cur[(size_t)l], alt[(size_t)l]);
         }
     }
@@ -541,14 +573,21 @@ private:
         LevelDev coarse = levels_[(size_t)l + 1];
         coarse.x = cur[(size_t)l + 1];
         launchMGRestrict(ctl_, levels_[(size_t)l], cur[(size_t)l], coarse, stream_);
+        mark("mg_restrict", (double)levels_[(size_t)l].N * (12.0 * levels_[(size_t)l].W + 28.0) + 20.0 * coarse.N);
         vcycle(l + 1, cur, alt);
         launchMGProlong(ctl_, levels_[(size_t)l], cur[(size_t)l], cur[(size_t)l + 1], stream_);
+        mark("mg_prolong", 20.0 * levels_[(size_t)l].N + 8.0 * levels_[(size_t)l + 1].N);
         smooth(l, cmg_.linearPostSweep, cur, alt);
     }
 
     void enqueueMultigrid() {
         const int L = (int)levels_.size();
-        for (int l = 1; l < L; l++) launchGalerkin(ctl_, levels_[(size_t)l - 1], levels_[(size_t)l], stream_);
+        for (int l = 1; l < L; l++) {
+            const LevelDev& f = levels_[(size_t)l - 1];
+            const LevelDev& c = levels_[(size_t)l];
+            launchGalerkin(ctl_, f, c, stream_);
+            mark("mg_galerkin", (double)f.N * (16.0 + 12.0 * f.W) + (double)c.N * (12.0 + 12.0 * c.W));
+        }
         std::vector<double*> cur((size_t)L), alt((size_t)L);
         for (int l = 0; l < L; l++) {
             cur[(size_t)l] = levels_[(size_t)l].x;
@@ -556,7 +595,10 @@ private:
         }
         const int cycles = cmg_.maxIter > 1 ? cmg_.maxIter : 1;
         for (int c = 0; c < cycles; c++) vcycle(0, cur, alt);
-        if (cur[0] != pp_) launchCopy(ctl_, pp_, cur[0], N_, stream_);
+        if (cur[0] != pp_) {
+            launchCopy(ctl_, pp_, cur[0], N_, stream_);
+            mark("copy", 16.0 * N_);
+        }
     }
 
     void enqueueLinear(double* x, double* xT, const double* AF, const double* b, const double* inv) {
@@ -565,16 +607,23 @@ private:
             for (int k = 0; k < iters; k++)
                 for (int c = 0; c < colorN_; c++) {
                     const int b0 = hColorStart_[(size_t)c], cnt = hColorStart_[(size_t)c + 1] - b0;
-                    if (cnt > 0) launchGaussSeidel1(mesh_, ctl_, AF, b, inv, x, dCellOrder_, b0, cnt, stream_);
+                    if (cnt > 0) {
+                        launchGaussSeidel1(mesh_, ctl_, AF, b, inv, x, dCellOrder_, b0, cnt, stream_);
+                        mark("gs_pp", (double)cnt * (12.0 * W_ + 28.0));
+                    }
                 }
             return;
         }
         double *live = x, *spare = xT;
         for (int k = 0; k < iters; k++) {
             launchJacobi1(mesh_, ctl_, AF, b, inv, live, spare, stream_);
+            mark("jacobi_pp", (double)N_ * (12.0 * W_ + 32.0));
             std::swap(live, spare);
         }
-        if (live != x) launchCopy(ctl_, x, live, N_, stream_);
+        if (live != x) {
+            launchCopy(ctl_, x, live, N_, stream_);
+            mark("copy", 16.0 * N_);
+        }
     }
 
     void enqueueIteration() {
@@ -584,6 +633,7 @@ private:
         const bool convNeedsGrad = conv && (scheme == 2 || scheme == 3);
         const int grad = cs_.gradientScheme;
         launchIterBegin(ctl_, hostStopDev_, stream_);
+        mark("iter_begin", 0.0);
         // gradients of u, v (when SOU / non-orthogonal) and p in one pass
         {
             const double* phi[3];
@@ -597,6 +647,7 @@ private:
             }
             phi[nf] = p_; bc[nf] = bc_[2]; gz[nf] = gPZ_; gr[nf] = gPR_; nf++;
             launchGradient(mesh_, ctl_, nf, phi, bc, gz, gr, grad, stream_);
+            mark("gradient", gradBytes(nf, grad));
         }
         MomentumArgs a{};
         a.mDot = mDot_; a.u = u_; a.v = v_; a.gUZ = gUZ_; a.gUR = gUR_; a.gVZ = gVZ_; a.gVR = gVR_;
@@ -605,29 +656,40 @@ private:
         a.DU = DU_; a.DV = DV_; a.mu = fluid_.mu; a.rho = fluid_.rho; a.dt = cs_.dt; a.alpha = alphaU_;
         a.conv = conv; a.scheme = (scheme == 3) ? 0 : scheme; a.nonOrtho = nonOrtho; a.transient = cs_.transient ? 1 : 0;
         launchMomentum(mesh_, ctl_, bc_[0], bc_[1], a, stream_);
+        {
+            double face = 32.0 + (scheme == 1 ? 8.0 : scheme == 2 ? 16.0 : 0.0);
+            double cell = 4.0 * W_ + 16.0 + 16.0 + 16.0 + 8.0 * W_ + 64.0 + (scheme == 2 ? 40.0 : 0.0);
+            if (cs_.transient) cell += 32.0;
+            mark("momentum", face * F_ + cell * N_);
+        }
         // momentum solves (LinearSolver::run for u then v; fused, identical arithmetic)
         const int iters = cs_.linearMaxIter;
         if (cs_.type == 1 && colorN_ > 0) {
             for (int k = 0; k < iters; k++)
                 for (int c = 0; c < colorN_; c++) {
                     const int b0 = hColorStart_[(size_t)c], cnt = hColorStart_[(size_t)c + 1] - b0;
-                    if (cnt > 0)
+                    if (cnt > 0) {
                         launchGaussSeidelUV(mesh_, ctl_, AFm_, bu_, bv_, iu_, iv_, u_, v_, dCellOrder_, b0, cnt, stream_);
+                        mark("gs_uv", (double)cnt * (12.0 * W_ + 52.0));
+                    }
                 }
         } else {
             double *lu = u_, *su = uT_, *lv = v_, *sv = vT_;
             for (int k = 0; k < iters; k++) {
                 launchJacobiUV(mesh_, ctl_, AFm_, bu_, bv_, iu_, iv_, lu, lv, su, sv, stream_);
+                mark("jacobi_uv", (double)N_ * (12.0 * W_ + 64.0));
                 std::swap(lu, su);
                 std::swap(lv, sv);
             }
             if (lu != u_) {
                 launchCopy(ctl_, u_, lu, N_, stream_);
                 launchCopy(ctl_, v_, lv, N_, stream_);
+                mark("copy", 32.0 * N_);
             }
         }
         launchPressureSystem(mesh_, ctl_, bc_[0], bc_[1], bc_[2], fluid_.rho, u_, v_, p_, gPZ_, gPR_, DU_, DV_, AFpp_,
                              ACpp_, ipp_, mDot_, stream_);
+        mark("pressure_rhiechow", 56.0 * F_ + (12.0 * W_ + 72.0) * N_);
         for (int corr = 0; corr <= nonOrtho; corr++) {
             const int cross = corr > 0;
             if (cross) {
@@ -635,8 +697,10 @@ private:
                 double* gz[1] = {gPZ_};
                 double* gr[1] = {gPR_};
                 launchGradient(mesh_, ctl_, 1, phi, &bc_[3], gz, gr, grad, stream_);
+                mark("gradient_pp", gradBytes(1, grad));
             }
             launchPressureRhs(mesh_, ctl_, fluid_.rho, mDot_, DU_, DV_, gPZ_, gPR_, cross, corr == 0, bpp_, pp_, stream_);
+            mark("pp_rhs", 16.0 * F_ + (4.0 * W_ + 16.0) * N_);
             if (cs_.useMultigrid) enqueueMultigrid();
             else enqueueLinear(pp_, ppT_, AFpp_, bpp_, ipp_);
         }
@@ -645,14 +709,94 @@ private:
             double* gz[1] = {gPZ_};
             double* gr[1] = {gPR_};
             launchGradient(mesh_, ctl_, 1, phi, &bc_[3], gz, gr, grad, stream_);
+            mark("gradient_pp", gradBytes(1, grad));
         }
         launchCorrect(mesh_, ctl_, bc_[2], fluid_.rho, alphaP_, nonOrtho, pp_, gPZ_, gPR_, DU_, DV_, u_, v_, p_, mDot_,
                       stream_);
+        mark("correct_massflux", 64.0 * F_ + (88.0 + 4.0 * W_) * N_);
         launchResiduals(mesh_, ctl_, AFm_, ACu_, ACv_, bu_, bv_, u_, v_, mDot_, resU_, resV_, resC_, scU_, scV_,
                         partial_, &residualBlocks_, stream_);
+        mark("residual", 16.0 * F_ + (16.0 * W_ + 88.0) * N_);
         launchIterEnd(ctl_, partial_, residualBlocks_, N_, stream_);
+        mark("iter_end", 40.0 * residualBlocks_);
     }
 
+    // Algorithmic bytes of one gradient launch: every array element counted once.
+    double gradBytes(int nf, int scheme) const {
+        const double face = scheme == 1 ? 24.0 : 48.0;
+        const double cell = 4.0 * W_ + 8.0 * nf + (scheme == 1 ? 24.0 : 8.0) + 16.0 * nf;
+        return face * F_ + cell * N_;
+    }
+
+public:
+    // Runs `iters` SIMPLE iterations eagerly from the current state with an
+    // event after every launch; returns per-kernel launches, time and bytes.
+    int profile(int iters, axisim_kernel_stat* out, int maxOut) {
+        if (!haveMesh_) throw StatusError(AXISIM_E_STATE, "no mesh");
+        uploadBC();
+        buildGraph();
+        Ctl h;
+        CK(cudaMemcpy(&h, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost));
+        const Ctl saved = h;
+        h.done = 0;
+        h.k = 0;
+        h.maxIter = 1 << 30;
+        h.checkConv = std::max(1, csim_.checkConv);
+        h.transient = cs_.transient ? 1 : 0;
+        for (int i = 0; i < 3; i++) {
+            h.tol[i] = -1.0;  // never converges: every profiled iteration runs in full
+            h.resNorm[i] = cres_[i].normType;
+            h.resScale[i] = cres_[i].scaleType;
+            h.resEnabled[i] = cres_[i].enabled;
+        }
+        CK(cudaMemcpyAsync(ctl_, &h, sizeof(Ctl), cudaMemcpyHostToDevice, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        profiling_ = true;
+        marks_.clear();
+        cudaEvent_t start;
+        CK(cudaEventCreate(&start));
+        CK(cudaEventRecord(start, stream_));
+        try {
+            for (int i = 0; i < iters; i++) enqueueIteration();
+        } catch (...) {
+            profiling_ = false;
+            throw;
+        }
+        profiling_ = false;
+        CK(cudaStreamSynchronize(stream_));
+        std::vector<axisim_kernel_stat> acc;
+        cudaEvent_t prev = start;
+        for (Mark& m : marks_) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, prev, m.ev));
+            auto it = std::find_if(acc.begin(), acc.end(),
+                                   [&](const axisim_kernel_stat& s) { return m.name == s.name; });
+            if (it == acc.end()) {
+                axisim_kernel_stat s{};
+                std::snprintf(s.name, sizeof(s.name), "%s", m.name.c_str());
+                acc.push_back(s);
+                it = acc.end() - 1;
+            }
+            it->launches++;
+            it->ms += ms;
+            it->bytes += m.bytes;
+            prev = m.ev;
+        }
+        for (Mark& m : marks_) cudaEventDestroy(m.ev);
+        marks_.clear();
+        cudaEventDestroy(start);
+        // restore the run's control block (iteration counters advanced by the profiled iterations)
+        Ctl after;
+        CK(cudaMemcpy(&after, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost));
+        Ctl restored = saved;
+        restored.currentIteration = after.currentIteration;
+        CK(cudaMemcpy(ctl_, &restored, sizeof(Ctl), cudaMemcpyHostToDevice));
+        const int n = (int)acc.size();
+        for (int i = 0; i < n && i < maxOut; i++) out[i] = acc[(size_t)i];
+        return n;
+    }
+
+private:
     void buildGraph() {
         if (exec_) return;
         if (cs_.useMultigrid) {
@@ -937,6 +1081,7 @@ template <class Fn>
 int guarded(axisim_handle* h, Fn&& fn) {
     if (!h) return AXISIM_E_ARG;
     try {
+        h->s->activate();
         return fn();
     } catch (const StatusError& e) {
         h->err = e.what();
@@ -956,7 +1101,7 @@ extern "C" {
 
 int axisim_abi_version(void) { return AXISIM_ABI_VERSION; }
 
-int axisim_create(const axisim_fluid* fluid, axisim_handle** out) {
+int axisim_create_on(int32_t device, const axisim_fluid* fluid, axisim_handle** out) {
     if (!out) return AXISIM_E_ARG;
     *out = nullptr;
     int n = 0;
@@ -964,17 +1109,20 @@ int axisim_create(const axisim_fluid* fluid, axisim_handle** out) {
         cudaGetLastError();
         return AXISIM_E_CUDA;
     }
+    if (device < 0 || device >= n) return AXISIM_E_ARG;
     try {
         axisim_fluid f{998.0, 0.0010518, 4180.0, 0.6, 3.0277e-9};
         if (fluid) f = *fluid;
         auto* h = new axisim_handle;
-        h->s.reset(new Solver(f));
+        h->s.reset(new Solver(device, f));
         *out = h;
         return AXISIM_OK;
     } catch (...) {
         return AXISIM_E_CUDA;
     }
 }
+
+int axisim_create(const axisim_fluid* fluid, axisim_handle** out) { return axisim_create_on(0, fluid, out); }
 
 int axisim_destroy(axisim_handle* h) {
     if (!h) return AXISIM_E_ARG;
@@ -1105,6 +1253,18 @@ int axisim_coloring(const axisim_handle* h, int32_t* colorOut, size_t n) {
         return AXISIM_OK;
     });
     return st == AXISIM_OK ? r : -st;
+}
+
+int axisim_profile_iteration(axisim_handle* h, int32_t iterations, axisim_kernel_stat* out, int32_t maxOut,
+                             int32_t* nOut) {
+    if (!h) return AXISIM_E_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    return guarded(h, [&] {
+        if (iterations < 1 || !out || maxOut < 1) throw StatusError(AXISIM_E_ARG, "bad profile arguments");
+        const int n = h->s->profile(iterations, out, maxOut);
+        if (nOut) *nOut = n;
+        return AXISIM_OK;
+    });
 }
 
 int axisim_multiblock_build(int32_t nBlocks, const axisim_block_spec* blocks, double tol, int32_t defaultGroup,

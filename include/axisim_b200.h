@@ -158,8 +158,11 @@ typedef void (*axisim_log_fn)(void* ctx, const char* line);
 
 /* ---- lifetime ---- */
 int axisim_abi_version(void);
-/* Solver::Solver(Config&) (solver.cpp:104-114). */
+/* Solver::Solver(Config&) (solver.cpp:104-114) on CUDA device 0. */
 int axisim_create(const axisim_fluid* fluid, axisim_handle** out);
+/* The same on a chosen CUDA device (one handle per GPU; the reference has a
+ * single device and stream per Solver, solver.cpp:110). */
+int axisim_create_on(int32_t device, const axisim_fluid* fluid, axisim_handle** out);
 /* Solver::reset + free (solver.cpp:118-144); frees every device allocation. */
 int axisim_destroy(axisim_handle* h);
 const char* axisim_last_error(const axisim_handle* h);
@@ -214,6 +217,22 @@ int64_t axisim_mg_level_maps(const axisim_handle* h, int32_t level, int32_t* cel
                              int32_t* coarseFaceNeighbor);
 /* MeshColoring (solver_struct.h:122-154): colour per cell; returns nColors. */
 int axisim_coloring(const axisim_handle* h, int32_t* colorOut, size_t n);
+
+/* ---- measurement ---- */
+/* Per-kernel statistics of the profiled iterations: launches, summed CUDA-event
+ * time between consecutive launches and the algorithmic bytes (each array
+ * element the kernel's arithmetic needs, counted once per launch). */
+typedef struct axisim_kernel_stat {
+    char name[32];
+    int32_t launches;
+    double ms;
+    double bytes;
+} axisim_kernel_stat;
+/* New (the reference times only the whole solve, solver.cpp:907-908,1318-1323):
+ * runs `iterations` SIMPLE iterations eagerly from the current state, with an
+ * event recorded after every kernel on the solver's stream. */
+int axisim_profile_iteration(axisim_handle* h, int32_t iterations, axisim_kernel_stat* out, int32_t maxOut,
+                             int32_t* nOut);
 
 /* ---- host case preparation ---- */
 /* Multiblock structured mesh (structs/multiblock.h): makeRectBlock +
