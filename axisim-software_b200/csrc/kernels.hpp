@@ -7,30 +7,40 @@
 
 namespace axisim {
 
-// One multigrid level on the device. Level 0 aliases the p' system.
+// One multigrid level on the device. Level 0 aliases the p' system and uses the
+// mesh's [W][N] slot block; coarser levels use sliced ELL: 32-row slices, slot
+// j of cell n at sliceOff[n/32] + 32 j + n%32, slice width (sliceOff[s+1] -
+// sliceOff[s]) / 32, unused slots with neighbour -1 and coefficient 0.
 struct LevelDev {
     int N = 0, W = 0;
-    int32_t* nb = nullptr;     // [W][N], -1 = no neighbour
-    double* AF = nullptr;      // [W][N]
+    int totalSlots = 0;
+    const int32_t* sliceOff = nullptr;  // null: [W][N] layout
+    int32_t* nb = nullptr;
+    double* AF = nullptr;
     double* AC = nullptr;
     double* b = nullptr;
     double* x = nullptr;
     double* xNew = nullptr;
-    double* xF = nullptr;      // single precision copy used by the mixed smoother
+    double* res = nullptr;     // fine residual / Galerkin diagonal scratch (N)
     int32_t* c2c = nullptr;    // fine -> coarse (null on the coarsest level)
-    // Galerkin / restriction gathers, stored on the COARSE level (built from level-1):
+    // restriction / Galerkin gathers, stored on the COARSE level:
     int32_t* mStart = nullptr;  // [N+1] members of each coarse cell
     int32_t* mList = nullptr;   // fine cell ids, ascending
-    int32_t* gStart = nullptr;  // [W*N+1] fine slots feeding each coarse ELL slot
-    int32_t* gList = nullptr;   // fine ELL slot indices, ascending fine cell then slot
+    int32_t* gStart = nullptr;  // [totalSlots+1] fine slots feeding each coarse slot
+    int32_t* gList = nullptr;   // fine slot positions, ascending fine cell then slot
     uint32_t* internalMask = nullptr;  // on the FINE level: slots folding into the coarse diagonal
-    // single precision copies for the mixed-precision cycle
-    float* AFf = nullptr;
-    float* ACf = nullptr;
-    float* invACf = nullptr;
-    float* bf = nullptr;
-    float* xf = nullptr;
-    float* xNewf = nullptr;
+};
+
+// Levels at and below `first` solved inside one CTA (V-cycle tail).
+constexpr int kMaxTail = 8;
+struct TailArgs {
+    int first = 0, count = 0;
+    LevelDev lv[kMaxTail];
+    int smemOff[kMaxTail];   // doubles: x, y, b per level
+    const double* resFine = nullptr;
+    double* xOut = nullptr;
+    double w = 0.6;
+    int pre = 1, post = 1, coarseSweeps = 30;
 };
 
 // ---- setup ----
@@ -75,11 +85,17 @@ void launchResiduals(const MeshDev& m, const Ctl* ctl, const double* AF, const d
 void launchIterEnd(Ctl* ctl, const double* partial, int nBlocks, int N, cudaStream_t s);
 void launchCopy(const Ctl* ctl, double* dst, const double* src, int n, cudaStream_t s);
 
-// ---- multigrid (FP64) ----
+// ---- multigrid (FP64, mg_fp64.cu) ----
 void launchGalerkin(const Ctl* ctl, const LevelDev& fine, const LevelDev& coarse, cudaStream_t s);
 void launchMGSmooth(const Ctl* ctl, const LevelDev& L, const double* x, double* y, double w, cudaStream_t s);
 void launchMGSmoothBlock(const Ctl* ctl, const LevelDev& L, double* x, double w, int sweeps, cudaStream_t s);
-void launchMGRestrict(const Ctl* ctl, const LevelDev& fine, const double* xFine, LevelDev& coarse, cudaStream_t s);
+void launchMGResidual(const Ctl* ctl, const LevelDev& L, const double* x, cudaStream_t s);
+// b_c = sum of the fine residuals of each agglomerate; x_c = 0, or with
+// firstSweep the result of one Jacobi sweep from zero written to xAlt
+void launchMGGather(const Ctl* ctl, const LevelDev& fine, const LevelDev& coarse, double* xCur, double* xAlt,
+                    int firstSweep, double w, cudaStream_t s);
 void launchMGProlong(const Ctl* ctl, const LevelDev& fine, double* xFine, const double* xCoarse, cudaStream_t s);
+size_t tailSharedBytes(const TailArgs& a);
+void launchMGTail(const Ctl* ctl, const TailArgs& a, cudaStream_t s);
 
 }  // namespace axisim

@@ -15,9 +15,7 @@
 //   k_pp_rhs     createPPRhs + the p' reset
 //   k_correct    updateMomentumPressure + updateMassFlux
 //   k_residual   residualAll + continuityResidual + first reduction pass
-// Multigrid: the Galerkin build and the restriction are deterministic gathers
-// (ascending fine-cell order) in place of the reference's atomicAdd scatters
-// (multigrid.cu:350-410); the residual is fused into the restriction.
+// The multigrid kernels live in mg_fp64.cu.
 #include <cmath>
 #include <cstdio>
 
@@ -844,122 +842,6 @@ __global__ void k_copy(const Ctl* ctl, double* dst, const double* src, int n) {
     if (i < n) dst[i] = src[i];
 }
 
-// ---------------- multigrid (multigrid.cu:350-541) ----------------
-// Galerkin A_H = P^T A P as a gather per coarse cell: the coarse diagonal sums
-// each member's AC plus its agglomerate-internal off-diagonals, the coarse
-// off-diagonals sum their feeding fine slots; both in ascending fine order.
-__global__ void __launch_bounds__(kThreads) k_galerkin(const Ctl* ctl, LevelDev F, LevelDev C) {
-    if (ctl->done) return;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= C.N) return;
-    double ac = 0.0;
-    for (int q = C.mStart[c]; q < C.mStart[c + 1]; q++) {
-        const int n = C.mList[q];
-        double diag = F.AC[n];
-        uint32_t mask = F.internalMask[n];
-        while (mask) {
-            const int j = __ffs(mask) - 1;
-            mask &= mask - 1;
-            diag += F.AF[(size_t)j * F.N + n];
-        }
-        ac += diag;
-    }
-    C.AC[c] = ac;
-    for (int j = 0; j < C.W; j++) {
-        const size_t s = (size_t)j * C.N + c;
-        double af = 0.0;
-        for (int q = C.gStart[s]; q < C.gStart[s + 1]; q++) af += F.AF[C.gList[q]];
-        C.AF[s] = af;
-    }
-}
-
-// weighted Jacobi, jacobiRow (multigrid.cu:447-484)
-__global__ void __launch_bounds__(kThreads) k_mg_smooth(const Ctl* ctl, int N, int W, const int32_t* __restrict__ nb,
-                                                        const double* __restrict__ AF, const double* __restrict__ AC,
-                                                        const double* __restrict__ b, const double* __restrict__ x,
-                                                        double* __restrict__ y, double w) {
-    if (ctl->done) return;
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N) return;
-    const double ac = AC[n];
-    if (fabs(ac) < 1.0e-30) {
-        y[n] = x[n];
-        return;
-    }
-    double Ax = ac * x[n];
-    for (int j = 0; j < W; j++) {
-        const size_t s = (size_t)j * N + n;
-        const int k = nb[s];
-        if (k != -1) Ax += AF[s] * x[k];
-    }
-    y[n] = x[n] + w * (b[n] - Ax) / ac;
-}
-
-// Whole-level weighted Jacobi inside one CTA with a shared-memory ping-pong
-// (jacobiSingleBlock, multigrid.cu:501-541). N <= blockDim.x.
-__global__ void k_mg_smooth_block(const Ctl* ctl, int N, int W, const int32_t* __restrict__ nb,
-                                  const double* __restrict__ AF, const double* __restrict__ AC,
-                                  const double* __restrict__ b, double* x, double w, int sweeps) {
-    if (ctl->done) return;
-    extern __shared__ double sx[];
-    double* xo = sx;
-    double* xn = sx + N;
-    const int n = threadIdx.x;
-    if (n < N) xo[n] = x[n];
-    __syncthreads();
-    for (int it = 0; it < sweeps; it++) {
-        if (n < N) {
-            const double ac = AC[n];
-            if (fabs(ac) < 1.0e-30) {
-                xn[n] = xo[n];
-            } else {
-                double Ax = ac * xo[n];
-                for (int j = 0; j < W; j++) {
-                    const size_t s = (size_t)j * N + n;
-                    const int k = nb[s];
-                    if (k != -1) Ax += AF[s] * xo[k];
-                }
-                xn[n] = xo[n] + w * (b[n] - Ax) / ac;
-            }
-        }
-        __syncthreads();
-        double* t = xo;
-        xo = xn;
-        xn = t;
-    }
-    if (n < N) x[n] = xo[n];
-}
-
-// residual (residualAll with sign) fused into the restriction: each coarse cell
-// sums its members' b - Ax in ascending order, and zeroes its correction.
-__global__ void __launch_bounds__(kThreads) k_mg_restrict(const Ctl* ctl, LevelDev F, const double* __restrict__ x,
-                                                          LevelDev C) {
-    if (ctl->done) return;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= C.N) return;
-    double sum = 0.0;
-    for (int q = C.mStart[c]; q < C.mStart[c + 1]; q++) {
-        const int n = C.mList[q];
-        double Ax = F.AC[n] * x[n];
-        for (int j = 0; j < F.W; j++) {
-            const size_t s = (size_t)j * F.N + n;
-            const int k = F.nb[s];
-            if (k >= 0) Ax += F.AF[s] * x[k];
-        }
-        sum += F.b[n] - Ax;
-    }
-    C.b[c] = sum;
-    C.x[c] = 0.0;
-}
-
-__global__ void __launch_bounds__(kThreads) k_mg_prolong(const Ctl* ctl, int N, const int32_t* __restrict__ c2c,
-                                                         double* x, const double* __restrict__ xc) {
-    if (ctl->done) return;
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N) return;
-    x[n] += xc[c2c[n]];
-}
-
 }  // namespace
 
 // ---------------- launchers ----------------
@@ -1063,28 +945,6 @@ void launchIterEnd(Ctl* ctl, const double* partial, int nBlocks, int N, cudaStre
 
 void launchCopy(const Ctl* ctl, double* dst, const double* src, int n, cudaStream_t s) {
     k_copy<<<blocksFor(n), kThreads, 0, s>>>(ctl, dst, src, n);
-}
-
-void launchGalerkin(const Ctl* ctl, const LevelDev& fine, const LevelDev& coarse, cudaStream_t s) {
-    k_galerkin<<<blocksFor(coarse.N), kThreads, 0, s>>>(ctl, fine, coarse);
-}
-
-void launchMGSmooth(const Ctl* ctl, const LevelDev& L, const double* x, double* y, double w, cudaStream_t s) {
-    k_mg_smooth<<<blocksFor(L.N), kThreads, 0, s>>>(ctl, L.N, L.W, L.nb, L.AF, L.AC, L.b, x, y, w);
-}
-
-void launchMGSmoothBlock(const Ctl* ctl, const LevelDev& L, double* x, double w, int sweeps, cudaStream_t s) {
-    const int threads = ((L.N + 31) / 32) * 32;
-    k_mg_smooth_block<<<1, threads, 2 * (size_t)L.N * sizeof(double), s>>>(ctl, L.N, L.W, L.nb, L.AF, L.AC, L.b, x,
-                                                                          w, sweeps);
-}
-
-void launchMGRestrict(const Ctl* ctl, const LevelDev& fine, const double* xFine, LevelDev& coarse, cudaStream_t s) {
-    k_mg_restrict<<<blocksFor(coarse.N), kThreads, 0, s>>>(ctl, fine, xFine, coarse);
-}
-
-void launchMGProlong(const Ctl* ctl, const LevelDev& fine, double* xFine, const double* xCoarse, cudaStream_t s) {
-    k_mg_prolong<<<blocksFor(fine.N), kThreads, 0, s>>>(ctl, fine.N, fine.c2c, xFine, xCoarse);
 }
 
 }  // namespace axisim

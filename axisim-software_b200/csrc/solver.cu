@@ -462,18 +462,26 @@ private:
         dCellOrder_ = meshArena_.upload(order.data(), order.size());
     }
 
-    // Device copies of the hierarchy: ELL topology, Galerkin/restriction gathers.
+    // Device copies of the hierarchy: level 0 aliases the p' system; coarser
+    // levels in sliced ELL; member lists and fine->coarse slot gathers for the
+    // restriction and the Galerkin build; the V-cycle tail for small levels.
     void ensureDeviceLevels() {
         ensureHierarchy();
         if (!levels_.empty()) return;
         const int L = (int)hier_.size();
         levels_.resize((size_t)L);
+        std::vector<std::vector<int32_t>> sliceOffH((size_t)L);
+        auto pos = [&](int l, int c, int j) -> int {
+            if (l == 0) return j * N_ + c;
+            return sliceOffH[(size_t)l][(size_t)(c >> 5)] + 32 * j + (c & 31);
+        };
         for (int l = 0; l < L; l++) {
             const GridLevel& g = hier_[(size_t)l];
             LevelDev& d = levels_[(size_t)l];
             d.N = g.nCells;
             if (l == 0) {
                 d.W = W_;
+                d.totalSlots = W_ * N_;
                 d.nb = const_cast<int32_t*>(mesh_.snb);
                 d.AF = AFpp_;
                 d.AC = ACpp_;
@@ -481,13 +489,24 @@ private:
                 d.x = pp_;
                 d.xNew = ppT_;
             } else {
+                const int nS = (g.nCells + 31) / 32;
+                std::vector<int32_t>& off = sliceOffH[(size_t)l];
+                off.assign((size_t)nS + 1, 0);
                 int W = 0;
-                for (int c = 0; c < g.nCells; c++) W = std::max(W, g.faceStart[(size_t)c + 1] - g.faceStart[(size_t)c]);
+                for (int sI = 0; sI < nS; sI++) {
+                    int w = 0;
+                    for (int c = sI * 32; c < std::min(g.nCells, sI * 32 + 32); c++)
+                        w = std::max(w, g.faceStart[(size_t)c + 1] - g.faceStart[(size_t)c]);
+                    off[(size_t)sI + 1] = off[(size_t)sI] + 32 * w;
+                    W = std::max(W, w);
+                }
                 d.W = W;
-                std::vector<int32_t> nb((size_t)W * g.nCells, -1);
+                d.totalSlots = off[(size_t)nS];
+                std::vector<int32_t> nb((size_t)std::max(d.totalSlots, 1), -1);
                 for (int c = 0; c < g.nCells; c++)
                     for (int k = g.faceStart[(size_t)c], j = 0; k < g.faceStart[(size_t)c + 1]; k++, j++)
-                        nb[(size_t)j * g.nCells + c] = g.faceNeighbor[(size_t)k];
+                        nb[(size_t)pos(l, c, j)] = g.faceNeighbor[(size_t)k];
+                d.sliceOff = mgArena_.upload(off.data(), off.size());
                 d.nb = mgArena_.upload(nb.data(), nb.size());
                 d.AF = mgArena_.alloc<double>(nb.size());
                 d.AC = mgArena_.alloc<double>((size_t)g.nCells);
@@ -495,15 +514,16 @@ private:
                 d.x = mgArena_.alloc<double>((size_t)g.nCells);
                 d.xNew = mgArena_.alloc<double>((size_t)g.nCells);
             }
-            if (!g.isCoarsest()) d.c2c = mgArena_.upload(g.cellToCoarse.data(), g.cellToCoarse.size());
+            if (!g.isCoarsest()) {
+                d.c2c = mgArena_.upload(g.cellToCoarse.data(), g.cellToCoarse.size());
+                d.res = mgArena_.alloc<double>((size_t)g.nCells);
+            }
         }
-        // gathers for coarse level l from fine level l-1
         for (int l = 1; l < L; l++) {
             const GridLevel& f = hier_[(size_t)l - 1];
             const GridLevel& c = hier_[(size_t)l];
             LevelDev& fd = levels_[(size_t)l - 1];
             LevelDev& cd = levels_[(size_t)l];
-            // members of each coarse cell, ascending fine id
             std::vector<int32_t> mStart((size_t)c.nCells + 1, 0), mList((size_t)f.nCells);
             for (int n = 0; n < f.nCells; n++) mStart[(size_t)f.cellToCoarse[(size_t)n] + 1]++;
             for (int k = 0; k < c.nCells; k++) mStart[(size_t)k + 1] += mStart[(size_t)k];
@@ -511,46 +531,60 @@ private:
                 std::vector<int32_t> fill(mStart);
                 for (int n = 0; n < f.nCells; n++) mList[(size_t)fill[(size_t)f.cellToCoarse[(size_t)n]]++] = n;
             }
-            // fine ELL slots feeding each coarse ELL slot; mask of diagonal-folding slots
-            const int Wc = cd.W;
-            std::vector<int32_t> coarseSlotOfCsr((size_t)c.nFaceRefs());
+            std::vector<int32_t> coarsePos((size_t)std::max(c.nFaceRefs(), 1));
             for (int cc = 0; cc < c.nCells; cc++)
                 for (int k = c.faceStart[(size_t)cc], j = 0; k < c.faceStart[(size_t)cc + 1]; k++, j++)
-                    coarseSlotOfCsr[(size_t)k] = j * c.nCells + cc;
-            std::vector<int32_t> gCount((size_t)Wc * c.nCells + 1, 0);
+                    coarsePos[(size_t)k] = pos(l, cc, j);
+            std::vector<int32_t> gCount((size_t)cd.totalSlots + 1, 0);
             std::vector<uint32_t> mask((size_t)f.nCells, 0u);
             for (int n = 0; n < f.nCells; n++)
                 for (int k = f.faceStart[(size_t)n], j = 0; k < f.faceStart[(size_t)n + 1]; k++, j++) {
                     if (f.faceNeighbor[(size_t)k] < 0) continue;
-                    const int s = f.fineSlotToCoarseSlot[(size_t)k];
-                    if (s >= 0) gCount[(size_t)coarseSlotOfCsr[(size_t)s] + 1]++;
+                    const int sI = f.fineSlotToCoarseSlot[(size_t)k];
+                    if (sI >= 0) gCount[(size_t)coarsePos[(size_t)sI] + 1]++;
                     else mask[(size_t)n] |= (1u << j);
                 }
             std::vector<int32_t> gStart(gCount.size(), 0);
             for (size_t i = 1; i < gCount.size(); i++) gStart[i] = gStart[i - 1] + gCount[i];
-            std::vector<int32_t> gList((size_t)gStart.back());
+            std::vector<int32_t> gList((size_t)std::max(gStart.back(), 1));
             {
                 std::vector<int32_t> fill(gStart);
                 for (int n = 0; n < f.nCells; n++)
                     for (int k = f.faceStart[(size_t)n], j = 0; k < f.faceStart[(size_t)n + 1]; k++, j++) {
                         if (f.faceNeighbor[(size_t)k] < 0) continue;
-                        const int s = f.fineSlotToCoarseSlot[(size_t)k];
-                        if (s >= 0) gList[(size_t)fill[(size_t)coarseSlotOfCsr[(size_t)s]]++] = j * f.nCells + n;
+                        const int sI = f.fineSlotToCoarseSlot[(size_t)k];
+                        if (sI >= 0) gList[(size_t)fill[(size_t)coarsePos[(size_t)sI]]++] = pos(l - 1, n, j);
                     }
             }
             cd.mStart = mgArena_.upload(mStart.data(), mStart.size());
             cd.mList = mgArena_.upload(mList.data(), mList.size());
             cd.gStart = mgArena_.upload(gStart.data(), gStart.size());
-            cd.gList = mgArena_.upload(gList.data(), std::max<size_t>(gList.size(), 1));
+            cd.gList = mgArena_.upload(gList.data(), gList.size());
             fd.internalMask = mgArena_.upload(mask.data(), mask.size());
         }
+        // V-cycle tail: the deepest levels that all fit one CTA's shared memory
+        tailStart_ = -1;
+        for (int t = 1; t < L; t++) {
+            if (L - t > kMaxTail) continue;
+            bool fits = true;
+            size_t bytes = 0;
+            for (int l = t; l < L; l++) {
+                fits = fits && levels_[(size_t)l].N <= 4096;
+                bytes += 3 * (size_t)levels_[(size_t)l].N * sizeof(double);
+            }
+            if (fits && bytes <= 200 * 1024) {
+                tailStart_ = t;
+                break;
+            }
+        }
     }
+    int tailStart_ = -1;
 
     // ---------- capture of one SIMPLE iteration (solver.cpp:1109-1284) ----------
     void smooth(int l, int sweeps, std::vector<double*>& cur, std::vector<double*>& alt) {
         LevelDev& L = levels_[(size_t)l];
         if (L.N <= 0 || sweeps <= 0) return;
-        if (sweeps > 1 && L.N <= 1024) {
+        if (sweeps > 1 && L.N <= 4096) {
             launchMGSmoothBlock(ctl_, L, cur[(size_t)l], cmg_.weight, sweeps, stream_);
             mark("mg_smooth_block", (double)L.N * (12.0 * L.W + 32.0));
             return;
@@ -562,21 +596,52 @@ private:
         }
     }
 
-    void vcycle(int l, std::vector<double*>& cur, std::vector<double*>& alt) {
+    // One V-cycle from level l (multigrid.cu:607-662). firstDone: the gather
+    // that produced this level's right-hand side already ran the first
+    // pre-smoothing sweep.
+    void vcycle(int l, std::vector<double*>& cur, std::vector<double*>& alt, bool firstDone) {
         const int L = (int)levels_.size();
         if (l < 0 || l >= L) return;
         if (hier_[(size_t)l].isCoarsest()) {
-            smooth(l, cmg_.linearSweep, cur, alt);
+            smooth(l, cmg_.linearSweep - (firstDone ? 1 : 0), cur, alt);
             return;
         }
-        smooth(l, cmg_.linearPreSweep, cur, alt);
-        LevelDev coarse = levels_[(size_t)l + 1];
-        coarse.x = cur[(size_t)l + 1];
-        launchMGRestrict(ctl_, levels_[(size_t)l], cur[(size_t)l], coarse, stream_);
-        mark("mg_restrict", (double)levels_[(size_t)l].N * (12.0 * levels_[(size_t)l].W + 28.0) + 20.0 * coarse.N);
-        vcycle(l + 1, cur, alt);
-        launchMGProlong(ctl_, levels_[(size_t)l], cur[(size_t)l], cur[(size_t)l + 1], stream_);
-        mark("mg_prolong", 20.0 * levels_[(size_t)l].N + 8.0 * levels_[(size_t)l + 1].N);
+        smooth(l, cmg_.linearPreSweep - (firstDone ? 1 : 0), cur, alt);
+        LevelDev& F = levels_[(size_t)l];
+        LevelDev& C = levels_[(size_t)l + 1];
+        launchMGResidual(ctl_, F, cur[(size_t)l], stream_);
+        mark("mg_residual", (double)F.N * (12.0 * F.W + 32.0));
+        if (l + 1 == tailStart_) {
+            TailArgs a;
+            a.first = l + 1;
+            a.count = L - (l + 1);
+            size_t off = 0;
+            for (int i = 0; i < a.count; i++) {
+                a.lv[i] = levels_[(size_t)(l + 1 + i)];
+                a.smemOff[i] = (int)off;
+                off += 3 * (size_t)a.lv[i].N;
+            }
+            a.resFine = F.res;
+            a.xOut = cur[(size_t)l + 1];
+            a.w = cmg_.weight;
+            a.pre = cmg_.linearPreSweep;
+            a.post = cmg_.linearPostSweep;
+            a.coarseSweeps = cmg_.linearSweep;
+            launchMGTail(ctl_, a, stream_);
+            double tb = 0.0;
+            for (int i = 0; i < a.count; i++) tb += (double)a.lv[i].N * (12.0 * a.lv[i].W + 32.0);
+            mark("mg_tail", tb);
+        } else {
+            const bool coarseIsCoarsest = hier_[(size_t)l + 1].isCoarsest();
+            const int sweepsBelow = coarseIsCoarsest ? cmg_.linearSweep : cmg_.linearPreSweep;
+            const bool fuse = sweepsBelow >= 1;
+            launchMGGather(ctl_, F, C, cur[(size_t)l + 1], alt[(size_t)l + 1], fuse ? 1 : 0, cmg_.weight, stream_);
+            mark("mg_gather", 12.0 * F.N + 32.0 * C.N);
+            if (fuse) std::swap(cur[(size_t)l + 1], alt[(size_t)l + 1]);
+            vcycle(l + 1, cur, alt, fuse);
+        }
+        launchMGProlong(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], stream_);
+        mark("mg_prolong", 20.0 * F.N + 8.0 * C.N);
         smooth(l, cmg_.linearPostSweep, cur, alt);
     }
 
@@ -586,7 +651,8 @@ private:
             const LevelDev& f = levels_[(size_t)l - 1];
             const LevelDev& c = levels_[(size_t)l];
             launchGalerkin(ctl_, f, c, stream_);
-            mark("mg_galerkin", (double)f.N * (16.0 + 12.0 * f.W) + (double)c.N * (12.0 + 12.0 * c.W));
+            mark("mg_galerkin", (double)f.N * (20.0 + 8.0 * std::max(1, f.W / 2)) + (double)c.totalSlots * 8.0 +
+                                    (double)c.N * 16.0);
         }
         std::vector<double*> cur((size_t)L), alt((size_t)L);
         for (int l = 0; l < L; l++) {
@@ -594,7 +660,7 @@ private:
             alt[(size_t)l] = levels_[(size_t)l].xNew;
         }
         const int cycles = cmg_.maxIter > 1 ? cmg_.maxIter : 1;
-        for (int c = 0; c < cycles; c++) vcycle(0, cur, alt);
+        for (int c = 0; c < cycles; c++) vcycle(0, cur, alt, false);
         if (cur[0] != pp_) {
             launchCopy(ctl_, pp_, cur[0], N_, stream_);
             mark("copy", 16.0 * N_);

@@ -44,6 +44,11 @@ def _variants():
     c.settings.update(convectionScheme=cases.CONV_QUICK, mgPreSweep=2, mgPostSweep=1, mgMaxIter=2,
                       resNorm=[1, 2, 0], resScale=[1, 2, 0], checkConv=2)
     v.append(("pipe_quick_norms", c))
+    c = cases.expansion(scale=1 / 4, max_iter=2, tol=1e-30)
+    v.append(("expansion_54k_deep_multigrid", c))
+    c = cases.expansion(scale=1 / 4, max_iter=2, tol=1e-30)
+    c.settings.update(mgPreSweep=0, mgPostSweep=2, mgLinearSweep=7, mgMaxIter=1)
+    v.append(("expansion_54k_mg_sweeps", c))
     c = cases.pulsatile_expansion(scale=1 / 32, dt=1e-3, steps=3, max_iter=3, tol=1e-30)
     v.append(("pulsatile_bdf2", c))
     c = cases.pulsatile_expansion(scale=1 / 32, dt=1e-3, steps=2, max_iter=3, tol=1e-30)
