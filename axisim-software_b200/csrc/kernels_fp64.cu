@@ -442,12 +442,56 @@ __global__ void __launch_bounds__(kThreads) k_momentum(MeshDev m, const Ctl* ctl
 }
 
 // ---------------- momentum sweeps (linear_solver.cu:9-72) ----------------
+template <int WC>
 __global__ void __launch_bounds__(kThreads) k_jacobi_uv(int N, int W, const int32_t* __restrict__ snb,
                                                         const Ctl* ctl, const double* __restrict__ AF,
                                                         const double* __restrict__ bu, const double* __restrict__ bv,
                                                         const double* __restrict__ iu, const double* __restrict__ iv,
                                                         const double* __restrict__ xu, const double* __restrict__ xv,
                                                         double* __restrict__ yu, double* __restrict__ yv) {
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    // All slot loads are issued before any neighbour gather (no load waits on
+    // the neighbour test); a boundary slot reads its own cell and is skipped.
+    int nbs[WC];
+    double af[WC];
+#pragma unroll
+    for (int j = 0; j < WC; j++) {
+        const size_t s = (size_t)j * N + n;
+        nbs[j] = snb[s];
+        af[j] = AF[s];
+    }
+    double gu[WC], gv[WC];
+#pragma unroll
+    for (int j = 0; j < WC; j++) {
+        const int k = nbs[j] >= 0 ? nbs[j] : n;
+        gu[j] = xu[k];
+        gv[j] = xv[k];
+    }
+    double vu = bu[n], vv = bv[n];
+#pragma unroll
+    for (int j = 0; j < WC; j++) {
+        if (nbs[j] >= 0) {
+            vu -= af[j] * gu[j];
+            vv -= af[j] * gv[j];
+        }
+    }
+    const double au = iu[n], av = iv[n];
+    yu[n] = (au != 0.0) ? vu * au : xu[n];
+    yv[n] = (av != 0.0) ? vv * av : xv[n];
+}
+
+// General-width fallback (cells with more than 8 faces).
+__global__ void __launch_bounds__(kThreads) k_jacobi_uv_wide(int N, int W, const int32_t* __restrict__ snb,
+                                                             const Ctl* ctl, const double* __restrict__ AF,
+                                                             const double* __restrict__ bu,
+                                                             const double* __restrict__ bv,
+                                                             const double* __restrict__ iu,
+                                                             const double* __restrict__ iv,
+                                                             const double* __restrict__ xu,
+                                                             const double* __restrict__ xv, double* __restrict__ yu,
+                                                             double* __restrict__ yv) {
     if (ctl->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
@@ -888,7 +932,9 @@ void launchMomentum(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, const BC
 void launchJacobiUV(const MeshDev& m, const Ctl* ctl, const double* AF, const double* bu, const double* bv,
                     const double* iu, const double* iv, const double* xu, const double* xv, double* yu, double* yv,
                     cudaStream_t s) {
-    k_jacobi_uv<<<blocksFor(m.N), kThreads, 0, s>>>(m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
+    if (m.W == 4) k_jacobi_uv<4><<<blocksFor(m.N), kThreads, 0, s>>>(m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
+    else if (m.W == 3) k_jacobi_uv<3><<<blocksFor(m.N), kThreads, 0, s>>>(m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
+    else k_jacobi_uv_wide<<<blocksFor(m.N), kThreads, 0, s>>>(m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
 }
 
 void launchGaussSeidelUV(const MeshDev& m, const Ctl* ctl, const double* AF, const double* bu, const double* bv,

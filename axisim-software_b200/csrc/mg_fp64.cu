@@ -9,9 +9,10 @@
 //   * the fine residual is a coalesced pass over the fine level; the gather of
 //     the coarse right-hand side also performs the coarse level's first
 //     pre-smoothing sweep (from x = 0 it needs no neighbour values);
-//   * every level at or below 4096 cells runs as ONE single-CTA kernel holding
-//     x, the Jacobi partner and b in shared memory (the reference launches
-//     three to four kernels per level per cycle there).
+//   * every level at or below 1024 cells runs as ONE single-CTA kernel holding
+//     x, the Jacobi partner, b and the residual in shared memory, with the
+//     coefficients L1-resident and the coarsest rows in registers (the
+//     reference launches three to four kernels per level per cycle there).
 // Compiled with --fmad=false like the rest of the FP64 path.
 #include <cmath>
 
@@ -23,6 +24,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kTailThreads = 1024;
+// tail levels are at most kTailThreads cells: one row per thread
 constexpr int kRegW = 16;
 
 inline int blocksFor(long long n, int t = kThreads) { return (int)((n + t - 1) / t); }
@@ -40,7 +42,67 @@ __device__ __forceinline__ Slots slotsOf(const LevelDev& L, int n) {
     return Slots{n, L.N, L.W};
 }
 
-// Weighted Jacobi row, jacobiRow (multigrid.cu:447-484).
+// Weighted Jacobi row, jacobiRow (multigrid.cu:447-484). Slot loads are
+// issued before the neighbour gathers; a slot without a neighbour reads the
+// cell itself and is skipped in the sum.
+__device__ __forceinline__ double jacobiRowT(const LevelDev& L, int n, const double* xo, double w, double bn) {
+    const double ac = L.AC[n];
+    if (fabs(ac) < 1.0e-30) return xo[n];
+    const Slots sl = slotsOf(L, n);
+    double Ax = ac * xo[n];
+    constexpr int kU = 8;
+    for (int j0 = 0; j0 < sl.width; j0 += kU) {
+        int k[kU];
+        double a[kU], g[kU];
+#pragma unroll
+        for (int j = 0; j < kU; j++) {
+            if (j0 + j < sl.width) {
+                const int p = sl.base + (j0 + j) * sl.stride;
+                k[j] = __ldg(L.nb + p);
+                a[j] = __ldg(L.AF + p);
+            } else {
+                k[j] = -1;
+                a[j] = 0.0;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kU; j++) g[j] = xo[k[j] != -1 ? k[j] : n];
+#pragma unroll
+        for (int j = 0; j < kU; j++)
+            if (k[j] != -1) Ax += a[j] * g[j];
+    }
+    return xo[n] + w * (bn - Ax) / ac;
+}
+
+// residualRaw with sign (residuals.cuh:17-48)
+__device__ __forceinline__ double residualRowT(const LevelDev& L, int n, const double* x, double bn) {
+    const Slots sl = slotsOf(L, n);
+    double Ax = L.AC[n] * x[n];
+    constexpr int kU = 8;
+    for (int j0 = 0; j0 < sl.width; j0 += kU) {
+        int k[kU];
+        double a[kU], g[kU];
+#pragma unroll
+        for (int j = 0; j < kU; j++) {
+            if (j0 + j < sl.width) {
+                const int p = sl.base + (j0 + j) * sl.stride;
+                k[j] = __ldg(L.nb + p);
+                a[j] = __ldg(L.AF + p);
+            } else {
+                k[j] = -1;
+                a[j] = 0.0;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kU; j++) g[j] = x[k[j] >= 0 ? k[j] : n];
+#pragma unroll
+        for (int j = 0; j < kU; j++)
+            if (k[j] >= 0) Ax += a[j] * g[j];
+    }
+    return bn - Ax;
+}
+
+// Plain rows for the multi-CTA sweeps (bandwidth-bound: occupancy first).
 __device__ __forceinline__ double jacobiRow(const LevelDev& L, int n, const double* xo, double w, double bn) {
     const double ac = L.AC[n];
     if (fabs(ac) < 1.0e-30) return xo[n];
@@ -54,7 +116,6 @@ __device__ __forceinline__ double jacobiRow(const LevelDev& L, int n, const doub
     return xo[n] + w * (bn - Ax) / ac;
 }
 
-// residualRaw with sign (residuals.cuh:17-48)
 __device__ __forceinline__ double residualRow(const LevelDev& L, int n, const double* x, double bn) {
     double Ax = L.AC[n] * x[n];
     const Slots sl = slotsOf(L, n);
@@ -64,6 +125,48 @@ __device__ __forceinline__ double residualRow(const LevelDev& L, int n, const do
         if (k >= 0) Ax += L.AF[p] * x[k];
     }
     return bn - Ax;
+}
+
+// Level 0 ([W][N] slots, W fixed at compile time): loads issued before gathers.
+template <int WC>
+__device__ __forceinline__ double ellAx(const LevelDev& L, int n, const double* x, bool jacobiTest) {
+    int k[WC];
+    double a[WC], g[WC];
+#pragma unroll
+    for (int j = 0; j < WC; j++) {
+        k[j] = L.nb[(size_t)j * L.N + n];
+        a[j] = L.AF[(size_t)j * L.N + n];
+    }
+#pragma unroll
+    for (int j = 0; j < WC; j++) g[j] = x[k[j] >= 0 ? k[j] : n];
+    double Ax = L.AC[n] * x[n];
+#pragma unroll
+    for (int j = 0; j < WC; j++)
+        if (jacobiTest ? (k[j] != -1) : (k[j] >= 0)) Ax += a[j] * g[j];
+    return Ax;
+}
+
+template <int WC>
+__global__ void __launch_bounds__(kThreads) k_mg_smooth_ell(const Ctl* ctl, LevelDev L, const double* __restrict__ x,
+                                                            double* __restrict__ y, double w) {
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L.N) return;
+    const double ac = L.AC[n];
+    if (fabs(ac) < 1.0e-30) {
+        y[n] = x[n];
+        return;
+    }
+    const double Ax = ellAx<WC>(L, n, x, true);
+    y[n] = x[n] + w * (L.b[n] - Ax) / ac;
+}
+
+template <int WC>
+__global__ void __launch_bounds__(kThreads) k_mg_residual_ell(const Ctl* ctl, LevelDev L, const double* __restrict__ x) {
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L.N) return;
+    L.res[n] = L.b[n] - ellAx<WC>(L, n, x, false);
 }
 
 __global__ void __launch_bounds__(kThreads) k_mg_smooth(const Ctl* ctl, LevelDev L, const double* __restrict__ x,
@@ -164,7 +267,7 @@ __global__ void __launch_bounds__(kThreads) k_gal_coarse(const Ctl* ctl, LevelDe
 __device__ __forceinline__ void tailSmooth(const LevelDev& L, double*& xo, double*& xn, const double* b, double w,
                                            int sweeps) {
     for (int it = 0; it < sweeps; it++) {
-        for (int n = threadIdx.x; n < L.N; n += blockDim.x) xn[n] = jacobiRow(L, n, xo, w, b[n]);
+        for (int n = threadIdx.x; n < L.N; n += blockDim.x) xn[n] = jacobiRowT(L, n, xo, w, b[n]);
         __syncthreads();
         double* t = xo;
         xo = xn;
@@ -222,11 +325,13 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_tail(const Ctl* ctl, TailAr
     double* X[kMaxTail];
     double* Y[kMaxTail];
     double* B[kMaxTail];
+    double* R[kMaxTail];
     for (int i = 0; i < a.count; i++) {
         const int N = a.lv[i].N;
         X[i] = sm + a.smemOff[i];
         Y[i] = X[i] + N;
         B[i] = Y[i] + N;
+        R[i] = B[i] + N;
     }
     // restriction into the first tail level from the finer level's residual
     {
@@ -243,13 +348,12 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_tail(const Ctl* ctl, TailAr
     for (int i = 0; i < last; i++) {
         const LevelDev& L = a.lv[i];
         tailSmooth(L, X[i], Y[i], B[i], a.w, a.pre);
+        for (int n = threadIdx.x; n < L.N; n += blockDim.x) R[i][n] = residualRowT(L, n, X[i], B[i][n]);
+        __syncthreads();
         const LevelDev& C = a.lv[i + 1];
         for (int c = threadIdx.x; c < C.N; c += blockDim.x) {
             double sum = 0.0;
-            for (int q = C.mStart[c]; q < C.mStart[c + 1]; q++) {
-                const int m = C.mList[q];
-                sum += residualRow(L, m, X[i], B[i][m]);
-            }
+            for (int q = C.mStart[c]; q < C.mStart[c + 1]; q++) sum += R[i][C.mList[q]];
             B[i + 1][c] = sum;
             X[i + 1][c] = 0.0;
         }
@@ -278,7 +382,9 @@ void launchGalerkin(const Ctl* ctl, const LevelDev& fine, const LevelDev& coarse
 }
 
 void launchMGSmooth(const Ctl* ctl, const LevelDev& L, const double* x, double* y, double w, cudaStream_t s) {
-    k_mg_smooth<<<blocksFor(L.N), kThreads, 0, s>>>(ctl, L, x, y, w);
+    if (!L.sliceOff && L.W == 4) k_mg_smooth_ell<4><<<blocksFor(L.N), kThreads, 0, s>>>(ctl, L, x, y, w);
+    else if (!L.sliceOff && L.W == 3) k_mg_smooth_ell<3><<<blocksFor(L.N), kThreads, 0, s>>>(ctl, L, x, y, w);
+    else k_mg_smooth<<<blocksFor(L.N), kThreads, 0, s>>>(ctl, L, x, y, w);
 }
 
 void launchMGSmoothBlock(const Ctl* ctl, const LevelDev& L, double* x, double w, int sweeps, cudaStream_t s) {
@@ -292,7 +398,9 @@ void launchMGSmoothBlock(const Ctl* ctl, const LevelDev& L, double* x, double w,
 }
 
 void launchMGResidual(const Ctl* ctl, const LevelDev& L, const double* x, cudaStream_t s) {
-    k_mg_residual<<<blocksFor(L.N), kThreads, 0, s>>>(ctl, L, x);
+    if (!L.sliceOff && L.W == 4) k_mg_residual_ell<4><<<blocksFor(L.N), kThreads, 0, s>>>(ctl, L, x);
+    else if (!L.sliceOff && L.W == 3) k_mg_residual_ell<3><<<blocksFor(L.N), kThreads, 0, s>>>(ctl, L, x);
+    else k_mg_residual<<<blocksFor(L.N), kThreads, 0, s>>>(ctl, L, x);
 }
 
 void launchMGGather(const Ctl* ctl, const LevelDev& fine, const LevelDev& coarse, double* xCur, double* xAlt,
@@ -306,7 +414,7 @@ void launchMGProlong(const Ctl* ctl, const LevelDev& fine, double* xFine, const 
 
 size_t tailSharedBytes(const TailArgs& a) {
     size_t d = 0;
-    for (int i = 0; i < a.count; i++) d += 3 * (size_t)a.lv[i].N;
+    for (int i = 0; i < a.count; i++) d += 4 * (size_t)a.lv[i].N;
     return d * sizeof(double);
 }
 

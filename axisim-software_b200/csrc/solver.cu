@@ -569,8 +569,8 @@ private:
             bool fits = true;
             size_t bytes = 0;
             for (int l = t; l < L; l++) {
-                fits = fits && levels_[(size_t)l].N <= 4096;
-                bytes += 3 * (size_t)levels_[(size_t)l].N * sizeof(double);
+                fits = fits && levels_[(size_t)l].N <= 1024;
+                bytes += 4 * (size_t)levels_[(size_t)l].N * sizeof(double);
             }
             if (fits && bytes <= 200 * 1024) {
                 tailStart_ = t;
@@ -619,7 +619,7 @@ private:
             for (int i = 0; i < a.count; i++) {
                 a.lv[i] = levels_[(size_t)(l + 1 + i)];
                 a.smemOff[i] = (int)off;
-                off += 3 * (size_t)a.lv[i].N;
+                off += 4 * (size_t)a.lv[i].N;
             }
             a.resFine = F.res;
             a.xOut = cur[(size_t)l + 1];
