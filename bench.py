@@ -202,6 +202,32 @@ def cpu_baseline_leg(case, mesh):
             "sample": f"{n} SIMPLE iterations of {case.name} from rest ({dt:.1f} s)"}
 
 
+def reference_cuda_leg(case, iters):
+    """The reference's own CUDA solver (compiled unchanged from its sources,
+    oracle/ref_build) on the same workload, timed by its CudaTimer span."""
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "axisim_ref")
+    if not os.path.exists(ref_bin):
+        return {"unavailable": "oracle/_ref/axisim_ref not built"}
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import tempfile
+    import make_golden
+    c = workload(1.0) if case is None else case
+    c.settings["maxIter"] = iters
+    c.settings["resTol"] = [0.0, 0.0, 0.0]
+    with tempfile.TemporaryDirectory() as d:
+        spec, out = os.path.join(d, "spec.txt"), os.path.join(d, "out.bin")
+        make_golden.write_spec(c, spec)
+        r = subprocess.run([ref_bin, spec, out], capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        return {"unavailable": "reference run failed: " + r.stderr.strip()[-200:]}
+    # "reference solver: N cells, K iterations, converged C, T ms"
+    import re
+    m = re.search(r"reference solver: (\d+) cells, (\d+) iterations, converged (\d+), ([0-9.]+) ms", r.stdout)
+    n, k, ms = int(m.group(1)), int(m.group(2)), float(m.group(4))
+    return {"value": n * k / (ms / 1e3) / 1e6, "unit": UNIT, "iterations": k, "ms": ms,
+            "note": "reference CUDA build (sm_100a, unchanged sources), CudaTimer over its SIMPLE loop"}
+
+
 def mesh_bytes(m):
     import numpy as np
     return int(sum(np.asarray(m[k]).nbytes for k in m if k not in ("nCells", "nFaces", "status")))
@@ -286,6 +312,7 @@ def run_b200(args):
                        "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                        "seconds": t_e2e, "note": "host clock around set_mesh/set_bc/set_field/solve/get_field"}
         line["cpu_baseline"] = cpu_baseline_leg(case, mesh)
+        line["reference_cuda"] = reference_cuda_leg(workload(args.scale), min(args.steps, 100))
         # time to residual 1e-6 on the pipe, CUDA-event time inside solve
         from axisim import cases
         pc = cases.pipe(max_iter=50000, tol=1e-6)
@@ -296,6 +323,10 @@ def run_b200(args):
                                     "converged": rr["converged"], "seconds": rr["ms"] / 1e3,
                                     "residuals": rr["residual"]}
         ps.close()
+        ref_pipe = reference_cuda_leg(cases.pipe(max_iter=50000, tol=1e-6), 50000)
+        if "ms" in ref_pipe:
+            line["time_to_residual"]["reference_cuda_seconds"] = ref_pipe["ms"] / 1e3
+            line["time_to_residual"]["reference_cuda_iterations"] = ref_pipe["iterations"]
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -1,0 +1,112 @@
+"""Generate golden vectors from the REFERENCE's own SIMPLE solver.
+
+Runs oracle/_ref/axisim_ref (the reference's solver translation units compiled
+unchanged from their sources by oracle/ref_build/Makefile, driven headless by
+oracle/ref_build/ref_driver.cu) on small cases and stores the solution fields
+and residual history as .npz fixtures next to this script. Needs a GPU (the
+reference is GPU-only); the committed fixtures are what the CPU tests read.
+
+    python tests/golden/make_golden.py [outdir]
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "axisim-software_b200"))
+from axisim import cases  # noqa: E402
+
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "axisim_ref")
+VAR_NAMES = {cases.U: "u", cases.V: "v", cases.P: "p"}
+
+
+def fixture_cases():
+    """(name, case, tolerance note) of every golden vector."""
+    out = []
+    out.append(("pipe10x50_fd_converged", cases.pipe(nr=10, nz=50, max_iter=5000, tol=1e-6, fully_developed=True)))
+    out.append(("pipe10x50_5it", cases.pipe(nr=10, nz=50, max_iter=5, tol=1e-30)))
+    c = cases.expansion(scale=1 / 32, max_iter=5, tol=1e-30)
+    out.append(("expansion864_sou_5it", c))
+    c = cases.expansion(scale=1 / 32, max_iter=20000, tol=1e-6)
+    out.append(("expansion864_sou_converged", c))
+    c = cases.expansion(scale=1 / 32, max_iter=4, tol=1e-30)
+    c.settings.update(convectionScheme=cases.CONV_CENTRAL, gradientScheme=cases.GRAD_GREEN_GAUSS)
+    out.append(("expansion864_gg_central_4it", c))
+    c = cases.pipe(nr=8, nz=40, max_iter=4, tol=1e-30)
+    c.settings.update(useMultigrid=0, linearType=cases.LINEAR_JACOBI, linearMaxIter=7)
+    out.append(("pipe8x40_nomg_jacobi7_4it", c))
+    c = cases.pulsatile_expansion(scale=1 / 32, dt=1e-3, steps=3, max_iter=3, tol=1e-30)
+    out.append(("pulsatile864_bdf2_3x3", c))
+    c = cases.pipe(max_iter=50000, tol=1e-6)
+    out.append(("pipe40x200_config1_converged", c))
+    return out
+
+
+def write_spec(case, path, tol=1e-9):
+    with open(path, "w") as f:
+        f.write(f"tol {tol!r}\n")
+        for b in case.blocks:
+            ax, rd = b["axial"], b["radial"]
+            f.write("block %r %r %r %d %d %r %r %d %d %r %d %d %d %d\n" % (
+                b["z0"], b["r0"], ax[0], ax[1], ax[2], ax[3], rd[0], rd[1], rd[2], rd[3], *b["edge_group"]))
+        for g in case.groups:
+            items = []
+            for var, bc in g.bcs.items():
+                t, val = bc[0], bc[1]
+                amp, freq = (bc[2], bc[3]) if len(bc) > 2 else (0.0, 0.0)
+                items.append(f"{VAR_NAMES[var]} {t} {val!r} {amp!r} {freq!r}")
+            f.write(f"group {g.id} {g.btype} {float(np.float32(g.total_length))!r} {len(items)} {' '.join(items)}\n")
+        s = case.settings
+        for k in ("convectionScheme", "gradientScheme", "linearType", "timeScheme", "linearMaxIter", "useMultigrid",
+                  "addConvectionTerm", "transient", "useNonOrthCorrector", "dt", "tEnd", "maxIter", "checkConv",
+                  "mgMaxIter", "mgWeight", "mgLinearSweep", "mgPreSweep", "mgPostSweep", "rho", "mu", "alphaU",
+                  "alphaP"):
+            f.write(f"set {k} {float(s[k])!r}\n")
+        for i in range(3):
+            f.write(f"set resNorm{i} {s['resNorm'][i]}\nset resScale{i} {s['resScale'][i]}\n"
+                    f"set resEnabled{i} {s['resEnabled'][i]}\nset resTol{i} {s['resTol'][i]!r}\n")
+
+
+FIELDS = ["u", "v", "p", "continuity", "gradPZ", "gradPR", "gradUZ", "gradUR", "gradVZ", "gradVR"]
+
+
+def read_out(path):
+    raw = open(path, "rb").read()
+    N, it, conv, rows = np.frombuffer(raw[:16], dtype=np.int32)
+    off = 16
+    out = {"iterations": int(it), "converged": int(conv)}
+    for name in FIELDS:
+        out[name] = np.frombuffer(raw[off:off + 8 * N], dtype=np.float64).copy()
+        off += 8 * N
+    out["residual_history"] = np.frombuffer(raw[off:off + 32 * rows], dtype=np.float64).reshape(rows, 4).copy()
+    return out
+
+
+def run_reference(case):
+    with tempfile.TemporaryDirectory() as d:
+        spec, out = os.path.join(d, "spec.txt"), os.path.join(d, "out.bin")
+        write_spec(case, spec)
+        r = subprocess.run([REF_BIN, spec, out], capture_output=True, text=True, timeout=1200)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference run failed: {r.stdout} {r.stderr}")
+        res = read_out(out)
+        res["log"] = r.stdout
+        return res
+
+
+def main(outdir=HERE):
+    for name, case in fixture_cases():
+        res = run_reference(case)
+        keep = {k: v for k, v in res.items() if k not in ("log",)}
+        if name.startswith("pipe40x200"):
+            keep = {k: keep[k] for k in ("u", "v", "p", "iterations", "converged", "residual_history")}
+        np.savez_compressed(os.path.join(outdir, name + ".npz"), **keep)
+        print(name, res["iterations"], res["converged"], res["log"].strip().splitlines()[0])
+
+
+if __name__ == "__main__":
+    main(*sys.argv[1:])

@@ -148,3 +148,19 @@ def test_errors_are_status_codes():
     with pytest.raises(abi.AxisimError) as e:
         abi.Solver(bad, case.bc_fields(), case.settings)
     assert e.value.status == abi.E_MESH
+
+
+@pytest.mark.parametrize("name", [n for n, _ in __import__("make_golden").fixture_cases()])
+def test_cuda_path_matches_reference_solver(name):
+    """The CUDA path against the reference's own solver (golden vectors)."""
+    import os
+    import make_golden
+    case = dict(make_golden.fixture_cases())[name]
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", name + ".npz"))
+    mesh = abi.multiblock(case.blocks)
+    gpu = abi.Solver(mesh, case.bc_fields(), case.settings)
+    r = gpu.solve()
+    assert r["iterations"] == int(g["iterations"]) and r["converged"] == bool(g["converged"])
+    for k in ("u", "v", "p", "gradPZ", "gradPR"):
+        if k in g:
+            assert rel_l2(gpu.get(k), g[k]) <= 1e-10, (name, k)

@@ -1,0 +1,52 @@
+"""The CPU oracle against golden vectors produced by the REFERENCE's own solver.
+
+tests/golden/*.npz come from tests/golden/make_golden.py, which runs the
+reference's solver translation units compiled unchanged from their sources
+(oracle/ref_build) on a B200. The reference sums its multigrid Galerkin and
+restriction with atomicAdd and contracts a*b+c into FMA, so agreement is to
+rounding: 1e-10 relative L2 on u, v, p and the gradients, and the same
+iteration count (also to convergence at 1e-6).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from helpers import rel_l2
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+import sys  # noqa: E402
+sys.path.insert(0, os.path.join(HERE, "golden"))
+import make_golden  # noqa: E402
+
+CASES = make_golden.fixture_cases()
+ORACLE_NAMES = {"u": "u", "v": "v", "p": "p", "gradPZ": "gradPZ", "gradPR": "gradPR", "gradUZ": "gradUZ",
+                "gradUR": "gradUR", "gradVZ": "gradVZ", "gradVR": "gradVR"}
+TOL = 1e-10
+
+
+@pytest.mark.parametrize("name,case", CASES, ids=[n for n, _ in CASES])
+def test_oracle_matches_reference_solver(name, case):
+    g = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    mesh = oracle.multiblock(case.blocks)
+    o = oracle.Oracle(mesh, case.bc_fields(), case.settings)
+    it, conv = o.run()
+    assert it == int(g["iterations"])
+    assert conv == bool(g["converged"])
+    for k, on in ORACLE_NAMES.items():
+        if k in g:
+            assert rel_l2(o.get(on), g[k]) <= TOL, (name, k, rel_l2(o.get(on), g[k]))
+    if "continuity" in g:
+        # per-cell mass imbalance after the last iteration (Solver::getMassImbalance)
+        scale = np.abs(o.get("mDot")).max()
+        assert np.max(np.abs(o.get("res_Continuity") - g["continuity"])) <= 1e-9 * scale
+    # the monitored residual history (U, V, Continuity) of the reference
+    hist = g["residual_history"]
+    assert hist.shape[0] == it
+    np.testing.assert_allclose(o.residuals(), hist[-1, 1:], rtol=1e-6)
+
+
+def test_fixture_cases_are_small():
+    for name, _ in CASES:
+        assert os.path.getsize(os.path.join(HERE, "golden", name + ".npz")) < 400_000
