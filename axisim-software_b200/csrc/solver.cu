@@ -1079,13 +1079,30 @@ int64_t Solver::getField(const std::string& name, double* out, size_t n) const {
         {"AC_v", ACv_, N, 0}, {"b_v", bv_, N, 0}, {"AF_v", AFm_, S, 1}, {"invAC_v", iv_, N, 0},
         {"AC_pp", ACpp_, N, 0}, {"b_pp", bpp_, N, 0}, {"AF_pp", AFpp_, S, 1}, {"invAC_pp", ipp_, N, 0},
         {"res_U", resU_, N, 0}, {"res_V", resV_, N, 0}, {"res_Continuity", resC_, N, 0},
-        {"continuity", resC_, N, 0},
         {"uOld", uOld_, N, 0}, {"vOld", vOld_, N, 0}, {"uOld2", uOld2_, N, 0}, {"vOld2", vOld2_, N, 0},
         {"invDPN", mesh_.invDPN, F, 0}, {"wP", mesh_.wP, F, 0}, {"dPB", mesh_.dPB, F, 0},
         {"length2D", mesh_.length2D, F, 0}, {"lsqWZ", mesh_.lsqWZ, F, 0}, {"lsqWR", mesh_.lsqWR, F, 0},
         {"invA2D", mesh_.invA2D, N, 0}, {"lsqInvZZ", mesh_.lsqIZZ, N, 0}, {"lsqInvZR", mesh_.lsqIZR, N, 0},
         {"lsqInvRR", mesh_.lsqIRR, N, 0},
     };
+    if (name == "continuity") {
+        // Solver::getMassImbalance (solver.cpp:298-331): per-cell net outflow
+        // of the final face mass fluxes.
+        if (!out || n < N) throw StatusError(AXISIM_E_ARG, "output buffer too small for continuity");
+        CK(cudaStreamSynchronize(stream_));
+        std::vector<double> md(F);
+        CK(cudaMemcpy(md.data(), mDot_, F * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int c = 0; c < N_; c++) {
+            double imb = 0.0;
+            for (int k = hCfs_[(size_t)c]; k < hCfs_[(size_t)c + 1]; k++) {
+                const int f = hCfi_[(size_t)k];
+                if (hOwner_[(size_t)f] == c) imb += md[(size_t)f];
+                else if (hNeighbor_[(size_t)f] == c) imb -= md[(size_t)f];
+            }
+            out[c] = imb;
+        }
+        return (int64_t)N;
+    }
     for (const E& e : tab) {
         if (name != e.n) continue;
         if (!out || n < e.len) throw StatusError(AXISIM_E_ARG, "output buffer too small for " + name);

@@ -120,3 +120,32 @@ def test_create_without_device_is_a_status_not_a_crash(lib):
     h = ctypes.c_void_p()
     st = lib.axisim_create(None, ctypes.byref(h))
     assert st == abi.E_CUDA and not h.value
+
+
+def test_cpp_adapter_compiles_and_links(lib, tmp_path):
+    """The header-only C++ adapter (reference Solver member names) builds against the library."""
+    src = tmp_path / "use_adapter.cpp"
+    src.write_text(r'''
+#include "axisim_solver.hpp"
+#include <cstdio>
+int main() {
+    axisim_fluid f{1000.0, 1e-3, 4180.0, 0.6, 3e-9};
+    try {
+        axisim_b200::Solver s(f);
+        s.configSimple.maxIter = 10;
+        std::string why;
+        std::printf("can continue: %d\n", (int)s.canContinue(&why));
+    } catch (const std::exception& e) {
+        std::printf("no device: %s\n", e.what());
+    }
+    return 0;
+}
+''')
+    exe = tmp_path / "use_adapter"
+    pkg = os.path.join(ROOT, "axisim-software_b200")
+    r = __import__("subprocess").run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                                      "-L", pkg, "-laxisim_b200", "-Wl,-rpath," + pkg, "-lpthread"],
+                                     capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = __import__("subprocess").run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0
