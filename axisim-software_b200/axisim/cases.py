@@ -129,9 +129,14 @@ class Case:
     groups: list
     settings: dict
     note: str = ""
+    mesh: dict = None   # packed mesh for unstructured cases (blocks empty)
 
     def bc_fields(self):
         return {v: resolve_bc_field(self.groups, v) for v in (U, V, P)}
+
+    def packed(self, builder):
+        """The packed mesh: the stored one, or `builder(blocks)` (the C++ or the oracle packer)."""
+        return self.mesh if self.mesh is not None else builder(self.blocks)
 
 
 def pipe(nr=40, nz=200, R=0.01, L=0.2, U0=0.05, rho=1000.0, mu=1e-3, fully_developed=False,
@@ -209,6 +214,29 @@ def pulsatile_expansion(scale=1.0, dt=1e-4, steps=2000, period=0.1, amplitude=0.
     c.settings.update(transient=1, timeScheme=TIME_SECOND_ORDER, dt=dt, tEnd=dt * steps)
     c.name = "pulsatile_" + c.name
     return c
+
+
+def bullet(scale=1.0, rho=1000.0, mu=1e-3, re=200.0, seed=0, max_iter=50000, tol=1e-6):
+    """Revolved bullet body (cylinder radius 5 mm, length 30 mm, hemispherical
+    nose) on the axis of a pipe of radius 20 mm and length 300 mm, triangulated
+    to ~485k cells at scale 1 (1250 x 200 quads split in two, body removed,
+    interior vertices jittered +-10 % of the spacing from a fixed seed).
+    Uniform inlet at Re 200 on the body diameter; the fluid is unstated in the
+    case description, so water (rho 1000, mu 1e-3, U = 0.02 m/s). Least-squares
+    gradients with the non-orthogonal corrector, agglomeration multigrid."""
+    from . import trimesh
+    nz, nr = max(8, round(1250 * scale)), max(4, round(200 * scale))
+    pts, tris, classify = trimesh.bullet_in_pipe(nz=nz, nr=nr, seed=seed)
+    mesh = trimesh.pack_triangles(pts, tris, classify)
+    u_in = re * mu / (rho * 0.01)
+    groups = [Group(0, VELOCITY_INLET, {U: (DIRICHLET, u_in)}, total_length=0.02),
+              Group(1, PRESSURE_OUTLET, {P: (DIRICHLET, 0.0)}, total_length=0.02),
+              Group(2, WALL, {}, total_length=0.3),
+              Group(3, SYMMETRY, {}, total_length=0.3)]
+    s = default_settings()
+    s.update(convectionScheme=CONV_UPWIND, gradientScheme=GRAD_LSQ, linearType=LINEAR_JACOBI, useNonOrthCorrector=1,
+             rho=rho, mu=mu, maxIter=max_iter, resTol=[tol, tol, tol])
+    return Case(f"bullet_{mesh['nCells']}", [], groups, s, note=f"U_in={u_in:.4g} m/s", mesh=mesh)
 
 
 def cell_count(case):

@@ -15,9 +15,38 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
+
 #include <cuda_runtime.h>
 
 namespace axisim {
+
+// Programmatic dependent launch: every kernel of the SIMPLE iteration is
+// launched with programmatic stream serialisation, so its launch and CTA
+// scheduling overlap the tail of the kernel before it. Each kernel waits for
+// its predecessor's results (griddepcontrol.wait) before reading anything,
+// then lets its own successor be scheduled (griddepcontrol.launch_dependents);
+// a successor's CTAs only start once the last CTA of this grid has started.
+__device__ __forceinline__ void pdlEnter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launchPDL(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                             Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 constexpr int kMaxHist = 128;   // residual history ring (>= largest graph batch)
 
@@ -105,6 +134,10 @@ struct MomentumArgs {
     double* DV;
     double mu, rho, dt, alpha;
     int conv, scheme, nonOrtho, transient;
+    // mixed precision: FP32 copies of AF and 1/AC for the correction sweeps (null on the FP64 path)
+    float* AF32;
+    float* invU32;
+    float* invV32;
 };
 
 }  // namespace axisim

@@ -7,21 +7,24 @@
 
 namespace axisim {
 
-// One multigrid level on the device. Level 0 aliases the p' system and uses the
-// mesh's [W][N] slot block; coarser levels use sliced ELL: 32-row slices, slot
-// j of cell n at sliceOff[n/32] + 32 j + n%32, slice width (sliceOff[s+1] -
-// sliceOff[s]) / 32, unused slots with neighbour -1 and coefficient 0.
-struct LevelDev {
+// One multigrid level on the device, values of type T (double on the FP64
+// path, float for the mixed-precision cycle). Level 0 aliases the p' system
+// and uses the mesh's [W][N] slot block; coarser levels use sliced ELL:
+// 32-row slices, slot j of cell n at sliceOff[n/32] + 32 j + n%32, slice width
+// (sliceOff[s+1] - sliceOff[s]) / 32, unused slots with neighbour -1 and
+// coefficient 0. Topology and transfer lists are shared by both precisions.
+template <class T>
+struct LevelT {
     int N = 0, W = 0;
     int totalSlots = 0;
     const int32_t* sliceOff = nullptr;  // null: [W][N] layout
     int32_t* nb = nullptr;
-    double* AF = nullptr;
-    double* AC = nullptr;
-    double* b = nullptr;
-    double* x = nullptr;
-    double* xNew = nullptr;
-    double* res = nullptr;     // fine residual / Galerkin diagonal scratch (N)
+    T* AF = nullptr;
+    T* AC = nullptr;
+    T* b = nullptr;
+    T* x = nullptr;
+    T* xNew = nullptr;
+    T* res = nullptr;          // fine residual / Galerkin diagonal scratch (N)
     int32_t* c2c = nullptr;    // fine -> coarse (null on the coarsest level)
     // restriction / Galerkin gathers, stored on the COARSE level:
     int32_t* mStart = nullptr;  // [N+1] members of each coarse cell
@@ -30,18 +33,22 @@ struct LevelDev {
     int32_t* gList = nullptr;   // fine slot positions, ascending fine cell then slot
     uint32_t* internalMask = nullptr;  // on the FINE level: slots folding into the coarse diagonal
 };
+using LevelDev = LevelT<double>;
+using LevelF = LevelT<float>;
 
 // Levels at and below `first` solved inside one CTA (V-cycle tail).
 constexpr int kMaxTail = 8;
-struct TailArgs {
+template <class T>
+struct TailArgsT {
     int first = 0, count = 0;
-    LevelDev lv[kMaxTail];
-    int smemOff[kMaxTail];   // doubles: x, y, b per level
-    const double* resFine = nullptr;
-    double* xOut = nullptr;
-    double w = 0.6;
+    LevelT<T> lv[kMaxTail];
+    int smemOff[kMaxTail];   // elements of T: x, y, b, r per level
+    const T* resFine = nullptr;
+    T* xOut = nullptr;
+    T w = T(0.6);
     int pre = 1, post = 1, coarseSweeps = 30;
 };
+using TailArgs = TailArgsT<double>;
 
 // ---- setup ----
 void launchPrecompute(const MeshDev& m, const int32_t* cfs, const int32_t* cfi, double* lsqDZ, double* lsqDR,
@@ -66,7 +73,8 @@ void launchGaussSeidelUV(const MeshDev& m, const Ctl* ctl, const double* AF, con
 void launchPressureSystem(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, const BCDev& bcV,
                           const BCDev& bcP, double rho, const double* u, const double* v, const double* p,
                           const double* gPZ, const double* gPR, const double* DU, const double* DV,
-                          double* AFpp, double* ACpp, double* invACpp, double* mDot, cudaStream_t s);
+                          double* AFpp, double* ACpp, double* invACpp, double* mDot, float* AF32, float* AC32,
+                          cudaStream_t s);
 void launchPressureRhs(const MeshDev& m, const Ctl* ctl, double rho, const double* mDot, const double* DU,
                        const double* DV, const double* gZ, const double* gR, int cross, int zeroPP, double* bpp,
                        double* pp, cudaStream_t s);
@@ -85,17 +93,42 @@ void launchResiduals(const MeshDev& m, const Ctl* ctl, const double* AF, const d
 void launchIterEnd(Ctl* ctl, const double* partial, int nBlocks, int N, cudaStream_t s);
 void launchCopy(const Ctl* ctl, double* dst, const double* src, int n, cudaStream_t s);
 
-// ---- multigrid (FP64, mg_fp64.cu) ----
-void launchGalerkin(const Ctl* ctl, const LevelDev& fine, const LevelDev& coarse, cudaStream_t s);
-void launchMGSmooth(const Ctl* ctl, const LevelDev& L, const double* x, double* y, double w, cudaStream_t s);
-void launchMGSmoothBlock(const Ctl* ctl, const LevelDev& L, double* x, double w, int sweeps, cudaStream_t s);
-void launchMGResidual(const Ctl* ctl, const LevelDev& L, const double* x, cudaStream_t s);
+// ---- multigrid (mg.cu), T = double or float ----
+// Galerkin P^T A P from a fine level of type TF into a coarse level of type TC
+template <class TF, class TC>
+void launchGalerkin(const Ctl* ctl, const LevelT<TF>& fine, const LevelT<TC>& coarse, cudaStream_t s);
+template <class T>
+void launchMGSmooth(const Ctl* ctl, const LevelT<T>& L, const T* x, T* y, T w, cudaStream_t s);
+template <class T>
+void launchMGSmoothBlock(const Ctl* ctl, const LevelT<T>& L, T* x, T w, int sweeps, cudaStream_t s);
+template <class T>
+void launchMGResidual(const Ctl* ctl, const LevelT<T>& L, const T* x, cudaStream_t s);
 // b_c = sum of the fine residuals of each agglomerate; x_c = 0, or with
 // firstSweep the result of one Jacobi sweep from zero written to xAlt
-void launchMGGather(const Ctl* ctl, const LevelDev& fine, const LevelDev& coarse, double* xCur, double* xAlt,
-                    int firstSweep, double w, cudaStream_t s);
-void launchMGProlong(const Ctl* ctl, const LevelDev& fine, double* xFine, const double* xCoarse, cudaStream_t s);
-size_t tailSharedBytes(const TailArgs& a);
-void launchMGTail(const Ctl* ctl, const TailArgs& a, cudaStream_t s);
+template <class T>
+void launchMGGather(const Ctl* ctl, const LevelT<T>& fine, const LevelT<T>& coarse, T* xCur, T* xAlt,
+                    int firstSweep, T w, cudaStream_t s);
+template <class T>
+void launchMGProlong(const Ctl* ctl, const LevelT<T>& fine, T* xFine, const T* xCoarse, cudaStream_t s);
+template <class T>
+size_t tailSharedBytes(const TailArgsT<T>& a);
+template <class T>
+void launchMGTail(const Ctl* ctl, const TailArgsT<T>& a, cudaStream_t s);
+
+// ---- mixed precision (kernels_mixed.cu) ----
+// p' cycle as iterative refinement: r = b - A x in FP64, stored as FP32 with
+// the first Jacobi sweep of the correction (from zero); x += e after the cycle.
+void launchIRResidualPP(const Ctl* ctl, const LevelDev& L0, float* r32, float* eFirst, double w, int firstSweep,
+                        cudaStream_t s);
+void launchIRUpdatePP(const Ctl* ctl, int N, double* x, const float* e, cudaStream_t s);
+// momentum in correction form: r = b - A u (FP64) -> FP32, first Jacobi sweep
+// delta = r / AC; FP32 sweeps on delta; u += delta
+void launchIRResidualUV(const MeshDev& m, const Ctl* ctl, const double* AF, const double* ACu, const double* ACv,
+                        const double* bu, const double* bv, const double* u, const double* v, const float* iu32,
+                        const float* iv32, float* ru, float* rv, float* du, float* dv, cudaStream_t s);
+void launchJacobiUV32(const MeshDev& m, const Ctl* ctl, const float* AF32, const float* ru, const float* rv,
+                      const float* iu32, const float* iv32, const float* du, const float* dv, float* du2, float* dv2,
+                      cudaStream_t s);
+void launchIRUpdateUV(const Ctl* ctl, int N, double* u, double* v, const float* du, const float* dv, cudaStream_t s);
 
 }  // namespace axisim

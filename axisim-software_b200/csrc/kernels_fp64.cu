@@ -96,6 +96,7 @@ __device__ __forceinline__ double nonOrthoFlux(const MeshDev& m, int c, int f, i
 // preComputeVariables, face part (memory_manger.cpp:528-591)
 __global__ void k_precompute_faces(MeshDev m, double* invDPN, double* wP, double* dPB, double* length2D,
                                    double* lsqWZ, double* lsqWR, double* lsqDZ, double* lsqDR) {
+    pdlEnter();
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= m.F) return;
     length2D[f] = m.area[f] / (2 * kPi * m.fcR[f]);
@@ -131,6 +132,7 @@ __global__ void k_precompute_faces(MeshDev m, double* invDPN, double* wP, double
 // preComputeVariables, cell part (memory_manger.cpp:524-526, 593-613)
 __global__ void k_precompute_cells(MeshDev m, const int32_t* cfs, const int32_t* cfi, const double* lsqDZ,
                                    const double* lsqDR, double* invA2D, double* IZZ, double* IZR, double* IRR) {
+    pdlEnter();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.N) return;
     invA2D[c] = 2.0 * kPi * m.ccR[c] / m.vol[c];
@@ -156,6 +158,7 @@ __global__ void k_precompute_cells(MeshDev m, const int32_t* cfs, const int32_t*
 // buildCellFaceCSR (memory_manger.cpp:287-323) into the [W][N] slot block
 __global__ void k_build_ell(int N, int W, const int32_t* cfs, const int32_t* cfi, const int32_t* owner,
                             const int32_t* neighbor, int32_t* sface, int32_t* snb) {
+    pdlEnter();
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
     const int k0 = cfs[n], deg = cfs[n + 1] - k0;
@@ -173,6 +176,7 @@ __global__ void k_build_ell(int N, int W, const int32_t* cfs, const int32_t* cfi
 
 // ---------------- iteration control ----------------
 __global__ void k_iter_begin(Ctl* ctl, const volatile int* hostStop) {
+    pdlEnter();
     if (ctl->done) return;
     if (hostStop && *hostStop) {
         ctl->done = 2;
@@ -195,6 +199,7 @@ struct GradArgs {
 
 template <int NF>
 __global__ void k_gradient(MeshDev m, const Ctl* ctl, GradArgs a, int scheme) {
+    pdlEnter();
     if (ctl && ctl->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m.N) return;
@@ -344,6 +349,7 @@ __device__ __forceinline__ void momentumBoundary(const MeshDev& m, int n, int f,
 
 __global__ void __launch_bounds__(kThreads) k_momentum(MeshDev m, const Ctl* ctl, BCDev bcU, BCDev bcV,
                                                        MomentumArgs a) {
+    pdlEnter();
     if (ctl->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m.N) return;
@@ -387,8 +393,10 @@ __global__ void __launch_bounds__(kThreads) k_momentum(MeshDev m, const Ctl* ctl
                 }
             }
             a.AF[s] = af;
+            if (a.AF32) a.AF32[s] = (float)af;
         } else {
             a.AF[s] = 0.0;
+            if (a.AF32) a.AF32[s] = 0.f;
             momentumBoundary(m, n, f, area, F, a.mu, bcU, ACu, bu);
             momentumBoundary(m, n, f, area, F, a.mu, bcV, ACv, bv);
         }
@@ -439,6 +447,10 @@ __global__ void __launch_bounds__(kThreads) k_momentum(MeshDev m, const Ctl* ctl
     a.invACv[n] = iv;
     a.DU[n] = V * iu;  // solver_util.cu:127-144
     a.DV[n] = V * iv;
+    if (a.invU32) {
+        a.invU32[n] = (float)iu;
+        a.invV32[n] = (float)iv;
+    }
 }
 
 // ---------------- momentum sweeps (linear_solver.cu:9-72) ----------------
@@ -449,6 +461,7 @@ __global__ void __launch_bounds__(kThreads) k_jacobi_uv(int N, int W, const int3
                                                         const double* __restrict__ iu, const double* __restrict__ iv,
                                                         const double* __restrict__ xu, const double* __restrict__ xv,
                                                         double* __restrict__ yu, double* __restrict__ yv) {
+    pdlEnter();
     if (ctl->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
@@ -492,6 +505,7 @@ __global__ void __launch_bounds__(kThreads) k_jacobi_uv_wide(int N, int W, const
                                                              const double* __restrict__ xu,
                                                              const double* __restrict__ xv, double* __restrict__ yu,
                                                              double* __restrict__ yv) {
+    pdlEnter();
     if (ctl->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
@@ -515,6 +529,7 @@ __global__ void __launch_bounds__(kThreads) k_gs_uv(int N, int W, const int32_t*
                                                     const double* __restrict__ bv, const double* __restrict__ iu,
                                                     const double* __restrict__ iv, double* xu, double* xv,
                                                     const int32_t* __restrict__ order, int begin, int count) {
+    pdlEnter();
     if (ctl->done) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
@@ -538,6 +553,7 @@ __global__ void __launch_bounds__(kThreads) k_jacobi1(int N, int W, const int32_
                                                       const double* __restrict__ AF, const double* __restrict__ b,
                                                       const double* __restrict__ inv, const double* __restrict__ x,
                                                       double* __restrict__ y) {
+    pdlEnter();
     if (ctl->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
@@ -555,6 +571,7 @@ __global__ void __launch_bounds__(kThreads) k_gs1(int N, int W, const int32_t* _
                                                   const double* __restrict__ AF, const double* __restrict__ b,
                                                   const double* __restrict__ inv, double* x,
                                                   const int32_t* __restrict__ order, int begin, int count) {
+    pdlEnter();
     if (ctl->done) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
@@ -583,10 +600,13 @@ struct PressureArgs {
     double* ACpp;
     double* invACpp;
     double* mDot;
+    float* AF32;  // FP32 copies for the mixed-precision cycle (null on the FP64 path)
+    float* AC32;
 };
 
 __global__ void __launch_bounds__(kThreads) k_pressure(MeshDev m, const Ctl* ctl, BCDev bcU, BCDev bcV, BCDev bcP,
                                                        PressureArgs a) {
+    pdlEnter();
     if (ctl->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m.N) return;
@@ -606,8 +626,10 @@ __global__ void __launch_bounds__(kThreads) k_pressure(MeshDev m, const Ctl* ctl
             const double K = rho * area * Df * m.invDPN[f];
             AC += K;
             a.AFpp[s] = 0.0 - K;
+            if (a.AF32) a.AF32[s] = (float)(0.0 - K);
         } else {
             a.AFpp[s] = 0.0;
+            if (a.AF32) a.AF32[s] = 0.f;
             const int g = m.group[f];
             if (g >= 0 && g < bcP.nGroups && bcP.type[g] == BC_DIRICHLET) {
                 const double K = rho * area * Df / m.dPB[f];
@@ -653,6 +675,7 @@ __global__ void __launch_bounds__(kThreads) k_pressure(MeshDev m, const Ctl* ctl
     }
     a.ACpp[n] = AC;
     a.invACpp[n] = (fabs(AC) < 1.0e-30) ? 0.0 : 1.0 / AC;
+    if (a.AC32) a.AC32[n] = (float)AC;
 }
 
 // createPPRhs (simple.cu:90-142) + the p' reset before the corrector loop
@@ -660,6 +683,7 @@ __global__ void __launch_bounds__(kThreads) k_pp_rhs(MeshDev m, const Ctl* ctl, 
                                                      const double* DU, const double* DV, const double* gZ,
                                                      const double* gR, int cross, int zeroPP, double* bpp,
                                                      double* pp) {
+    pdlEnter();
     if (ctl->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m.N) return;
@@ -698,6 +722,7 @@ struct CorrectArgs {
 };
 
 __global__ void __launch_bounds__(kThreads) k_correct(MeshDev m, const Ctl* ctl, BCDev bcP, CorrectArgs a) {
+    pdlEnter();
     if (ctl->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m.N) return;
@@ -769,6 +794,7 @@ __global__ void __launch_bounds__(kThreads) k_residual(MeshDev m, const Ctl* ctl
                                                        const double* u, const double* v, const double* mDot,
                                                        double* resU, double* resV, double* resC, double* scaleU,
                                                        double* scaleV, double* partial) {
+    pdlEnter();
     if (ctl->done || !ctl->checked) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     const int N = m.N;
@@ -815,6 +841,7 @@ __global__ void __launch_bounds__(kThreads) k_residual(MeshDev m, const Ctl* ctl
 // Second reduction pass + residualAllHost's host arithmetic + convergence test
 // + iteration counters, all on the device (no host synchronisation).
 __global__ void __launch_bounds__(kThreads) k_iter_end(Ctl* ctl, const double* partial, int nBlocks, int N) {
+    pdlEnter();
     if (ctl->done) return;
     __shared__ double sh[kThreads][kResQ];
     if (ctl->checked) {
@@ -881,6 +908,7 @@ __global__ void __launch_bounds__(kThreads) k_iter_end(Ctl* ctl, const double* p
 }
 
 __global__ void k_copy(const Ctl* ctl, double* dst, const double* src, int n) {
+    pdlEnter();
     if (ctl && ctl->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] = src[i];
@@ -891,22 +919,22 @@ __global__ void k_copy(const Ctl* ctl, double* dst, const double* src, int n) {
 // ---------------- launchers ----------------
 void launchPrecompute(const MeshDev& m, const int32_t* cfs, const int32_t* cfi, double* lsqDZ, double* lsqDR,
                       cudaStream_t s) {
-    k_precompute_faces<<<blocksFor(m.F), kThreads, 0, s>>>(m, const_cast<double*>(m.invDPN), const_cast<double*>(m.wP),
+    launchPDL(k_precompute_faces, dim3(blocksFor(m.F)), dim3(kThreads), 0, s, m, const_cast<double*>(m.invDPN), const_cast<double*>(m.wP),
                                                             const_cast<double*>(m.dPB), const_cast<double*>(m.length2D),
                                                             const_cast<double*>(m.lsqWZ), const_cast<double*>(m.lsqWR),
                                                             lsqDZ, lsqDR);
-    k_precompute_cells<<<blocksFor(m.N), kThreads, 0, s>>>(m, cfs, cfi, lsqDZ, lsqDR, const_cast<double*>(m.invA2D),
+    launchPDL(k_precompute_cells, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, cfs, cfi, lsqDZ, lsqDR, const_cast<double*>(m.invA2D),
                                                             const_cast<double*>(m.lsqIZZ), const_cast<double*>(m.lsqIZR),
                                                             const_cast<double*>(m.lsqIRR));
 }
 
 void launchBuildEll(int N, int W, const int32_t* cfs, const int32_t* cfi, const int32_t* owner,
                     const int32_t* neighbor, int32_t* sface, int32_t* snb, cudaStream_t s) {
-    k_build_ell<<<blocksFor(N), kThreads, 0, s>>>(N, W, cfs, cfi, owner, neighbor, sface, snb);
+    launchPDL(k_build_ell, dim3(blocksFor(N)), dim3(kThreads), 0, s, N, W, cfs, cfi, owner, neighbor, sface, snb);
 }
 
 void launchIterBegin(Ctl* ctl, const volatile int* hostStop, cudaStream_t s) {
-    k_iter_begin<<<1, 1, 0, s>>>(ctl, hostStop);
+    launchPDL(k_iter_begin, dim3(1), dim3(1), 0, s, ctl, hostStop);
 }
 
 void launchGradient(const MeshDev& m, const Ctl* ctl, int nFields, const double* const* phi, const BCDev* bc,
@@ -919,60 +947,60 @@ void launchGradient(const MeshDev& m, const Ctl* ctl, int nFields, const double*
         a.gR[q] = gR[q];
     }
     const int b = blocksFor(m.N);
-    if (nFields == 1) k_gradient<1><<<b, kThreads, 0, s>>>(m, ctl, a, scheme);
-    else if (nFields == 2) k_gradient<2><<<b, kThreads, 0, s>>>(m, ctl, a, scheme);
-    else k_gradient<3><<<b, kThreads, 0, s>>>(m, ctl, a, scheme);
+    if (nFields == 1) launchPDL(k_gradient<1>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme);
+    else if (nFields == 2) launchPDL(k_gradient<2>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme);
+    else launchPDL(k_gradient<3>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme);
 }
 
 void launchMomentum(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, const BCDev& bcV, const MomentumArgs& a,
                     cudaStream_t s) {
-    k_momentum<<<blocksFor(m.N), kThreads, 0, s>>>(m, ctl, bcU, bcV, a);
+    launchPDL(k_momentum, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcU, bcV, a);
 }
 
 void launchJacobiUV(const MeshDev& m, const Ctl* ctl, const double* AF, const double* bu, const double* bv,
                     const double* iu, const double* iv, const double* xu, const double* xv, double* yu, double* yv,
                     cudaStream_t s) {
-    if (m.W == 4) k_jacobi_uv<4><<<blocksFor(m.N), kThreads, 0, s>>>(m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
-    else if (m.W == 3) k_jacobi_uv<3><<<blocksFor(m.N), kThreads, 0, s>>>(m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
-    else k_jacobi_uv_wide<<<blocksFor(m.N), kThreads, 0, s>>>(m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
+    if (m.W == 4) launchPDL(k_jacobi_uv<4>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
+    else if (m.W == 3) launchPDL(k_jacobi_uv<3>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
+    else launchPDL(k_jacobi_uv_wide, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
 }
 
 void launchGaussSeidelUV(const MeshDev& m, const Ctl* ctl, const double* AF, const double* bu, const double* bv,
                          const double* iu, const double* iv, double* xu, double* xv, const int32_t* order, int begin,
                          int count, cudaStream_t s) {
-    k_gs_uv<<<blocksFor(count), kThreads, 0, s>>>(m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, order, begin,
+    launchPDL(k_gs_uv, dim3(blocksFor(count)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, order, begin,
                                                   count);
 }
 
 void launchPressureSystem(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, const BCDev& bcV, const BCDev& bcP,
                           double rho, const double* u, const double* v, const double* p, const double* gPZ,
                           const double* gPR, const double* DU, const double* DV, double* AFpp, double* ACpp,
-                          double* invACpp, double* mDot, cudaStream_t s) {
-    PressureArgs a{rho, u, v, p, gPZ, gPR, DU, DV, AFpp, ACpp, invACpp, mDot};
-    k_pressure<<<blocksFor(m.N), kThreads, 0, s>>>(m, ctl, bcU, bcV, bcP, a);
+                          double* invACpp, double* mDot, float* AF32, float* AC32, cudaStream_t s) {
+    PressureArgs a{rho, u, v, p, gPZ, gPR, DU, DV, AFpp, ACpp, invACpp, mDot, AF32, AC32};
+    launchPDL(k_pressure, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcU, bcV, bcP, a);
 }
 
 void launchPressureRhs(const MeshDev& m, const Ctl* ctl, double rho, const double* mDot, const double* DU,
                        const double* DV, const double* gZ, const double* gR, int cross, int zeroPP, double* bpp,
                        double* pp, cudaStream_t s) {
-    k_pp_rhs<<<blocksFor(m.N), kThreads, 0, s>>>(m, ctl, rho, mDot, DU, DV, gZ, gR, cross, zeroPP, bpp, pp);
+    launchPDL(k_pp_rhs, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, rho, mDot, DU, DV, gZ, gR, cross, zeroPP, bpp, pp);
 }
 
 void launchJacobi1(const MeshDev& m, const Ctl* ctl, const double* AF, const double* b, const double* inv,
                    const double* x, double* y, cudaStream_t s) {
-    k_jacobi1<<<blocksFor(m.N), kThreads, 0, s>>>(m.N, m.W, m.snb, ctl, AF, b, inv, x, y);
+    launchPDL(k_jacobi1, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF, b, inv, x, y);
 }
 
 void launchGaussSeidel1(const MeshDev& m, const Ctl* ctl, const double* AF, const double* b, const double* inv,
                         double* x, const int32_t* order, int begin, int count, cudaStream_t s) {
-    k_gs1<<<blocksFor(count), kThreads, 0, s>>>(m.N, m.W, m.snb, ctl, AF, b, inv, x, order, begin, count);
+    launchPDL(k_gs1, dim3(blocksFor(count)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF, b, inv, x, order, begin, count);
 }
 
 void launchCorrect(const MeshDev& m, const Ctl* ctl, const BCDev& bcP, double rho, double alphaP, int nonOrtho,
                    const double* pp, const double* gZ, const double* gR, const double* DU, const double* DV, double* u,
                    double* v, double* p, double* mDot, cudaStream_t s) {
     CorrectArgs a{rho, alphaP, nonOrtho, pp, gZ, gR, DU, DV, u, v, p, mDot};
-    k_correct<<<blocksFor(m.N), kThreads, 0, s>>>(m, ctl, bcP, a);
+    launchPDL(k_correct, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcP, a);
 }
 
 void launchResiduals(const MeshDev& m, const Ctl* ctl, const double* AF, const double* ACu, const double* ACv,
@@ -981,16 +1009,16 @@ void launchResiduals(const MeshDev& m, const Ctl* ctl, const double* AF, const d
                      int* nBlocksOut, cudaStream_t s) {
     const int b = blocksFor(m.N);
     *nBlocksOut = b;
-    k_residual<<<b, kThreads, 0, s>>>(m, ctl, AF, ACu, ACv, bu, bv, u, v, mDot, resU, resV, resC, scaleU, scaleV,
+    launchPDL(k_residual, dim3(b), dim3(kThreads), 0, s, m, ctl, AF, ACu, ACv, bu, bv, u, v, mDot, resU, resV, resC, scaleU, scaleV,
                                       partial);
 }
 
 void launchIterEnd(Ctl* ctl, const double* partial, int nBlocks, int N, cudaStream_t s) {
-    k_iter_end<<<1, kThreads, 0, s>>>(ctl, partial, nBlocks, N);
+    launchPDL(k_iter_end, dim3(1), dim3(kThreads), 0, s, ctl, partial, nBlocks, N);
 }
 
 void launchCopy(const Ctl* ctl, double* dst, const double* src, int n, cudaStream_t s) {
-    k_copy<<<blocksFor(n), kThreads, 0, s>>>(ctl, dst, src, n);
+    launchPDL(k_copy, dim3(blocksFor(n)), dim3(kThreads), 0, s, ctl, dst, src, n);
 }
 
 }  // namespace axisim

@@ -1,0 +1,468 @@
+// mg.cu -- agglomeration multigrid V-cycle for the pressure correction (sm_100a).
+//
+// Same algorithm as MultigridSolver (solver/source/multigrid.cu:350-662):
+// Galerkin coarse operator P^T A P with piecewise-constant P, restriction by
+// summing fine residuals per agglomerate, prolongation by injection,
+// weighted-Jacobi smoothing (jacobiRow, multigrid.cu:447-484). B200 design:
+//   * no atomics: the Galerkin sums and the restriction are gathers over
+//     host-built member / slot lists in ascending fine order (bit-reproducible);
+//   * the fine residual is a coalesced pass over the fine level; the gather of
+//     the coarse right-hand side also performs the coarse level's first
+//     pre-smoothing sweep (from x = 0 it needs no neighbour values);
+//   * every level at or below 1024 cells runs as ONE single-CTA kernel holding
+//     x, the Jacobi partner, b and the residual in shared memory, with the
+//     coefficients L1-resident and the coarsest rows in registers (the
+//     reference launches three to four kernels per level per cycle there).
+// Every kernel is a template on the value type: double for the FP64 path
+// (compiled with --fmad=false, bit-exact with the CPU oracle), float for the
+// inner cycles of the mixed-precision path.
+#include <cmath>
+
+#include "kernels.hpp"
+
+namespace axisim {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kTailThreads = 1024;  // tail levels hold at most this many cells: one row per thread
+constexpr int kRegW = 16;
+
+inline int blocksFor(long long n, int t = kThreads) { return (int)((n + t - 1) / t); }
+
+template <class T>
+__device__ __forceinline__ T tiny();
+template <>
+__device__ __forceinline__ double tiny<double>() {
+    return 1.0e-30;
+}
+template <>
+__device__ __forceinline__ float tiny<float>() {
+    return 1.0e-30f;
+}
+
+struct Slots {
+    int base, stride, width;
+};
+
+template <class T>
+__device__ __forceinline__ Slots slotsOf(const LevelT<T>& L, int n) {
+    if (L.sliceOff) {
+        const int s = n >> 5;
+        const int o = L.sliceOff[s];
+        return Slots{o + (n & 31), 32, (L.sliceOff[s + 1] - o) >> 5};
+    }
+    return Slots{n, L.N, L.W};
+}
+
+// Weighted Jacobi row, jacobiRow (multigrid.cu:447-484).
+template <class T>
+__device__ __forceinline__ T jacobiRow(const LevelT<T>& L, int n, const T* xo, T w, T bn) {
+    const T ac = L.AC[n];
+    if (fabs(ac) < tiny<T>()) return xo[n];
+    T Ax = ac * xo[n];
+    const Slots sl = slotsOf(L, n);
+    for (int j = 0; j < sl.width; j++) {
+        const int p = sl.base + j * sl.stride;
+        const int k = L.nb[p];
+        if (k != -1) Ax += L.AF[p] * xo[k];
+    }
+    return xo[n] + w * (bn - Ax) / ac;
+}
+
+// residualRaw with sign (residuals.cuh:17-48)
+template <class T>
+__device__ __forceinline__ T residualRow(const LevelT<T>& L, int n, const T* x, T bn) {
+    T Ax = L.AC[n] * x[n];
+    const Slots sl = slotsOf(L, n);
+    for (int j = 0; j < sl.width; j++) {
+        const int p = sl.base + j * sl.stride;
+        const int k = L.nb[p];
+        if (k >= 0) Ax += L.AF[p] * x[k];
+    }
+    return bn - Ax;
+}
+
+// The same rows with every slot load issued before the neighbour gathers
+// (latency-bound single-CTA tail).
+template <class T>
+__device__ __forceinline__ T axEager(const LevelT<T>& L, int n, const T* x, bool jacobiTest) {
+    const Slots sl = slotsOf(L, n);
+    T Ax = L.AC[n] * x[n];
+    constexpr int kU = 8;
+    for (int j0 = 0; j0 < sl.width; j0 += kU) {
+        int k[kU];
+        T a[kU], g[kU];
+#pragma unroll
+        for (int j = 0; j < kU; j++) {
+            if (j0 + j < sl.width) {
+                const int p = sl.base + (j0 + j) * sl.stride;
+                k[j] = __ldg(L.nb + p);
+                a[j] = __ldg(L.AF + p);
+            } else {
+                k[j] = -1;
+                a[j] = T(0);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kU; j++) g[j] = x[k[j] >= 0 ? k[j] : n];
+#pragma unroll
+        for (int j = 0; j < kU; j++)
+            if (jacobiTest ? (k[j] != -1) : (k[j] >= 0)) Ax += a[j] * g[j];
+    }
+    return Ax;
+}
+
+template <class T>
+__device__ __forceinline__ T jacobiRowT(const LevelT<T>& L, int n, const T* xo, T w, T bn) {
+    const T ac = L.AC[n];
+    if (fabs(ac) < tiny<T>()) return xo[n];
+    const T Ax = axEager(L, n, xo, true);
+    return xo[n] + w * (bn - Ax) / ac;
+}
+
+// Level 0 ([W][N] slots, W fixed at compile time): loads issued before gathers.
+template <class T, int WC>
+__device__ __forceinline__ T ellAx(const LevelT<T>& L, int n, const T* x, bool jacobiTest) {
+    int k[WC];
+    T a[WC], g[WC];
+#pragma unroll
+    for (int j = 0; j < WC; j++) {
+        k[j] = L.nb[(size_t)j * L.N + n];
+        a[j] = L.AF[(size_t)j * L.N + n];
+    }
+#pragma unroll
+    for (int j = 0; j < WC; j++) g[j] = x[k[j] >= 0 ? k[j] : n];
+    T Ax = L.AC[n] * x[n];
+#pragma unroll
+    for (int j = 0; j < WC; j++)
+        if (jacobiTest ? (k[j] != -1) : (k[j] >= 0)) Ax += a[j] * g[j];
+    return Ax;
+}
+
+template <class T, int WC>
+__global__ void __launch_bounds__(kThreads) k_mg_smooth_ell(const Ctl* ctl, LevelT<T> L, const T* __restrict__ x,
+                                                            T* __restrict__ y, T w) {
+    pdlEnter();
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L.N) return;
+    const T ac = L.AC[n];
+    if (fabs(ac) < tiny<T>()) {
+        y[n] = x[n];
+        return;
+    }
+    const T Ax = ellAx<T, WC>(L, n, x, true);
+    y[n] = x[n] + w * (L.b[n] - Ax) / ac;
+}
+
+template <class T, int WC>
+__global__ void __launch_bounds__(kThreads) k_mg_residual_ell(const Ctl* ctl, LevelT<T> L, const T* __restrict__ x) {
+    pdlEnter();
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L.N) return;
+    L.res[n] = L.b[n] - ellAx<T, WC>(L, n, x, false);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_mg_smooth(const Ctl* ctl, LevelT<T> L, const T* __restrict__ x,
+                                                        T* __restrict__ y, T w) {
+    pdlEnter();
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L.N) return;
+    y[n] = jacobiRow(L, n, x, w, L.b[n]);
+}
+
+template <class T>
+__global__ void k_mg_smooth_block(const Ctl* ctl, LevelT<T> L, T* x, T w, int sweeps) {
+    pdlEnter();
+    if (ctl->done) return;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* xo = reinterpret_cast<T*>(smraw);
+    T* xn = xo + L.N;
+    for (int n = threadIdx.x; n < L.N; n += blockDim.x) xo[n] = x[n];
+    __syncthreads();
+    for (int it = 0; it < sweeps; it++) {
+        for (int n = threadIdx.x; n < L.N; n += blockDim.x) xn[n] = jacobiRow(L, n, xo, w, L.b[n]);
+        __syncthreads();
+        T* t = xo;
+        xo = xn;
+        xn = t;
+    }
+    for (int n = threadIdx.x; n < L.N; n += blockDim.x) x[n] = xo[n];
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_mg_residual(const Ctl* ctl, LevelT<T> L, const T* __restrict__ x) {
+    pdlEnter();
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L.N) return;
+    L.res[n] = residualRow(L, n, x, L.b[n]);
+}
+
+// Restriction (multigrid.cu:398-410) as a gather; optionally the coarse
+// level's first Jacobi sweep from x = 0: x1 = 0 + w (b - A 0) / AC.
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_mg_gather(const Ctl* ctl, const T* __restrict__ resFine, LevelT<T> C,
+                                                        T* xCur, T* xAlt, int firstSweep, T w) {
+    pdlEnter();
+    if (ctl->done) return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C.N) return;
+    T sum = T(0);
+    for (int q = C.mStart[c]; q < C.mStart[c + 1]; q++) sum += resFine[C.mList[q]];
+    C.b[c] = sum;
+    if (!firstSweep) {
+        xCur[c] = T(0);
+        return;
+    }
+    const T ac = C.AC[c];
+    xAlt[c] = (fabs(ac) < tiny<T>()) ? T(0) : T(0) + w * (sum - ac * T(0)) / ac;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_mg_prolong(const Ctl* ctl, int N, const int32_t* __restrict__ c2c, T* x,
+                                                         const T* __restrict__ xc) {
+    pdlEnter();
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    x[n] += xc[c2c[n]];
+}
+
+// Galerkin, step 1 (coalesced over fine cells): each row's contribution to
+// its coarse diagonal, AC plus the agglomerate-internal off-diagonals in slot
+// order (multigrid.cu:371-386).
+template <class TF>
+__global__ void __launch_bounds__(kThreads) k_gal_diag(const Ctl* ctl, LevelT<TF> F) {
+    pdlEnter();
+    if (ctl->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= F.N) return;
+    TF diag = F.AC[n];
+    uint32_t mask = F.internalMask[n];
+    const Slots sl = slotsOf(F, n);
+    while (mask) {
+        const int j = __ffs(mask) - 1;
+        mask &= mask - 1;
+        diag += F.AF[sl.base + j * sl.stride];
+    }
+    F.res[n] = diag;
+}
+
+// Galerkin, step 2: one thread per coarse slot sums its feeding fine slots;
+// the first N threads also sum their members' diagonal contributions. Sums
+// run in the fine type and are stored in the coarse type.
+template <class TF, class TC>
+__global__ void __launch_bounds__(kThreads) k_gal_coarse(const Ctl* ctl, LevelT<TF> F, LevelT<TC> C) {
+    pdlEnter();
+    if (ctl->done) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < C.totalSlots) {
+        TF af = TF(0);
+        for (int q = C.gStart[t]; q < C.gStart[t + 1]; q++) af += F.AF[C.gList[q]];
+        C.AF[t] = (TC)af;
+    }
+    if (t < C.N) {
+        TF ac = TF(0);
+        for (int q = C.mStart[t]; q < C.mStart[t + 1]; q++) ac += F.res[C.mList[q]];
+        C.AC[t] = (TC)ac;
+    }
+}
+
+// ---------------- V-cycle tail inside one CTA ----------------
+template <class T>
+__device__ __forceinline__ void tailSmooth(const LevelT<T>& L, T*& xo, T*& xn, const T* b, T w, int sweeps) {
+    for (int it = 0; it < sweeps; it++) {
+        for (int n = threadIdx.x; n < L.N; n += blockDim.x) xn[n] = jacobiRowT(L, n, xo, w, b[n]);
+        __syncthreads();
+        T* t = xo;
+        xo = xn;
+        xn = t;
+    }
+}
+
+// Coarsest level with one row per thread held in registers.
+template <class T>
+__device__ __forceinline__ void tailCoarsest(const LevelT<T>& L, T*& xo, T*& xn, const T* b, T w, int sweeps) {
+    const int n = threadIdx.x;
+    const bool active = n < L.N;
+    T af[kRegW];
+    int nb[kRegW];
+    int width = 0;
+    T ac = T(0), bn = T(0);
+    if (active) {
+        const Slots sl = slotsOf(L, n);
+        width = sl.width;
+        for (int j = 0; j < kRegW; j++) {
+            if (j < width) {
+                af[j] = L.AF[sl.base + j * sl.stride];
+                nb[j] = L.nb[sl.base + j * sl.stride];
+            } else {
+                af[j] = T(0);
+                nb[j] = -1;
+            }
+        }
+        ac = L.AC[n];
+        bn = b[n];
+    }
+    const bool empty = fabs(ac) < tiny<T>();
+    for (int it = 0; it < sweeps; it++) {
+        if (active) {
+            if (empty) {
+                xn[n] = xo[n];
+            } else {
+                T Ax = ac * xo[n];
+#pragma unroll
+                for (int j = 0; j < kRegW; j++)
+                    if (j < width && nb[j] != -1) Ax += af[j] * xo[nb[j]];
+                xn[n] = xo[n] + w * (bn - Ax) / ac;
+            }
+        }
+        __syncthreads();
+        T* t = xo;
+        xo = xn;
+        xn = t;
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kTailThreads) k_mg_tail(const Ctl* ctl, TailArgsT<T> a) {
+    pdlEnter();
+    if (ctl->done) return;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* sm = reinterpret_cast<T*>(smraw);
+    T* X[kMaxTail];
+    T* Y[kMaxTail];
+    T* B[kMaxTail];
+    T* R[kMaxTail];
+    for (int i = 0; i < a.count; i++) {
+        const int N = a.lv[i].N;
+        X[i] = sm + a.smemOff[i];
+        Y[i] = X[i] + N;
+        B[i] = Y[i] + N;
+        R[i] = B[i] + N;
+    }
+    // restriction into the first tail level from the finer level's residual
+    {
+        const LevelT<T>& C = a.lv[0];
+        for (int c = threadIdx.x; c < C.N; c += blockDim.x) {
+            T sum = T(0);
+            for (int q = C.mStart[c]; q < C.mStart[c + 1]; q++) sum += a.resFine[C.mList[q]];
+            B[0][c] = sum;
+            X[0][c] = T(0);
+        }
+        __syncthreads();
+    }
+    const int last = a.count - 1;
+    for (int i = 0; i < last; i++) {
+        const LevelT<T>& L = a.lv[i];
+        tailSmooth(L, X[i], Y[i], B[i], a.w, a.pre);
+        for (int n = threadIdx.x; n < L.N; n += blockDim.x) R[i][n] = B[i][n] - axEager(L, n, X[i], false);
+        __syncthreads();
+        const LevelT<T>& C = a.lv[i + 1];
+        for (int c = threadIdx.x; c < C.N; c += blockDim.x) {
+            T sum = T(0);
+            for (int q = C.mStart[c]; q < C.mStart[c + 1]; q++) sum += R[i][C.mList[q]];
+            B[i + 1][c] = sum;
+            X[i + 1][c] = T(0);
+        }
+        __syncthreads();
+    }
+    {
+        const LevelT<T>& L = a.lv[last];
+        if (L.N <= (int)blockDim.x && L.W <= kRegW) tailCoarsest(L, X[last], Y[last], B[last], a.w, a.coarseSweeps);
+        else tailSmooth(L, X[last], Y[last], B[last], a.w, a.coarseSweeps);
+    }
+    for (int i = last - 1; i >= 0; i--) {
+        const LevelT<T>& L = a.lv[i];
+        for (int n = threadIdx.x; n < L.N; n += blockDim.x) X[i][n] += X[i + 1][L.c2c[n]];
+        __syncthreads();
+        tailSmooth(L, X[i], Y[i], B[i], a.w, a.post);
+    }
+    for (int n = threadIdx.x; n < a.lv[0].N; n += blockDim.x) a.xOut[n] = X[0][n];
+}
+
+}  // namespace
+
+template <class TF, class TC>
+void launchGalerkin(const Ctl* ctl, const LevelT<TF>& fine, const LevelT<TC>& coarse, cudaStream_t s) {
+    launchPDL(k_gal_diag<TF>, dim3(blocksFor(fine.N)), dim3(kThreads), 0, s, ctl, fine);
+    const int n = coarse.totalSlots > coarse.N ? coarse.totalSlots : coarse.N;
+    launchPDL(k_gal_coarse<TF, TC>, dim3(blocksFor(n)), dim3(kThreads), 0, s, ctl, fine, coarse);
+}
+
+template <class T>
+void launchMGSmooth(const Ctl* ctl, const LevelT<T>& L, const T* x, T* y, T w, cudaStream_t s) {
+    if (!L.sliceOff && L.W == 4) launchPDL(k_mg_smooth_ell<T, 4>, dim3(blocksFor(L.N)), dim3(kThreads), 0, s, ctl, L, x, y, w);
+    else if (!L.sliceOff && L.W == 3) launchPDL(k_mg_smooth_ell<T, 3>, dim3(blocksFor(L.N)), dim3(kThreads), 0, s, ctl, L, x, y, w);
+    else launchPDL(k_mg_smooth<T>, dim3(blocksFor(L.N)), dim3(kThreads), 0, s, ctl, L, x, y, w);
+}
+
+template <class T>
+void launchMGSmoothBlock(const Ctl* ctl, const LevelT<T>& L, T* x, T w, int sweeps, cudaStream_t s) {
+    const int threads = L.N < 1024 ? ((L.N + 31) / 32) * 32 : 1024;
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_mg_smooth_block<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        configured = true;
+    }
+    launchPDL(k_mg_smooth_block<T>, dim3(1), dim3(threads), 2 * (size_t)L.N * sizeof(T), s, ctl, L, x, w, sweeps);
+}
+
+template <class T>
+void launchMGResidual(const Ctl* ctl, const LevelT<T>& L, const T* x, cudaStream_t s) {
+    if (!L.sliceOff && L.W == 4) launchPDL(k_mg_residual_ell<T, 4>, dim3(blocksFor(L.N)), dim3(kThreads), 0, s, ctl, L, x);
+    else if (!L.sliceOff && L.W == 3) launchPDL(k_mg_residual_ell<T, 3>, dim3(blocksFor(L.N)), dim3(kThreads), 0, s, ctl, L, x);
+    else launchPDL(k_mg_residual<T>, dim3(blocksFor(L.N)), dim3(kThreads), 0, s, ctl, L, x);
+}
+
+template <class T>
+void launchMGGather(const Ctl* ctl, const LevelT<T>& fine, const LevelT<T>& coarse, T* xCur, T* xAlt, int firstSweep,
+                    T w, cudaStream_t s) {
+    launchPDL(k_mg_gather<T>, dim3(blocksFor(coarse.N)), dim3(kThreads), 0, s, ctl, fine.res, coarse, xCur, xAlt, firstSweep, w);
+}
+
+template <class T>
+void launchMGProlong(const Ctl* ctl, const LevelT<T>& fine, T* xFine, const T* xCoarse, cudaStream_t s) {
+    launchPDL(k_mg_prolong<T>, dim3(blocksFor(fine.N)), dim3(kThreads), 0, s, ctl, fine.N, fine.c2c, xFine, xCoarse);
+}
+
+template <class T>
+size_t tailSharedBytes(const TailArgsT<T>& a) {
+    size_t d = 0;
+    for (int i = 0; i < a.count; i++) d += 4 * (size_t)a.lv[i].N;
+    return d * sizeof(T);
+}
+
+template <class T>
+void launchMGTail(const Ctl* ctl, const TailArgsT<T>& a, cudaStream_t s) {
+    const size_t smem = tailSharedBytes(a);
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_mg_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        configured = true;
+    }
+    launchPDL(k_mg_tail<T>, dim3(1), dim3(kTailThreads), smem, s, ctl, a);
+}
+
+// explicit instantiations: FP64 path, mixed-precision cycle
+template void launchGalerkin<double, double>(const Ctl*, const LevelT<double>&, const LevelT<double>&, cudaStream_t);
+template void launchGalerkin<double, float>(const Ctl*, const LevelT<double>&, const LevelT<float>&, cudaStream_t);
+template void launchGalerkin<float, float>(const Ctl*, const LevelT<float>&, const LevelT<float>&, cudaStream_t);
+#define AXISIM_MG_INSTANTIATE(T)                                                                               \
+    template void launchMGSmooth<T>(const Ctl*, const LevelT<T>&, const T*, T*, T, cudaStream_t);               \
+    template void launchMGSmoothBlock<T>(const Ctl*, const LevelT<T>&, T*, T, int, cudaStream_t);               \
+    template void launchMGResidual<T>(const Ctl*, const LevelT<T>&, const T*, cudaStream_t);                    \
+    template void launchMGGather<T>(const Ctl*, const LevelT<T>&, const LevelT<T>&, T*, T*, int, T, cudaStream_t); \
+    template void launchMGProlong<T>(const Ctl*, const LevelT<T>&, T*, const T*, cudaStream_t);                 \
+    template size_t tailSharedBytes<T>(const TailArgsT<T>&);                                                   \
+    template void launchMGTail<T>(const Ctl*, const TailArgsT<T>&, cudaStream_t);
+AXISIM_MG_INSTANTIATE(double)
+AXISIM_MG_INSTANTIATE(float)
+#undef AXISIM_MG_INSTANTIATE
+
+}  // namespace axisim

@@ -136,7 +136,6 @@ public:
 
     void setPrecision(int mode) {
         if (mode != AXISIM_PREC_FP64 && mode != AXISIM_PREC_MIXED) throw StatusError(AXISIM_E_ARG, "unknown precision mode");
-        if (mode == AXISIM_PREC_MIXED) throw StatusError(AXISIM_E_CONFIG, "mixed precision is not built in this library");
         precision_ = mode;
         destroyGraph();
     }
@@ -166,6 +165,9 @@ public:
             if (pm.faceNeighbor[f] >= N) throw StatusError(AXISIM_E_MESH, "faceNeighbor out of range");
         }
         destroyGraph();
+        mixArena_.release();
+        levels32_.clear();
+        AF32m_ = nullptr;
         mgArena_.release();
         levels_.clear();
         hier_.clear();
@@ -378,6 +380,12 @@ private:
     std::vector<GridLevel> hier_;
     bool haveHierarchy_ = false;
     std::vector<LevelDev> levels_;
+    // mixed precision: FP32 copies of the hierarchy and the inner-solve vectors
+    Arena mixArena_;
+    std::vector<LevelF> levels32_;
+    float *AF32m_ = nullptr, *iu32_ = nullptr, *iv32_ = nullptr, *ru32_ = nullptr, *rv32_ = nullptr;
+    float *du32_[2] = {nullptr, nullptr}, *dv32_[2] = {nullptr, nullptr};
+    float *AF32pp_ = nullptr, *AC32pp_ = nullptr, *r32pp_ = nullptr, *e32_[2] = {nullptr, nullptr}, *res32_ = nullptr;
     std::vector<int32_t> hColor_, hColorStart_;
     int colorN_ = 0;
     int32_t* dCellOrder_ = nullptr;
@@ -446,6 +454,7 @@ private:
         hier_ = buildHierarchy(finestLevel(N_, F_, hCfs_.data(), hCfi_.data(), hOwner_.data(), hNeighbor_.data()));
         haveHierarchy_ = true;
         levels_.clear();
+        levels32_.clear();
         mgArena_.release();
     }
 
@@ -580,72 +589,170 @@ private:
     }
     int tailStart_ = -1;
 
+    void ensureMixedBuffers() {
+        if (precision_ != AXISIM_PREC_MIXED) return;
+        if (!AF32m_) {
+            const size_t N = (size_t)N_, WN = (size_t)W_ * N;
+            Arena& A = mixArena_;
+            AF32m_ = A.alloc<float>(WN);
+            iu32_ = A.alloc<float>(N); iv32_ = A.alloc<float>(N);
+            ru32_ = A.alloc<float>(N); rv32_ = A.alloc<float>(N);
+            for (int i = 0; i < 2; i++) {
+                du32_[i] = A.alloc<float>(N);
+                dv32_[i] = A.alloc<float>(N);
+                e32_[i] = A.alloc<float>(N);
+            }
+            AF32pp_ = A.alloc<float>(WN);
+            AC32pp_ = A.alloc<float>(N);
+            r32pp_ = A.alloc<float>(N);
+            res32_ = A.alloc<float>(N);
+        }
+        if (!cs_.useMultigrid || !levels32_.empty()) return;
+        // FP32 hierarchy: the same topology and transfer lists as levels_
+        const int L = (int)levels_.size();
+        levels32_.resize((size_t)L);
+        for (int l = 0; l < L; l++) {
+            const LevelDev& d = levels_[(size_t)l];
+            LevelF& f = levels32_[(size_t)l];
+            f.N = d.N;
+            f.W = d.W;
+            f.totalSlots = d.totalSlots;
+            f.sliceOff = d.sliceOff;
+            f.nb = d.nb;
+            f.c2c = d.c2c;
+            f.mStart = d.mStart;
+            f.mList = d.mList;
+            f.gStart = d.gStart;
+            f.gList = d.gList;
+            f.internalMask = d.internalMask;
+            if (l == 0) {
+                f.AF = AF32pp_;
+                f.AC = AC32pp_;
+                f.b = r32pp_;
+                f.x = e32_[0];
+                f.xNew = e32_[1];
+                f.res = res32_;
+            } else {
+                f.AF = mixArena_.alloc<float>((size_t)std::max(d.totalSlots, 1));
+                f.AC = mixArena_.alloc<float>((size_t)d.N);
+                f.b = mixArena_.alloc<float>((size_t)d.N);
+                f.x = mixArena_.alloc<float>((size_t)d.N);
+                f.xNew = mixArena_.alloc<float>((size_t)d.N);
+                f.res = d.c2c ? mixArena_.alloc<float>((size_t)d.N) : nullptr;
+            }
+        }
+    }
+
     // ---------- capture of one SIMPLE iteration (solver.cpp:1109-1284) ----------
-    void smooth(int l, int sweeps, std::vector<double*>& cur, std::vector<double*>& alt) {
-        LevelDev& L = levels_[(size_t)l];
+    template <class T>
+    void smoothT(std::vector<LevelT<T>>& lv, int l, int sweeps, std::vector<T*>& cur, std::vector<T*>& alt) {
+        LevelT<T>& L = lv[(size_t)l];
         if (L.N <= 0 || sweeps <= 0) return;
+        const T w = (T)cmg_.weight;
+        const char* tag = sizeof(T) == 8 ? "" : "32";
         if (sweeps > 1 && L.N <= 4096) {
-            launchMGSmoothBlock(ctl_, L, cur[(size_t)l], cmg_.weight, sweeps, stream_);
-            mark("mg_smooth_block", (double)L.N * (12.0 * L.W + 32.0));
+            launchMGSmoothBlock<T>(ctl_, L, cur[(size_t)l], w, sweeps, stream_);
+            mark((std::string("mg_smooth_block") + tag).c_str(), (double)L.N * ((4.0 + 2 * sizeof(T)) * L.W + 4.0 * sizeof(T)));
             return;
         }
         for (int i = 0; i < sweeps; i++) {
-            launchMGSmooth(ctl_, L, cur[(size_t)l], alt[(size_t)l], cmg_.weight, stream_);
-            mark(l == 0 ? "mg_smooth_l0" : "mg_smooth", (double)L.N * (12.0 * L.W + 32.0));
+            launchMGSmooth<T>(ctl_, L, cur[(size_t)l], alt[(size_t)l], w, stream_);
+            mark((std::string(l == 0 ? "mg_smooth_l0" : "mg_smooth") + tag).c_str(),
+                 (double)L.N * ((4.0 + sizeof(T)) * L.W + 4.0 * sizeof(T)));
             std::swap(cur[(size_t)l], alt[(size_t)l]);
         }
     }
 
     // One V-cycle from level l (multigrid.cu:607-662). firstDone: the gather
-    // that produced this level's right-hand side already ran the first
+    // (or, on level 0 of the mixed cycle, the refinement residual) that
+    // produced this level's right-hand side already ran its first
     // pre-smoothing sweep.
-    void vcycle(int l, std::vector<double*>& cur, std::vector<double*>& alt, bool firstDone) {
-        const int L = (int)levels_.size();
+    template <class T>
+    void vcycleT(std::vector<LevelT<T>>& lv, int l, std::vector<T*>& cur, std::vector<T*>& alt, bool firstDone) {
+        const int L = (int)lv.size();
         if (l < 0 || l >= L) return;
+        const T w = (T)cmg_.weight;
+        const char* tag = sizeof(T) == 8 ? "" : "32";
+        const double vb = (double)sizeof(T);
         if (hier_[(size_t)l].isCoarsest()) {
-            smooth(l, cmg_.linearSweep - (firstDone ? 1 : 0), cur, alt);
+            smoothT<T>(lv, l, cmg_.linearSweep - (firstDone ? 1 : 0), cur, alt);
             return;
         }
-        smooth(l, cmg_.linearPreSweep - (firstDone ? 1 : 0), cur, alt);
-        LevelDev& F = levels_[(size_t)l];
-        LevelDev& C = levels_[(size_t)l + 1];
-        launchMGResidual(ctl_, F, cur[(size_t)l], stream_);
-        mark("mg_residual", (double)F.N * (12.0 * F.W + 32.0));
+        smoothT<T>(lv, l, cmg_.linearPreSweep - (firstDone ? 1 : 0), cur, alt);
+        LevelT<T>& F = lv[(size_t)l];
+        LevelT<T>& C = lv[(size_t)l + 1];
+        launchMGResidual<T>(ctl_, F, cur[(size_t)l], stream_);
+        mark((std::string("mg_residual") + tag).c_str(), (double)F.N * ((4.0 + vb) * F.W + 4.0 * vb));
         if (l + 1 == tailStart_) {
-            TailArgs a;
+            TailArgsT<T> a;
             a.first = l + 1;
             a.count = L - (l + 1);
             size_t off = 0;
             for (int i = 0; i < a.count; i++) {
-                a.lv[i] = levels_[(size_t)(l + 1 + i)];
+                a.lv[i] = lv[(size_t)(l + 1 + i)];
                 a.smemOff[i] = (int)off;
                 off += 4 * (size_t)a.lv[i].N;
             }
             a.resFine = F.res;
             a.xOut = cur[(size_t)l + 1];
-            a.w = cmg_.weight;
+            a.w = w;
             a.pre = cmg_.linearPreSweep;
             a.post = cmg_.linearPostSweep;
             a.coarseSweeps = cmg_.linearSweep;
-            launchMGTail(ctl_, a, stream_);
+            launchMGTail<T>(ctl_, a, stream_);
             double tb = 0.0;
-            for (int i = 0; i < a.count; i++) tb += (double)a.lv[i].N * (12.0 * a.lv[i].W + 32.0);
-            mark("mg_tail", tb);
+            for (int i = 0; i < a.count; i++) tb += (double)a.lv[i].N * ((4.0 + vb) * a.lv[i].W + 4.0 * vb);
+            mark((std::string("mg_tail") + tag).c_str(), tb);
         } else {
             const bool coarseIsCoarsest = hier_[(size_t)l + 1].isCoarsest();
             const int sweepsBelow = coarseIsCoarsest ? cmg_.linearSweep : cmg_.linearPreSweep;
             const bool fuse = sweepsBelow >= 1;
-            launchMGGather(ctl_, F, C, cur[(size_t)l + 1], alt[(size_t)l + 1], fuse ? 1 : 0, cmg_.weight, stream_);
-            mark("mg_gather", 12.0 * F.N + 32.0 * C.N);
+            launchMGGather<T>(ctl_, F, C, cur[(size_t)l + 1], alt[(size_t)l + 1], fuse ? 1 : 0, w, stream_);
+            mark((std::string("mg_gather") + tag).c_str(), (4.0 + vb) * F.N + 4.0 * vb * C.N);
             if (fuse) std::swap(cur[(size_t)l + 1], alt[(size_t)l + 1]);
-            vcycle(l + 1, cur, alt, fuse);
+            vcycleT<T>(lv, l + 1, cur, alt, fuse);
         }
-        launchMGProlong(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], stream_);
-        mark("mg_prolong", 20.0 * F.N + 8.0 * C.N);
-        smooth(l, cmg_.linearPostSweep, cur, alt);
+        launchMGProlong<T>(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], stream_);
+        mark((std::string("mg_prolong") + tag).c_str(), (4.0 + 2 * vb) * F.N + vb * C.N);
+        smoothT<T>(lv, l, cmg_.linearPostSweep, cur, alt);
+    }
+
+    // Mixed precision: every V-cycle is one refinement step on the FP64 system
+    // (residual and update in FP64, the cycle for the correction in FP32).
+    void enqueueMultigridMixed() {
+        const int L = (int)levels_.size();
+        if (L > 1) {
+            launchGalerkin<double, float>(ctl_, levels_[0], levels32_[1], stream_);
+            mark("mg_galerkin", (double)levels_[0].N * (20.0 + 8.0 * levels_[0].W) + 12.0 * levels32_[1].totalSlots);
+        }
+        for (int l = 2; l < L; l++) {
+            launchGalerkin<float, float>(ctl_, levels32_[(size_t)l - 1], levels32_[(size_t)l], stream_);
+            mark("mg_galerkin32", (double)levels32_[(size_t)l - 1].N * (12.0 + 4.0 * levels32_[(size_t)l - 1].W) +
+                                      8.0 * levels32_[(size_t)l].totalSlots);
+        }
+        const bool coarsest0 = hier_[0].isCoarsest();
+        const int first = coarsest0 ? cmg_.linearSweep : cmg_.linearPreSweep;
+        const bool firstSweep = first >= 1;
+        const int cycles = cmg_.maxIter > 1 ? cmg_.maxIter : 1;
+        for (int c = 0; c < cycles; c++) {
+            std::vector<float*> cur((size_t)L), alt((size_t)L);
+            for (int l = 0; l < L; l++) {
+                cur[(size_t)l] = levels32_[(size_t)l].x;
+                alt[(size_t)l] = levels32_[(size_t)l].xNew;
+            }
+            launchIRResidualPP(ctl_, levels_[0], r32pp_, cur[0], cmg_.weight, firstSweep ? 1 : 0, stream_);
+            mark("ir_residual_pp", (double)N_ * (12.0 * W_ + 32.0 + 8.0));
+            vcycleT<float>(levels32_, 0, cur, alt, firstSweep);
+            launchIRUpdatePP(ctl_, N_, pp_, cur[0], stream_);
+            mark("ir_update_pp", 20.0 * N_);
+        }
     }
 
     void enqueueMultigrid() {
+        if (precision_ == AXISIM_PREC_MIXED) {
+            enqueueMultigridMixed();
+            return;
+        }
         const int L = (int)levels_.size();
         for (int l = 1; l < L; l++) {
             const LevelDev& f = levels_[(size_t)l - 1];
@@ -660,7 +767,7 @@ private:
             alt[(size_t)l] = levels_[(size_t)l].xNew;
         }
         const int cycles = cmg_.maxIter > 1 ? cmg_.maxIter : 1;
-        for (int c = 0; c < cycles; c++) vcycle(0, cur, alt, false);
+        for (int c = 0; c < cycles; c++) vcycleT<double>(levels_, 0, cur, alt, false);
         if (cur[0] != pp_) {
             launchCopy(ctl_, pp_, cur[0], N_, stream_);
             mark("copy", 16.0 * N_);
@@ -721,6 +828,10 @@ private:
         a.AF = AFm_; a.ACu = ACu_; a.ACv = ACv_; a.bu = bu_; a.bv = bv_; a.invACu = iu_; a.invACv = iv_;
         a.DU = DU_; a.DV = DV_; a.mu = fluid_.mu; a.rho = fluid_.rho; a.dt = cs_.dt; a.alpha = alphaU_;
         a.conv = conv; a.scheme = (scheme == 3) ? 0 : scheme; a.nonOrtho = nonOrtho; a.transient = cs_.transient ? 1 : 0;
+        const bool mixedMomentum = precision_ == AXISIM_PREC_MIXED && cs_.type != 1;
+        a.AF32 = mixedMomentum ? AF32m_ : nullptr;
+        a.invU32 = mixedMomentum ? iu32_ : nullptr;
+        a.invV32 = mixedMomentum ? iv32_ : nullptr;
         launchMomentum(mesh_, ctl_, bc_[0], bc_[1], a, stream_);
         {
             double face = 32.0 + (scheme == 1 ? 8.0 : scheme == 2 ? 16.0 : 0.0);
@@ -739,6 +850,20 @@ private:
                         mark("gs_uv", (double)cnt * (12.0 * W_ + 52.0));
                     }
                 }
+        } else if (mixedMomentum) {
+            // correction form: FP64 residual, FP32 Jacobi sweeps on the correction, FP64 update
+            launchIRResidualUV(mesh_, ctl_, AFm_, ACu_, ACv_, bu_, bv_, u_, v_, iu32_, iv32_, ru32_, rv32_, du32_[0],
+                               dv32_[0], stream_);
+            mark("ir_residual_uv", (double)N_ * (12.0 * W_ + 64.0 + 24.0));
+            int c = 0;
+            for (int k = 1; k < iters; k++) {
+                launchJacobiUV32(mesh_, ctl_, AF32m_, ru32_, rv32_, iu32_, iv32_, du32_[c], dv32_[c], du32_[1 - c],
+                                 dv32_[1 - c], stream_);
+                mark("jacobi_uv32", (double)N_ * (8.0 * W_ + 32.0));
+                c = 1 - c;
+            }
+            launchIRUpdateUV(ctl_, N_, u_, v_, du32_[c], dv32_[c], stream_);
+            mark("ir_update_uv", 40.0 * N_);
         } else {
             double *lu = u_, *su = uT_, *lv = v_, *sv = vT_;
             for (int k = 0; k < iters; k++) {
@@ -753,8 +878,9 @@ private:
                 mark("copy", 32.0 * N_);
             }
         }
+        const bool mixedPP = precision_ == AXISIM_PREC_MIXED && cs_.useMultigrid;
         launchPressureSystem(mesh_, ctl_, bc_[0], bc_[1], bc_[2], fluid_.rho, u_, v_, p_, gPZ_, gPR_, DU_, DV_, AFpp_,
-                             ACpp_, ipp_, mDot_, stream_);
+                             ACpp_, ipp_, mDot_, mixedPP ? AF32pp_ : nullptr, mixedPP ? AC32pp_ : nullptr, stream_);
         mark("pressure_rhiechow", 56.0 * F_ + (12.0 * W_ + 72.0) * N_);
         for (int corr = 0; corr <= nonOrtho; corr++) {
             const int cross = corr > 0;
@@ -865,9 +991,8 @@ public:
 private:
     void buildGraph() {
         if (exec_) return;
-        if (cs_.useMultigrid) {
-            ensureDeviceLevels();
-        }
+        if (cs_.useMultigrid) ensureDeviceLevels();
+        ensureMixedBuffers();
         if (cs_.type == 1) ensureColoring();
         CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
         try {

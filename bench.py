@@ -39,6 +39,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="cell-count scale of the workload (1 = full size)")
     ap.add_argument("--no-extras", action="store_true", help="skip cpu baseline / e2e / time-to-residual legs")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="mixed: FP32 inner solves inside FP64 refinement (the workload's setting); fp64: plain")
     return ap.parse_args()
 
 
@@ -246,7 +248,8 @@ def run_b200(args):
     s = dict(case.settings)
     s["maxIter"] = max(3, args.warmup)
     s["resTol"] = [0.0, 0.0, 0.0]
-    solver = abi.Solver(mesh, bcs, s, device=local)
+    prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
+    solver = abi.Solver(mesh, bcs, s, device=local, precision=prec)
     solver.solve()                       # warm-up: W SIMPLE iterations (+ capture of the iteration graph)
     solver.set_max_iter(args.steps, tol=0.0)
     sampler = ClockSampler(local) if rank == 0 else None
@@ -273,7 +276,7 @@ def run_b200(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": case.name, "cells": N, "faces": mesh["nFaces"], "precision": "fp64",
+        "config": {"workload": case.name, "cells": N, "faces": mesh["nFaces"], "precision": args.precision,
                    "convection": "second-order upwind", "gradient": "least squares",
                    "momentum_solver": "Jacobi x20 (u,v fused)", "pressure_solver": "agglomeration MG, 3 V-cycles",
                    "parallelism": f"replicas{world}" if world > 1 else "single",

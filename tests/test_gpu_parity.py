@@ -49,6 +49,11 @@ def _variants():
     c = cases.expansion(scale=1 / 4, max_iter=2, tol=1e-30)
     c.settings.update(mgPreSweep=0, mgPostSweep=2, mgLinearSweep=7, mgMaxIter=1)
     v.append(("expansion_54k_mg_sweeps", c))
+    c = cases.bullet(scale=0.1, max_iter=4, tol=1e-30)
+    v.append(("bullet_triangles_lsq_nonortho", c))
+    c = cases.bullet(scale=0.25, max_iter=2, tol=1e-30)
+    c.settings.update(gradientScheme=cases.GRAD_GREEN_GAUSS, convectionScheme=cases.CONV_SOU)
+    v.append(("bullet_triangles_gg_sou_deep_mg", c))
     c = cases.pulsatile_expansion(scale=1 / 32, dt=1e-3, steps=3, max_iter=3, tol=1e-30)
     v.append(("pulsatile_bdf2", c))
     c = cases.pulsatile_expansion(scale=1 / 32, dt=1e-3, steps=2, max_iter=3, tol=1e-30)
@@ -62,7 +67,7 @@ VARIANTS = _variants()
 
 @pytest.mark.parametrize("name,case", VARIANTS, ids=[n for n, _ in VARIANTS])
 def test_bitexact_after_iterations(name, case):
-    mesh = oracle.multiblock(case.blocks)
+    mesh = case.packed(oracle.multiblock)
     orc = oracle.Oracle(mesh, case.bc_fields(), case.settings)
     gpu = abi.Solver(mesh, case.bc_fields(), case.settings)
     it_o, conv_o = orc.run()
