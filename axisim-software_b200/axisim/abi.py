@@ -30,7 +30,7 @@ EXPORTS = [
     "axisim_solve", "axisim_can_continue", "axisim_request_stop", "axisim_get_field", "axisim_set_field",
     "axisim_mg_levels", "axisim_mg_level_maps", "axisim_coloring", "axisim_multiblock_build",
     "axisim_mesh_sizes", "axisim_mesh_view", "axisim_mesh_free", "axisim_resolve_bc",
-    "axisim_profile_iteration", "axisim_create_on",
+    "axisim_profile_iteration", "axisim_create_on", "axisim_set_batch", "axisim_batch_status",
 ]
 
 
@@ -145,6 +145,8 @@ def lib():
             "axisim_resolve_bc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, _u8p,
                                             _f64p, _u8p]),
             "axisim_profile_iteration": (C.c_int, [vp, C.c_int32, C.POINTER(KernelStat), C.c_int32, _i32p]),
+            "axisim_set_batch": (C.c_int, [vp, C.c_int32, _i32p]),
+            "axisim_batch_status": (C.c_int, [vp, _i32p, _f64p, C.c_int32]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -332,6 +334,20 @@ class Solver:
         self._check(lib().axisim_profile_iteration(self.h, iterations, out, 64, C.byref(n)))
         return [dict(name=out[i].name.decode(), launches=out[i].launches, ms=out[i].ms, bytes=out[i].bytes)
                 for i in range(min(n.value, 64))]
+
+    def set_batch(self, case_cell_start):
+        cs = np.ascontiguousarray(case_cell_start, dtype=np.int32)
+        self._check(lib().axisim_set_batch(self.h, len(cs) - 1, cs.ctypes.data_as(_i32p)))
+        self.n_cases = len(cs) - 1
+
+    def batch_status(self):
+        n = self.n_cases
+        conv = np.zeros(n, np.int32)
+        res = np.zeros((n, 3))
+        k = lib().axisim_batch_status(self.h, conv.ctypes.data_as(_i32p), res.ctypes.data_as(_f64p), n)
+        if k < 0:
+            self._check(-k)
+        return conv, res
 
     def can_continue(self):
         buf = C.create_string_buffer(256)

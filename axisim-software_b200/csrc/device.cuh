@@ -107,6 +107,20 @@ struct Ctl {
     int resEnabled[3];
     int histCount;        // entries written since the host last drained
     double hist[kMaxHist][4];  // iteration, U, V, Continuity
+    // batch of independent cases packed into one mesh (nCases = 0: one case)
+    int nCases;
+    int casesConverged;
+};
+
+// Per-case monitoring of a batch: raw sums per case and the reference's
+// residual arithmetic (residuals.cu:37-100) applied case by case.
+struct BatchDev {
+    int nCases = 0;
+    const int32_t* cellStart = nullptr;  // nCases + 1
+    double* raw = nullptr;               // 5 per case: |rU|, scaleU, |rV|, scaleV, |continuity|
+    double* resVal = nullptr;            // 3 per case
+    double* scaleVal = nullptr;          // 3 per case
+    int32_t* convergedAt = nullptr;      // first converged iteration, -1 before
 };
 
 struct MomentumArgs {

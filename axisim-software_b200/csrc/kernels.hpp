@@ -91,6 +91,9 @@ void launchResiduals(const MeshDev& m, const Ctl* ctl, const double* AF, const d
                      double* resU, double* resV, double* resC, double* scaleU, double* scaleV, double* partial,
                      int* nBlocksOut, cudaStream_t s);
 void launchIterEnd(Ctl* ctl, const double* partial, int nBlocks, int N, cudaStream_t s);
+// batch: per-case reduction of the per-cell residual arrays, then per-case norms + convergence
+void launchBatchIterEnd(Ctl* ctl, const BatchDev& b, const double* resU, const double* resV, const double* resC,
+                        const double* scaleU, const double* scaleV, cudaStream_t s);
 void launchCopy(const Ctl* ctl, double* dst, const double* src, int n, cudaStream_t s);
 
 // ---- multigrid (mg.cu), T = double or float ----

@@ -907,6 +907,102 @@ __global__ void __launch_bounds__(kThreads) k_iter_end(Ctl* ctl, const double* p
     ctl->itersThisCall++;
 }
 
+// One CTA per case: sums over the case's cell range of the per-cell residual
+// arrays k_residual wrote (fixed strided order, deterministic).
+__global__ void __launch_bounds__(kThreads) k_case_reduce(const Ctl* ctl, BatchDev b, const double* resU,
+                                                          const double* resV, const double* resC,
+                                                          const double* scaleU, const double* scaleV) {
+    pdlEnter();
+    if (ctl->done || !ctl->checked) return;
+    const int c = blockIdx.x;
+    const int n0 = b.cellStart[c], n1 = b.cellStart[c + 1];
+    const int normU = ctl->resNorm[0], normV = ctl->resNorm[1];
+    const int isMax[kResQ] = {normU == 2, 0, normV == 2, 0, 0};
+    double acc[kResQ];
+    for (int q = 0; q < kResQ; q++) acc[q] = isMax[q] ? -INFINITY : 0.0;
+    for (int n = n0 + (int)threadIdx.x; n < n1; n += blockDim.x) {
+        acc[0] = combine(acc[0], normStat(resU[n], normU), isMax[0]);
+        acc[1] += fabs(scaleU[n]);
+        acc[2] = combine(acc[2], normStat(resV[n], normV), isMax[2]);
+        acc[3] += fabs(scaleV[n]);
+        acc[4] += fabs(resC[n]);
+    }
+    blockReduce<kThreads>(acc, isMax, b.raw + (size_t)c * kResQ);
+}
+
+// residualAllHost's arithmetic and the convergence test, case by case; the
+// batch is done once every case has converged.
+__global__ void __launch_bounds__(kThreads) k_batch_iter_end(Ctl* ctl, BatchDev b, int N) {
+    pdlEnter();
+    if (ctl->done) return;
+    __shared__ int nConv, nBad;
+    if (threadIdx.x == 0) {
+        nConv = 0;
+        nBad = 0;
+    }
+    __syncthreads();
+    if (ctl->checked) {
+        const int scaleIteration = ctl->transient ? ctl->k : ctl->currentIteration;
+        for (int c = threadIdx.x; c < b.nCases; c += blockDim.x) {
+            const double* raw = b.raw + (size_t)c * kResQ;
+            double* rv = b.resVal + (size_t)c * 3;
+            double* sv = b.scaleVal + (size_t)c * 3;
+            const double rawv[3] = {raw[0], raw[2], raw[4]};
+            const double diag[2] = {raw[1], raw[3]};
+            const double Nc = (double)(b.cellStart[c + 1] - b.cellStart[c]);
+            for (int i = 0; i < 3; i++) {
+                if (!ctl->resEnabled[i]) continue;
+                rv[i] = rawv[i];
+                if (i < 2) {
+                    switch (ctl->resScale[i]) {
+                        case 0: sv[i] = 1.0; break;
+                        case 1: sv[i] = Nc; break;
+                        case 2: sv[i] = sqrt(Nc); break;
+                        case 3: sv[i] = diag[i]; break;
+                        default: break;
+                    }
+                }
+            }
+            bool any = false, conv = true, finite = true;
+            for (int i = 0; i < 3; i++) {
+                if (!ctl->resEnabled[i]) continue;
+                if (i == 2 && scaleIteration < 5) sv[i] = fmax(rv[i], 0.0);
+                if (sv[i] != 0.0) {
+                    if (ctl->resNorm[i] == 1) rv[i] = sqrt(rv[i]);
+                    rv[i] /= sv[i];
+                }
+                any = true;
+                if (!(rv[i] <= ctl->tol[i])) conv = false;
+                if (!isfinite(rv[i])) finite = false;
+            }
+            if (any && conv) {
+                atomicAdd(&nConv, 1);
+                if (b.convergedAt[c] < 0) b.convergedAt[c] = ctl->currentIteration;
+            }
+            if (!finite) atomicAdd(&nBad, 1);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    if (ctl->checked) {
+        ctl->casesConverged = nConv;
+        ctl->converged = nConv == b.nCases;
+        for (int i = 0; i < 3; i++) ctl->resVal[i] = b.resVal[i];  // first case, for the summary line
+        const int h = ctl->histCount % kMaxHist;
+        ctl->hist[h][0] = (double)ctl->currentIteration;
+        ctl->hist[h][1] = b.resVal[0];
+        ctl->hist[h][2] = b.resVal[1];
+        ctl->hist[h][3] = b.resVal[2];
+        ctl->histCount++;
+        if (ctl->converged) ctl->done = 1;
+        else if (nBad) ctl->done = 4;
+    }
+    ctl->k++;
+    ctl->currentIteration++;
+    ctl->itersThisCall++;
+    (void)N;
+}
+
 __global__ void k_copy(const Ctl* ctl, double* dst, const double* src, int n) {
     pdlEnter();
     if (ctl && ctl->done) return;
@@ -1015,6 +1111,12 @@ void launchResiduals(const MeshDev& m, const Ctl* ctl, const double* AF, const d
 
 void launchIterEnd(Ctl* ctl, const double* partial, int nBlocks, int N, cudaStream_t s) {
     launchPDL(k_iter_end, dim3(1), dim3(kThreads), 0, s, ctl, partial, nBlocks, N);
+}
+
+void launchBatchIterEnd(Ctl* ctl, const BatchDev& b, const double* resU, const double* resV, const double* resC,
+                        const double* scaleU, const double* scaleV, cudaStream_t s) {
+    launchPDL(k_case_reduce, dim3(b.nCases), dim3(kThreads), 0, s, ctl, b, resU, resV, resC, scaleU, scaleV);
+    launchPDL(k_batch_iter_end, dim3(1), dim3(kThreads), 0, s, ctl, b, 0);
 }
 
 void launchCopy(const Ctl* ctl, double* dst, const double* src, int n, cudaStream_t s) {

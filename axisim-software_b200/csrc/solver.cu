@@ -165,6 +165,8 @@ public:
             if (pm.faceNeighbor[f] >= N) throw StatusError(AXISIM_E_MESH, "faceNeighbor out of range");
         }
         destroyGraph();
+        batchArena_.release();
+        batch_ = BatchDev{};
         mixArena_.release();
         levels32_.clear();
         AF32m_ = nullptr;
@@ -239,6 +241,51 @@ public:
         CK(cudaStreamSynchronize(stream_));
         haveMesh_ = true;
         isReady_ = false;
+    }
+
+    // Cases [caseStart[c], caseStart[c+1]) of the packed mesh are independent
+    // problems monitored and converged separately (nCases = 0 clears).
+    void setBatch(int nCases, const int32_t* caseStart) {
+        if (!haveMesh_) throw StatusError(AXISIM_E_STATE, "set the mesh before the batch layout");
+        if (nCases < 0 || (nCases > 0 && !caseStart)) throw StatusError(AXISIM_E_ARG, "bad batch layout");
+        if (nCases > 0) {
+            if (caseStart[0] != 0 || caseStart[nCases] != N_) throw StatusError(AXISIM_E_ARG, "case ranges must cover the mesh");
+            for (int c = 0; c < nCases; c++)
+                if (caseStart[c + 1] <= caseStart[c]) throw StatusError(AXISIM_E_ARG, "empty or decreasing case range");
+            // no face may connect two cases
+            for (int f = 0; f < F_; f++) {
+                const int nb = hNeighbor_[(size_t)f];
+                if (nb < 0) continue;
+                const int co = (int)(std::upper_bound(caseStart, caseStart + nCases + 1, hOwner_[(size_t)f]) - caseStart);
+                const int cn = (int)(std::upper_bound(caseStart, caseStart + nCases + 1, nb) - caseStart);
+                if (co != cn) throw StatusError(AXISIM_E_MESH, "a face connects two cases");
+            }
+        }
+        destroyGraph();
+        batchArena_.release();
+        batch_ = BatchDev{};
+        hCaseStart_.clear();
+        if (nCases == 0) return;
+        hCaseStart_.assign(caseStart, caseStart + nCases + 1);
+        batch_.nCases = nCases;
+        batch_.cellStart = batchArena_.upload(caseStart, (size_t)nCases + 1);
+        batch_.raw = batchArena_.alloc<double>((size_t)nCases * 5);
+        batch_.resVal = batchArena_.alloc<double>((size_t)nCases * 3);
+        batch_.scaleVal = batchArena_.alloc<double>((size_t)nCases * 3);
+        batch_.convergedAt = batchArena_.alloc<int32_t>((size_t)nCases);
+        std::vector<int32_t> neg((size_t)nCases, -1);
+        CK(cudaMemcpy(batch_.convergedAt, neg.data(), neg.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    }
+
+    int batchStatus(int32_t* convergedAt, double* residuals, int n) const {
+        if (batch_.nCases == 0) throw StatusError(AXISIM_E_STATE, "no batch layout set");
+        if (n < batch_.nCases) throw StatusError(AXISIM_E_ARG, "buffer too small");
+        CK(cudaStreamSynchronize(stream_));
+        if (convergedAt)
+            CK(cudaMemcpy(convergedAt, batch_.convergedAt, sizeof(int32_t) * (size_t)batch_.nCases, cudaMemcpyDeviceToHost));
+        if (residuals)
+            CK(cudaMemcpy(residuals, batch_.resVal, sizeof(double) * 3 * (size_t)batch_.nCases, cudaMemcpyDeviceToHost));
+        return batch_.nCases;
     }
 
     void setBC(int var, const axisim_bc_field& b) {
@@ -405,6 +452,11 @@ private:
         CK(cudaEventRecord(m.ev, stream_));
         marks_.push_back(m);
     }
+
+    // batch of independent cases packed into one mesh
+    Arena batchArena_;
+    BatchDev batch_;
+    std::vector<int32_t> hCaseStart_;
 
     // graph
     cudaGraph_t graph_ = nullptr;
@@ -909,8 +961,13 @@ private:
         launchResiduals(mesh_, ctl_, AFm_, ACu_, ACv_, bu_, bv_, u_, v_, mDot_, resU_, resV_, resC_, scU_, scV_,
                         partial_, &residualBlocks_, stream_);
         mark("residual", 16.0 * F_ + (16.0 * W_ + 88.0) * N_);
-        launchIterEnd(ctl_, partial_, residualBlocks_, N_, stream_);
-        mark("iter_end", 40.0 * residualBlocks_);
+        if (batch_.nCases > 0) {
+            launchBatchIterEnd(ctl_, batch_, resU_, resV_, resC_, scU_, scV_, stream_);
+            mark("batch_iter_end", 40.0 * N_);
+        } else {
+            launchIterEnd(ctl_, partial_, residualBlocks_, N_, stream_);
+            mark("iter_end", 40.0 * residualBlocks_);
+        }
     }
 
     // Algorithmic bytes of one gradient launch: every array element counted once.
@@ -1067,6 +1124,11 @@ int Solver::solve(int continueRun, axisim_result* res) {
     if (!cont) {
         zeroState();
         simTime_ = 0.0;
+        if (batch_.nCases > 0) {
+            std::vector<int32_t> neg((size_t)batch_.nCases, -1);
+            CK(cudaMemcpy(batch_.convergedAt, neg.data(), neg.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+            CK(cudaMemset(batch_.scaleVal, 0, sizeof(double) * 3 * (size_t)batch_.nCases));
+        }
     }
     buildGraph();
     // control block: settings for this run
@@ -1473,6 +1535,23 @@ int axisim_profile_iteration(axisim_handle* h, int32_t iterations, axisim_kernel
         if (nOut) *nOut = n;
         return AXISIM_OK;
     });
+}
+
+int axisim_set_batch(axisim_handle* h, int32_t nCases, const int32_t* caseCellStart) {
+    return guarded(h, [&] {
+        h->s->setBatch(nCases, caseCellStart);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_batch_status(const axisim_handle* h, int32_t* convergedAt, double* residuals, int32_t n) {
+    auto* hh = const_cast<axisim_handle*>(h);
+    int r = 0;
+    const int st = guarded(hh, [&] {
+        r = hh->s->batchStatus(convergedAt, residuals, n);
+        return AXISIM_OK;
+    });
+    return st == AXISIM_OK ? r : -st;
 }
 
 int axisim_multiblock_build(int32_t nBlocks, const axisim_block_spec* blocks, double tol, int32_t defaultGroup,

@@ -208,6 +208,18 @@ int64_t axisim_get_field(const axisim_handle* h, const char* name, double* out, 
 /* Initial state for u v p mDot (and uOld vOld for a transient restart). */
 int64_t axisim_set_field(axisim_handle* h, const char* name, const double* in, size_t n);
 
+/* ---- batches (new: the reference solves one case per Solver, solver.h:18-185) ---- */
+/* Declares the packed mesh to be nCases independent problems occupying the
+ * contiguous cell ranges [caseCellStart[c], caseCellStart[c+1]) (no face may
+ * join two ranges; boundary group ids are per case). Every kernel and every
+ * graph node then advances all cases at once; residuals are formed and
+ * normalised per case and the solve ends when every case has converged.
+ * nCases = 0 returns to a single problem. */
+int axisim_set_batch(axisim_handle* h, int32_t nCases, const int32_t* caseCellStart);
+/* Per case: the first SIMPLE iteration at which it met the tolerances (-1 if
+ * not yet) and its last U, V, Continuity residuals (3 per case). */
+int axisim_batch_status(const axisim_handle* h, int32_t* convergedAt, double* residuals, int32_t n);
+
 /* ---- multigrid hierarchy (MultigridSolver::describeHierarchy, multigrid.cu:727-764) ---- */
 int axisim_mg_levels(const axisim_handle* h, int32_t* cellsPerLevel, int32_t maxLevels);
 /* fine->coarse maps of level `level` (GridLevel::cellToCoarse / fineSlotToCoarseSlot,

@@ -1,0 +1,79 @@
+"""Multi-rank batch host logic on CPU (gloo, world size 2): cases are sharded
+by a greedy bin pack, each rank solves its own with the CPU oracle (the CUDA
+path is the same per case), and a gather merges the per-case results; the
+merged result equals the single-process one."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from axisim import batch
+
+N_CASES = 6
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _solve_cases(indices):
+    import oracle
+    cs = batch.random_cases(N_CASES, seed=11, scale=0.01, max_iter=4, tol=1e-30)
+    out = {}
+    for i in indices:
+        c = cs[i]
+        m = oracle.multiblock(c.blocks)
+        o = oracle.Oracle(m, c.bc_fields(), c.settings, threads=1)
+        o.run()
+        out[i] = {"u": o.get("u"), "p": o.get("p")}
+    return out
+
+
+def _worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    sizes = [sum(b["axial"][1] * b["radial"][1] for b in c.blocks)
+             for c in batch.random_cases(N_CASES, seed=11, scale=0.01)]
+    parts = batch.shard(sizes, world)
+    local = _solve_cases(parts[rank])
+    merged = batch.gather_results(local, world, dist)
+    if rank == 0:
+        q.put({k: {f: v[f].tolist() for f in v} for k, v in merged.items()})
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_shard_covers_every_case_once_and_balances():
+    sizes = [5, 9, 1, 7, 3, 8, 2]
+    for world in (1, 2, 3, 4):
+        parts = batch.shard(sizes, world)
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(sizes)))
+        loads = [sum(sizes[i] for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(sizes)
+
+
+@pytest.mark.timeout(300)
+def test_two_rank_batch_equals_single_process():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    merged = q.get(timeout=240)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    ref = _solve_cases(range(N_CASES))
+    assert sorted(int(k) for k in merged) == list(range(N_CASES))
+    for i in range(N_CASES):
+        for f in ("u", "p"):
+            np.testing.assert_array_equal(np.array(merged[i][f]), ref[i][f])
