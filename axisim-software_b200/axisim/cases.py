@@ -241,3 +241,38 @@ def bullet(scale=1.0, rho=1000.0, mu=1e-3, re=200.0, seed=0, max_iter=50000, tol
 
 def cell_count(case):
     return sum(int(b["axial"][1]) * int(b["radial"][1]) for b in case.blocks)
+
+
+def expansion_metrics(mesh, u, p, r_in=0.002, r_out=0.006, l_in=0.04, l_total=0.16):
+    """Flow quantities of the sudden expansion used to compare precisions:
+    centreline axial velocity u(z) (cells next to the axis), pressure drop
+    (area-weighted p next to the inlet minus next to the outlet) and the corner
+    recirculation length (from the step to where u next to the outer wall
+    turns positive)."""
+    zc, rc, vol = mesh["cellCenterZ"], mesh["cellCenterR"], mesh["cellVolume"]
+    r_axis = rc.min()
+    axis = np.isclose(rc, r_axis, rtol=0, atol=1e-12)
+    order = np.argsort(zc[axis])
+    centre_z, centre_u = zc[axis][order], u[axis][order]
+    dz_in = np.sort(np.unique(zc))[:1]
+    first_col = np.isclose(zc, zc.min(), rtol=0, atol=1e-12)
+    last_col = np.isclose(zc, zc.max(), rtol=0, atol=1e-12)
+    p_in = np.sum(p[first_col] * vol[first_col]) / np.sum(vol[first_col])
+    p_out = np.sum(p[last_col] * vol[last_col]) / np.sum(vol[last_col])
+    wall = np.isclose(rc, rc[zc > l_in].max(), rtol=0, atol=1e-12) & (zc > l_in)
+    wz, wu = zc[wall], u[wall]
+    o = np.argsort(wz)
+    wz, wu = wz[o], wu[o]
+    # primary recirculation: the longest run of reversed flow along the outer
+    # wall (a small corner eddy can sit right at the step)
+    recirc, to_outlet = 0.0, False
+    neg = wu < 0
+    if neg.any():
+        edges = np.diff(np.concatenate([[0], neg.astype(np.int8), [0]]))
+        starts, ends = np.nonzero(edges == 1)[0], np.nonzero(edges == -1)[0]
+        k = int(np.argmax(ends - starts))
+        to_outlet = ends[k] == len(wu)
+        recirc = (l_total if to_outlet else wz[ends[k]]) - l_in
+    del dz_in
+    return {"centre_z": centre_z, "centre_u": centre_u, "dp": p_in - p_out, "recirculation_length": float(recirc),
+            "recirculation_reaches_outlet": to_outlet}

@@ -204,7 +204,7 @@ def cpu_baseline_leg(case, mesh):
             "sample": f"{n} SIMPLE iterations of {case.name} from rest ({dt:.1f} s)"}
 
 
-def reference_cuda_leg(case, iters):
+def reference_cuda_leg(case, iters, tol=0.0):
     """The reference's own CUDA solver (compiled unchanged from its sources,
     oracle/ref_build) on the same workload, timed by its CudaTimer span."""
     ref_bin = os.path.join(ROOT, "oracle", "_ref", "axisim_ref")
@@ -215,7 +215,7 @@ def reference_cuda_leg(case, iters):
     import make_golden
     c = workload(1.0) if case is None else case
     c.settings["maxIter"] = iters
-    c.settings["resTol"] = [0.0, 0.0, 0.0]
+    c.settings["resTol"] = [tol, tol, tol]
     with tempfile.TemporaryDirectory() as d:
         spec, out = os.path.join(d, "spec.txt"), os.path.join(d, "out.bin")
         make_golden.write_spec(c, spec)
@@ -230,52 +230,136 @@ def reference_cuda_leg(case, iters):
             "note": "reference CUDA build (sm_100a, unchanged sources), CudaTimer over its SIMPLE loop"}
 
 
+# DRAM bytes per launch per cell of the top kernels from one ncu capture of this
+# workload (profiles/k_jacobi_uv_expansion874k.md: dram__bytes_read.sum +
+# dram__bytes_write.sum = 88.4 MB per launch at 874,496 cells).
+NCU_TRAFFIC_PER_CELL = {"jacobi_uv": 88.36e6 / 874496}
+
+
 def mesh_bytes(m):
     import numpy as np
     return int(sum(np.asarray(m[k]).nbytes for k in m if k not in ("nCells", "nFaces", "status")))
+
+
+def measure(abi, mesh, bcs, settings, args, local, dist, prec, sampler=None):
+    """W warm-up iterations, then K timed SIMPLE iterations (CUDA events inside
+    the library) on one solver handle; returns the solver and the timing."""
+    s = dict(settings)
+    s["maxIter"] = max(3, args.warmup)
+    s["resTol"] = [0.0, 0.0, 0.0]
+    solver = abi.Solver(mesh, bcs, s, device=local, precision=prec)
+    solver.solve()                       # warm-up (+ capture of the iteration graph)
+    solver.set_max_iter(args.steps, tol=0.0)
+    barrier(dist)
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    r = solver.solve(cont=True)          # K timed iterations
+    barrier(dist)
+    clocks = sampler.stop() if sampler else None
+    assert r["iterations"] == args.steps, r
+    return solver, max_over_ranks(dist, r["ms"]), clocks
+
+
+def time_to_residual(abi, case, local, prec, tol=1e-6):
+    c = dict(case.settings)
+    c["resTol"] = [tol, tol, tol]
+    mesh = case.packed(abi.multiblock)
+    s = abi.Solver(mesh, case.bc_fields(), c, device=local, precision=prec)
+    r = s.solve()
+    out = {"iterations": r["iterations"], "converged": r["converged"], "seconds": r["ms"] / 1e3,
+           "residuals": r["residual"]}
+    fields = {f: s.get(f) for f in ("u", "v", "p")}
+    s.close()
+    return out, mesh, fields
+
+
+def batch_leg(abi, local, n_cases=64, steps=50):
+    """Config 4: cases advanced together in one packed mesh vs one handle per
+    case, same K SIMPLE iterations, device (CUDA-event) time."""
+    from axisim import batch
+    cs = batch.random_cases(n_cases, seed=0)
+    meshes = [abi.multiblock(c.blocks) for c in cs]
+    union, start, bcs = batch.pack_union(meshes, [c.groups for c in cs])
+    settings = dict(cs[0].settings)
+    settings.update(maxIter=3, resTol=[0.0] * 3)
+    g = abi.Solver(union, bcs, settings, device=local)
+    g.set_batch(start)
+    g.solve()
+    g.set_max_iter(steps, tol=0.0)
+    rb = g.solve(cont=True)
+    g.close()
+    seq_ms = 0.0
+    for c, m in zip(cs, meshes):
+        s = dict(c.settings)
+        s.update(maxIter=3, resTol=[0.0] * 3)
+        h = abi.Solver(m, c.bc_fields(), s, device=local)
+        h.solve()
+        h.set_max_iter(steps, tol=0.0)
+        seq_ms += h.solve(cont=True)["ms"]
+        h.close()
+    cells = union["nCells"]
+    return {"cases": n_cases, "cells": int(cells), "steps": steps,
+            "batched_Mcell_iter_s": cells * steps / (rb["ms"] / 1e3) / 1e6,
+            "sequential_Mcell_iter_s": cells * steps / (seq_ms / 1e3) / 1e6,
+            "speedup": seq_ms / rb["ms"], "batched_ms": rb["ms"], "sequential_ms": seq_ms,
+            "note": "config-4 case mix (seed 0), first %d cases; one packed mesh vs one handle per case" % n_cases}
+
+
+def batch_converge_leg(abi, local, n_cases=16, scale=0.05, max_iter=20000):
+    """Time to all-converged for a small batch vs the sum of the sequential solves."""
+    from axisim import batch
+    cs = batch.random_cases(n_cases, seed=0, scale=scale, max_iter=max_iter, tol=1e-6)
+    meshes = [abi.multiblock(c.blocks) for c in cs]
+    union, start, bcs = batch.pack_union(meshes, [c.groups for c in cs])
+    g = abi.Solver(union, bcs, cs[0].settings, device=local)
+    g.set_batch(start)
+    rb = g.solve()
+    conv_at, _ = g.batch_status()
+    g.close()
+    seq_ms, seq_conv = 0.0, 0
+    for c, m in zip(cs, meshes):
+        h = abi.Solver(m, c.bc_fields(), c.settings, device=local)
+        r = h.solve()
+        seq_ms += r["ms"]
+        seq_conv += int(r["converged"])
+        h.close()
+    return {"cases": n_cases, "cells": int(union["nCells"]), "batched_seconds": rb["ms"] / 1e3,
+            "batched_iterations": rb["iterations"], "batched_converged_cases": int((conv_at >= 0).sum()),
+            "sequential_seconds": seq_ms / 1e3, "sequential_converged_cases": seq_conv,
+            "note": f"config-4 case mix at scale {scale}, tolerance 1e-6, at most {max_iter} iterations"}
 
 
 def run_b200(args):
     world, rank, local, dist = dist_setup(args.gpus)
     import numpy as np
     import axisim.abi as abi
+    from axisim import cases
     if not os.path.exists(abi.LIB_PATH):
         abi.build()
     case = workload(args.scale)
     mesh = abi.multiblock(case.blocks)
     N = mesh["nCells"]
     bcs = case.bc_fields()
-    s = dict(case.settings)
-    s["maxIter"] = max(3, args.warmup)
-    s["resTol"] = [0.0, 0.0, 0.0]
     prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
-    solver = abi.Solver(mesh, bcs, s, device=local, precision=prec)
-    solver.solve()                       # warm-up: W SIMPLE iterations (+ capture of the iteration graph)
-    solver.set_max_iter(args.steps, tol=0.0)
     sampler = ClockSampler(local) if rank == 0 else None
-    barrier(dist)
-    if sampler:
-        sampler.start()
-        time.sleep(0.3)
-    r = solver.solve(cont=True)          # K timed SIMPLE iterations (CUDA events inside)
-    barrier(dist)
-    clocks = sampler.stop() if sampler else None
-    assert r["iterations"] == args.steps, r
-    ms = max_over_ranks(dist, r["ms"])
+    solver, ms, clocks = measure(abi, mesh, bcs, case.settings, args, local, dist, prec, sampler)
     value = world * N * args.steps / (ms / 1e3) / 1e6
 
     # per-kernel roofline: two eagerly replayed iterations with events after every launch
     stats = solver.profile(iterations=2)
+    solver.close()
     launches_per_iter = sum(k["launches"] for k in stats) / 2.0
     top = max(stats, key=lambda k: k["ms"])
     peak, peak_kind = peaks()
     achieved = (top["bytes"] / top["launches"]) / (top["ms"] / top["launches"] / 1e3) / 1e9
     total_bytes = sum(k["bytes"] for k in stats) / 2.0
     total_ms = sum(k["ms"] for k in stats) / 2.0
+    traffic = NCU_TRAFFIC_PER_CELL.get(top["name"])
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64+f32" if prec == abi.PREC_MIXED else "f64", "data": "synthetic",
         "config": {"workload": case.name, "cells": N, "faces": mesh["nFaces"], "precision": args.precision,
                    "convection": "second-order upwind", "gradient": "least squares",
                    "momentum_solver": "Jacobi x20 (u,v fused)", "pressure_solver": "agglomeration MG, 3 V-cycles",
@@ -283,7 +367,8 @@ def run_b200(args):
                    "l2": "inputs larger than L2 (mesh + fields ~%.0f MB per iteration)" % (
                        (mesh_bytes(mesh) + N * 8 * 40) / 1e6)},
         "roofline": {"bound": "hbm", "kernel": top["name"], "achieved": achieved, "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic * N if traffic else None,
                      "bytes_per_launch": top["bytes"] / top["launches"],
                      "ms_per_launch": top["ms"] / top["launches"],
                      "iteration_algorithmic_GBps": total_bytes / (total_ms / 1e3) / 1e9},
@@ -293,14 +378,18 @@ def run_b200(args):
         "gpu_launches": int(round(launches_per_iter * args.steps)),
         "clocks": clocks,
     }
-    solver.close()
+    if prec == abi.PREC_MIXED:
+        s64, ms64, _ = measure(abi, mesh, bcs, case.settings, args, local, dist, abi.PREC_FP64)
+        s64.close()
+        line["plain_fp64"] = {"value": world * N * args.steps / (ms64 / 1e3) / 1e6, "unit": UNIT,
+                              "ms_per_step": ms64 / args.steps}
     if rank == 0 and not args.no_extras and world == 1:
         # e2e through the public API from host buffers: case upload + K iterations + field download
         t0 = time.perf_counter()
         s2 = dict(case.settings)
         s2["maxIter"] = args.steps
         s2["resTol"] = [0.0, 0.0, 0.0]
-        sol2 = abi.Solver(mesh, bcs, s2, device=local)
+        sol2 = abi.Solver(mesh, bcs, s2, device=local, precision=prec)
         zeros = np.zeros(N)
         for f in ("u", "v", "p"):
             sol2.set(f, zeros)
@@ -316,20 +405,34 @@ def run_b200(args):
                        "seconds": t_e2e, "note": "host clock around set_mesh/set_bc/set_field/solve/get_field"}
         line["cpu_baseline"] = cpu_baseline_leg(case, mesh)
         line["reference_cuda"] = reference_cuda_leg(workload(args.scale), min(args.steps, 100))
-        # time to residual 1e-6 on the pipe, CUDA-event time inside solve
-        from axisim import cases
+        # time to the 1e-6 residual: the workload in both precisions, errors of the mixed run
+        ttr = {}
+        full = cases.expansion(scale=args.scale, max_iter=60000, tol=1e-6)
+        t64, m64, f64 = time_to_residual(abi, full, local, abi.PREC_FP64)
+        tmx, _, fmx = time_to_residual(abi, full, local, abi.PREC_MIXED)
+        e64 = cases.expansion_metrics(m64, f64["u"], f64["p"])
+        emx = cases.expansion_metrics(m64, fmx["u"], fmx["p"])
+        rel = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))  # noqa: E731
+        tmx["error_vs_fp64"] = {
+            "u_rel_l2": rel(fmx["u"], f64["u"]), "v_rel_l2": rel(fmx["v"], f64["v"]),
+            "p_rel_l2": rel(fmx["p"], f64["p"]),
+            "centreline_u_rel_l2": rel(emx["centre_u"], e64["centre_u"]),
+            "pressure_drop_rel": abs(emx["dp"] - e64["dp"]) / abs(e64["dp"]),
+            "recirculation_length_abs_m": abs(emx["recirculation_length"] - e64["recirculation_length"])}
+        t64["pressure_drop_Pa"] = e64["dp"]
+        t64["recirculation_length_m"] = e64["recirculation_length"]
+        t64["recirculation_reaches_outlet"] = e64["recirculation_reaches_outlet"]
+        ttr[case.name] = {"plain_fp64": t64, "mixed": tmx, "speedup_mixed_vs_plain": t64["seconds"] / tmx["seconds"]}
         pc = cases.pipe(max_iter=50000, tol=1e-6)
-        pm = abi.multiblock(pc.blocks)
-        ps = abi.Solver(pm, pc.bc_fields(), pc.settings, device=local)
-        rr = ps.solve()
-        line["time_to_residual"] = {"case": pc.name, "cells": pm["nCells"], "iterations": rr["iterations"],
-                                    "converged": rr["converged"], "seconds": rr["ms"] / 1e3,
-                                    "residuals": rr["residual"]}
-        ps.close()
-        ref_pipe = reference_cuda_leg(cases.pipe(max_iter=50000, tol=1e-6), 50000)
+        p64, _, _ = time_to_residual(abi, pc, local, abi.PREC_FP64)
+        pmx, _, _ = time_to_residual(abi, pc, local, abi.PREC_MIXED)
+        ref_pipe = reference_cuda_leg(cases.pipe(max_iter=50000, tol=1e-6), 50000, tol=1e-6)
+        ttr[pc.name] = {"plain_fp64": p64, "mixed": pmx}
         if "ms" in ref_pipe:
-            line["time_to_residual"]["reference_cuda_seconds"] = ref_pipe["ms"] / 1e3
-            line["time_to_residual"]["reference_cuda_iterations"] = ref_pipe["iterations"]
+            ttr[pc.name]["reference_cuda"] = {"seconds": ref_pipe["ms"] / 1e3, "iterations": ref_pipe["iterations"]}
+        line["time_to_residual"] = ttr
+        line["batch"] = batch_leg(abi, local)
+        line["batch_to_converged"] = batch_converge_leg(abi, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

