@@ -22,6 +22,7 @@ OK, E_ARG, E_CONFIG, E_MESH, E_CUDA, E_DIVERGED, E_STOPPED, E_STATE, E_TIMEOUT =
 STATUS_NAMES = {0: "OK", 1: "E_ARG", 2: "E_CONFIG", 3: "E_MESH", 4: "E_CUDA", 5: "E_DIVERGED",
                 6: "E_STOPPED", 7: "E_STATE", 8: "E_TIMEOUT"}
 PREC_FP64, PREC_MIXED = 0, 1
+PSOLVE_VCYCLES, PSOLVE_FCG = 0, 1
 
 # Every entry point include/axisim_b200.h declares.
 EXPORTS = [
@@ -31,6 +32,7 @@ EXPORTS = [
     "axisim_mg_levels", "axisim_mg_level_maps", "axisim_coloring", "axisim_multiblock_build",
     "axisim_mesh_sizes", "axisim_mesh_view", "axisim_mesh_free", "axisim_resolve_bc",
     "axisim_profile_iteration", "axisim_create_on", "axisim_set_batch", "axisim_batch_status",
+    "axisim_set_pressure_solver",
 ]
 
 
@@ -129,6 +131,7 @@ def lib():
                                             C.c_double, C.c_double]),
             "axisim_set_fluid": (C.c_int, [vp, C.POINTER(Fluid)]),
             "axisim_set_precision": (C.c_int, [vp, C.c_int32]),
+            "axisim_set_pressure_solver": (C.c_int, [vp, C.c_int32]),
             "axisim_solve": (C.c_int, [vp, C.c_int32, C.POINTER(Result)]),
             "axisim_can_continue": (C.c_int, [vp, C.c_char_p, C.c_size_t]),
             "axisim_request_stop": (C.c_int, [vp]),
@@ -269,7 +272,7 @@ def settings_structs(s):
 class Solver:
     """One solver handle (Solver in the reference): case in, fields out."""
 
-    def __init__(self, mesh, bcs, settings, precision=PREC_FP64, device=0):
+    def __init__(self, mesh, bcs, settings, precision=PREC_FP64, device=0, pressure_solver=PSOLVE_VCYCLES):
         L = lib()
         cs, sim, mg, res, fluid = settings_structs(settings)
         self.h = C.c_void_p()
@@ -288,6 +291,8 @@ class Solver:
                                         settings["alphaU"], settings["alphaP"]))
         if precision != PREC_FP64:
             self._check(L.axisim_set_precision(self.h, precision))
+        if pressure_solver != PSOLVE_VCYCLES:
+            self._check(L.axisim_set_pressure_solver(self.h, pressure_solver))
 
     def _check(self, st):
         if st != OK:

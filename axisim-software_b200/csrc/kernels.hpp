@@ -134,4 +134,23 @@ void launchJacobiUV32(const MeshDev& m, const Ctl* ctl, const float* AF32, const
                       cudaStream_t s);
 void launchIRUpdateUV(const Ctl* ctl, int N, double* u, double* v, const float* du, const float* dv, cudaStream_t s);
 
+// ---- flexible CG on the p' system, FP32 V-cycle preconditioner (krylov.cu) ----
+// partial: one FP64 pair per block of 256 cells; counter[2] start at zero;
+// scalars[0] = (r, z), [1] = (z, q_prev), [2] and [3] = (p, q) of alternate
+// iterations.
+struct FcgScratch {
+    double* partial = nullptr;
+    unsigned int* counter = nullptr;
+    double* scalars = nullptr;
+};
+void launchFcgInit(const Ctl* ctl, const LevelDev& L0, const double* x, double* r, float* r32, float* eFirst, double w,
+                   int firstSweep, cudaStream_t s);
+void launchFcgDots(const Ctl* ctl, int N, const float* e, const double* r, const double* q, int useQ, FcgScratch& f,
+                   cudaStream_t s);
+void launchFcgSpmv(const Ctl* ctl, const LevelDev& L0, const float* e, const double* pOld, double* pNew, double* q,
+                   int first, int pqOld, int pqNew, FcgScratch& f, cudaStream_t s);
+// next: 0 = last iteration (x only), 1 = also r, 2 = also the first sweep
+void launchFcgUpdate(const Ctl* ctl, const LevelDev& L0, double* x, double* r, const double* p, const double* q,
+                     const FcgScratch& f, int pqSlot, float* r32, float* eFirst, double w, int next, cudaStream_t s);
+
 }  // namespace axisim

@@ -140,6 +140,13 @@ public:
         destroyGraph();
     }
 
+    void setPressureSolver(int mode) {
+        if (mode != AXISIM_PSOLVE_VCYCLES && mode != AXISIM_PSOLVE_FCG)
+            throw StatusError(AXISIM_E_ARG, "unknown pressure solver mode");
+        psolve_ = mode;
+        destroyGraph();
+    }
+
     // ---------------- mesh ----------------
     void setMesh(const axisim_mesh_packed& pm) {
         const int N = pm.nCells, F = pm.nFaces;
@@ -170,6 +177,7 @@ public:
         mixArena_.release();
         levels32_.clear();
         AF32m_ = nullptr;
+        fcgR_ = nullptr;
         mgArena_.release();
         levels_.clear();
         hier_.clear();
@@ -392,6 +400,7 @@ private:
     axisim_config_residual cres_[3];
     double alphaU_ = 0.7, alphaP_ = 0.3;
     int precision_ = AXISIM_PREC_FP64;
+    int psolve_ = AXISIM_PSOLVE_VCYCLES;
 
     cudaStream_t stream_ = nullptr;
     volatile int* hostStop_ = nullptr;
@@ -433,6 +442,9 @@ private:
     float *AF32m_ = nullptr, *iu32_ = nullptr, *iv32_ = nullptr, *ru32_ = nullptr, *rv32_ = nullptr;
     float *du32_[2] = {nullptr, nullptr}, *dv32_[2] = {nullptr, nullptr};
     float *AF32pp_ = nullptr, *AC32pp_ = nullptr, *r32pp_ = nullptr, *e32_[2] = {nullptr, nullptr}, *res32_ = nullptr;
+    // flexible CG on the p' system: FP64 residual, directions (two, alternating), A p
+    double *fcgR_ = nullptr, *fcgP_[2] = {nullptr, nullptr}, *fcgQ_ = nullptr;
+    FcgScratch fcg_;
     std::vector<int32_t> hColor_, hColorStart_;
     int colorN_ = 0;
     int32_t* dCellOrder_ = nullptr;
@@ -641,8 +653,25 @@ private:
     }
     int tailStart_ = -1;
 
+    // FP32 p' hierarchy: used by the mixed-precision cycle and as the
+    // preconditioner of the flexible CG solve in either precision
+    bool fp32PressureCycle() const {
+        return cs_.useMultigrid && (precision_ == AXISIM_PREC_MIXED || psolve_ == AXISIM_PSOLVE_FCG);
+    }
+
     void ensureMixedBuffers() {
-        if (precision_ != AXISIM_PREC_MIXED) return;
+        if (precision_ != AXISIM_PREC_MIXED && !fp32PressureCycle()) return;
+        if (psolve_ == AXISIM_PSOLVE_FCG && !fcgR_) {
+            const size_t N = (size_t)N_;
+            Arena& A = mixArena_;
+            fcgR_ = A.alloc<double>(N);
+            fcgP_[0] = A.alloc<double>(N);
+            fcgP_[1] = A.alloc<double>(N);
+            fcgQ_ = A.alloc<double>(N);
+            fcg_.partial = A.alloc<double>((N + 255) / 256 * 2);
+            fcg_.counter = A.alloc<unsigned int>(2);
+            fcg_.scalars = A.alloc<double>(4);
+        }
         if (!AF32m_) {
             const size_t N = (size_t)N_, WN = (size_t)W_ * N;
             Arena& A = mixArena_;
@@ -771,7 +800,7 @@ private:
 
     // Mixed precision: every V-cycle is one refinement step on the FP64 system
     // (residual and update in FP64, the cycle for the correction in FP32).
-    void enqueueMultigridMixed() {
+    void enqueueGalerkin32() {
         const int L = (int)levels_.size();
         if (L > 1) {
             launchGalerkin<double, float>(ctl_, levels_[0], levels32_[1], stream_);
@@ -782,6 +811,11 @@ private:
             mark("mg_galerkin32", (double)levels32_[(size_t)l - 1].N * (12.0 + 4.0 * levels32_[(size_t)l - 1].W) +
                                       8.0 * levels32_[(size_t)l].totalSlots);
         }
+    }
+
+    void enqueueMultigridMixed() {
+        enqueueGalerkin32();
+        const int L = (int)levels_.size();
         const bool coarsest0 = hier_[0].isCoarsest();
         const int first = coarsest0 ? cmg_.linearSweep : cmg_.linearPreSweep;
         const bool firstSweep = first >= 1;
@@ -800,7 +834,43 @@ private:
         }
     }
 
+    // Flexible CG on the FP64 p' system with one FP32 V-cycle (from zero) as the
+    // preconditioner of each iteration; cmg_.maxIter iterations.
+    void enqueuePressureFcg() {
+        enqueueGalerkin32();
+        const bool firstSweep = (hier_[0].isCoarsest() ? cmg_.linearSweep : cmg_.linearPreSweep) >= 1;
+        const int L = (int)levels_.size();
+        const int iters = cmg_.maxIter > 1 ? cmg_.maxIter : 1;
+        const double vb = 4.0;
+        launchFcgInit(ctl_, levels_[0], pp_, fcgR_, r32pp_, levels32_[0].x, cmg_.weight, firstSweep ? 1 : 0, stream_);
+        mark("fcg_init", (double)N_ * (12.0 * W_ + 8.0 + 8.0 + 8.0 + 8.0 + vb + (firstSweep ? vb : 0.0)));
+        for (int it = 0; it < iters; it++) {
+            std::vector<float*> cur((size_t)L), alt((size_t)L);
+            for (int l = 0; l < L; l++) {
+                cur[(size_t)l] = levels32_[(size_t)l].x;
+                alt[(size_t)l] = levels32_[(size_t)l].xNew;
+            }
+            vcycleT<float>(levels32_, 0, cur, alt, firstSweep);
+            const float* e = cur[0];
+            launchFcgDots(ctl_, N_, e, fcgR_, fcgQ_, it > 0 ? 1 : 0, fcg_, stream_);
+            mark("fcg_dots", (double)N_ * (vb + 8.0 + (it > 0 ? 8.0 : 0.0)));
+            double* pOld = fcgP_[(it + 1) & 1];
+            double* pNew = fcgP_[it & 1];
+            const int pqOld = 2 + ((it + 1) & 1), pqNew = 2 + (it & 1);
+            launchFcgSpmv(ctl_, levels_[0], e, pOld, pNew, fcgQ_, it == 0 ? 1 : 0, pqOld, pqNew, fcg_, stream_);
+            mark("fcg_spmv", (double)N_ * (12.0 * W_ + 8.0 + vb + (it > 0 ? 8.0 : 0.0) + 16.0));
+            const int next = it + 1 < iters ? (firstSweep ? 2 : 1) : 0;
+            launchFcgUpdate(ctl_, levels_[0], pp_, fcgR_, pNew, fcgQ_, fcg_, pqNew, r32pp_, levels32_[0].x,
+                            cmg_.weight, next, stream_);
+            mark("fcg_update", (double)N_ * (24.0 + (next ? 24.0 + vb + (next > 1 ? 8.0 + vb : 0.0) : 0.0)));
+        }
+    }
+
     void enqueueMultigrid() {
+        if (psolve_ == AXISIM_PSOLVE_FCG) {
+            enqueuePressureFcg();
+            return;
+        }
         if (precision_ == AXISIM_PREC_MIXED) {
             enqueueMultigridMixed();
             return;
@@ -930,7 +1000,7 @@ private:
                 mark("copy", 32.0 * N_);
             }
         }
-        const bool mixedPP = precision_ == AXISIM_PREC_MIXED && cs_.useMultigrid;
+        const bool mixedPP = fp32PressureCycle();
         launchPressureSystem(mesh_, ctl_, bc_[0], bc_[1], bc_[2], fluid_.rho, u_, v_, p_, gPZ_, gPR_, DU_, DV_, AFpp_,
                              ACpp_, ipp_, mDot_, mixedPP ? AF32pp_ : nullptr, mixedPP ? AC32pp_ : nullptr, stream_);
         mark("pressure_rhiechow", 56.0 * F_ + (12.0 * W_ + 72.0) * N_);
@@ -1447,6 +1517,13 @@ int axisim_set_fluid(axisim_handle* h, const axisim_fluid* fluid) {
 int axisim_set_precision(axisim_handle* h, int32_t mode) {
     return guarded(h, [&] {
         h->s->setPrecision(mode);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_set_pressure_solver(axisim_handle* h, int32_t mode) {
+    return guarded(h, [&] {
+        h->s->setPressureSolver(mode);
         return AXISIM_OK;
     });
 }

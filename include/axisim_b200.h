@@ -46,6 +46,8 @@ enum { AXISIM_WALL = 0, AXISIM_VELOCITY_INLET = 1, AXISIM_PRESSURE_OUTLET = 2, A
 enum { AXISIM_VAR_U = 0, AXISIM_VAR_V = 1, AXISIM_VAR_P = 2 };
 /* Precision of the pressure-correction multigrid (new; no reference counterpart) */
 enum { AXISIM_PREC_FP64 = 0, AXISIM_PREC_MIXED = 1 };
+/* Method of the pressure-correction solve (new; no reference counterpart) */
+enum { AXISIM_PSOLVE_VCYCLES = 0, AXISIM_PSOLVE_FCG = 1 };
 
 /* Mirror of FVMeshHostPacked (structs/solver_struct.h:400-429). */
 typedef struct axisim_mesh_packed {
@@ -183,6 +185,12 @@ int axisim_set_config(axisim_handle* h, const axisim_config_solver* solver,
 int axisim_set_fluid(axisim_handle* h, const axisim_fluid* fluid);
 /* New: precision of the pressure-correction solve (AXISIM_PREC_*). */
 int axisim_set_precision(axisim_handle* h, int32_t mode);
+/* New: method of the pressure-correction solve when configSolver.useMultigrid
+ * is set (AXISIM_PSOLVE_*). VCYCLES is the reference's configMultigrid.maxIter
+ * V-cycles (multigrid.cu:794-798); FCG runs configMultigrid.maxIter iterations
+ * of flexible conjugate gradients in FP64 with one FP32 V-cycle as the
+ * preconditioner of each, in either precision mode. */
+int axisim_set_pressure_solver(axisim_handle* h, int32_t mode);
 
 /* ---- solve / continue / stop ---- */
 /* Solver::run + runSimple (solver.cpp:146-173, 753-1396), synchronous on the
