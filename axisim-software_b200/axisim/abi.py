@@ -32,7 +32,7 @@ EXPORTS = [
     "axisim_mg_levels", "axisim_mg_level_maps", "axisim_coloring", "axisim_multiblock_build",
     "axisim_mesh_sizes", "axisim_mesh_view", "axisim_mesh_free", "axisim_resolve_bc",
     "axisim_profile_iteration", "axisim_create_on", "axisim_set_batch", "axisim_batch_status",
-    "axisim_set_pressure_solver",
+    "axisim_set_pressure_solver", "axisim_residual_static",
 ]
 
 
@@ -132,6 +132,9 @@ def lib():
             "axisim_set_fluid": (C.c_int, [vp, C.POINTER(Fluid)]),
             "axisim_set_precision": (C.c_int, [vp, C.c_int32]),
             "axisim_set_pressure_solver": (C.c_int, [vp, C.c_int32]),
+            # device pointers as integers (e.g. torch data_ptr()), stream as cudaStream_t
+            "axisim_residual_static": (C.c_int, [C.c_int32] * 3 + [vp] * 12 + [C.c_int32] * 2 + [vp] * 5 +
+                                       [C.c_char_p, C.c_size_t]),
             "axisim_solve": (C.c_int, [vp, C.c_int32, C.POINTER(Result)]),
             "axisim_can_continue": (C.c_int, [vp, C.c_char_p, C.c_size_t]),
             "axisim_request_stop": (C.c_int, [vp]),

@@ -254,6 +254,36 @@ typedef struct axisim_kernel_stat {
 int axisim_profile_iteration(axisim_handle* h, int32_t iterations, axisim_kernel_stat* out, int32_t maxOut,
                              int32_t* nOut);
 
+/* New; no counterpart in the reference. The SIMPLE residuals of caller-owned
+ * device arrays, computed with the same arithmetic as a solve's residual step
+ * (residualAll + continuityResidual, residuals.cu:5-100) but with NO device
+ * allocation: for callers that cannot allocate at that point -- a host whose
+ * GPU memory is all held by another allocator or capped, or a monitoring hook
+ * inside a time-critical loop where cudaMalloc/cudaFree would stall the device.
+ * The reduction scratch is a fixed file-scope device array sized for at most
+ * AXISIM_STATIC_MAX_CELLS cells; larger nCells is rejected with AXISIM_E_ARG.
+ * Inputs, all device pointers on the current device, in the reference's CSR
+ * slot order: cellFaceStart[nCells + 1], cellFaceIDs[nSlots],
+ * faceOwner/faceNeighbor/mDot[nFaces], AF[nSlots] (u and v share it),
+ * ACu/ACv/bu/bv/u/v[nCells]; normU/normV 0 = L1, 1 = L2, 2 = LINF.
+ * Outputs: resU/resV = |b - A x| and resC = the signed mass imbalance per cell,
+ * sums[5] = the U statistic (sum, sum of squares or max by norm), sum |AC_u u|,
+ * the V statistic, sum |AC_v v| and sum |imbalance| -- the values before
+ * residualAllHost's scaling. Runs on the calling thread's current device, on
+ * `stream` (a cudaStream_t; NULL = default stream), and returns once the results
+ * are written. Out-of-range indices are skipped and reported as AXISIM_E_MESH.
+ * The first call on each device looks up the scratch address, so make it before
+ * any stream capture. All calls share the scratch: calls that overlap in time
+ * (other threads, or other streams still running) race and give wrong sums.
+ * Messages go to err[errLen] (may be NULL). */
+#define AXISIM_STATIC_MAX_CELLS 4194304
+int axisim_residual_static(int32_t nCells, int32_t nFaces, int32_t nSlots, const int32_t* cellFaceStart,
+                           const int32_t* cellFaceIDs, const int32_t* faceOwner, const int32_t* faceNeighbor,
+                           const double* AF, const double* ACu, const double* ACv, const double* bu,
+                           const double* bv, const double* u, const double* v, const double* mDot,
+                           int32_t normU, int32_t normV, double* resU, double* resV, double* resC, double* sums,
+                           void* stream, char* err, size_t errLen);
+
 /* ---- host case preparation ---- */
 /* Multiblock structured mesh (structs/multiblock.h): makeRectBlock +
  * autoDetectInterfaces + assignGlobalNumbering + toPackedMesh. */
