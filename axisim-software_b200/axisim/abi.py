@@ -32,7 +32,7 @@ EXPORTS = [
     "axisim_mg_levels", "axisim_mg_level_maps", "axisim_coloring", "axisim_multiblock_build",
     "axisim_mesh_sizes", "axisim_mesh_view", "axisim_mesh_free", "axisim_resolve_bc",
     "axisim_profile_iteration", "axisim_create_on", "axisim_set_batch", "axisim_batch_status",
-    "axisim_set_pressure_solver", "axisim_residual_static",
+    "axisim_set_pressure_solver", "axisim_residual_static", "axisim_pressure_stats",
 ]
 
 
@@ -131,7 +131,8 @@ def lib():
                                             C.c_double, C.c_double]),
             "axisim_set_fluid": (C.c_int, [vp, C.POINTER(Fluid)]),
             "axisim_set_precision": (C.c_int, [vp, C.c_int32]),
-            "axisim_set_pressure_solver": (C.c_int, [vp, C.c_int32]),
+            "axisim_set_pressure_solver": (C.c_int, [vp, C.c_int32, C.c_double, C.c_double]),
+            "axisim_pressure_stats": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
             # device pointers as integers (e.g. torch data_ptr()), stream as cudaStream_t
             "axisim_residual_static": (C.c_int, [C.c_int32] * 3 + [vp] * 12 + [C.c_int32] * 2 + [vp] * 5 +
                                        [C.c_char_p, C.c_size_t]),
@@ -275,7 +276,8 @@ def settings_structs(s):
 class Solver:
     """One solver handle (Solver in the reference): case in, fields out."""
 
-    def __init__(self, mesh, bcs, settings, precision=PREC_FP64, device=0, pressure_solver=PSOLVE_VCYCLES):
+    def __init__(self, mesh, bcs, settings, precision=PREC_FP64, device=0, pressure_solver=PSOLVE_VCYCLES,
+                 pressure_tol=0.0, prolong_scale=1.0):
         L = lib()
         cs, sim, mg, res, fluid = settings_structs(settings)
         self.h = C.c_void_p()
@@ -295,7 +297,7 @@ class Solver:
         if precision != PREC_FP64:
             self._check(L.axisim_set_precision(self.h, precision))
         if pressure_solver != PSOLVE_VCYCLES:
-            self._check(L.axisim_set_pressure_solver(self.h, pressure_solver))
+            self._check(L.axisim_set_pressure_solver(self.h, pressure_solver, pressure_tol, prolong_scale))
 
     def _check(self, st):
         if st != OK:
@@ -356,6 +358,12 @@ class Solver:
         if k < 0:
             self._check(-k)
         return conv, res
+
+    def pressure_stats(self):
+        """(Krylov p' solves started, Krylov iterations completed)."""
+        a, b = C.c_int64(), C.c_int64()
+        self._check(lib().axisim_pressure_stats(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def can_continue(self):
         buf = C.create_string_buffer(256)

@@ -110,6 +110,21 @@ struct Ctl {
     // batch of independent cases packed into one mesh (nCases = 0: one case)
     int nCases;
     int casesConverged;
+    // Krylov p' solve: set once its residual meets the tolerance, so the
+    // remaining kernels of that solve (cycles included) return at entry;
+    // cleared when the solve ends
+    int ppSkip;
+    int ppPad;
+    long long ppSolves;      // Krylov solves started
+    long long ppIterations;  // Krylov iterations completed
+};
+
+// Counters of the learned first Krylov step (device memory, one per solver).
+struct NetStats {
+    long long applied;    // p' solves whose first Krylov step used the network
+    long long fallbacks;  // of those, steps rolled back because the V-cycle reduces the residual more
+    double logRhoV;       // running mean of log(||r_new|| / ||r_old||) over V-cycle-preconditioned steps
+    long long vSteps;     // V-cycle steps in that mean
 };
 
 // Per-case monitoring of a batch: raw sums per case and the reference's

@@ -46,6 +46,7 @@ struct TailArgsT {
     const T* resFine = nullptr;
     T* xOut = nullptr;
     T w = T(0.6);
+    T prolongScale = T(1);  // coarse correction x += s P e (1 in the reference's cycle)
     int pre = 1, post = 1, coarseSweeps = 30;
 };
 using TailArgs = TailArgsT<double>;
@@ -112,7 +113,7 @@ template <class T>
 void launchMGGather(const Ctl* ctl, const LevelT<T>& fine, const LevelT<T>& coarse, T* xCur, T* xAlt,
                     int firstSweep, T w, cudaStream_t s);
 template <class T>
-void launchMGProlong(const Ctl* ctl, const LevelT<T>& fine, T* xFine, const T* xCoarse, cudaStream_t s);
+void launchMGProlong(const Ctl* ctl, const LevelT<T>& fine, T* xFine, const T* xCoarse, T scale, cudaStream_t s);
 template <class T>
 size_t tailSharedBytes(const TailArgsT<T>& a);
 template <class T>
@@ -137,20 +138,28 @@ void launchIRUpdateUV(const Ctl* ctl, int N, double* u, double* v, const float* 
 // ---- flexible CG on the p' system, FP32 V-cycle preconditioner (krylov.cu) ----
 // partial: one FP64 pair per block of 256 cells; counter[2] start at zero;
 // scalars[0] = (r, z), [1] = (z, q_prev), [2] and [3] = (p, q) of alternate
-// iterations.
+// iterations, [4] = (b, b), [5] = (r, r), [6] = restart flag, [7] = (r0, r0).
 struct FcgScratch {
     double* partial = nullptr;
     unsigned int* counter = nullptr;
     double* scalars = nullptr;
 };
-void launchFcgInit(const Ctl* ctl, const LevelDev& L0, const double* x, double* r, float* r32, float* eFirst, double w,
-                   int firstSweep, cudaStream_t s);
+void launchFcgInit(Ctl* ctl, const LevelDev& L0, const double* x, double* r, float* r32, float* eFirst, double w,
+                   int firstSweep, double relTol, FcgScratch& f, cudaStream_t s);
 void launchFcgDots(const Ctl* ctl, int N, const float* e, const double* r, const double* q, int useQ, FcgScratch& f,
                    cudaStream_t s);
 void launchFcgSpmv(const Ctl* ctl, const LevelDev& L0, const float* e, const double* pOld, double* pNew, double* q,
                    int first, int pqOld, int pqNew, FcgScratch& f, cudaStream_t s);
-// next: 0 = last iteration (x only), 1 = also r, 2 = also the first sweep
-void launchFcgUpdate(const Ctl* ctl, const LevelDev& L0, double* x, double* r, const double* p, const double* q,
-                     const FcgScratch& f, int pqSlot, float* r32, float* eFirst, double w, int next, cudaStream_t s);
+// next: 0 = last iteration (x only), 1 = also r, 2 = also the first sweep;
+// ns (nullable): records the step's residual reduction as a V-cycle step
+void launchFcgUpdate(Ctl* ctl, const LevelDev& L0, double* x, double* r, const double* p, const double* q,
+                     FcgScratch& f, int pqSlot, float* r32, float* eFirst, double w, int next, double relTol,
+                     NetStats* ns, cudaStream_t s);
+// keeps or rolls back a first step preconditioned by the learned network
+void launchFcgJudge(Ctl* ctl, const LevelDev& L0, double* x, double* r, const double* p, const double* q,
+                    FcgScratch& f, int pqSlot, float* r32, float* eFirst, double w, int firstSweep, NetStats* ns,
+                    cudaStream_t s);
+// clears Ctl::ppSkip after the solve
+void launchFcgEnd(Ctl* ctl, cudaStream_t s);
 
 }  // namespace axisim

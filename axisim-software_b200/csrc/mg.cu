@@ -144,7 +144,7 @@ template <class T, int WC>
 __global__ void __launch_bounds__(kThreads) k_mg_smooth_ell(const Ctl* ctl, LevelT<T> L, const T* __restrict__ x,
                                                             T* __restrict__ y, T w) {
     pdlEnter();
-    if (ctl->done) return;
+    if (ctl->done || ctl->ppSkip) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= L.N) return;
     const T ac = L.AC[n];
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(kThreads) k_mg_smooth_ell(const Ctl* ctl, Leve
 template <class T, int WC>
 __global__ void __launch_bounds__(kThreads) k_mg_residual_ell(const Ctl* ctl, LevelT<T> L, const T* __restrict__ x) {
     pdlEnter();
-    if (ctl->done) return;
+    if (ctl->done || ctl->ppSkip) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= L.N) return;
     L.res[n] = L.b[n] - ellAx<T, WC>(L, n, x, false);
@@ -169,7 +169,7 @@ template <class T>
 __global__ void __launch_bounds__(kThreads) k_mg_smooth(const Ctl* ctl, LevelT<T> L, const T* __restrict__ x,
                                                         T* __restrict__ y, T w) {
     pdlEnter();
-    if (ctl->done) return;
+    if (ctl->done || ctl->ppSkip) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= L.N) return;
     y[n] = jacobiRow(L, n, x, w, L.b[n]);
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(kThreads) k_mg_smooth(const Ctl* ctl, LevelT<T
 template <class T>
 __global__ void k_mg_smooth_block(const Ctl* ctl, LevelT<T> L, T* x, T w, int sweeps) {
     pdlEnter();
-    if (ctl->done) return;
+    if (ctl->done || ctl->ppSkip) return;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* xo = reinterpret_cast<T*>(smraw);
     T* xn = xo + L.N;
@@ -197,7 +197,7 @@ __global__ void k_mg_smooth_block(const Ctl* ctl, LevelT<T> L, T* x, T w, int sw
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_mg_residual(const Ctl* ctl, LevelT<T> L, const T* __restrict__ x) {
     pdlEnter();
-    if (ctl->done) return;
+    if (ctl->done || ctl->ppSkip) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= L.N) return;
     L.res[n] = residualRow(L, n, x, L.b[n]);
@@ -209,7 +209,7 @@ template <class T>
 __global__ void __launch_bounds__(kThreads) k_mg_gather(const Ctl* ctl, const T* __restrict__ resFine, LevelT<T> C,
                                                         T* xCur, T* xAlt, int firstSweep, T w) {
     pdlEnter();
-    if (ctl->done) return;
+    if (ctl->done || ctl->ppSkip) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= C.N) return;
     T sum = T(0);
@@ -225,12 +225,12 @@ __global__ void __launch_bounds__(kThreads) k_mg_gather(const Ctl* ctl, const T*
 
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_mg_prolong(const Ctl* ctl, int N, const int32_t* __restrict__ c2c, T* x,
-                                                         const T* __restrict__ xc) {
+                                                         const T* __restrict__ xc, T scale) {
     pdlEnter();
-    if (ctl->done) return;
+    if (ctl->done || ctl->ppSkip) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
-    x[n] += xc[c2c[n]];
+    x[n] += scale * xc[c2c[n]];
 }
 
 // Galerkin, step 1 (coalesced over fine cells): each row's contribution to
@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(kThreads) k_mg_prolong(const Ctl* ctl, int N, 
 template <class TF>
 __global__ void __launch_bounds__(kThreads) k_gal_diag(const Ctl* ctl, LevelT<TF> F) {
     pdlEnter();
-    if (ctl->done) return;
+    if (ctl->done || ctl->ppSkip) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= F.N) return;
     TF diag = F.AC[n];
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(kThreads) k_gal_diag(const Ctl* ctl, LevelT<TF
 template <class TF, class TC>
 __global__ void __launch_bounds__(kThreads) k_gal_coarse(const Ctl* ctl, LevelT<TF> F, LevelT<TC> C) {
     pdlEnter();
-    if (ctl->done) return;
+    if (ctl->done || ctl->ppSkip) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < C.totalSlots) {
         TF af = TF(0);
@@ -332,7 +332,7 @@ __device__ __forceinline__ void tailCoarsest(const LevelT<T>& L, T*& xo, T*& xn,
 template <class T>
 __global__ void __launch_bounds__(kTailThreads) k_mg_tail(const Ctl* ctl, TailArgsT<T> a) {
     pdlEnter();
-    if (ctl->done) return;
+    if (ctl->done || ctl->ppSkip) return;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* sm = reinterpret_cast<T*>(smraw);
     T* X[kMaxTail];
@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_tail(const Ctl* ctl, TailAr
     }
     for (int i = last - 1; i >= 0; i--) {
         const LevelT<T>& L = a.lv[i];
-        for (int n = threadIdx.x; n < L.N; n += blockDim.x) X[i][n] += X[i + 1][L.c2c[n]];
+        for (int n = threadIdx.x; n < L.N; n += blockDim.x) X[i][n] += a.prolongScale * X[i + 1][L.c2c[n]];
         __syncthreads();
         tailSmooth(L, X[i], Y[i], B[i], a.w, a.post);
     }
@@ -427,8 +427,9 @@ void launchMGGather(const Ctl* ctl, const LevelT<T>& fine, const LevelT<T>& coar
 }
 
 template <class T>
-void launchMGProlong(const Ctl* ctl, const LevelT<T>& fine, T* xFine, const T* xCoarse, cudaStream_t s) {
-    launchPDL(k_mg_prolong<T>, dim3(blocksFor(fine.N)), dim3(kThreads), 0, s, ctl, fine.N, fine.c2c, xFine, xCoarse);
+void launchMGProlong(const Ctl* ctl, const LevelT<T>& fine, T* xFine, const T* xCoarse, T scale, cudaStream_t s) {
+    launchPDL(k_mg_prolong<T>, dim3(blocksFor(fine.N)), dim3(kThreads), 0, s, ctl, fine.N, fine.c2c, xFine, xCoarse,
+              scale);
 }
 
 template <class T>
@@ -458,7 +459,7 @@ template void launchGalerkin<float, float>(const Ctl*, const LevelT<float>&, con
     template void launchMGSmoothBlock<T>(const Ctl*, const LevelT<T>&, T*, T, int, cudaStream_t);               \
     template void launchMGResidual<T>(const Ctl*, const LevelT<T>&, const T*, cudaStream_t);                    \
     template void launchMGGather<T>(const Ctl*, const LevelT<T>&, const LevelT<T>&, T*, T*, int, T, cudaStream_t); \
-    template void launchMGProlong<T>(const Ctl*, const LevelT<T>&, T*, const T*, cudaStream_t);                 \
+    template void launchMGProlong<T>(const Ctl*, const LevelT<T>&, T*, const T*, T, cudaStream_t);                 \
     template size_t tailSharedBytes<T>(const TailArgsT<T>&);                                                   \
     template void launchMGTail<T>(const Ctl*, const TailArgsT<T>&, cudaStream_t);
 AXISIM_MG_INSTANTIATE(double)

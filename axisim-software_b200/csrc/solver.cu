@@ -140,11 +140,28 @@ public:
         destroyGraph();
     }
 
-    void setPressureSolver(int mode) {
+    void setPressureSolver(int mode, double relTol, double prolongScale) {
         if (mode != AXISIM_PSOLVE_VCYCLES && mode != AXISIM_PSOLVE_FCG)
             throw StatusError(AXISIM_E_ARG, "unknown pressure solver mode");
+        if (!(relTol >= 0.0 && relTol < 1.0)) throw StatusError(AXISIM_E_ARG, "relTol must be in [0, 1)");
+        if (!(prolongScale > 0.0 && prolongScale <= 4.0)) throw StatusError(AXISIM_E_ARG, "prolongScale must be in (0, 4]");
         psolve_ = mode;
+        psolveTol_ = relTol;
+        prolongScale_ = prolongScale;
         destroyGraph();
+    }
+
+    void pressureStats(int64_t* solves, int64_t* iterations) {
+        Ctl h;
+        CK(cudaMemcpy(&h, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost));
+        if (solves) *solves = h.ppSolves;
+        if (iterations) *iterations = h.ppIterations;
+    }
+
+    void ensureNetStats() {
+        if (netStats_) return;
+        netStats_ = netArena_.alloc<NetStats>(1);
+        nnE_ = netArena_.alloc<float>((size_t)N_);
     }
 
     // ---------------- mesh ----------------
@@ -178,6 +195,9 @@ public:
         levels32_.clear();
         AF32m_ = nullptr;
         fcgR_ = nullptr;
+        netArena_.release();
+        netStats_ = nullptr;
+        nnE_ = nullptr;
         mgArena_.release();
         levels_.clear();
         hier_.clear();
@@ -401,6 +421,9 @@ private:
     double alphaU_ = 0.7, alphaP_ = 0.3;
     int precision_ = AXISIM_PREC_FP64;
     int psolve_ = AXISIM_PSOLVE_VCYCLES;
+    double psolveTol_ = 0.0;
+    double prolongScale_ = 1.0;  // coarse-correction scale inside the FCG preconditioner
+    double curProlong_ = 1.0;    // scale of the cycle being captured
 
     cudaStream_t stream_ = nullptr;
     volatile int* hostStop_ = nullptr;
@@ -445,6 +468,10 @@ private:
     // flexible CG on the p' system: FP64 residual, directions (two, alternating), A p
     double *fcgR_ = nullptr, *fcgP_[2] = {nullptr, nullptr}, *fcgQ_ = nullptr;
     FcgScratch fcg_;
+    // counters of the Krylov steps (V-cycle reduction, learned-step outcomes)
+    Arena netArena_;
+    NetStats* netStats_ = nullptr;
+    float* nnE_ = nullptr;
     std::vector<int32_t> hColor_, hColorStart_;
     int colorN_ = 0;
     int32_t* dCellOrder_ = nullptr;
@@ -670,7 +697,7 @@ private:
             fcgQ_ = A.alloc<double>(N);
             fcg_.partial = A.alloc<double>((N + 255) / 256 * 2);
             fcg_.counter = A.alloc<unsigned int>(2);
-            fcg_.scalars = A.alloc<double>(4);
+            fcg_.scalars = A.alloc<double>(8);
         }
         if (!AF32m_) {
             const size_t N = (size_t)N_, WN = (size_t)W_ * N;
@@ -780,6 +807,7 @@ private:
             a.pre = cmg_.linearPreSweep;
             a.post = cmg_.linearPostSweep;
             a.coarseSweeps = cmg_.linearSweep;
+            a.prolongScale = (T)curProlong_;
             launchMGTail<T>(ctl_, a, stream_);
             double tb = 0.0;
             for (int i = 0; i < a.count; i++) tb += (double)a.lv[i].N * ((4.0 + vb) * a.lv[i].W + 4.0 * vb);
@@ -793,7 +821,7 @@ private:
             if (fuse) std::swap(cur[(size_t)l + 1], alt[(size_t)l + 1]);
             vcycleT<T>(lv, l + 1, cur, alt, fuse);
         }
-        launchMGProlong<T>(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], stream_);
+        launchMGProlong<T>(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], (T)curProlong_, stream_);
         mark((std::string("mg_prolong") + tag).c_str(), (4.0 + 2 * vb) * F.N + vb * C.N);
         smoothT<T>(lv, l, cmg_.linearPostSweep, cur, alt);
     }
@@ -838,11 +866,13 @@ private:
     // preconditioner of each iteration; cmg_.maxIter iterations.
     void enqueuePressureFcg() {
         enqueueGalerkin32();
+        curProlong_ = prolongScale_;
         const bool firstSweep = (hier_[0].isCoarsest() ? cmg_.linearSweep : cmg_.linearPreSweep) >= 1;
         const int L = (int)levels_.size();
         const int iters = cmg_.maxIter > 1 ? cmg_.maxIter : 1;
         const double vb = 4.0;
-        launchFcgInit(ctl_, levels_[0], pp_, fcgR_, r32pp_, levels32_[0].x, cmg_.weight, firstSweep ? 1 : 0, stream_);
+        launchFcgInit(ctl_, levels_[0], pp_, fcgR_, r32pp_, levels32_[0].x, cmg_.weight, firstSweep ? 1 : 0,
+                      psolveTol_, fcg_, stream_);
         mark("fcg_init", (double)N_ * (12.0 * W_ + 8.0 + 8.0 + 8.0 + 8.0 + vb + (firstSweep ? vb : 0.0)));
         for (int it = 0; it < iters; it++) {
             std::vector<float*> cur((size_t)L), alt((size_t)L);
@@ -861,9 +891,12 @@ private:
             mark("fcg_spmv", (double)N_ * (12.0 * W_ + 8.0 + vb + (it > 0 ? 8.0 : 0.0) + 16.0));
             const int next = it + 1 < iters ? (firstSweep ? 2 : 1) : 0;
             launchFcgUpdate(ctl_, levels_[0], pp_, fcgR_, pNew, fcgQ_, fcg_, pqNew, r32pp_, levels32_[0].x,
-                            cmg_.weight, next, stream_);
+                            cmg_.weight, next, psolveTol_, netStats_, stream_);
             mark("fcg_update", (double)N_ * (24.0 + (next ? 24.0 + vb + (next > 1 ? 8.0 + vb : 0.0) : 0.0)));
         }
+        launchFcgEnd(ctl_, stream_);
+        mark("fcg_end", 0.0);
+        curProlong_ = 1.0;
     }
 
     void enqueueMultigrid() {
@@ -1120,6 +1153,7 @@ private:
         if (exec_) return;
         if (cs_.useMultigrid) ensureDeviceLevels();
         ensureMixedBuffers();
+        if (cs_.useMultigrid && psolve_ == AXISIM_PSOLVE_FCG) ensureNetStats();
         if (cs_.type == 1) ensureColoring();
         CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
         try {
@@ -1521,9 +1555,16 @@ int axisim_set_precision(axisim_handle* h, int32_t mode) {
     });
 }
 
-int axisim_set_pressure_solver(axisim_handle* h, int32_t mode) {
+int axisim_set_pressure_solver(axisim_handle* h, int32_t mode, double relTol, double prolongScale) {
     return guarded(h, [&] {
-        h->s->setPressureSolver(mode);
+        h->s->setPressureSolver(mode, relTol, prolongScale);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_pressure_stats(axisim_handle* h, int64_t* solves, int64_t* iterations) {
+    return guarded(h, [&] {
+        h->s->pressureStats(solves, iterations);
         return AXISIM_OK;
     });
 }

@@ -187,10 +187,17 @@ int axisim_set_fluid(axisim_handle* h, const axisim_fluid* fluid);
 int axisim_set_precision(axisim_handle* h, int32_t mode);
 /* New: method of the pressure-correction solve when configSolver.useMultigrid
  * is set (AXISIM_PSOLVE_*). VCYCLES is the reference's configMultigrid.maxIter
- * V-cycles (multigrid.cu:794-798); FCG runs configMultigrid.maxIter iterations
- * of flexible conjugate gradients in FP64 with one FP32 V-cycle as the
- * preconditioner of each, in either precision mode. */
-int axisim_set_pressure_solver(axisim_handle* h, int32_t mode);
+ * V-cycles (multigrid.cu:794-798); FCG runs up to configMultigrid.maxIter
+ * iterations of flexible conjugate gradients in FP64 with one FP32 V-cycle as
+ * the preconditioner of each, in either precision mode, stopping once
+ * ||b - A p'||_2 <= relTol ||b||_2 (relTol = 0: always maxIter iterations).
+ * prolongScale multiplies the coarse-level corrections inside that V-cycle
+ * (1 = the reference's injection; > 1 over-corrects, which offsets the weak
+ * coarse correction of piecewise-constant aggregation). */
+int axisim_set_pressure_solver(axisim_handle* h, int32_t mode, double relTol, double prolongScale);
+/* New: Krylov p' solves started and iterations completed since the handle's
+ * mesh was set. */
+int axisim_pressure_stats(axisim_handle* h, int64_t* solves, int64_t* iterations);
 
 /* ---- solve / continue / stop ---- */
 /* Solver::run + runSimple (solver.cpp:146-173, 753-1396), synchronous on the

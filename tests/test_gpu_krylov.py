@@ -42,7 +42,7 @@ def test_fcg_runs_krylov_kernels_and_rejects_unknown_mode():
     assert {"fcg_init", "fcg_dots", "fcg_spmv", "fcg_update"} <= names
     assert any(n.startswith("mg_smooth") and n.endswith("32") for n in names)
     assert "ir_update_pp" not in names
-    st = abi.lib().axisim_set_pressure_solver(gpu.h, 7)
+    st = abi.lib().axisim_set_pressure_solver(gpu.h, 7, 0.0, 1.0)
     assert st == abi.E_ARG
 
 
@@ -54,3 +54,31 @@ def test_fcg_reaches_lower_continuity_than_vcycles_in_same_iterations():
     ra, rb = a.solve(), b.solve()
     assert ra["iterations"] == rb["iterations"] == 400
     assert rb["residual"][2] < ra["residual"][2], (rb["residual"], ra["residual"])
+
+
+def test_fcg_relative_tolerance_stops_early_and_keeps_the_solution():
+    case = cases.expansion(scale=1 / 16, max_iter=40000, tol=1e-8)
+    mesh = abi.multiblock(case.blocks)
+    st = dict(case.settings)
+    st["mgMaxIter"] = 40
+    full = abi.Solver(mesh, case.bc_fields(), case.settings, pressure_solver=abi.PSOLVE_FCG)
+    early = abi.Solver(mesh, case.bc_fields(), st, pressure_solver=abi.PSOLVE_FCG, pressure_tol=1e-2)
+    rf, re = full.solve(), early.solve()
+    assert rf["converged"] and re["converged"]
+    solves, iters = early.pressure_stats()
+    assert solves == re["iterations"] and 0 < iters < 40 * solves
+    for f in ("u", "v", "p"):
+        assert rel_l2(early.get(f), full.get(f)) <= 1e-6, f
+    assert abi.lib().axisim_set_pressure_solver(early.h, abi.PSOLVE_FCG, 1.5, 1.0) == abi.E_ARG
+    assert abi.lib().axisim_set_pressure_solver(early.h, abi.PSOLVE_FCG, 0.1, 0.0) == abi.E_ARG
+
+
+def test_fcg_over_corrected_preconditioner_converges_to_the_same_solution():
+    case = cases.expansion(scale=1 / 16, max_iter=40000, tol=1e-8)
+    mesh = abi.multiblock(case.blocks)
+    a = abi.Solver(mesh, case.bc_fields(), case.settings, pressure_solver=abi.PSOLVE_FCG)
+    b = abi.Solver(mesh, case.bc_fields(), case.settings, pressure_solver=abi.PSOLVE_FCG, prolong_scale=2.0)
+    ra, rb = a.solve(), b.solve()
+    assert ra["converged"] and rb["converged"]
+    for f in ("u", "v", "p"):
+        assert rel_l2(b.get(f), a.get(f)) <= 1e-6, f
