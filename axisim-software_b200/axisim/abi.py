@@ -23,6 +23,8 @@ STATUS_NAMES = {0: "OK", 1: "E_ARG", 2: "E_CONFIG", 3: "E_MESH", 4: "E_CUDA", 5:
                 6: "E_STOPPED", 7: "E_STATE", 8: "E_TIMEOUT"}
 PREC_FP64, PREC_MIXED = 0, 1
 PSOLVE_VCYCLES, PSOLVE_FCG = 0, 1
+LEARNED_OFF, LEARNED_FIRST_STEP, LEARNED_ALWAYS = 0, 1, 2
+NET_FP32, NET_BF16, NET_BF16_WEIGHTS = 0, 1, 2
 
 # Every entry point include/axisim_b200.h declares.
 EXPORTS = [
@@ -33,6 +35,9 @@ EXPORTS = [
     "axisim_mesh_sizes", "axisim_mesh_view", "axisim_mesh_free", "axisim_resolve_bc",
     "axisim_profile_iteration", "axisim_create_on", "axisim_set_batch", "axisim_batch_status",
     "axisim_set_pressure_solver", "axisim_residual_static", "axisim_pressure_stats",
+    "axisim_learned_harvest", "axisim_learned_sample_count", "axisim_learned_add_sample",
+    "axisim_learned_get_sample", "axisim_learned_init", "axisim_learned_params", "axisim_learned_grad",
+    "axisim_learned_train", "axisim_learned_enable", "axisim_learned_stats", "axisim_learned_predict",
 ]
 
 
@@ -133,6 +138,18 @@ def lib():
             "axisim_set_precision": (C.c_int, [vp, C.c_int32]),
             "axisim_set_pressure_solver": (C.c_int, [vp, C.c_int32, C.c_double, C.c_double]),
             "axisim_pressure_stats": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+            "axisim_learned_harvest": (C.c_int, [vp, C.c_int32, C.c_int32]),
+            "axisim_learned_sample_count": (C.c_int, [vp, C.POINTER(C.c_int32)]),
+            "axisim_learned_add_sample": (C.c_int, [vp, vp, vp, vp, vp, vp]),
+            "axisim_learned_get_sample": (C.c_int, [vp, C.c_int32, vp, vp, vp, vp, vp, vp]),
+            "axisim_learned_init": (C.c_int, [vp, C.c_int32, C.c_uint64, C.POINTER(C.c_int64)]),
+            "axisim_learned_params": (C.c_int, [vp, vp, C.c_int64, C.c_int32]),
+            "axisim_learned_grad": (C.c_int, [vp, C.c_int32, vp, vp, C.c_int64]),
+            "axisim_learned_train": (C.c_int, [vp, C.c_int32, C.c_float, C.c_uint64, C.c_int32, C.c_int32, vp]),
+            "axisim_learned_enable": (C.c_int, [vp, C.c_int32]),
+            "axisim_learned_predict": (C.c_int, [vp, vp, vp, vp, vp]),
+            "axisim_learned_stats": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                               C.POINTER(C.c_double), C.POINTER(C.c_double)]),
             # device pointers as integers (e.g. torch data_ptr()), stream as cudaStream_t
             "axisim_residual_static": (C.c_int, [C.c_int32] * 3 + [vp] * 12 + [C.c_int32] * 2 + [vp] * 5 +
                                        [C.c_char_p, C.c_size_t]),
@@ -358,6 +375,71 @@ class Solver:
         if k < 0:
             self._check(-k)
         return conv, res
+
+    # ---- learned p' preconditioner ----
+    def learned_harvest(self, every, capacity=0):
+        self._check(lib().axisim_learned_harvest(self.h, every, capacity))
+
+    def learned_sample_count(self):
+        c = C.c_int32()
+        self._check(lib().axisim_learned_sample_count(self.h, C.byref(c)))
+        return c.value
+
+    def learned_add_sample(self, b, target, ac, deficit, af):
+        """af: off-diagonals in the mesh's slot order (len(cellFaceIDs))."""
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (b, target, ac, deficit, af)]
+        self._check(lib().axisim_learned_add_sample(self.h, *[a.ctypes.data for a in arrs]))
+
+    def learned_get_sample(self, i):
+        """(b, target, A_C, deficit, A_F in slot order, relative residual of the
+        solve that made it)."""
+        n = self.mesh["nCells"]
+        out = [np.zeros(n, np.float32) for _ in range(4)] + [np.zeros(len(self.mesh["cellFaceIDs"]), np.float32)]
+        rr = np.zeros(1, np.float32)
+        self._check(lib().axisim_learned_get_sample(self.h, i, *[a.ctypes.data for a in out], rr.ctypes.data))
+        return out + [float(rr[0])]
+
+    def learned_init(self, precision=NET_BF16_WEIGHTS, seed=0):
+        n = C.c_int64()
+        self._check(lib().axisim_learned_init(self.h, precision, seed, C.byref(n)))
+        self._n_params = n.value
+        return n.value
+
+    def learned_params(self):
+        p = np.zeros(self._n_params, np.float32)
+        self._check(lib().axisim_learned_params(self.h, p.ctypes.data, p.size, 0))
+        return p
+
+    def learned_set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        self._check(lib().axisim_learned_params(self.h, p.ctypes.data, p.size, 1))
+
+    def learned_grad(self, i):
+        loss = np.zeros(1, np.float32)
+        g = np.zeros(self._n_params, np.float32)
+        self._check(lib().axisim_learned_grad(self.h, i, loss.ctypes.data, g.ctypes.data, g.size))
+        return float(loss[0]), g
+
+    def learned_train(self, steps, lr=1e-3, seed=0, first=0, count=0):
+        out = np.zeros(steps, np.float32)
+        self._check(lib().axisim_learned_train(self.h, steps, lr, seed, first, count, out.ctypes.data))
+        return out
+
+    def learned_predict(self, r, ac, deficit):
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (r, ac, deficit)]
+        out = np.zeros(self.mesh["nCells"], np.float32)
+        self._check(lib().axisim_learned_predict(self.h, *[a.ctypes.data for a in arrs], out.ctypes.data))
+        return out
+
+    def learned_enable(self, mode=LEARNED_FIRST_STEP):
+        self._check(lib().axisim_learned_enable(self.h, mode))
+
+    def learned_stats(self):
+        """Solves with the network, fallbacks to the V-cycle, and the running
+        scores (mean log residual reduction per Krylov iteration) of both."""
+        a, f, sn, sv = C.c_int64(), C.c_int64(), C.c_double(), C.c_double()
+        self._check(lib().axisim_learned_stats(self.h, C.byref(a), C.byref(f), C.byref(sn), C.byref(sv)))
+        return dict(applied=a.value, fallbacks=f.value, score_net=sn.value, score_vcycle=sv.value)
 
     def pressure_stats(self):
         """(Krylov p' solves started, Krylov iterations completed)."""

@@ -119,12 +119,19 @@ struct Ctl {
     long long ppIterations;  // Krylov iterations completed
 };
 
-// Counters of the learned first Krylov step (device memory, one per solver).
+// The learned first Krylov step: which p' solves use it, and the running means
+// the choice is made from (device memory, one per solver). Each solve's score
+// is its mean log residual reduction per Krylov iteration, log(||r_end|| /
+// ||r_0||) / iterations, from the FP64 residual.
 struct NetStats {
-    long long applied;    // p' solves whose first Krylov step used the network
-    long long fallbacks;  // of those, steps rolled back because the V-cycle reduces the residual more
-    double logRhoV;       // running mean of log(||r_new|| / ||r_old||) over V-cycle-preconditioned steps
-    long long vSteps;     // V-cycle steps in that mean
+    long long applied;    // solves whose first step used the network
+    long long fallbacks;  // solves that ran the plain V-cycle because its score was better
+    double logRhoNet;     // running mean score of solves with the network
+    double logRhoV;       // running mean score of solves without it
+    long long nNet, nV;   // solves in those means
+    long long solveIdx;   // learned-enabled solves so far (probe schedule)
+    int curNet;           // this solve uses the network
+    int pad;
 };
 
 // Per-case monitoring of a batch: raw sums per case and the reference's

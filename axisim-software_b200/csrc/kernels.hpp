@@ -138,7 +138,8 @@ void launchIRUpdateUV(const Ctl* ctl, int N, double* u, double* v, const float* 
 // ---- flexible CG on the p' system, FP32 V-cycle preconditioner (krylov.cu) ----
 // partial: one FP64 pair per block of 256 cells; counter[2] start at zero;
 // scalars[0] = (r, z), [1] = (z, q_prev), [2] and [3] = (p, q) of alternate
-// iterations, [4] = (b, b), [5] = (r, r), [6] = restart flag, [7] = (r0, r0).
+// iterations, [4] = (b, b), [5] = (r, r), [6] = Krylov iteration counter at
+// the solve's start, [7] = (r0, r0), [8..10] = learned step scale and its dots.
 struct FcgScratch {
     double* partial = nullptr;
     unsigned int* counter = nullptr;
@@ -150,16 +151,20 @@ void launchFcgDots(const Ctl* ctl, int N, const float* e, const double* r, const
                    cudaStream_t s);
 void launchFcgSpmv(const Ctl* ctl, const LevelDev& L0, const float* e, const double* pOld, double* pNew, double* q,
                    int first, int pqOld, int pqNew, FcgScratch& f, cudaStream_t s);
-// next: 0 = last iteration (x only), 1 = also r, 2 = also the first sweep;
-// ns (nullable): records the step's residual reduction as a V-cycle step
+// next: 0 = x only, 1 = also r and (r, r), 2 = also the first sweep
 void launchFcgUpdate(Ctl* ctl, const LevelDev& L0, double* x, double* r, const double* p, const double* q,
                      FcgScratch& f, int pqSlot, float* r32, float* eFirst, double w, int next, double relTol,
-                     NetStats* ns, cudaStream_t s);
-// keeps or rolls back a first step preconditioned by the learned network
-void launchFcgJudge(Ctl* ctl, const LevelDev& L0, double* x, double* r, const double* p, const double* q,
-                    FcgScratch& f, int pqSlot, float* r32, float* eFirst, double w, int firstSweep, NetStats* ns,
-                    cudaStream_t s);
-// clears Ctl::ppSkip after the solve
-void launchFcgEnd(Ctl* ctl, cudaStream_t s);
+                     cudaStream_t s);
+// per-solve choice between the learned first preconditioner and the V-cycle;
+// the learned one is z = alpha y + V-cycle(r - alpha A y), y the network's
+// output and alpha = (y, r) / (y, A y) its best scale (scalars [8..10])
+void launchFcgGate(Ctl* ctl, NetStats* ns, int always, cudaStream_t s);
+void launchFcgUngate(Ctl* ctl, cudaStream_t s);
+void launchNnResidual(const Ctl* ctl, const LevelDev& L0, const double* r, const float* y, double* Ay,
+                      FcgScratch& f, float* r32, float* eFirst, double w, int firstSweep, cudaStream_t s);
+void launchNnCombine(const Ctl* ctl, const NetStats* ns, int N, const float* y, const FcgScratch& f, float* e,
+                     cudaStream_t s);
+// clears Ctl::ppSkip after the solve; with ns, scores the solve
+void launchFcgEnd(Ctl* ctl, const FcgScratch& f, NetStats* ns, cudaStream_t s);
 
 }  // namespace axisim

@@ -94,7 +94,7 @@ __device__ __forceinline__ bool gridSum(const double (&v)[NQ], double* __restric
 
 // r = b - A x in FP64, r in FP32 for the V-cycle and, when firstSweep, the
 // V-cycle's first weighted Jacobi sweep from zero.
-// s[4] = (b, b), s[5] = (r, r), s[7] = (r0, r0), s[6] = 0; a solve that
+// s[4] = (b, b), s[5] = (r, r), s[7] = (r0, r0), s[6] = iteration counter; a solve that
 // already meets the tolerance (b = 0 included) is skipped whole.
 __global__ void __launch_bounds__(kThreads) k_fcg_init(Ctl* ctl, LevelDev L, const double* __restrict__ x,
                                                        double* __restrict__ r, float* __restrict__ r32,
@@ -119,8 +119,8 @@ __global__ void __launch_bounds__(kThreads) k_fcg_init(Ctl* ctl, LevelDev L, con
     }
     if (gridSum<2>(acc, partial, counter, s + 4)) {
         ctl->ppSolves++;
-        s[6] = 0.0;   // restart flag (set when a learned step is rolled back)
-        s[7] = s[5];  // (r0, r0)
+        s[6] = (double)ctl->ppIterations;  // Krylov iterations before this solve
+        s[7] = s[5];                       // (r0, r0)
         if (s[5] <= relTol * relTol * s[4]) ctl->ppSkip = 1;
     }
 }
@@ -133,12 +133,11 @@ __global__ void __launch_bounds__(kThreads) k_fcg_dots(const Ctl* ctl, int N, co
     pdlEnter();
     if (ctl->done || ctl->ppSkip) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool withQ = useQ && s[6] == 0.0;  // after a rollback the search restarts
     double acc[2] = {0.0, 0.0};
     if (n < N) {
         const double z = (double)e[n];
         acc[0] = r[n] * z;
-        if (withQ) acc[1] = z * q[n];
+        if (useQ) acc[1] = z * q[n];
     }
     gridSum<2>(acc, partial, counter, s);
 }
@@ -185,11 +184,10 @@ __global__ void __launch_bounds__(kThreads) k_fcg_update(Ctl* ctl, LevelDev L, d
                                                          const double* __restrict__ q, double* s, int pqSlot,
                                                          float* __restrict__ r32, float* __restrict__ eFirst, double w,
                                                          int next, double relTol, double* __restrict__ partial,
-                                                         unsigned int* counter, NetStats* ns) {
+                                                         unsigned int* counter) {
     pdlEnter();
     if (ctl->done || ctl->ppSkip) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    const double rrOld = s[5];
     const double pq = s[pqSlot];
     const double alpha = (pq != 0.0 && isfinite(pq)) ? s[0] / pq : 0.0;
     double acc[1] = {0.0};
@@ -212,47 +210,68 @@ __global__ void __launch_bounds__(kThreads) k_fcg_update(Ctl* ctl, LevelDev L, d
     }
     if (gridSum<1>(acc, partial, counter, s + 5)) {
         ctl->ppIterations++;
-        if (ns && rrOld > 0.0 && s[5] > 0.0 && isfinite(s[5])) {
-            // running mean of the V-cycle step's log residual reduction (window ~100)
-            const double lr = 0.5 * log(s[5] / rrOld);
-            const long long k = ns->vSteps < 100 ? ns->vSteps + 1 : 100;
-            ns->logRhoV += (lr - ns->logRhoV) / (double)k;
-            ns->vSteps++;
-        }
         if (s[5] <= relTol * relTol * s[4]) ctl->ppSkip = 1;
     }
 }
 
-// After a first step preconditioned by the learned network: keep it when its
-// residual reduction ||r1|| / ||r0|| is at least as good as the V-cycle's
-// running mean, else undo it (x -= alpha p, r += alpha q, r in FP32 and the
-// first sweep again) and flag a restart of the search directions.
-__global__ void __launch_bounds__(kThreads) k_fcg_judge(Ctl* ctl, LevelDev L, double* __restrict__ x,
-                                                        double* __restrict__ r, const double* __restrict__ p,
-                                                        const double* __restrict__ q, double* s, int pqSlot,
-                                                        float* __restrict__ r32, float* __restrict__ eFirst, double w,
-                                                        int firstSweep, NetStats* ns) {
+// Chooses, for this solve, between the learned first preconditioner and the
+// plain V-cycle: the network when its running score is at least as good as
+// the V-cycle's (or either has no score yet), with every 16th solve a probe of
+// the V-cycle and every 16th + 8 a probe of the network so both scores stay
+// current (always: the network on every solve). Using the network sets
+// Ctl::ppSkip = 2 for the network's kernels and k_nn_residual; k_fcg_ungate
+// then clears it before the V-cycle on the remaining residual.
+__global__ void k_fcg_gate(Ctl* ctl, NetStats* ns, int always) {
     pdlEnter();
     if (ctl->done) return;
+    const long long k = ns->solveIdx++ % 16;
+    int use;
+    if (always) use = 1;
+    else if (k == 0) use = 0;
+    else if (k == 8) use = 1;
+    else use = (ns->nNet == 0 || ns->nV == 0 || ns->logRhoNet <= ns->logRhoV) ? 1 : 0;
+    ns->curNet = use && ctl->ppSkip == 0;
+    if (use) ns->applied++;
+    else if (k != 0) ns->fallbacks++;
+    if (use && ctl->ppSkip == 0) ctl->ppSkip = 2;
+}
+
+// With the network's step (ppSkip == 2), step 1: Ay = A y (FP64) and the
+// best scale of y in the energy norm, alpha = (y, r) / (y, A y), in sn[0].
+__global__ void __launch_bounds__(kThreads) k_nn_scale(const Ctl* ctl, LevelDev L, const double* __restrict__ r,
+                                                       const float* __restrict__ y, double* __restrict__ Ay,
+                                                       double* __restrict__ partial, unsigned int* counter,
+                                                       double* sn) {
+    pdlEnter();
+    if (ctl->done || ctl->ppSkip != 2) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    const double rr0 = s[7], rr1 = s[5];
-    const double lr = (rr0 > 0.0 && rr1 >= 0.0) ? 0.5 * log(rr1 / rr0) : 0.0;
-    const bool ok = isfinite(rr1) && (ns->vSteps == 0 || lr <= ns->logRhoV);
-    if (n == 0) {
-        ns->applied++;
-        if (!ok) {
-            ns->fallbacks++;
-            s[6] = 1.0;
-            s[5] = rr0;
-            ctl->ppSkip = 0;
+    double acc[2] = {0.0, 0.0};
+    if (n < L.N) {
+        const double yn = (double)y[n];
+        double a = L.AC[n] * yn;
+        for (int j = 0; j < L.W; j++) {
+            const size_t s = (size_t)j * L.N + n;
+            const int k = L.nb[s];
+            if (k >= 0) a += L.AF[s] * (double)y[k];
         }
+        Ay[n] = a;
+        acc[0] = yn * r[n];
+        acc[1] = yn * a;
     }
-    if (ok || n >= L.N) return;
-    const double pq = s[pqSlot];
-    const double alpha = (pq != 0.0 && isfinite(pq)) ? s[0] / pq : 0.0;
-    x[n] -= alpha * p[n];
-    const double rv = r[n] + alpha * q[n];
-    r[n] = rv;
+    if (gridSum<2>(acc, partial, counter, sn + 1)) sn[0] = (sn[2] > 0.0 && isfinite(sn[1])) ? sn[1] / sn[2] : 0.0;
+}
+
+// Step 2: r' = r - alpha A y in FP64, r' in FP32 for the V-cycle that follows,
+// and that V-cycle's first sweep from zero.
+__global__ void __launch_bounds__(kThreads) k_nn_residual(const Ctl* ctl, LevelDev L, const double* __restrict__ r,
+                                                          const double* __restrict__ Ay, const double* sn,
+                                                          float* __restrict__ r32, float* __restrict__ eFirst,
+                                                          double w, int firstSweep) {
+    pdlEnter();
+    if (ctl->done || ctl->ppSkip != 2) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L.N) return;
+    const double rv = r[n] - sn[0] * Ay[n];
     r32[n] = (float)rv;
     if (firstSweep) {
         const double ac = L.AC[n];
@@ -260,10 +279,41 @@ __global__ void __launch_bounds__(kThreads) k_fcg_judge(Ctl* ctl, LevelDev L, do
     }
 }
 
-__global__ void k_fcg_end(Ctl* ctl) {
+// z = alpha y + V-cycle(r - alpha A y) when this solve uses the network.
+__global__ void __launch_bounds__(kThreads) k_nn_combine(const Ctl* ctl, const NetStats* ns, int N,
+                                                         const float* __restrict__ y, const double* sn,
+                                                         float* __restrict__ e) {
+    pdlEnter();
+    if (ctl->done || ctl->ppSkip || !ns->curNet) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n < N) e[n] = (float)((double)e[n] + sn[0] * (double)y[n]);
+}
+
+__global__ void k_fcg_ungate(Ctl* ctl) {
+    pdlEnter();
+    if (ctl->ppSkip == 2) ctl->ppSkip = 0;
+}
+
+// Ends the solve: clears Ctl::ppSkip and, with ns, adds the solve's score to
+// the running mean (window 32) of the method it used.
+__global__ void k_fcg_end(Ctl* ctl, const double* s, NetStats* ns) {
     pdlEnter();
     ctl->ppSkip = 0;
+    if (!ns || ctl->done) return;
+    const double iters = (double)ctl->ppIterations - s[6];
+    if (!(iters >= 1.0) || !(s[7] > 0.0) || !(s[5] > 0.0) || !isfinite(s[5])) return;
+    const double score = 0.5 * log(s[5] / s[7]) / iters;
+    if (ns->curNet) {
+        const long long m = ns->nNet < 32 ? ns->nNet + 1 : 32;
+        ns->logRhoNet += (score - ns->logRhoNet) / (double)m;
+        ns->nNet++;
+    } else {
+        const long long m = ns->nV < 32 ? ns->nV + 1 : 32;
+        ns->logRhoV += (score - ns->logRhoV) / (double)m;
+        ns->nV++;
+    }
 }
+
 
 }  // namespace
 
@@ -287,18 +337,34 @@ void launchFcgSpmv(const Ctl* ctl, const LevelDev& L0, const float* e, const dou
 
 void launchFcgUpdate(Ctl* ctl, const LevelDev& L0, double* x, double* r, const double* p, const double* q,
                      FcgScratch& f, int pqSlot, float* r32, float* eFirst, double w, int next, double relTol,
-                     NetStats* ns, cudaStream_t s) {
+                     cudaStream_t s) {
     launchPDL(k_fcg_update, dim3(blocksFor(L0.N)), dim3(kThreads), 0, s, ctl, L0, x, r, p, q, f.scalars, pqSlot, r32,
-              eFirst, w, next, relTol, f.partial, f.counter + 1, ns);
+              eFirst, w, next, relTol, f.partial, f.counter + 1);
 }
 
-void launchFcgJudge(Ctl* ctl, const LevelDev& L0, double* x, double* r, const double* p, const double* q,
-                    FcgScratch& f, int pqSlot, float* r32, float* eFirst, double w, int firstSweep, NetStats* ns,
-                    cudaStream_t s) {
-    launchPDL(k_fcg_judge, dim3(blocksFor(L0.N)), dim3(kThreads), 0, s, ctl, L0, x, r, p, q, f.scalars, pqSlot, r32,
-              eFirst, w, firstSweep, ns);
+void launchFcgGate(Ctl* ctl, NetStats* ns, int always, cudaStream_t s) {
+    launchPDL(k_fcg_gate, dim3(1), dim3(1), 0, s, ctl, ns, always);
 }
 
-void launchFcgEnd(Ctl* ctl, cudaStream_t s) { launchPDL(k_fcg_end, dim3(1), dim3(1), 0, s, ctl); }
+void launchNnResidual(const Ctl* ctl, const LevelDev& L0, const double* r, const float* y, double* Ay,
+                      FcgScratch& f, float* r32, float* eFirst, double w, int firstSweep, cudaStream_t s) {
+    double* sn = f.scalars + 8;
+    launchPDL(k_nn_scale, dim3(blocksFor(L0.N)), dim3(kThreads), 0, s, ctl, L0, r, y, Ay, f.partial, f.counter,
+              sn);
+    launchPDL(k_nn_residual, dim3(blocksFor(L0.N)), dim3(kThreads), 0, s, ctl, L0, r, (const double*)Ay,
+              (const double*)sn, r32, eFirst, w, firstSweep);
+}
+
+void launchNnCombine(const Ctl* ctl, const NetStats* ns, int N, const float* y, const FcgScratch& f, float* e,
+                     cudaStream_t s) {
+    launchPDL(k_nn_combine, dim3(blocksFor(N)), dim3(kThreads), 0, s, ctl, ns, N, y, (const double*)(f.scalars + 8),
+              e);
+}
+
+void launchFcgUngate(Ctl* ctl, cudaStream_t s) { launchPDL(k_fcg_ungate, dim3(1), dim3(1), 0, s, ctl); }
+
+void launchFcgEnd(Ctl* ctl, const FcgScratch& f, NetStats* ns, cudaStream_t s) {
+    launchPDL(k_fcg_end, dim3(1), dim3(1), 0, s, ctl, (const double*)f.scalars, ns);
+}
 
 }  // namespace axisim

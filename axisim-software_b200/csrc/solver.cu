@@ -24,6 +24,7 @@
 #include "../../include/axisim_b200.h"
 #include "host_prep.hpp"
 #include "kernels.hpp"
+#include "learned.hpp"
 
 namespace axisim {
 
@@ -158,10 +159,189 @@ public:
         if (iterations) *iterations = h.ppIterations;
     }
 
+    void resetLearned() {
+        net_.reset();
+        learnedMode_ = 0;
+        adamT_ = 0;
+        sampleArena_.release();
+        harvestEvery_ = 0;
+        sampleCap_ = 0;
+        samples_ = nullptr;
+        sampleCount_ = nullptr;
+        sampleRelres_ = nullptr;
+        harvestCounter_ = nullptr;
+    }
+
+    // ---------------- learned preconditioner ----------------
+    void learnedHarvest(int every, int capacity) {
+        if (!haveMesh_) throw StatusError(AXISIM_E_STATE, "no mesh");
+        if (every < 0 || capacity < 0) throw StatusError(AXISIM_E_ARG, "every and capacity must be >= 0");
+        if (capacity > 0 && capacity != sampleCap_) {
+            sampleArena_.release();
+            samples_ = sampleArena_.alloc<float>((size_t)capacity * sampleStride());
+            sampleCount_ = sampleArena_.alloc<int>(1);
+            sampleRelres_ = sampleArena_.alloc<float>((size_t)capacity);
+            harvestCounter_ = sampleArena_.alloc<unsigned int>(1);
+            sampleCap_ = capacity;
+        }
+        harvestEvery_ = samples_ ? every : 0;
+        destroyGraph();
+    }
+
+    int learnedSampleCount() {
+        if (!sampleCount_) return 0;
+        int c = 0;
+        CK(cudaMemcpy(&c, sampleCount_, sizeof(int), cudaMemcpyDeviceToHost));
+        return c;
+    }
+
+    size_t sampleStride() const { return (size_t)(4 + W_) * (size_t)N_; }
+
+    // A_F in the mesh's CSR slot order (cellFaceStart) <-> ELL [W][N]
+    std::vector<float> csrToEll(const float* csr) const {
+        std::vector<float> ell((size_t)W_ * N_, 0.f);
+        for (int n = 0; n < N_; n++)
+            for (int k = hCfs_[(size_t)n], j = 0; k < hCfs_[(size_t)n + 1]; k++, j++)
+                ell[(size_t)j * N_ + n] = csr[(size_t)k];
+        return ell;
+    }
+
+    void learnedAddSample(const float* b, const float* t, const float* ac, const float* d, const float* afCsr) {
+        if (!samples_) throw StatusError(AXISIM_E_STATE, "no sample store: call axisim_learned_harvest with a capacity");
+        if (!b || !t || !ac || !d || !afCsr) throw StatusError(AXISIM_E_ARG, "sample array is null");
+        const int c = learnedSampleCount();
+        if (c >= sampleCap_) throw StatusError(AXISIM_E_ARG, "sample store is full");
+        float* base = samples_ + (size_t)c * sampleStride();
+        const float* src[4] = {b, t, ac, d};
+        for (int k = 0; k < 4; k++)
+            CK(cudaMemcpy(base + (size_t)k * N_, src[k], (size_t)N_ * sizeof(float), cudaMemcpyHostToDevice));
+        const std::vector<float> ell = csrToEll(afCsr);
+        CK(cudaMemcpy(base + 4 * (size_t)N_, ell.data(), ell.size() * sizeof(float), cudaMemcpyHostToDevice));
+        const float rr = -1.f;
+        const int c1 = c + 1;
+        CK(cudaMemcpy(sampleRelres_ + c, &rr, sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(sampleCount_, &c1, sizeof(int), cudaMemcpyHostToDevice));
+    }
+
+    void learnedGetSample(int idx, float* b, float* t, float* ac, float* d, float* afCsr, float* relres) {
+        if (idx < 0 || idx >= learnedSampleCount()) throw StatusError(AXISIM_E_ARG, "sample index out of range");
+        const float* base = samples_ + (size_t)idx * sampleStride();
+        float* dst[4] = {b, t, ac, d};
+        for (int k = 0; k < 4; k++)
+            if (dst[k])
+                CK(cudaMemcpy(dst[k], base + (size_t)k * N_, (size_t)N_ * sizeof(float), cudaMemcpyDeviceToHost));
+        if (afCsr) {
+            std::vector<float> ell((size_t)W_ * N_);
+            CK(cudaMemcpy(ell.data(), base + 4 * (size_t)N_, ell.size() * sizeof(float), cudaMemcpyDeviceToHost));
+            for (int n = 0; n < N_; n++)
+                for (int k = hCfs_[(size_t)n], j = 0; k < hCfs_[(size_t)n + 1]; k++, j++)
+                    afCsr[(size_t)k] = ell[(size_t)j * N_ + n];
+        }
+        if (relres) CK(cudaMemcpy(relres, sampleRelres_ + idx, sizeof(float), cudaMemcpyDeviceToHost));
+    }
+
+    size_t learnedInit(int precision, uint64_t seed) {
+        if (!haveMesh_) throw StatusError(AXISIM_E_STATE, "no mesh");
+        if (precision < 0 || precision > 2) throw StatusError(AXISIM_E_ARG, "unknown network precision");
+        ensureHierarchy();
+        net_.init(hier_, mesh_.snb, W_, precision, seed, stream_);
+        adamT_ = 0;
+        destroyGraph();
+        return net_.numParams();
+    }
+
+    void requireNet() const {
+        if (!net_.ready()) throw StatusError(AXISIM_E_STATE, "network not initialised (axisim_learned_init)");
+    }
+
+    void learnedParams(float* host, int64_t n, int set) {
+        requireNet();
+        if (!host || n != (int64_t)net_.numParams()) throw StatusError(AXISIM_E_ARG, "parameter count mismatch");
+        if (set) {
+            CK(cudaMemcpy(net_.params(), host, (size_t)n * sizeof(float), cudaMemcpyHostToDevice));
+            net_.syncLowPrecision(stream_);
+            CK(cudaStreamSynchronize(stream_));
+        } else {
+            CK(cudaMemcpy(host, net_.params(), (size_t)n * sizeof(float), cudaMemcpyDeviceToHost));
+        }
+    }
+
+    LearnedNet::Sample sample(int idx) const {
+        const float* base = samples_ + (size_t)idx * sampleStride();
+        const size_t N = (size_t)N_;
+        return LearnedNet::Sample{base, base + N, base + 2 * N, base + 3 * N, base + 4 * N};
+    }
+
+    float learnedGrad(int idx, float* grad, int64_t n) {
+        requireNet();
+        if (idx < 0 || idx >= learnedSampleCount()) throw StatusError(AXISIM_E_ARG, "sample index out of range");
+        if (grad && n != (int64_t)net_.numParams()) throw StatusError(AXISIM_E_ARG, "parameter count mismatch");
+        Arena tmp;
+        float* loss = tmp.alloc<float>(1);
+        net_.lossAndGrad(sample(idx), loss, stream_);
+        CK(cudaStreamSynchronize(stream_));
+        float h = 0.f;
+        CK(cudaMemcpy(&h, loss, sizeof(float), cudaMemcpyDeviceToHost));
+        if (grad) CK(cudaMemcpy(grad, net_.grad(), (size_t)n * sizeof(float), cudaMemcpyDeviceToHost));
+        return h;
+    }
+
+    // Adam on samples [first, first + count) drawn uniformly (with replacement)
+    // by a seeded linear congruential generator.
+    void learnedTrain(int steps, float lr, uint64_t seed, int first, int count, float* lossHost) {
+        requireNet();
+        const int have = learnedSampleCount();
+        if (count <= 0) count = have - first;
+        if (first < 0 || count <= 0 || first + count > have)
+            throw StatusError(AXISIM_E_ARG, "sample range outside the store");
+        if (steps <= 0 || !(lr > 0.f)) throw StatusError(AXISIM_E_ARG, "steps and lr must be positive");
+        Arena tmp;
+        float* loss = tmp.alloc<float>((size_t)steps);
+        uint64_t st = seed * 6364136223846793005ull + 1442695040888963407ull;
+        for (int i = 0; i < steps; i++) {
+            st = st * 6364136223846793005ull + 1442695040888963407ull;
+            const int idx = first + (int)((st >> 33) % (uint64_t)count);
+            net_.trainStep(sample(idx), lr, ++adamT_, loss + i, stream_);
+        }
+        CK(cudaStreamSynchronize(stream_));
+        if (lossHost) CK(cudaMemcpy(lossHost, loss, (size_t)steps * sizeof(float), cudaMemcpyDeviceToHost));
+    }
+
+    void learnedPredict(const float* r, const float* ac, const float* d, float* out) {
+        requireNet();
+        if (!r || !ac || !d || !out) throw StatusError(AXISIM_E_ARG, "array is null");
+        Arena tmp;
+        float* dev = tmp.alloc<float>(4 * (size_t)N_);
+        const float* src[3] = {r, ac, d};
+        for (int k = 0; k < 3; k++)
+            CK(cudaMemcpy(dev + (size_t)k * N_, src[k], (size_t)N_ * sizeof(float), cudaMemcpyHostToDevice));
+        net_.predict(dev, dev + N_, dev + 2 * (size_t)N_, dev + 3 * (size_t)N_, stream_);
+        CK(cudaStreamSynchronize(stream_));
+        CK(cudaMemcpy(out, dev + 3 * (size_t)N_, (size_t)N_ * sizeof(float), cudaMemcpyDeviceToHost));
+    }
+
+    void learnedEnable(int mode) {
+        if (mode != AXISIM_LEARNED_OFF && mode != AXISIM_LEARNED_FIRST_STEP && mode != AXISIM_LEARNED_ALWAYS)
+            throw StatusError(AXISIM_E_ARG, "unknown learned mode");
+        if (mode != AXISIM_LEARNED_OFF) requireNet();
+        learnedMode_ = mode;
+        destroyGraph();
+    }
+
+    void learnedStats(int64_t* applied, int64_t* fallbacks, double* scoreNet, double* scoreV) {
+        NetStats h{};
+        if (netStats_) CK(cudaMemcpy(&h, netStats_, sizeof(NetStats), cudaMemcpyDeviceToHost));
+        if (applied) *applied = h.applied;
+        if (fallbacks) *fallbacks = h.fallbacks;
+        if (scoreNet) *scoreNet = h.logRhoNet;
+        if (scoreV) *scoreV = h.logRhoV;
+    }
+
     void ensureNetStats() {
         if (netStats_) return;
         netStats_ = netArena_.alloc<NetStats>(1);
-        nnE_ = netArena_.alloc<float>((size_t)N_);
+        nnY_ = netArena_.alloc<float>((size_t)N_);
+        nnAy_ = netArena_.alloc<double>((size_t)N_);
     }
 
     // ---------------- mesh ----------------
@@ -197,7 +377,9 @@ public:
         fcgR_ = nullptr;
         netArena_.release();
         netStats_ = nullptr;
-        nnE_ = nullptr;
+        nnY_ = nullptr;
+        nnAy_ = nullptr;
+        resetLearned();
         mgArena_.release();
         levels_.clear();
         hier_.clear();
@@ -471,7 +653,19 @@ private:
     // counters of the Krylov steps (V-cycle reduction, learned-step outcomes)
     Arena netArena_;
     NetStats* netStats_ = nullptr;
-    float* nnE_ = nullptr;
+    float* nnY_ = nullptr;    // the network's output in the first Krylov iteration
+    double* nnAy_ = nullptr;  // A times it
+    // learned preconditioner and its harvested (b, p', A_C, deficit, A_F)
+    // training samples, FP32 [cap][4 + W][N] (A_F as ELL)
+    LearnedNet net_;
+    int learnedMode_ = 0;
+    int adamT_ = 0;
+    Arena sampleArena_;
+    int harvestEvery_ = 0, sampleCap_ = 0;
+    float* samples_ = nullptr;
+    int* sampleCount_ = nullptr;
+    float* sampleRelres_ = nullptr;
+    unsigned int* harvestCounter_ = nullptr;
     std::vector<int32_t> hColor_, hColorStart_;
     int colorN_ = 0;
     int32_t* dCellOrder_ = nullptr;
@@ -697,7 +891,7 @@ private:
             fcgQ_ = A.alloc<double>(N);
             fcg_.partial = A.alloc<double>((N + 255) / 256 * 2);
             fcg_.counter = A.alloc<unsigned int>(2);
-            fcg_.scalars = A.alloc<double>(8);
+            fcg_.scalars = A.alloc<double>(16);
         }
         if (!AF32m_) {
             const size_t N = (size_t)N_, WN = (size_t)W_ * N;
@@ -874,14 +1068,33 @@ private:
         launchFcgInit(ctl_, levels_[0], pp_, fcgR_, r32pp_, levels32_[0].x, cmg_.weight, firstSweep ? 1 : 0,
                       psolveTol_, fcg_, stream_);
         mark("fcg_init", (double)N_ * (12.0 * W_ + 8.0 + 8.0 + 8.0 + 8.0 + vb + (firstSweep ? vb : 0.0)));
+        const bool useNet = learnedMode_ != AXISIM_LEARNED_OFF && net_.ready();
         for (int it = 0; it < iters; it++) {
             std::vector<float*> cur((size_t)L), alt((size_t)L);
             for (int l = 0; l < L; l++) {
                 cur[(size_t)l] = levels32_[(size_t)l].x;
                 alt[(size_t)l] = levels32_[(size_t)l].xNew;
             }
+            const bool netStep = useNet && it == 0;
+            // first iteration with the network: the gate picks the learned
+            // preconditioner z = alpha y + V-cycle(r - alpha A y), y =
+            // network(r), whose kernels run while ppSkip == 2, or the plain
+            // V-cycle
+            if (netStep) {
+                launchFcgGate(ctl_, netStats_, learnedMode_ == AXISIM_LEARNED_ALWAYS ? 1 : 0, stream_);
+                net_.infer(ctl_, 1, fcgR_, ACpp_, AFpp_, mesh_.snb, W_, nnY_, stream_);
+                mark("nn_infer", 0.0);
+                launchNnResidual(ctl_, levels_[0], fcgR_, nnY_, nnAy_, fcg_, r32pp_, levels32_[0].x, cmg_.weight,
+                                 firstSweep ? 1 : 0, stream_);
+                mark("nn_residual", (double)N_ * (12.0 * W_ + 8.0 + 4.0 * W_ + 8.0 + 8.0 + 8.0 + 8.0 + 4.0 + 4.0));
+                launchFcgUngate(ctl_, stream_);
+            }
             vcycleT<float>(levels32_, 0, cur, alt, firstSweep);
             const float* e = cur[0];
+            if (netStep) {
+                launchNnCombine(ctl_, netStats_, N_, nnY_, fcg_, cur[0], stream_);
+                mark("nn_combine", 12.0 * N_);
+            }
             launchFcgDots(ctl_, N_, e, fcgR_, fcgQ_, it > 0 ? 1 : 0, fcg_, stream_);
             mark("fcg_dots", (double)N_ * (vb + 8.0 + (it > 0 ? 8.0 : 0.0)));
             double* pOld = fcgP_[(it + 1) & 1];
@@ -889,12 +1102,12 @@ private:
             const int pqOld = 2 + ((it + 1) & 1), pqNew = 2 + (it & 1);
             launchFcgSpmv(ctl_, levels_[0], e, pOld, pNew, fcgQ_, it == 0 ? 1 : 0, pqOld, pqNew, fcg_, stream_);
             mark("fcg_spmv", (double)N_ * (12.0 * W_ + 8.0 + vb + (it > 0 ? 8.0 : 0.0) + 16.0));
-            const int next = it + 1 < iters ? (firstSweep ? 2 : 1) : 0;
+            const int next = it + 1 < iters ? (firstSweep ? 2 : 1) : 1;
             launchFcgUpdate(ctl_, levels_[0], pp_, fcgR_, pNew, fcgQ_, fcg_, pqNew, r32pp_, levels32_[0].x,
-                            cmg_.weight, next, psolveTol_, netStats_, stream_);
-            mark("fcg_update", (double)N_ * (24.0 + (next ? 24.0 + vb + (next > 1 ? 8.0 + vb : 0.0) : 0.0)));
+                            cmg_.weight, next, psolveTol_, stream_);
+            mark("fcg_update", (double)N_ * (24.0 + 24.0 + vb + (next > 1 ? 8.0 + vb : 0.0)));
         }
-        launchFcgEnd(ctl_, stream_);
+        launchFcgEnd(ctl_, fcg_, useNet ? netStats_ : nullptr, stream_);
         mark("fcg_end", 0.0);
         curProlong_ = 1.0;
     }
@@ -1050,6 +1263,12 @@ private:
             mark("pp_rhs", 16.0 * F_ + (4.0 * W_ + 16.0) * N_);
             if (cs_.useMultigrid) enqueueMultigrid();
             else enqueueLinear(pp_, ppT_, AFpp_, bpp_, ipp_);
+        }
+        if (harvestEvery_ > 0 && samples_) {
+            launchHarvest(ctl_, N_, harvestEvery_, sampleCap_, bpp_, pp_, ACpp_, AFpp_, mesh_.snb, W_,
+                          psolve_ == AXISIM_PSOLVE_FCG ? fcg_.scalars : nullptr, samples_, sampleCount_, sampleRelres_,
+                          harvestCounter_, stream_);
+            mark("harvest", 0.0);
         }
         {
             const double* phi[1] = {pp_};
@@ -1558,6 +1777,90 @@ int axisim_set_precision(axisim_handle* h, int32_t mode) {
 int axisim_set_pressure_solver(axisim_handle* h, int32_t mode, double relTol, double prolongScale) {
     return guarded(h, [&] {
         h->s->setPressureSolver(mode, relTol, prolongScale);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_learned_harvest(axisim_handle* h, int32_t every, int32_t capacity) {
+    return guarded(h, [&] {
+        h->s->learnedHarvest(every, capacity);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_learned_sample_count(axisim_handle* h, int32_t* count) {
+    return guarded(h, [&] {
+        if (!count) throw StatusError(AXISIM_E_ARG, "count is null");
+        *count = h->s->learnedSampleCount();
+        return AXISIM_OK;
+    });
+}
+
+int axisim_learned_add_sample(axisim_handle* h, const float* b, const float* target, const float* acDiag,
+                              const float* deficit, const float* afSlots) {
+    return guarded(h, [&] {
+        h->s->learnedAddSample(b, target, acDiag, deficit, afSlots);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_learned_get_sample(axisim_handle* h, int32_t index, float* b, float* target, float* acDiag,
+                              float* deficit, float* afSlots, float* relResidual) {
+    return guarded(h, [&] {
+        h->s->learnedGetSample(index, b, target, acDiag, deficit, afSlots, relResidual);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_learned_init(axisim_handle* h, int32_t precision, uint64_t seed, int64_t* nParams) {
+    return guarded(h, [&] {
+        const size_t n = h->s->learnedInit(precision, seed);
+        if (nParams) *nParams = (int64_t)n;
+        return AXISIM_OK;
+    });
+}
+
+int axisim_learned_params(axisim_handle* h, float* params, int64_t n, int32_t set) {
+    return guarded(h, [&] {
+        h->s->learnedParams(params, n, set);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_learned_grad(axisim_handle* h, int32_t sample, float* loss, float* grad, int64_t n) {
+    return guarded(h, [&] {
+        const float l = h->s->learnedGrad(sample, grad, n);
+        if (loss) *loss = l;
+        return AXISIM_OK;
+    });
+}
+
+int axisim_learned_train(axisim_handle* h, int32_t steps, float lr, uint64_t seed, int32_t first, int32_t count,
+                         float* lossOut) {
+    return guarded(h, [&] {
+        h->s->learnedTrain(steps, lr, seed, first, count, lossOut);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_learned_predict(axisim_handle* h, const float* r, const float* acDiag, const float* deficit, float* out) {
+    return guarded(h, [&] {
+        h->s->learnedPredict(r, acDiag, deficit, out);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_learned_enable(axisim_handle* h, int32_t mode) {
+    return guarded(h, [&] {
+        h->s->learnedEnable(mode);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_learned_stats(axisim_handle* h, int64_t* applied, int64_t* fallbacks, double* scoreNet,
+                         double* scoreVcycle) {
+    return guarded(h, [&] {
+        h->s->learnedStats(applied, fallbacks, scoreNet, scoreVcycle);
         return AXISIM_OK;
     });
 }

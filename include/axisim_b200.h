@@ -199,6 +199,64 @@ int axisim_set_pressure_solver(axisim_handle* h, int32_t mode, double relTol, do
  * mesh was set. */
 int axisim_pressure_stats(axisim_handle* h, int64_t* solves, int64_t* iterations);
 
+/* ---- learned p' preconditioner (new; no reference counterpart) ----
+ * A U-Net over the multigrid's agglomeration hierarchy maps a p' residual r to
+ * a correction y. It is trained on (p' right-hand side, converged p') pairs
+ * that the solver's own FCG + V-cycle solve produces, with the energy-norm
+ * error left after the best scaling of y as the loss. In the first FCG
+ * iteration of a p' solve the preconditioner becomes
+ * z = a y + V(r - a A y), a = (y, r) / (y, A y): the network's step, scaled
+ * for the least energy error, then a V-cycle on the residual it leaves. Each solve is scored
+ * by its mean log reduction of the FP64 residual per Krylov iteration; with
+ * FIRST_STEP the network is used while its running score is at least as good
+ * as the plain V-cycle's, else the solve falls back to the V-cycle (every 16th
+ * solve probes each method so both scores stay current); ALWAYS uses it on
+ * every solve. */
+enum { AXISIM_LEARNED_OFF = 0, AXISIM_LEARNED_FIRST_STEP = 1, AXISIM_LEARNED_ALWAYS = 2 };
+/* Sample store of `capacity` samples (0 keeps the current store) and harvest
+ * of one sample every `every` SIMPLE iterations (0 = off) during solves; a
+ * harvested sample is the p' system of that iteration after its solve, so run
+ * the FCG solver with a tight relTol while harvesting. */
+int axisim_learned_harvest(axisim_handle* h, int32_t every, int32_t capacity);
+int axisim_learned_sample_count(axisim_handle* h, int32_t* count);
+/* Host arrays: right-hand side, target p' (A p' = b), A_C diagonal and
+ * boundary deficit 1 - sum|A_F| / A_C (nCells floats each), and the
+ * off-diagonals A_F in the mesh's slot order (cellFaceStart[nCells] floats, 0
+ * on boundary slots). */
+int axisim_learned_add_sample(axisim_handle* h, const float* b, const float* target, const float* acDiag,
+                              const float* deficit, const float* afSlots);
+/* Any output may be NULL; relResidual = ||b - A p'|| / ||b|| of the solve that
+ * produced it (-1 when added by hand). */
+int axisim_learned_get_sample(axisim_handle* h, int32_t index, float* b, float* target, float* acDiag,
+                              float* deficit, float* afSlots, float* relResidual);
+/* (Re)initialises the network for the handle's mesh (AXISIM_NET_*): weights
+ * and activations in FP32, both in BF16, or BF16 weights with FP32
+ * activations; products always accumulate in FP32. */
+enum { AXISIM_NET_FP32 = 0, AXISIM_NET_BF16 = 1, AXISIM_NET_BF16_WEIGHTS = 2 };
+int axisim_learned_init(axisim_handle* h, int32_t precision, uint64_t seed, int64_t* nParams);
+/* Reads (set = 0) or writes (set = 1) the n FP32 master parameters. */
+int axisim_learned_params(axisim_handle* h, float* params, int64_t n, int32_t set);
+/* Loss 1 - (y.b)^2 / ((y.A y)(b.p')) of the network output y on stored
+ * sample `sample` (the energy-norm error left after the best scaling of y,
+ * which is what one Krylov step along y removes) and its gradient with respect
+ * to the parameters; grad may be NULL. */
+int axisim_learned_grad(axisim_handle* h, int32_t sample, float* loss, float* grad, int64_t n);
+/* `steps` Adam steps (learning rate lr) on samples drawn from store entries
+ * [first, first + count) (count <= 0: to the end) with a seeded generator;
+ * lossOut[steps] (may be NULL) receives each step's loss. */
+int axisim_learned_train(axisim_handle* h, int32_t steps, float lr, uint64_t seed, int32_t first, int32_t count,
+                         float* lossOut);
+/* The network's correction out[nCells] (its output times rms(r / A_C)) for a
+ * residual r, A_C diagonal and boundary deficit (host arrays). */
+int axisim_learned_predict(axisim_handle* h, const float* r, const float* acDiag, const float* deficit, float* out);
+/* AXISIM_LEARNED_*; takes effect in the FCG pressure solver. */
+int axisim_learned_enable(axisim_handle* h, int32_t mode);
+/* Solves that used the network, solves that fell back to the V-cycle because
+ * its score was better, and the two running scores (mean log residual
+ * reduction per Krylov iteration; more negative is better). */
+int axisim_learned_stats(axisim_handle* h, int64_t* applied, int64_t* fallbacks, double* scoreNet,
+                         double* scoreVcycle);
+
 /* ---- solve / continue / stop ---- */
 /* Solver::run + runSimple (solver.cpp:146-173, 753-1396), synchronous on the
  * caller's thread. continueRun mirrors Solver::continueSolver: the device fields

@@ -1,0 +1,92 @@
+"""Learned p' preconditioner on the GPU: the hand-written forward/backward
+kernels against the CPU oracle, and training.
+
+Gradient tolerances: FP32 mode accumulates in FP32 in a different order from
+the float64 oracle, so loss and gradient agree to ~1e-5 relative. The sample is
+a random symmetric, diagonally dominant matrix on the mesh with t = A^-1 b. BF16 mode
+rounds every stored activation to 8 mantissa bits through ~30 layers, and the
+loss gradient is a difference of two nearly cancelling terms, so there the
+check is what training needs: the gradient's direction (cosine >= 0.99 with the
+oracle's, relative L2 error <= 0.1), against an oracle run on the same
+BF16-rounded weights.
+"""
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spla
+
+from axisim import cases
+import axisim.abi as abi
+import learned_ref as LR
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16_round(x):
+    u = np.asarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32)
+
+
+def _solver_with_sample(nr=10, nz=50, seed=0):
+    case = cases.pipe(nr=nr, nz=nz, max_iter=1, tol=1e-30)
+    mesh = abi.multiblock(case.blocks)
+    s = abi.Solver(mesh, case.bc_fields(), case.settings)
+    rng = np.random.default_rng(seed)
+    N = int(mesh["nCells"])
+    s.learned_harvest(0, 2)
+    ac, af = LR.random_spd_system(mesh, rng)
+    A = LR.matrix(mesh, ac, af)
+    b = rng.standard_normal(N)
+    t = spla.spsolve(A.tocsc(), b)
+    d = 1.0 - (np.asarray(abs(A).sum(1)).ravel() - ac) / ac
+    s.learned_add_sample(b, t, ac, d, af)
+    levels = s.mg_levels()
+    net = LR.NetRef(LR.hierarchy(mesh, s.mg_level_maps, len(levels)))
+    return s, net
+
+
+@pytest.mark.parametrize("prec", [abi.NET_FP32, abi.NET_BF16, abi.NET_BF16_WEIGHTS], ids=["fp32", "bf16", "bf16w"])
+def test_gpu_loss_and_gradient_match_oracle(prec):
+    s, net = _solver_with_sample()
+    n = s.learned_init(prec, seed=3)
+    assert n == net.n_params
+    bf16 = prec == abi.NET_BF16
+    p = s.learned_params().astype(np.float64)
+    if prec != abi.NET_FP32:
+        p = _bf16_round(p).astype(np.float64)
+    b, t, ac, d, af, _ = s.learned_get_sample(0)
+    A = LR.matrix(s.mesh, ac, af)
+    loss_ref, g_ref = net.loss_and_grad(p, b, t, ac, d, A)
+    loss, g = s.learned_grad(0)
+    tol_loss, tol_grad = (1e-5, 1e-4) if not bf16 else (2e-2, 1e-1)  # BF16 weights alone: FP32 tolerances
+    assert abs(loss - loss_ref) <= tol_loss * loss_ref, (loss, loss_ref)
+    err = np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref)
+    assert err <= tol_grad, err
+    cos = float(g @ g_ref / (np.linalg.norm(g) * np.linalg.norm(g_ref)))
+    assert cos >= (0.99 if bf16 else 1 - 1e-6), cos
+    # per group too, so no small group hides behind a large one
+    for key, (off, K, Co) in net.groups.items():
+        sl = slice(off, off + K * Co + Co)
+        gn = np.linalg.norm(g_ref[sl])
+        if gn > 1e-3 * np.linalg.norm(g_ref):
+            assert np.linalg.norm(g[sl] - g_ref[sl]) / gn <= 10 * tol_grad, key
+
+
+def test_training_step_is_adam_on_the_gradient():
+    s, _ = _solver_with_sample()
+    s.learned_init(abi.NET_FP32, seed=4)
+    p0 = s.learned_params().astype(np.float64)
+    _, g = s.learned_grad(0)
+    lr = 1e-3
+    losses = s.learned_train(1, lr=lr, seed=0)
+    p1 = s.learned_params().astype(np.float64)
+    # first Adam step, bias-corrected: p1 = p0 - lr g / (|g| + eps)
+    np.testing.assert_allclose(p1, p0 - lr * g / (np.abs(g) + 1e-8), rtol=1e-4, atol=1e-7)
+    assert np.isfinite(losses).all()
+
+
+def test_training_reduces_the_loss_on_one_sample():
+    s, _ = _solver_with_sample()
+    s.learned_init(abi.NET_BF16_WEIGHTS, seed=5)
+    losses = s.learned_train(200, lr=3e-3, seed=0)
+    assert np.mean(losses[-20:]) < 0.5 * np.mean(losses[:5]), (losses[:5], losses[-20:])
