@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <random>
 #include <stdexcept>
 #include <string>
@@ -211,6 +212,205 @@ __global__ void k_layer_fwd(const Ctl* ctl, int gated, NetLayer L, const TW* __r
             if (L.relu) v = fmaxf(v, 0.f);
             stv(Y, (size_t)n * Cout + o0 + j, v);
         }
+    }
+}
+
+// Tiled layers: a block computes a 64-row tile of Y = act(Z W + b [+ add])
+// for all Cout = 16 CPT outputs. The tile's Z (64 x K, FP32) is gathered into
+// shared memory (lanes along the channels, so source rows load coalesced),
+// W is staged in 32-row chunks, and each of the 256 threads accumulates a
+// 4-row x CPT-column register block (columns tx + 16 j: conflict-free
+// weight reads, broadcast Z reads).
+constexpr int kTileRows = 64;
+constexpr int kChunk = 32;
+
+// Every channel count here divides 256, so thread t handles channel t % C of
+// rows t / C, t / C + 256 / C, ... of each input (no per-element division).
+// For a mean over a CSR list, the tile's list bounds are first staged in
+// shared memory (idx: TR + 1 ints) so the C threads of a row do not each
+// re-read them.
+template <class TA, int TR>
+__device__ __forceinline__ void gatherTile(const NetLayer& L, int row0, float* zs, int ldz, int* idx) {
+    int off = 0;
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        if (i >= L.nIn) break;
+        const NetIn& I = L.in[i];
+        const int C = I.C;
+        const int c = threadIdx.x % C, rstep = blockDim.x / C;
+        const TA* x = (const TA*)I.x;
+        const bool mean = I.xf == NX_NBMEAN || I.xf == NX_POOL;
+        if (mean) {
+            __syncthreads();
+            for (int r = threadIdx.x; r <= TR; r += blockDim.x) idx[r] = I.s[min(row0 + r, L.N)];
+            __syncthreads();
+        }
+        for (int r = threadIdx.x / C; r < TR; r += rstep) {
+            const int n = row0 + r;
+            float v = 0.f;
+            if (n < L.N) {
+                if (I.xf == NX_ID) v = ldv(x, (size_t)n * C + c);
+                else if (I.xf == NX_UNPOOL) v = ldv(x, (size_t)I.map[n] * C + c);
+                else {
+                    // four independent list loads, then four independent row
+                    // loads: coarse levels have long lists and few rows, so
+                    // the loop is bound by load latency, not bandwidth
+                    int q = idx[r];
+                    const int q1 = idx[r + 1];
+                    for (; q + 4 <= q1; q += 4) {
+                        const int k0 = __ldg(I.list + q), k1 = __ldg(I.list + q + 1);
+                        const int k2 = __ldg(I.list + q + 2), k3 = __ldg(I.list + q + 3);
+                        const float a0 = ldv(x, (size_t)k0 * C + c), a1 = ldv(x, (size_t)k1 * C + c);
+                        const float a2 = ldv(x, (size_t)k2 * C + c), a3 = ldv(x, (size_t)k3 * C + c);
+                        v += (a0 + a1) + (a2 + a3);
+                    }
+                    for (; q < q1; q++) v += ldv(x, (size_t)__ldg(I.list + q) * C + c);
+                    v *= __ldg(I.inv + n);
+                }
+            }
+            zs[r * ldz + off + c] = v;
+        }
+        off += C;
+    }
+}
+
+template <class TA, class TW, int CPT, int RPT>
+__global__ void __launch_bounds__(256) k_layer_tile(const Ctl* ctl, int gated, NetLayer L, const TW* __restrict__ P) {
+    if (idle(ctl, gated)) return;
+    constexpr int COUT = 16 * CPT;
+    constexpr int TR = 16 * RPT;  // rows per tile
+    extern __shared__ float sm[];
+    const int K = L.K;
+    const int ldz = K + 1;
+    float* zs = sm;                   // [TR][K + 1]
+    float* ws = sm + TR * ldz;        // [32][COUT]
+    const int row0 = blockIdx.x * TR;
+    gatherTile<TA, TR>(L, row0, zs, ldz, (int*)(ws + kChunk * COUT));
+    __syncthreads();
+    if (L.Z) {
+        TA* Z = (TA*)L.Z;
+        const int k = threadIdx.x % K, rstep = blockDim.x / K;
+        for (int r = threadIdx.x / K; r < TR; r += rstep)
+            if (row0 + r < L.N) stv(Z, (size_t)(row0 + r) * K + k, zs[r * ldz + k]);
+    }
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 x 16 threads
+    const TW* W = P + L.wOff;
+    float acc[RPT][CPT];
+#pragma unroll
+    for (int j = 0; j < CPT; j++) {
+        const float bj = ldv(W + (size_t)K * COUT, tx + 16 * j);
+#pragma unroll
+        for (int i = 0; i < RPT; i++) acc[i][j] = bj;
+    }
+    for (int k0 = 0; k0 < K; k0 += kChunk) {
+        const int kn = min(kChunk, K - k0);
+        // the chunk's weights: all of a thread's loads issued before any
+        // shared-memory store, so they are in flight together
+        constexpr int PER = kChunk * COUT / 256;
+        float wv[PER];
+#pragma unroll
+        for (int u = 0; u < PER; u++) {
+            const int idx = threadIdx.x + 256 * u;
+            wv[u] = idx < kn * COUT ? ldv(W, (size_t)k0 * COUT + idx) : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < PER; u++) ws[threadIdx.x + 256 * u] = wv[u];
+        __syncthreads();
+        for (int kk = 0; kk < kn; kk++) {
+            float z[RPT];
+#pragma unroll
+            for (int i = 0; i < RPT; i++) z[i] = zs[(ty * RPT + i) * ldz + k0 + kk];
+#pragma unroll
+            for (int j = 0; j < CPT; j++) {
+                const float w = ws[kk * COUT + tx + 16 * j];
+#pragma unroll
+                for (int i = 0; i < RPT; i++) acc[i][j] = fmaf(z[i], w, acc[i][j]);
+            }
+        }
+    }
+    const TA* add = (const TA*)L.add;
+    TA* Y = (TA*)L.Y;
+#pragma unroll
+    for (int i = 0; i < RPT; i++) {
+        const int n = row0 + ty * RPT + i;
+        if (n >= L.N) continue;
+#pragma unroll
+        for (int j = 0; j < CPT; j++) {
+            const int o = tx + 16 * j;
+            float v = acc[i][j];
+            if (add) v += ldv(add, (size_t)n * COUT + o);
+            if (L.relu) v = fmaxf(v, 0.f);
+            stv(Y, (size_t)n * COUT + o, v);
+        }
+    }
+}
+
+// Tiled backward: G = gY * act'(Y) for a 64-row tile (kept in shared memory
+// and written out for the weight gradient), then dZ = G W^T for K = 16 KPT
+// columns, W^T staged in 32-output chunks.
+template <class TA, class TW, int KPT>
+__global__ void __launch_bounds__(256) k_layer_dz_tile(NetLayer L, const TW* __restrict__ P, float* __restrict__ G,
+                                                       float* __restrict__ dZ) {
+    constexpr int KD = 16 * KPT;
+    extern __shared__ float sm[];
+    const int Cout = L.Cout;
+    const int ldg = Cout + 1;
+    float* gs = sm;                       // [64][Cout + 1]
+    float* wt = sm + kTileRows * ldg;     // [32][KD]: W^T chunk
+    const int row0 = blockIdx.x * kTileRows;
+    const TA* Y = (const TA*)L.Y;
+    const int o = threadIdx.x % Cout, rstep = blockDim.x / Cout;  // Cout divides 256
+    for (int r = threadIdx.x / Cout; r < kTileRows; r += rstep) {
+        const int n = row0 + r;
+        float v = 0.f;
+        if (n < L.N) {
+            v = L.gY[(size_t)n * Cout + o];
+            if (L.relu && ldv(Y, (size_t)n * Cout + o) <= 0.f) v = 0.f;
+            G[(size_t)n * Cout + o] = v;
+        }
+        gs[r * ldg + o] = v;
+    }
+    if (!dZ) return;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const TW* W = P + L.wOff;
+    float acc[4][KPT];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < KPT; j++) acc[i][j] = 0.f;
+    for (int o0 = 0; o0 < Cout; o0 += kChunk) {
+        const int on = min(kChunk, Cout - o0);
+        constexpr int PER = kChunk * KD / 256;
+        float wv[PER];
+#pragma unroll
+        for (int u = 0; u < PER; u++) {
+            const int idx = threadIdx.x + 256 * u;
+            const int oo = idx / KD, k = idx % KD;
+            wv[u] = oo < on ? ldv(W, (size_t)k * Cout + o0 + oo) : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < PER; u++) wt[threadIdx.x + 256 * u] = wv[u];
+        __syncthreads();
+        for (int oo = 0; oo < on; oo++) {
+            float g[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) g[i] = gs[(ty * 4 + i) * ldg + o0 + oo];
+#pragma unroll
+            for (int j = 0; j < KPT; j++) {
+                const float w = wt[oo * KD + tx + 16 * j];
+#pragma unroll
+                for (int i = 0; i < 4; i++) acc[i][j] = fmaf(g[i], w, acc[i][j]);
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int n = row0 + ty * 4 + i;
+        if (n >= L.N) continue;
+#pragma unroll
+        for (int j = 0; j < KPT; j++) dZ[(size_t)n * KD + tx + 16 * j] = acc[i][j];
     }
 }
 
@@ -467,8 +667,61 @@ __global__ void __launch_bounds__(kThreads) k_harvest(const Ctl* ctl, int N, int
 
 // ---------------- host helpers ----------------
 
+// Opts a kernel into more than 48 KB of dynamic shared memory, once per device.
+template <class F>
+void allowSmem(F* f, size_t bytes) {
+    if (bytes <= 48 * 1024) return;
+    static std::mutex mu;
+    static std::vector<std::pair<int, const void*>> done;
+    int dev = 0;
+    NCK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto& d : done)
+        if (d.first == dev && d.second == (const void*)f) return;
+    NCK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    done.push_back({dev, (const void*)f});
+}
+
+template <class TA, class TW, int CPT, int RPT>
+void launchTileR(const Ctl* ctl, int gated, const NetLayer& L, const void* P, cudaStream_t s) {
+    const size_t smem =
+        ((size_t)16 * RPT * (L.K + 1) + (size_t)kChunk * 16 * CPT + 16 * RPT + 1) * sizeof(float);
+    allowSmem(k_layer_tile<TA, TW, CPT, RPT>, smem);
+    k_layer_tile<TA, TW, CPT, RPT><<<blocksFor(L.N, 16 * RPT), 256, smem, s>>>(ctl, gated, L, (const TW*)P);
+}
+
+// 64-row tiles on large levels; 16-row tiles (4 x the blocks, 1/4 the work
+// per thread) where a level has too few rows to fill the GPU.
+template <class TA, class TW, int CPT>
+void launchTile(const Ctl* ctl, int gated, const NetLayer& L, const void* P, cudaStream_t s) {
+    if (L.N >= 148 * 64 * 4) launchTileR<TA, TW, CPT, 4>(ctl, gated, L, P, s);
+    else launchTileR<TA, TW, CPT, 1>(ctl, gated, L, P, s);
+}
+
+template <class TA, class TW, int KPT>
+void launchDzTile(const NetLayer& L, const void* P, float* G, float* dZ, cudaStream_t s) {
+    const size_t smem = ((size_t)kTileRows * (L.Cout + 1) + (size_t)kChunk * 16 * KPT) * sizeof(float);
+    allowSmem(k_layer_dz_tile<TA, TW, KPT>, smem);
+    k_layer_dz_tile<TA, TW, KPT><<<blocksFor(L.N, kTileRows), 256, smem, s>>>(L, (const TW*)P, G, dZ);
+}
+
+// The tiled kernels assume every channel count divides their 256 threads.
+inline bool tileable(const NetLayer& L) {
+    if (L.K > 256 || 256 % L.K != 0 || L.Cout > 256 || 256 % L.Cout != 0) return false;
+    for (int i = 0; i < L.nIn; i++)
+        if (256 % L.in[i].C != 0) return false;
+    return true;
+}
+
 template <class TA, class TW>
 void launchLayerFwd(const Ctl* ctl, int gated, const NetLayer& L, const void* P, cudaStream_t s) {
+    switch (tileable(L) ? L.Cout : 0) {
+        case 16: launchTile<TA, TW, 1>(ctl, gated, L, P, s); return;
+        case 32: launchTile<TA, TW, 2>(ctl, gated, L, P, s); return;
+        case 64: launchTile<TA, TW, 4>(ctl, gated, L, P, s); return;
+        case 128: launchTile<TA, TW, 8>(ctl, gated, L, P, s); return;
+        default: break;
+    }
     const int rows = L.K <= 64 ? 128 : 32;
     const size_t smem = (size_t)rows * (L.K + 1) * sizeof(float);
     const dim3 grid(blocksFor(L.N, rows));
@@ -480,6 +733,16 @@ void launchLayerFwd(const Ctl* ctl, int gated, const NetLayer& L, const void* P,
 
 template <class TA, class TW>
 void launchLayerDz(const NetLayer& L, const void* P, float* G, float* dZ, cudaStream_t s) {
+    if (dZ && tileable(L)) {
+        switch (L.K) {
+            case 16: launchDzTile<TA, TW, 1>(L, P, G, dZ, s); return;
+            case 32: launchDzTile<TA, TW, 2>(L, P, G, dZ, s); return;
+            case 64: launchDzTile<TA, TW, 4>(L, P, G, dZ, s); return;
+            case 128: launchDzTile<TA, TW, 8>(L, P, G, dZ, s); return;
+            case 256: launchDzTile<TA, TW, 16>(L, P, G, dZ, s); return;
+            default: break;
+        }
+    }
     k_layer_dz<TA, TW, 16><<<blocksFor(L.N), kThreads, 0, s>>>(L, (const TW*)P, G, dZ);
 }
 
