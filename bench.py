@@ -261,11 +261,15 @@ def measure(abi, mesh, bcs, settings, args, local, dist, prec, sampler=None):
     return solver, max_over_ranks(dist, r["ms"]), clocks
 
 
-def time_to_residual(abi, case, local, prec, tol=1e-6):
+def time_to_residual(abi, case, local, prec, tol=1e-6, fcg_iters=0):
     c = dict(case.settings)
     c["resTol"] = [tol, tol, tol]
     mesh = case.packed(abi.multiblock)
-    s = abi.Solver(mesh, case.bc_fields(), c, device=local, precision=prec)
+    if fcg_iters:
+        c["mgMaxIter"] = fcg_iters
+        s = abi.Solver(mesh, case.bc_fields(), c, device=local, precision=prec, pressure_solver=abi.PSOLVE_FCG)
+    else:
+        s = abi.Solver(mesh, case.bc_fields(), c, device=local, precision=prec)
     r = s.solve()
     out = {"iterations": r["iterations"], "converged": r["converged"], "seconds": r["ms"] / 1e3,
            "residuals": r["residual"]}
@@ -328,6 +332,81 @@ def batch_converge_leg(abi, local, n_cases=16, scale=0.05, max_iter=20000):
             "batched_iterations": rb["iterations"], "batched_converged_cases": int((conv_at >= 0).sum()),
             "sequential_seconds": seq_ms / 1e3, "sequential_converged_cases": seq_conv,
             "note": f"config-4 case mix at scale {scale}, tolerance 1e-6, at most {max_iter} iterations"}
+
+
+def transient_leg(abi, local, scale=1.512, warm_steps=2, timed_steps=3, max_iter=300, train_steps=600):
+    """The transient pulsatile sudden expansion (1,998,855 cells at scale
+    1.512, BDF2, dt 1e-4): after `warm_steps` untimed steps, time-to-residual
+    1e-6 of each of `timed_steps` steps (at most `max_iter` SIMPLE iterations
+    per step) for the reference method (FP64, 3 V-cycles), mixed precision with
+    the FCG p' solve, and the same with the learned first Krylov step, whose
+    network is trained beforehand on p' systems harvested during its warm-up
+    steps. Fields are compared with the FP64 FCG run over the same steps."""
+    import numpy as np
+    from axisim import cases
+    case = cases.pulsatile_expansion(scale=scale, dt=1e-4, steps=warm_steps, max_iter=max_iter, tol=1e-6)
+    mesh = case.packed(abi.multiblock)
+    dt = case.settings["dt"]
+
+    def arm(prec, psolve, tol=1e-2, learned=False):
+        st = dict(case.settings)
+        if psolve == abi.PSOLVE_FCG:
+            st["mgMaxIter"] = 300 if learned else 100  # the learned arm harvests converged p' while warming up
+        s = abi.Solver(mesh, case.bc_fields(), st, device=local, precision=prec, pressure_solver=psolve,
+                       pressure_tol=tol if not learned else 1e-6, prolong_scale=2.0)
+        info = {}
+        if learned:
+            s.learned_harvest(1, 64)
+        s.solve()  # warm-up steps (harvesting for the learned arm)
+        if learned:
+            s.learned_harvest(0)
+            n = s.learned_sample_count()
+            s.learned_init(abi.NET_BF16_WEIGHTS, seed=1)
+            t0 = time.perf_counter()
+            losses = s.learned_train(train_steps, lr=1e-3, seed=0, first=0, count=max(1, n - 8))
+            t_train = time.perf_counter() - t0
+            held = [s.learned_grad(i)[0] for i in range(max(1, n - 8), n)]
+            info["training"] = {"samples": n, "steps": train_steps, "seconds": t_train,
+                                "loss_first_50": float(np.mean(losses[:50])),
+                                "loss_last_50": float(np.mean(losses[-50:])),
+                                "held_out_loss": float(np.mean(held)) if held else None,
+                                "loss": "energy-norm error left after the best scaling of the output"}
+            s.settings["mgMaxIter"] = 100
+            abi.lib().axisim_set_pressure_solver(s.h, abi.PSOLVE_FCG, tol, 2.0)
+            s.learned_enable(abi.LEARNED_FIRST_STEP)
+        s.settings["tEnd"] = dt
+        steps, secs, iters = [], 0.0, 0
+        pp0 = s.pressure_stats() if psolve == abi.PSOLVE_FCG else (0, 0)
+        for _ in range(timed_steps):
+            s.set_max_iter(max_iter, tol=1e-6)
+            r = s.solve(cont=True)
+            steps.append({"iterations": r["iterations"], "converged": r["converged"], "seconds": r["ms"] / 1e3,
+                          "residual": r["residual"]})
+            secs += r["ms"] / 1e3
+            iters += r["iterations"]
+        info.update(steps=steps, seconds=secs, iterations=iters,
+                    steps_converged=sum(1 for x in steps if x["converged"]))
+        if psolve == abi.PSOLVE_FCG:
+            pp1 = s.pressure_stats()
+            info["krylov_iterations_per_solve"] = (pp1[1] - pp0[1]) / max(1, pp1[0] - pp0[0])
+        if learned:
+            info["learned"] = s.learned_stats()
+            a, f = info["learned"]["applied"], info["learned"]["fallbacks"]
+            info["fallback_rate"] = f / max(1, a + f)
+        fields = {k: s.get(k) for k in ("u", "v", "p")}
+        s.close()
+        return info, fields
+
+    out = {"workload": case.name, "cells": int(mesh["nCells"]), "dt": dt, "warm_steps": warm_steps,
+           "timed_steps": timed_steps, "max_iter_per_step": max_iter, "tol": 1e-6}
+    out["plain_fp64"], _ = arm(abi.PREC_FP64, abi.PSOLVE_VCYCLES)
+    out["fcg_fp64"], f64 = arm(abi.PREC_FP64, abi.PSOLVE_FCG)
+    out["mixed_fcg"], fmx = arm(abi.PREC_MIXED, abi.PSOLVE_FCG)
+    out["learned_mixed_fcg"], fln = arm(abi.PREC_MIXED, abi.PSOLVE_FCG, learned=True)
+    rel = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))  # noqa: E731
+    for key, f in (("mixed_fcg", fmx), ("learned_mixed_fcg", fln)):
+        out[key]["error_vs_fp64"] = {k: rel(f[k], f64[k]) for k in ("u", "v", "p")}
+    return out
 
 
 def run_b200(args):
@@ -422,7 +501,13 @@ def run_b200(args):
         t64["pressure_drop_Pa"] = e64["dp"]
         t64["recirculation_length_m"] = e64["recirculation_length"]
         t64["recirculation_reaches_outlet"] = e64["recirculation_reaches_outlet"]
-        ttr[case.name] = {"plain_fp64": t64, "mixed": tmx, "speedup_mixed_vs_plain": t64["seconds"] / tmx["seconds"]}
+        tfc, _, ffc = time_to_residual(abi, full, local, abi.PREC_MIXED, fcg_iters=5)
+        tfc["error_vs_fp64"] = {"u_rel_l2": rel(ffc["u"], f64["u"]), "v_rel_l2": rel(ffc["v"], f64["v"]),
+                                "p_rel_l2": rel(ffc["p"], f64["p"])}
+        tfc["pressure_solver"] = "flexible CG, 5 iterations, FP32 V-cycle preconditioner"
+        ttr[case.name] = {"plain_fp64": t64, "mixed": tmx, "mixed_fcg": tfc,
+                          "speedup_mixed_vs_plain": t64["seconds"] / tmx["seconds"],
+                          "speedup_mixed_fcg_vs_plain": t64["seconds"] / tfc["seconds"]}
         pc = cases.pipe(max_iter=50000, tol=1e-6)
         p64, _, _ = time_to_residual(abi, pc, local, abi.PREC_FP64)
         pmx, _, _ = time_to_residual(abi, pc, local, abi.PREC_MIXED)
@@ -431,6 +516,7 @@ def run_b200(args):
         if "ms" in ref_pipe:
             ttr[pc.name]["reference_cuda"] = {"seconds": ref_pipe["ms"] / 1e3, "iterations": ref_pipe["iterations"]}
         line["time_to_residual"] = ttr
+        line["transient"] = transient_leg(abi, local, scale=1.512 * args.scale)
         line["batch"] = batch_leg(abi, local)
         line["batch_to_converged"] = batch_converge_leg(abi, local)
     if rank == 0:
