@@ -31,6 +31,13 @@ METRIC = "time-to-residual 1e-6 & SIMPLE iter/s per Mcell, learned+mixed vs plai
 UNIT = "Mcell-iter/s"
 
 
+def _json_scalar(o):
+    # numpy scalars (numpy's bool_ included) as plain Python values
+    if hasattr(o, "item"):
+        return o.item()
+    raise TypeError(f"not JSON serializable: {type(o).__name__}")
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -180,7 +187,7 @@ def run_reference(args):
                              "sample": f"{done} SIMPLE iterations of {case.name} ({t_total:.1f} s)"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference has no CPU solver path; this arm runs the oracle's C restatement of it"}
-    print(json.dumps(line), flush=True)
+    print(json.dumps(line, default=_json_scalar), flush=True)
 
 
 def cpu_baseline_leg(case, mesh):
@@ -520,7 +527,7 @@ def run_b200(args):
         line["batch"] = batch_leg(abi, local)
         line["batch_to_converged"] = batch_converge_leg(abi, local)
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        print(json.dumps(line, default=_json_scalar), flush=True)
     if dist is not None:
         dist.destroy_process_group()
 
