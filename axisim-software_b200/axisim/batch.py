@@ -17,7 +17,7 @@ GROUPS_PER_CASE = 4
 
 
 def random_cases(n=256, seed=0, lo=8_000, hi=260_000, rho=1056.0, mu=3.5e-3, scale=1.0, max_iter=50000, tol=1e-6):
-    """n cases with cell count log-uniform in [lo, hi]; each a
+    """The batch workload: n cases with cell count log-uniform in [lo, hi]; each a
     pipe or a sudden expansion (expansion ratio uniform in [1.5, 4]), throat
     Reynolds number uniform in [50, 1500], inlet uniform or fully developed with
     50/50 odds; all drawn from `seed`. `scale` multiplies the cell counts."""

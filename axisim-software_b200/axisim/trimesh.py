@@ -10,7 +10,7 @@ Boundary groups come from a caller-supplied classifier of the boundary face
 centres (the reference matches them to the nearest sketch edge,
 mesh.cpp:1835-1846).
 
-`bullet_in_pipe` builds the BASELINE unstructured case: a revolved bullet body
+`bullet_in_pipe` builds the unstructured bullet case: a revolved bullet body
 (cylinder, hemispherical nose) on the axis of a pipe, triangulated from a quad
 grid, the body removed cell by cell, interior vertices jittered from a fixed
 seed.

@@ -237,10 +237,12 @@ def reference_cuda_leg(case, iters, tol=0.0):
             "note": "reference CUDA build (sm_100a, unchanged sources), CudaTimer over its SIMPLE loop"}
 
 
-# DRAM bytes per launch per cell of the top kernels from one ncu capture of this
-# workload (profiles/k_jacobi_uv_expansion874k.md: dram__bytes_read.sum +
-# dram__bytes_write.sum = 88.4 MB per launch at 874,496 cells).
-NCU_TRAFFIC_PER_CELL = {"jacobi_uv": 88.36e6 / 874496}
+# DRAM bytes per launch per cell of the top kernels, from one ncu capture of this
+# workload each (dram__bytes_read.sum + dram__bytes_write.sum per launch at
+# 874,496 cells; FP64 sweep 88.4 MB).
+NCU_TRAFFIC_PER_CELL = {"jacobi_uv": 88.36e6 / 874496,
+                        # dram__bytes_read.sum 48.976 MB + dram__bytes_write.sum 0.179 MB per launch
+                        "jacobi_uv32": (48.976384e6 + 0.178688e6) / 874496}
 
 
 def mesh_bytes(m):
@@ -286,7 +288,7 @@ def time_to_residual(abi, case, local, prec, tol=1e-6, fcg_iters=0):
 
 
 def batch_leg(abi, local, n_cases=64, steps=50):
-    """Config 4: cases advanced together in one packed mesh vs one handle per
+    """Batch of random cases advanced together in one packed mesh vs one handle per
     case, same K SIMPLE iterations, device (CUDA-event) time."""
     from axisim import batch
     cs = batch.random_cases(n_cases, seed=0)
@@ -314,7 +316,7 @@ def batch_leg(abi, local, n_cases=64, steps=50):
             "batched_Mcell_iter_s": cells * steps / (rb["ms"] / 1e3) / 1e6,
             "sequential_Mcell_iter_s": cells * steps / (seq_ms / 1e3) / 1e6,
             "speedup": seq_ms / rb["ms"], "batched_ms": rb["ms"], "sequential_ms": seq_ms,
-            "note": "config-4 case mix (seed 0), first %d cases; one packed mesh vs one handle per case" % n_cases}
+            "note": "random pipe/expansion case mix (seed 0), first %d cases; one packed mesh vs one handle per case" % n_cases}
 
 
 def batch_converge_leg(abi, local, n_cases=16, scale=0.05, max_iter=20000):
@@ -338,7 +340,7 @@ def batch_converge_leg(abi, local, n_cases=16, scale=0.05, max_iter=20000):
     return {"cases": n_cases, "cells": int(union["nCells"]), "batched_seconds": rb["ms"] / 1e3,
             "batched_iterations": rb["iterations"], "batched_converged_cases": int((conv_at >= 0).sum()),
             "sequential_seconds": seq_ms / 1e3, "sequential_converged_cases": seq_conv,
-            "note": f"config-4 case mix at scale {scale}, tolerance 1e-6, at most {max_iter} iterations"}
+            "note": f"random pipe/expansion case mix at scale {scale}, tolerance 1e-6, at most {max_iter} iterations"}
 
 
 def transient_leg(abi, local, scale=1.512, warm_steps=2, timed_steps=3, max_iter=300, train_steps=600):
