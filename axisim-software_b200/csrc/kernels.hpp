@@ -114,6 +114,11 @@ void launchMGGather(const Ctl* ctl, const LevelT<T>& fine, const LevelT<T>& coar
                     int firstSweep, T w, cudaStream_t s);
 template <class T>
 void launchMGProlong(const Ctl* ctl, const LevelT<T>& fine, T* xFine, const T* xCoarse, T scale, cudaStream_t s);
+// prolongation fused into the first post-smoothing sweep (ELL levels with
+// W = 3 or 4): y = smooth(x + s P e); returns false when not applicable
+template <class T>
+bool launchMGProlongSmooth(const Ctl* ctl, const LevelT<T>& fine, const T* xFine, const T* xCoarse, T* y, T w,
+                           T scale, cudaStream_t s);
 template <class T>
 size_t tailSharedBytes(const TailArgsT<T>& a);
 template <class T>

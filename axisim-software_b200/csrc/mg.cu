@@ -156,6 +156,46 @@ __global__ void __launch_bounds__(kThreads) k_mg_smooth_ell(const Ctl* ctl, Leve
     y[n] = x[n] + w * (L.b[n] - Ax) / ac;
 }
 
+// Prolongation fused into the first post-smoothing sweep on an ELL level:
+// x' = x + s P e is formed on the fly for the cell and its neighbours, and
+// y = x' + w (b - A x') / A_C, with the expressions and their order of the
+// separate prolongation and sweep kernels, so the result is the same bit for
+// bit; x' itself is never stored (one pass over x instead of three).
+template <class T, int WC>
+__global__ void __launch_bounds__(kThreads) k_mg_prolong_smooth_ell(const Ctl* ctl, LevelT<T> L,
+                                                                    const T* __restrict__ x,
+                                                                    const T* __restrict__ xc, T* __restrict__ y,
+                                                                    T w, T scale) {
+    pdlEnter();
+    if (ctl->done || ctl->ppSkip) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L.N) return;
+    const int32_t* __restrict__ c2c = L.c2c;
+    const T xn = x[n] + scale * xc[c2c[n]];
+    const T ac = L.AC[n];
+    if (fabs(ac) < tiny<T>()) {
+        y[n] = xn;
+        return;
+    }
+    int k[WC];
+    T a[WC], g[WC];
+#pragma unroll
+    for (int j = 0; j < WC; j++) {
+        k[j] = L.nb[(size_t)j * L.N + n];
+        a[j] = L.AF[(size_t)j * L.N + n];
+    }
+#pragma unroll
+    for (int j = 0; j < WC; j++) {
+        const int m = k[j] >= 0 ? k[j] : n;
+        g[j] = x[m] + scale * xc[c2c[m]];
+    }
+    T Ax = L.AC[n] * xn;
+#pragma unroll
+    for (int j = 0; j < WC; j++)
+        if (k[j] != -1) Ax += a[j] * g[j];
+    y[n] = xn + w * (L.b[n] - Ax) / ac;
+}
+
 template <class T, int WC>
 __global__ void __launch_bounds__(kThreads) k_mg_residual_ell(const Ctl* ctl, LevelT<T> L, const T* __restrict__ x) {
     pdlEnter();
@@ -433,6 +473,21 @@ void launchMGProlong(const Ctl* ctl, const LevelT<T>& fine, T* xFine, const T* x
 }
 
 template <class T>
+bool launchMGProlongSmooth(const Ctl* ctl, const LevelT<T>& fine, const T* xFine, const T* xCoarse, T* y, T w,
+                           T scale, cudaStream_t s) {
+    if (fine.sliceOff || !fine.c2c) return false;
+    if (fine.W == 4)
+        launchPDL(k_mg_prolong_smooth_ell<T, 4>, dim3(blocksFor(fine.N)), dim3(kThreads), 0, s, ctl, fine, xFine,
+                  xCoarse, y, w, scale);
+    else if (fine.W == 3)
+        launchPDL(k_mg_prolong_smooth_ell<T, 3>, dim3(blocksFor(fine.N)), dim3(kThreads), 0, s, ctl, fine, xFine,
+                  xCoarse, y, w, scale);
+    else
+        return false;
+    return true;
+}
+
+template <class T>
 size_t tailSharedBytes(const TailArgsT<T>& a) {
     size_t d = 0;
     for (int i = 0; i < a.count; i++) d += 4 * (size_t)a.lv[i].N;
@@ -460,6 +515,7 @@ template void launchGalerkin<float, float>(const Ctl*, const LevelT<float>&, con
     template void launchMGResidual<T>(const Ctl*, const LevelT<T>&, const T*, cudaStream_t);                    \
     template void launchMGGather<T>(const Ctl*, const LevelT<T>&, const LevelT<T>&, T*, T*, int, T, cudaStream_t); \
     template void launchMGProlong<T>(const Ctl*, const LevelT<T>&, T*, const T*, T, cudaStream_t);                 \
+    template bool launchMGProlongSmooth<T>(const Ctl*, const LevelT<T>&, const T*, const T*, T*, T, T, cudaStream_t); \
     template size_t tailSharedBytes<T>(const TailArgsT<T>&);                                                   \
     template void launchMGTail<T>(const Ctl*, const TailArgsT<T>&, cudaStream_t);
 AXISIM_MG_INSTANTIATE(double)

@@ -83,7 +83,11 @@ class Solver {
 public:
     Solver(int device, const axisim_fluid& f) : fluid_(f), device_(device) {
         CK(cudaSetDevice(device_));
-        CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        // A blocking stream: set-up work (cudaMalloc'd buffers zeroed by
+        // cudaMemset, uploads by cudaMemcpy from pageable memory, which may
+        // return before the DMA lands) runs on the legacy default stream, and
+        // the solver's kernels must be ordered after it.
+        CK(cudaStreamCreate(&stream_));
         CK(cudaHostAlloc(&hostStop_, sizeof(int), cudaHostAllocMapped));
         *hostStop_ = 0;
         CK(cudaHostGetDevicePointer((void**)&hostStopDev_, (void*)hostStop_, 0));
@@ -1015,9 +1019,20 @@ private:
             if (fuse) std::swap(cur[(size_t)l + 1], alt[(size_t)l + 1]);
             vcycleT<T>(lv, l + 1, cur, alt, fuse);
         }
-        launchMGProlong<T>(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], (T)curProlong_, stream_);
-        mark((std::string("mg_prolong") + tag).c_str(), (4.0 + 2 * vb) * F.N + vb * C.N);
-        smoothT<T>(lv, l, cmg_.linearPostSweep, cur, alt);
+        const int post = cmg_.linearPostSweep;
+        const bool blockSmoother = post > 1 && F.N <= 4096;
+        if (post >= 1 && !blockSmoother &&
+            launchMGProlongSmooth<T>(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], alt[(size_t)l], w,
+                                     (T)curProlong_, stream_)) {
+            mark((std::string("mg_prolong_smooth") + tag).c_str(),
+                 (double)F.N * ((4.0 + vb) * F.W + 4.0 + 4.0 * vb) + vb * C.N);
+            std::swap(cur[(size_t)l], alt[(size_t)l]);
+            smoothT<T>(lv, l, post - 1, cur, alt);
+        } else {
+            launchMGProlong<T>(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], (T)curProlong_, stream_);
+            mark((std::string("mg_prolong") + tag).c_str(), (4.0 + 2 * vb) * F.N + vb * C.N);
+            smoothT<T>(lv, l, post, cur, alt);
+        }
     }
 
     // Mixed precision: every V-cycle is one refinement step on the FP64 system
@@ -1449,8 +1464,10 @@ int Solver::solve(int continueRun, axisim_result* res) {
         simTime_ = 0.0;
         if (batch_.nCases > 0) {
             std::vector<int32_t> neg((size_t)batch_.nCases, -1);
-            CK(cudaMemcpy(batch_.convergedAt, neg.data(), neg.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-            CK(cudaMemset(batch_.scaleVal, 0, sizeof(double) * 3 * (size_t)batch_.nCases));
+            CK(cudaMemcpyAsync(batch_.convergedAt, neg.data(), neg.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                               stream_));
+            CK(cudaMemsetAsync(batch_.scaleVal, 0, sizeof(double) * 3 * (size_t)batch_.nCases, stream_));
+            CK(cudaStreamSynchronize(stream_));
         }
     }
     buildGraph();
