@@ -376,6 +376,20 @@ class Solver:
             self._check(-k)
         return conv, res
 
+    def save_solution_npy(self, directory, quads=True, triangles=None, **kw):
+        """The reference's NumPy export (solution.npy, points.npy, cells.npy,
+        meta.json; see axisim.export) of this handle's current fields. quads:
+        derive the corner polygons of an axis-aligned structured mesh;
+        triangles: (points, tris) of an unstructured one."""
+        from . import export
+        s = self.settings
+        fluid = {"rho": s["rho"], "mu": s["mu"], "cp": 4180.0, "k": 0.6, "D": 3.0277e-9}
+        sols = export.solutions_from(self.get, self.mesh, fluid)
+        kw.setdefault("transient", bool(s.get("transient", 0)))
+        kw.setdefault("dt", s.get("dt", 0.0))
+        q = export.quad_corners(self.mesh) if quads and triangles is None else None
+        return export.save_solution_npy(directory, self.mesh, sols, fluid, quads=q, triangles=triangles, **kw)
+
     # ---- learned p' preconditioner ----
     def learned_harvest(self, every, capacity=0):
         self._check(lib().axisim_learned_harvest(self.h, every, capacity))
