@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="cell-count scale of the workload (1 = full size)")
     ap.add_argument("--no-extras", action="store_true", help="skip cpu baseline / e2e / time-to-residual legs")
+    ap.add_argument("--network-only", action="store_true",
+                    help="time the learned p' network alone (inference and training steps, 2M-cell mesh)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="mixed: FP32 inner solves inside FP64 refinement (the workload's setting); fp64: plain")
     return ap.parse_args()
@@ -418,6 +420,37 @@ def transient_leg(abi, local, scale=1.512, warm_steps=2, timed_steps=3, max_iter
     return out
 
 
+def network_leg(abi, local, scale=1.512, infer=5, train=5):
+    """The learned p' network alone on the transient mesh (1,998,855 cells at
+    scale 1.512): mean host-clock time of `infer` predictions and `train` Adam
+    steps on a synthetic sample (after one warm-up of each)."""
+    import numpy as np
+    from axisim import cases
+    case = cases.pulsatile_expansion(scale=scale, dt=1e-4, steps=1, max_iter=1, tol=1e-30)
+    mesh = case.packed(abi.multiblock)
+    N = int(mesh["nCells"])
+    s = abi.Solver(mesh, case.bc_fields(), case.settings, device=local)
+    rng = np.random.default_rng(0)
+    af = np.where(mesh["faceNeighbor"][mesh["cellFaceIDs"]] >= 0, -1.0, 0.0)
+    s.learned_harvest(0, 1)
+    s.learned_add_sample(rng.standard_normal(N), rng.standard_normal(N), np.full(N, 4.1), np.zeros(N), af)
+    n_params = s.learned_init(abi.NET_BF16_WEIGHTS, seed=0)
+    r, ac, d = rng.standard_normal(N), np.full(N, 4.1), np.zeros(N)
+    s.learned_predict(r, ac, d)
+    s.learned_train(1)
+    t0 = time.perf_counter()
+    for _ in range(infer):
+        s.learned_predict(r, ac, d)
+    t_inf = (time.perf_counter() - t0) / infer
+    t0 = time.perf_counter()
+    s.learned_train(train)
+    t_tr = (time.perf_counter() - t0) / train
+    s.close()
+    return {"cells": N, "parameters": n_params,
+            "predict_ms": t_inf * 1e3, "train_step_ms": t_tr * 1e3,
+            "note": "predict includes the host copies of r, A_C, deficit and the result"}
+
+
 def run_b200(args):
     world, rank, local, dist = dist_setup(args.gpus)
     import numpy as np
@@ -425,6 +458,10 @@ def run_b200(args):
     from axisim import cases
     if not os.path.exists(abi.LIB_PATH):
         abi.build()
+    if args.network_only:
+        if rank == 0:
+            print(json.dumps(network_leg(abi, local, scale=1.512 * args.scale), default=_json_scalar), flush=True)
+        return
     case = workload(args.scale)
     mesh = abi.multiblock(case.blocks)
     N = mesh["nCells"]
