@@ -62,7 +62,8 @@ def pack_union(meshes, groups_list):
     cell_off = np.cumsum([0] + [m["nCells"] for m in meshes])
     face_off = np.cumsum([0] + [m["nFaces"] for m in meshes])
     ref_off = np.cumsum([0] + [len(m["cellFaceIDs"]) for m in meshes])
-    out = {"nCells": int(cell_off[-1]), "nFaces": int(face_off[-1]), "status": 0}
+    out = {"nCells": int(cell_off[-1]), "nFaces": int(face_off[-1]), "status": 0,
+           "meshType": 0 if all(m.get("meshType", 1) == 0 for m in meshes) else 1}
     cat = lambda k: np.concatenate([m[k] for m in meshes])  # noqa: E731
     for k in ("faceNormalZ", "faceNormalR", "faceCenterZ", "faceCenterR", "faceArea", "cellCenterZ", "cellCenterR",
               "cellArea2D", "cellVolume"):

@@ -16,8 +16,9 @@ import numpy as np
 DIRICHLET, NEUMANN, FULLY_DEVELOPED, MICHAELIS_MENTEN, HILL, NONE, PULSATILE = range(7)
 # BoundaryType (structs/boundary_struct.h:342-348)
 WALL, VELOCITY_INLET, PRESSURE_OUTLET, SYMMETRY, FAR_FIELD = range(5)
-# BoundaryVariable
-U, V, P = "u", "v", "p"
+# BoundaryVariable: velocity components, pressure, static temperature, concentration
+U, V, P, TEMP, CONC = "u", "v", "p", "T", "C"
+SCALARS = (TEMP, CONC)
 # ConvectionScheme / GradientScheme / LinearSolverType / TimeScheme
 CONV_UPWIND, CONV_CENTRAL, CONV_SOU, CONV_QUICK = range(4)
 GRAD_GREEN_GAUSS, GRAD_LSQ = range(2)
@@ -29,43 +30,59 @@ WEST, EAST, SOUTH, NORTH = range(4)
 
 
 def default_bc_type(btype, var):
-    """getDefaultBCType (boundary_func.cpp:117-201) for u, v, p."""
+    """getDefaultBCType (boundary_func.cpp:117-201): the scalars are Dirichlet
+    at a velocity inlet and zero-gradient everywhere else."""
     table = {
-        VELOCITY_INLET: {U: DIRICHLET, V: DIRICHLET, P: NEUMANN},
-        PRESSURE_OUTLET: {U: NEUMANN, V: NEUMANN, P: DIRICHLET},
-        WALL: {U: DIRICHLET, V: DIRICHLET, P: NEUMANN},
-        SYMMETRY: {U: NEUMANN, V: DIRICHLET, P: NEUMANN},
-        FAR_FIELD: {U: DIRICHLET, V: DIRICHLET, P: NEUMANN},
+        VELOCITY_INLET: {U: DIRICHLET, V: DIRICHLET, P: NEUMANN, TEMP: DIRICHLET, CONC: DIRICHLET},
+        PRESSURE_OUTLET: {U: NEUMANN, V: NEUMANN, P: DIRICHLET, TEMP: NEUMANN, CONC: NEUMANN},
+        WALL: {U: DIRICHLET, V: DIRICHLET, P: NEUMANN, TEMP: NEUMANN, CONC: NEUMANN},
+        SYMMETRY: {U: NEUMANN, V: DIRICHLET, P: NEUMANN, TEMP: NEUMANN, CONC: NEUMANN},
+        FAR_FIELD: {U: DIRICHLET, V: DIRICHLET, P: NEUMANN, TEMP: NEUMANN, CONC: NEUMANN},
     }
     return table.get(btype, {}).get(var, NONE)
 
 
 def variable_editable(var, btype):
-    """isVariableInBoundaryType (boundary_func.cpp:333-378) for u, v, p."""
+    """isVariableInBoundaryType (boundary_func.cpp:333-378)."""
     if btype == WALL:
-        return var in (U, V)
+        return var in (U, V, TEMP, CONC)
     if btype == SYMMETRY:
         return False
     if btype == FAR_FIELD:
         return var in (U, V)
     if btype == VELOCITY_INLET:
-        return var in (U, V)
+        return var in (U, V, TEMP, CONC)
     if btype == PRESSURE_OUTLET:
-        return var == P
+        return var in (P, TEMP, CONC)
     return False
+
+
+def michaelis_menten(vmax, km, inhibition=None):
+    """MichaelisMentenParams (boundary_struct.h:111): J = Vmax c / (Km + c),
+    times 1 - V2 c^m / (K2^m + c^m) when inhibition = (m, K2, V2) is given."""
+    return (MICHAELIS_MENTEN, dict(Vmax=vmax, Km=km, n=1.0, inhibition=inhibition))
+
+
+def hill(vmax, km, n, inhibition=None):
+    """HillParams (boundary_struct.h:112): J = Vmax c^n / (Km^n + c^n)."""
+    return (HILL, dict(Vmax=vmax, Km=km, n=n, inhibition=inhibition))
 
 
 @dataclass
 class Group:
     """BoundarySegmentGroup (boundary_struct.h:501-533): id, type, user BCs, totalLength.
 
-    bcs maps variable -> (bcType, value) or (PULSATILE, mean, amplitude, frequency).
+    bcs maps variable -> (bcType, value), (PULSATILE, mean, amplitude, frequency)
+    or a kinetics condition from michaelis_menten() / hill(). layers maps a
+    scalar variable to its wall stack [(k, d), ...], a series resistance
+    sum d / k (Layer::resistance, boundary_struct.h:24-39).
     total_length is stored as float32, as the reference's float totalLength is.
     """
     id: int
     btype: int
     bcs: dict = field(default_factory=dict)
     total_length: float = 0.0
+    layers: dict = field(default_factory=dict)
 
 
 def effective_bc(group, var):
@@ -83,6 +100,9 @@ def resolve_bc_field(groups, var):
     out = dict(type=np.full(G, NONE, np.uint8), btype=np.full(G, WALL, np.uint8),
                value=np.zeros(G), length=np.zeros(G), puls=np.zeros(G, np.uint8),
                amp=np.zeros(G), freq=np.zeros(G))
+    if var in SCALARS:  # kinetics defaults (memory_manger.cpp:72-83)
+        out.update(vmax=np.zeros(G), km=np.zeros(G), n=np.ones(G), m=np.ones(G), k2=np.zeros(G),
+                   v2=np.zeros(G), Rtot=np.zeros(G))
     for g in groups:
         if g.id < 0:
             continue
@@ -90,8 +110,23 @@ def resolve_bc_field(groups, var):
         t = bc[0]
         out["type"][g.id] = DIRICHLET if t == PULSATILE else t
         out["btype"][g.id] = g.btype
-        out["value"][g.id] = bc[1]
         out["length"][g.id] = float(np.float32(g.total_length))
+        if t in (MICHAELIS_MENTEN, HILL):
+            # memory_manger.cpp:110-131: a kinetics condition has no single value
+            k = bc[1]
+            out["vmax"][g.id] = k["Vmax"]
+            out["km"][g.id] = k["Km"]
+            if t == HILL:
+                out["n"][g.id] = k["n"]
+            if k.get("inhibition"):
+                out["m"][g.id], out["k2"][g.id], out["v2"][g.id] = k["inhibition"]
+        else:
+            out["value"][g.id] = bc[1]
+        if var in SCALARS and var in g.layers:  # memory_manger.cpp:133-145
+            R = 0.0
+            for (k_layer, d_layer) in g.layers[var]:
+                R += (d_layer / k_layer) if k_layer != 0.0 else 0.0
+            out["Rtot"][g.id] = R
         if t == PULSATILE:
             out["puls"][g.id] = 1
             out["amp"][g.id] = bc[2]
@@ -119,7 +154,10 @@ def default_settings():
                 transient=0, useNonOrthCorrector=0, dt=0.1, tEnd=2.0, maxIter=50, checkConv=1,
                 mgMaxIter=3, mgWeight=0.6, mgLinearSweep=30, mgPreSweep=1, mgPostSweep=1,
                 rho=998.0, mu=0.0010518, alphaU=0.7, alphaP=0.3,
-                resNorm=[0, 0, 0], resScale=[3, 3, 3], resEnabled=[1, 1, 1], resTol=[1e-3, 1e-3, 1e-3])
+                resNorm=[0, 0, 0], resScale=[3, 3, 3], resEnabled=[1, 1, 1], resTol=[1e-3, 1e-3, 1e-3],
+                solveEnergy=0, solveConcentration=0, cp=4180.0, k=0.6, D=3.0277e-9,
+                scalarResNorm=[0, 0], scalarResScale=[3, 3], scalarResEnabled=[0, 0],
+                scalarResTol=[1e-3, 1e-3])
 
 
 @dataclass
@@ -132,7 +170,13 @@ class Case:
     mesh: dict = None   # packed mesh for unstructured cases (blocks empty)
 
     def bc_fields(self):
-        return {v: resolve_bc_field(self.groups, v) for v in (U, V, P)}
+        """Per-variable boundary fields: u, v, p, and T / C when the settings solve them."""
+        out = {v: resolve_bc_field(self.groups, v) for v in (U, V, P)}
+        if self.settings.get("solveEnergy"):
+            out[TEMP] = resolve_bc_field(self.groups, TEMP)
+        if self.settings.get("solveConcentration"):
+            out[CONC] = resolve_bc_field(self.groups, CONC)
+        return out
 
     def packed(self, builder):
         """The packed mesh: the stored one, or `builder(blocks)` (the C++ or the oracle packer)."""
@@ -237,6 +281,36 @@ def bullet(scale=1.0, rho=1000.0, mu=1e-3, re=200.0, seed=0, max_iter=50000, tol
     s.update(convectionScheme=CONV_UPWIND, gradientScheme=GRAD_LSQ, linearType=LINEAR_JACOBI, useNonOrthCorrector=1,
              rho=rho, mu=mu, maxIter=max_iter, resTol=[tol, tol, tol])
     return Case(f"bullet_{mesh['nCells']}", [], groups, s, note=f"U_in={u_in:.4g} m/s", mesh=mesh)
+
+
+def with_scalars(case, energy=True, concentration=True, t_in=310.0, t_wall=300.0, c_in=1.0, wall_c=None,
+                 wall_layers=None, k=None, D=None):
+    """Adds energy and/or concentration transport to a case: Dirichlet T and C
+    at every velocity inlet; at every wall, T fixed at t_wall (None keeps the
+    zero-gradient default) and C by wall_c (a michaelis_menten() / hill()
+    condition, a (type, value) pair, or None for zero gradient) behind the
+    layer stack wall_layers [(k, d), ...]. k / D override the conductivity and
+    the mass diffusivity."""
+    for g in case.groups:
+        if g.btype == VELOCITY_INLET:
+            if energy:
+                g.bcs[TEMP] = (DIRICHLET, t_in)
+            if concentration:
+                g.bcs[CONC] = (DIRICHLET, c_in)
+        elif g.btype == WALL:
+            if energy and t_wall is not None:
+                g.bcs[TEMP] = (DIRICHLET, t_wall)
+            if concentration and wall_c is not None:
+                g.bcs[CONC] = wall_c
+            if concentration and wall_layers:
+                g.layers[CONC] = list(wall_layers)
+    case.settings.update(solveEnergy=int(bool(energy)), solveConcentration=int(bool(concentration)))
+    if k is not None:
+        case.settings["k"] = k
+    if D is not None:
+        case.settings["D"] = D
+    case.name += "_scalars"
+    return case
 
 
 def cell_count(case):

@@ -53,17 +53,23 @@ def write_npy(path, array, descr):
         f.write(a.tobytes(order="C"))
 
 
-def solutions_from(get, mesh, fluid):
+def solutions_from(get, mesh, fluid, energy=False, concentration=False):
     """Solver::createSolutions + createDerivedVelocitySolutions (solver.cpp:186-262)
     from a field getter (axisim.abi.Solver.get or oracle.Oracle.get): velocity
     magnitude |V| and the cell Reynolds number rho |V| sqrt(area2D) / mu are derived
     from the final u and v; the continuity field is the per-cell net outflow
-    of the face mass fluxes (Solver::getMassImbalance, solver.cpp:298-331)."""
+    of the face mass fluxes (Solver::getMassImbalance, solver.cpp:298-331).
+    energy / concentration add Temperature, dT/dz, dT/dr and Concentration,
+    dC/dz, dC/dr (solver.cpp:199-209)."""
     N = int(mesh["nCells"])
     u, v, p = get("u")[:N], get("v")[:N], get("p")[:N]
     out = {"Axial Velocity": u, "Radial Velocity": v, "Pressure": p,
            "dU/dz": get("gradUZ")[:N], "dU/dr": get("gradUR")[:N], "dV/dz": get("gradVZ")[:N],
            "dV/dr": get("gradVR")[:N], "dP/dz": get("gradPZ")[:N], "dP/dr": get("gradPR")[:N]}
+    if energy:
+        out.update({"Temperature": get("T")[:N], "dT/dz": get("gradTZ")[:N], "dT/dr": get("gradTR")[:N]})
+    if concentration:
+        out.update({"Concentration": get("C")[:N], "dC/dz": get("gradCZ")[:N], "dC/dr": get("gradCR")[:N]})
     out["Continuity"] = mass_imbalance(mesh, get("mDot")[:int(mesh["nFaces"])])
     speed = np.sqrt(u * u + v * v)
     h = np.sqrt(np.maximum(np.asarray(mesh["cellArea2D"], np.float64), 0.0))

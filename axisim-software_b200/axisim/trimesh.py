@@ -72,7 +72,7 @@ def pack_triangles(points, tris, classify):
                 faceCenterZ=fz, faceCenterR=fr, faceArea=farea, faceBoundaryGroupID=group, cellCenterZ=cz,
                 cellCenterR=cr, cellArea2D=area2d, cellVolume=vol,
                 cellFaceStart=(3 * np.arange(T + 1)).astype(np.int32),
-                cellFaceIDs=face_of_edge.astype(np.int32), status=0)
+                cellFaceIDs=face_of_edge.astype(np.int32), status=0, meshType=1)
 
 
 def bullet_in_pipe(nz=1250, nr=200, L=0.3, R=0.02, body_r=0.005, body_len=0.03, nose_tip=0.1, jitter=0.1, seed=0):

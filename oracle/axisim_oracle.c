@@ -32,7 +32,7 @@
 
 #define ORC_PI 3.14159265358979323846
 
-enum { BC_DIRICHLET = 0, BC_NEUMANN = 1, BC_FULLY_DEVELOPED = 2 };
+enum { BC_DIRICHLET = 0, BC_NEUMANN = 1, BC_FULLY_DEVELOPED = 2, BC_MICHAELIS_MENTEN = 3, BC_HILL = 4 };
 enum { CONV_UPWIND = 0, CONV_CENTRAL = 1, CONV_SOU = 2, CONV_QUICK = 3 };
 enum { GRAD_GG = 0, GRAD_LSQ = 1 };
 enum { NORM_L1 = 0, NORM_L2 = 1, NORM_LINF = 2 };
@@ -362,6 +362,9 @@ typedef struct {
     uint8_t* puls;
     double* amp;
     double* freq;
+    /* wall kinetics (BoundaryFieldDevice, solver_struct.h:436-451) with the
+     * host-precomputed Km^n and K2^m (memory_manger.cpp:122-136) */
+    double *vmax, *km, *nexp, *mexp, *k2, *v2, *Rtot, *kmN, *k2M;
 } bcf;
 
 typedef struct {
@@ -388,13 +391,18 @@ struct orc_solver {
     double *invDPN, *wP, *dPB, *invA2D, *length2D, *lsqWZ, *lsqWR, *lsqIZZ, *lsqIZR, *lsqIRR;
     /* level-0 CSR neighbour, memory_manger.cpp:287-323 */
     int32_t* slotNb;
-    bcf bcU, bcV, bcP, bcPP;
-    coeffs cu, cv, cpp;
+    bcf bcU, bcV, bcP, bcPP, bcT, bcC;
+    coeffs cu, cv, cpp, ct, cc;
     double *u, *v, *p, *pp, *uTemp, *vTemp, *ppTemp, *DU, *DV;
     double *gradPZ, *gradPR, *gradUZ, *gradUR, *gradVZ, *gradVR;
     double *uOld, *vOld, *uOld2, *vOld2, *mDot;
     double *resU, *resV, *resC, *scaleU, *scaleV;
     double resVal[3], scaleVal[3];
+    /* scalar transport: temperature, concentration, their work and old levels,
+     * gradients, residuals; wall concentration and consumption per face */
+    double *T, *C, *TTemp, *CTemp, *TOld, *COld, *TOld2, *COld2, *gradTZ, *gradTR, *gradCZ, *gradCR;
+    double *resT, *resCc, *scaleT, *scaleCc, *cw, *ocrWall;
+    double resValS[2], scaleValS[2];
     int currentIteration;
     double simTime;
     /* multigrid */
@@ -533,6 +541,57 @@ static void compute_gradient(const orc_solver* s, const bcf* bc, const double* p
     }
 }
 
+/* ---------------- wall kinetics, concentration_equation.cu:6-160 ---------------- */
+static inline double kin_mm(const bcf* bc, int g, double c) { return (bc->vmax[g] * c) / (bc->km[g] + c); }
+static inline double kin_dmm(const bcf* bc, int g, double c) {
+    const double inv = 1.0 / (bc->km[g] + c);
+    return bc->vmax[g] * bc->km[g] * inv * inv;
+}
+static inline double kin_inhib(const bcf* bc, int g, double c) {
+    const double V2 = bc->v2[g];
+    if (V2 == 0.0) return 1.0;
+    const double cm = pow(c, bc->mexp[g]);
+    return (1.0 - (V2 * cm / (bc->k2M[g] + cm)));
+}
+static inline double kin_dinhib(const bcf* bc, int g, double c) {
+    const double V2 = bc->v2[g];
+    if (V2 == 0.0) return 0.0;
+    const double m = bc->mexp[g], K2m = bc->k2M[g];
+    const double cm = pow(c, m);
+    const double cm1 = pow(c, m - 1.0);
+    return (-(m * V2 * K2m) * (cm1) / ((K2m + cm) * (K2m + cm)));
+}
+static inline double kin_hill(const bcf* bc, int g, double c) {
+    const double cn = pow(c, bc->nexp[g]);
+    return (bc->vmax[g] * cn) / (bc->kmN[g] + cn);
+}
+static inline double kin_dhill(const bcf* bc, int g, double c) {
+    const double n = bc->nexp[g], Kmn = bc->kmN[g];
+    const double cn = pow(c, n);
+    const double cn1 = pow(c, n - 1.0);
+    return ((n * bc->vmax[g] * Kmn) * (cn1) / ((Kmn + cn) * (Kmn + cn)));
+}
+/* wallConcentrationMichaelisMenten / wallConcentrationHill: Newton on
+ * h (c_P - c_w) = J(c_w), from c_w = c_P, clipped at 0, at most 100 steps. */
+static double wall_concentration(const bcf* bc, int g, int hill, double cp, double h) {
+    double cw = cp;
+    const double relTol = 1e-10, absTol = 1e-14;
+    for (int i = 0; i < 100; i++) {
+        const double rate = hill ? kin_hill(bc, g, cw) : kin_mm(bc, g, cw);
+        const double inhib = kin_inhib(bc, g, cw);
+        const double J = rate * inhib;
+        const double drate = hill ? kin_dhill(bc, g, cw) : kin_dmm(bc, g, cw);
+        const double dJ = rate * kin_dinhib(bc, g, cw) + drate * inhib;
+        const double F = h * (cp - cw) - J;
+        const double dF = -h - dJ;
+        const double step = F / dF;
+        cw -= step;
+        cw = fmax(0.0, cw);
+        if (fabs(step) < absTol + relTol * fabs(cw)) break;
+    }
+    return cw;
+}
+
 /* ---------------- momentum assembly, solver_util.cu:218-448, cuh:715-865 ---------------- */
 static void add_transport(orc_solver* s, coeffs* c, const bcf* bc, const double* phi,
                           const double* gZ, const double* gR, int nonOrtho, double gamma, int conv,
@@ -596,6 +655,16 @@ static void add_transport(orc_solver* s, coeffs* c, const bcf* bc, const double*
                     } else if (t == BC_FULLY_DEVELOPED) {
                         AC[n] += K;
                         b[n] += K * prescribed(s, f, t, val, len);
+                    } else if (t == BC_MICHAELIS_MENTEN || t == BC_HILL) {
+                        /* solver_util.cu:388-411 reactive wall */
+                        const int hill = t == BC_HILL;
+                        const double Rtot = (dPF / gamma) + bc->Rtot[g];
+                        const double h = 1 / Rtot;
+                        const double cw = wall_concentration(bc, g, hill, phi[n], h);
+                        s->cw[f] = cw;
+                        s->ocrWall[f] = a * (hill ? kin_hill(bc, g, cw) : kin_mm(bc, g, cw)) * kin_inhib(bc, g, cw);
+                        AC[n] += a * h;
+                        b[n] += a * h * cw;
                     }
                 }
                 if (F != 0.0) {
@@ -1057,45 +1126,58 @@ static void continuity_residual(orc_solver* s) {
     }
 }
 
-/* residuals.cu:37-100 residualAllHost (U, V, Continuity) */
+/* residuals.cu:37-100 residualAllHost: U, V, Continuity, Temperature,
+ * Concentration (entries 3 and 4 read the scalar settings). */
 static void residual_host(orc_solver* s, int scaleIteration) {
-    double* res[3] = { s->resU, s->resV, s->resC };
-    double* scl[2] = { s->scaleU, s->scaleV };
+    const orc_config* c = &s->cfg;
+    double* res[5] = { s->resU, s->resV, s->resC, s->resT, s->resCc };
+    double* scl[5] = { s->scaleU, s->scaleV, NULL, s->scaleT, s->scaleCc };
+    double* val[5] = { &s->resVal[0], &s->resVal[1], &s->resVal[2], &s->resValS[0], &s->resValS[1] };
+    double* sv[5] = { &s->scaleVal[0], &s->scaleVal[1], &s->scaleVal[2], &s->scaleValS[0], &s->scaleValS[1] };
+    const int norm[5] = { c->resNorm[0], c->resNorm[1], c->resNorm[2], c->scalarResNorm[0], c->scalarResNorm[1] };
+    const int scale[5] = { c->resScale[0], c->resScale[1], c->resScale[2], c->scalarResScale[0], c->scalarResScale[1] };
+    const int en[5] = { c->resEnabled[0], c->resEnabled[1], c->resEnabled[2], c->scalarResEnabled[0],
+                        c->scalarResEnabled[1] };
     const int N = s->N;
-    for (int i = 0; i < 3; i++) {
-        if (!s->cfg.resEnabled[i]) continue;
+    for (int i = 0; i < 5; i++) {
+        if (!en[i]) continue;
         if (i == 2) {
-            s->resVal[i] = reduce(res[i], N, 1, 0);
+            *val[i] = reduce(res[i], N, 1, 0);
         } else {
-            switch (s->cfg.resNorm[i]) {
-            case NORM_L1: s->resVal[i] = reduce(res[i], N, 1, 0); break;
-            case NORM_L2: s->resVal[i] = reduce(res[i], N, 2, 0); break;
-            case NORM_LINF: s->resVal[i] = reduce(res[i], N, 1, 1); break;
+            switch (norm[i]) {
+            case NORM_L1: *val[i] = reduce(res[i], N, 1, 0); break;
+            case NORM_L2: *val[i] = reduce(res[i], N, 2, 0); break;
+            case NORM_LINF: *val[i] = reduce(res[i], N, 1, 1); break;
             }
-            switch (s->cfg.resScale[i]) {
-            case SCALE_NONE: s->scaleVal[i] = 1.0; break;
-            case SCALE_N: s->scaleVal[i] = N; break;
-            case SCALE_SQRT_N: s->scaleVal[i] = sqrt((double)N); break;
-            case SCALE_DIAG: s->scaleVal[i] = reduce(scl[i], N, 1, 0); break;
+            switch (scale[i]) {
+            case SCALE_NONE: *sv[i] = 1.0; break;
+            case SCALE_N: *sv[i] = N; break;
+            case SCALE_SQRT_N: *sv[i] = sqrt((double)N); break;
+            case SCALE_DIAG: *sv[i] = reduce(scl[i], N, 1, 0); break;
             }
         }
     }
-    for (int i = 0; i < 3; i++) {
-        if (!s->cfg.resEnabled[i]) continue;
-        if (i == 2 && scaleIteration < 5) s->scaleVal[i] = fmax(s->resVal[i], 0.0);
-        if (s->scaleVal[i] == 0.0) continue;
-        if (s->cfg.resNorm[i] == NORM_L2) s->resVal[i] = sqrt(s->resVal[i]);
-        s->resVal[i] /= s->scaleVal[i];
+    for (int i = 0; i < 5; i++) {
+        if (!en[i]) continue;
+        if (i == 2 && scaleIteration < 5) *sv[i] = fmax(*val[i], 0.0);
+        if (*sv[i] == 0.0) continue;
+        if (norm[i] == NORM_L2) *val[i] = sqrt(*val[i]);
+        *val[i] /= *sv[i];
     }
 }
 
 /* solver.cpp:59-72 residualsConverged */
 static int residuals_converged(const orc_solver* s) {
+    const orc_config* c = &s->cfg;
+    const int en[5] = { c->resEnabled[0], c->resEnabled[1], c->resEnabled[2], c->scalarResEnabled[0],
+                        c->scalarResEnabled[1] };
+    const double val[5] = { s->resVal[0], s->resVal[1], s->resVal[2], s->resValS[0], s->resValS[1] };
+    const double tol[5] = { c->resTol[0], c->resTol[1], c->resTol[2], c->scalarResTol[0], c->scalarResTol[1] };
     int any = 0;
-    for (int i = 0; i < 3; i++) {
-        if (!s->cfg.resEnabled[i]) continue;
+    for (int i = 0; i < 5; i++) {
+        if (!en[i]) continue;
         any = 1;
-        if (!(s->resVal[i] <= s->cfg.resTol[i])) return 0;
+        if (!(val[i] <= tol[i])) return 0;
     }
     return any;
 }
@@ -1106,6 +1188,20 @@ static void copy_bc(bcf* d, const orc_bc_field* h, int zeroValues) {
     if (!h || h->nGroups <= 0) return;
     const int G = h->nGroups;
     d->nGroups = G;
+    /* memory_manger.cpp:72-83 defaults, 110-136 kinetics and Km^n, K2^m */
+    double** kin[9] = { &d->vmax, &d->km, &d->nexp, &d->mexp, &d->k2, &d->v2, &d->Rtot, &d->kmN, &d->k2M };
+    for (int i = 0; i < 9; i++) *kin[i] = (double*)xcalloc((size_t)G, 8);
+    for (int g = 0; g < G; g++) {
+        d->vmax[g] = h->vmaxByGroup ? h->vmaxByGroup[g] : 0.0;
+        d->km[g] = h->kmByGroup ? h->kmByGroup[g] : 0.0;
+        d->nexp[g] = h->nByGroup ? h->nByGroup[g] : 1.0;
+        d->mexp[g] = h->mByGroup ? h->mByGroup[g] : 1.0;
+        d->k2[g] = h->k2ByGroup ? h->k2ByGroup[g] : 0.0;
+        d->v2[g] = h->v2ByGroup ? h->v2ByGroup[g] : 0.0;
+        d->Rtot[g] = h->RtotByGroup ? h->RtotByGroup[g] : 0.0;
+        d->kmN[g] = pow(d->km[g], d->nexp[g]);
+        d->k2M[g] = pow(d->k2[g], d->mexp[g]);
+    }
     d->type = (uint8_t*)xcalloc((size_t)G, 1);
     d->btype = (uint8_t*)xcalloc((size_t)G, 1);
     d->value = (double*)xcalloc((size_t)G, 8);
@@ -1130,6 +1226,8 @@ static void copy_bc(bcf* d, const orc_bc_field* h, int zeroValues) {
 static void free_bc(bcf* d) {
     free(d->type); free(d->btype); free(d->value); free(d->mean); free(d->length);
     free(d->puls); free(d->amp); free(d->freq);
+    free(d->vmax); free(d->km); free(d->nexp); free(d->mexp); free(d->k2); free(d->v2); free(d->Rtot);
+    free(d->kmN); free(d->k2M);
 }
 
 #define DUP(dst, src, n, T) do { dst = (T*)xcalloc((size_t)(n) ? (size_t)(n) : 1, sizeof(T)); memcpy(dst, src, (size_t)(n) * sizeof(T)); } while (0)
@@ -1174,13 +1272,24 @@ static void build_coloring(orc_solver* s) {
 
 orc_solver* orc_create(const orc_mesh* m, const orc_bc_field* bu, const orc_bc_field* bv,
                        const orc_bc_field* bp, const orc_config* cfg) {
+    return orc_create_ex(m, bu, bv, bp, NULL, NULL, cfg);
+}
+
+orc_solver* orc_create_ex(const orc_mesh* m, const orc_bc_field* bu, const orc_bc_field* bv,
+                          const orc_bc_field* bp, const orc_bc_field* bt, const orc_bc_field* bcc,
+                          const orc_config* cfg) {
     if (!m || m->nCells <= 0 || !cfg) return NULL;
+    if ((cfg->solveEnergy && !bt) || (cfg->solveConcentration && !bcc)) return NULL;
+    /* solver.cpp:887-889: both scalars are divided through by rho */
+    if ((cfg->solveEnergy || cfg->solveConcentration) && !(cfg->rho > 0.0)) return NULL;
     orc_solver* s = (orc_solver*)xcalloc(1, sizeof(orc_solver));
     s->cfg = *cfg;
     /* solver.cpp:537-547 runCheck clamps */
     if (s->cfg.maxIter < 1) s->cfg.maxIter = 50;
     if (s->cfg.checkConv < 1) s->cfg.checkConv = 1;
     if (s->cfg.linearMaxIter < 1) s->cfg.linearMaxIter = 20;
+    /* solver.cpp:548-555: no non-orthogonal corrector on a structured mesh */
+    if (s->cfg.structuredMesh) s->cfg.useNonOrthCorrector = 0;
     const int N = m->nCells, F = m->nFaces;
     s->N = N;
     s->F = F;
@@ -1274,9 +1383,11 @@ orc_solver* orc_create(const orc_mesh* m, const orc_bc_field* bu, const orc_bc_f
     copy_bc(&s->bcV, bv, 0);
     copy_bc(&s->bcP, bp, 0);
     copy_bc(&s->bcPP, bp, 1); /* solver.cpp:791-795: p types, zero values */
+    if (cfg->solveEnergy) copy_bc(&s->bcT, bt, 0);
+    if (cfg->solveConcentration) copy_bc(&s->bcC, bcc, 0);
 
-    coeffs* cs[3] = { &s->cu, &s->cv, &s->cpp };
-    for (int i = 0; i < 3; i++) {
+    coeffs* cs[5] = { &s->cu, &s->cv, &s->cpp, &s->ct, &s->cc };
+    for (int i = 0; i < 5; i++) {
         cs[i]->N = N;
         cs[i]->S = s->S;
         cs[i]->AC = (double*)xcalloc((size_t)N, 8);
@@ -1291,6 +1402,9 @@ orc_solver* orc_create(const orc_mesh* m, const orc_bc_field* bu, const orc_bc_f
     AL(s->DU, N); AL(s->DV, N); AL(s->gradPZ, N); AL(s->gradPR, N); AL(s->gradUZ, N); AL(s->gradUR, N);
     AL(s->gradVZ, N); AL(s->gradVR, N); AL(s->uOld, N); AL(s->vOld, N); AL(s->uOld2, N); AL(s->vOld2, N);
     AL(s->mDot, F); AL(s->resU, N); AL(s->resV, N); AL(s->resC, N); AL(s->scaleU, N); AL(s->scaleV, N);
+    AL(s->T, N); AL(s->C, N); AL(s->TTemp, N); AL(s->CTemp, N); AL(s->TOld, N); AL(s->COld, N);
+    AL(s->TOld2, N); AL(s->COld2, N); AL(s->gradTZ, N); AL(s->gradTR, N); AL(s->gradCZ, N); AL(s->gradCR, N);
+    AL(s->resT, N); AL(s->resCc, N); AL(s->scaleT, N); AL(s->scaleCc, N); AL(s->cw, F); AL(s->ocrWall, F);
 #undef AL
     if (s->cfg.linearType == 1) build_coloring(s);
     if (s->cfg.useMultigrid) build_levels(s);
@@ -1347,8 +1461,27 @@ static void update_pulsatile(bcf* bc, double t) {
     }
 }
 
-/* One SIMPLE iteration, solver.cpp:1116-1217 */
-static void simple_iteration(orc_solver* s, const double* uOld2, const double* vOld2) {
+/* One transported scalar after the corrections (solver.cpp:1218-1238): the
+ * volumetric flux mDot / rho convects it, `gamma` is its kinematic
+ * diffusivity, the unsteady term has capacity 1. */
+static void scalar_transport(orc_solver* s, coeffs* cf, const bcf* bc, double* phi, double* phiTemp, double* gZ,
+                             double* gR, const double* old, const double* old2, double gamma, double alpha) {
+    const orc_config* c = &s->cfg;
+    const int applyNonOrtho = c->useNonOrthCorrector ? 1 : 0;
+    const int conv = c->addConvectionTerm ? 1 : 0;
+    const int convNeedsGrad = conv && (c->convectionScheme == CONV_SOU || c->convectionScheme == CONV_QUICK);
+    if (applyNonOrtho || convNeedsGrad) compute_gradient(s, bc, phi, gZ, gR);
+    add_transport(s, cf, bc, phi, gZ, gR, applyNonOrtho, gamma, conv, c->convectionScheme, 1.0 / c->rho);
+    if (c->transient) add_transient(s, cf, old, old2, 1.0, c->dt);
+    under_relax(s, cf, phi, alpha);
+    inverse_diag(cf);
+    linear_solve(s, cf, phi, phiTemp);
+}
+
+/* One SIMPLE iteration, solver.cpp:1116-1238. sOld / sOld2 are the scalar
+ * time levels the scalar step reads (T, C); see orc_run for which buffers. */
+static void simple_iteration(orc_solver* s, const double* uOld2, const double* vOld2, int bdf2,
+                             const double* const sOld[2], const double* const sOld2[2]) {
     const orc_config* c = &s->cfg;
     const int applyNonOrtho = c->useNonOrthCorrector ? 1 : 0;
     const int conv = c->addConvectionTerm ? 1 : 0;
@@ -1356,6 +1489,8 @@ static void simple_iteration(orc_solver* s, const double* uOld2, const double* v
     clear_coeffs(&s->cu);
     clear_coeffs(&s->cv);
     clear_coeffs(&s->cpp);
+    if (c->solveEnergy) clear_coeffs(&s->ct);
+    if (c->solveConcentration) clear_coeffs(&s->cc);
     if (applyNonOrtho || convNeedsGrad) {
         compute_gradient(s, &s->bcU, s->u, s->gradUZ, s->gradUR);
         compute_gradient(s, &s->bcV, s->v, s->gradVZ, s->gradVR);
@@ -1412,6 +1547,13 @@ static void simple_iteration(orc_solver* s, const double* uOld2, const double* v
         s->p[n] += c->alphaP * s->pp[n];
     }
     update_mass_flux(s, applyNonOrtho);
+    /* energy (k / (rho cp), relaxed with alphaU) then concentration (D, unrelaxed) */
+    if (c->solveEnergy)
+        scalar_transport(s, &s->ct, &s->bcT, s->T, s->TTemp, s->gradTZ, s->gradTR, sOld[0], bdf2 ? sOld2[0] : NULL,
+                         c->k / (c->rho * c->cp), c->alphaU);
+    if (c->solveConcentration)
+        scalar_transport(s, &s->cc, &s->bcC, s->C, s->CTemp, s->gradCZ, s->gradCR, sOld[1], bdf2 ? sOld2[1] : NULL,
+                         c->D, 1.0);
 }
 
 int orc_run(orc_solver* s, int continueRun, int* converged) {
@@ -1422,6 +1564,14 @@ int orc_run(orc_solver* s, int continueRun, int* converged) {
     const double timeOffset = (c->transient && continueRun) ? s->simTime : 0.0;
     const int useBDF2 = c->transient && c->timeScheme == 1;
     const int numSteps = c->transient ? (int)ceil(c->tEnd / c->dt) : 1;
+    /* solver.cpp:985-1009: the scalar step reads the time levels through
+     * pointers taken from simple.tempOld / tempOld2 (concOld / concOld2) once,
+     * before the time loop, while the BDF2 shift below swaps the names
+     * simple.tempOld <-> tempOld2 every step. The scalar step therefore keeps
+     * reading the same two buffers: correct levels on odd steps, the two
+     * levels exchanged on even steps from the third on. Reproduced as is. */
+    const double* const sOld[2] = { s->TOld, s->COld };
+    const double* const sOld2[2] = { s->TOld2, s->COld2 };
     int iters = 0;
     int conv = 0;
     for (int t = 0; t < numSteps; t++) {
@@ -1433,17 +1583,26 @@ int orc_run(orc_solver* s, int continueRun, int* converged) {
                 double* tmp;
                 tmp = s->uOld2; s->uOld2 = s->uOld; s->uOld = tmp;
                 tmp = s->vOld2; s->vOld2 = s->vOld; s->vOld = tmp;
+                tmp = s->TOld2; s->TOld2 = s->TOld; s->TOld = tmp;
+                tmp = s->COld2; s->COld2 = s->COld; s->COld = tmp;
             }
             memcpy(s->uOld, s->u, (size_t)s->N * 8);
             memcpy(s->vOld, s->v, (size_t)s->N * 8);
+            if (c->solveEnergy) memcpy(s->TOld, s->T, (size_t)s->N * 8);
+            if (c->solveConcentration) memcpy(s->COld, s->C, (size_t)s->N * 8);
         }
         const int bdf2 = useBDF2 && t > 0;
         conv = 0;
         for (int k = 0; k < c->maxIter; k++) {
-            simple_iteration(s, bdf2 ? s->uOld2 : NULL, bdf2 ? s->vOld2 : NULL);
+            simple_iteration(s, bdf2 ? s->uOld2 : NULL, bdf2 ? s->vOld2 : NULL, bdf2, sOld, sOld2);
             if (k % c->checkConv == 0) {
                 residual_raw(s, &s->cu, s->u, s->resU, s->scaleU, c->resScale[0] == SCALE_DIAG);
                 residual_raw(s, &s->cv, s->v, s->resV, s->scaleV, c->resScale[1] == SCALE_DIAG);
+                /* unsolved scalars keep all-zero systems and residuals */
+                if (c->solveEnergy)
+                    residual_raw(s, &s->ct, s->T, s->resT, s->scaleT, c->scalarResScale[0] == SCALE_DIAG);
+                if (c->solveConcentration)
+                    residual_raw(s, &s->cc, s->C, s->resCc, s->scaleCc, c->scalarResScale[1] == SCALE_DIAG);
                 continuity_residual(s);
                 residual_host(s, c->transient ? k : s->currentIteration);
                 conv = residuals_converged(s);
@@ -1458,6 +1617,8 @@ int orc_run(orc_solver* s, int continueRun, int* converged) {
     compute_gradient(s, &s->bcU, s->u, s->gradUZ, s->gradUR);
     compute_gradient(s, &s->bcV, s->v, s->gradVZ, s->gradVR);
     compute_gradient(s, &s->bcP, s->p, s->gradPZ, s->gradPR);
+    if (c->solveEnergy) compute_gradient(s, &s->bcT, s->T, s->gradTZ, s->gradTR);
+    if (c->solveConcentration) compute_gradient(s, &s->bcC, s->C, s->gradCZ, s->gradCR);
     if (converged) *converged = conv;
     return iters;
 }
@@ -1477,6 +1638,12 @@ static double* field_ptr(const orc_solver* s, const char* name, size_t* len) {
         { "invDPN", s->invDPN, F }, { "wP", s->wP, F }, { "dPB", s->dPB, F }, { "length2D", s->length2D, F },
         { "lsqWZ", s->lsqWZ, F }, { "lsqWR", s->lsqWR, F }, { "invA2D", s->invA2D, N },
         { "lsqInvZZ", s->lsqIZZ, N }, { "lsqInvZR", s->lsqIZR, N }, { "lsqInvRR", s->lsqIRR, N },
+        { "T", s->T, N }, { "C", s->C, N }, { "gradTZ", s->gradTZ, N }, { "gradTR", s->gradTR, N },
+        { "gradCZ", s->gradCZ, N }, { "gradCR", s->gradCR, N },
+        { "AC_T", s->ct.AC, N }, { "b_T", s->ct.b, N }, { "AF_T", s->ct.AF, S }, { "invAC_T", s->ct.invAC, N },
+        { "AC_C", s->cc.AC, N }, { "b_C", s->cc.b, N }, { "AF_C", s->cc.AF, S }, { "invAC_C", s->cc.invAC, N },
+        { "TOld", s->TOld, N }, { "COld", s->COld, N }, { "TOld2", s->TOld2, N }, { "COld2", s->COld2, N },
+        { "res_T", s->resT, N }, { "res_C", s->resCc, N }, { "cw", s->cw, F }, { "ocrWall", s->ocrWall, F },
     };
     for (size_t i = 0; i < sizeof(t) / sizeof(t[0]); i++)
         if (strcmp(t[i].n, name) == 0) { *len = t[i].l; return t[i].p; }
@@ -1501,6 +1668,11 @@ int orc_set(orc_solver* s, const char* name, const double* in, size_t n) {
 
 void orc_last_residuals(const orc_solver* s, double out[3]) {
     for (int i = 0; i < 3; i++) out[i] = s->resVal[i];
+}
+
+void orc_scalar_residuals(const orc_solver* s, double out[2]) {
+    out[0] = s->resValS[0];
+    out[1] = s->resValS[1];
 }
 
 int orc_iterations(const orc_solver* s) { return s->currentIteration; }
@@ -1533,9 +1705,12 @@ void orc_destroy(orc_solver* s) {
     free(s->nZ); free(s->nR); free(s->fcZ); free(s->fcR); free(s->area); free(s->ccZ); free(s->ccR); free(s->vol);
     free(s->invDPN); free(s->wP); free(s->dPB); free(s->invA2D); free(s->length2D);
     free(s->lsqWZ); free(s->lsqWR); free(s->lsqIZZ); free(s->lsqIZR); free(s->lsqIRR); free(s->slotNb);
-    free_bc(&s->bcU); free_bc(&s->bcV); free_bc(&s->bcP); free_bc(&s->bcPP);
-    coeffs* cs[3] = { &s->cu, &s->cv, &s->cpp };
-    for (int i = 0; i < 3; i++) { free(cs[i]->AC); free(cs[i]->b); free(cs[i]->invAC); free(cs[i]->AF); }
+    free_bc(&s->bcU); free_bc(&s->bcV); free_bc(&s->bcP); free_bc(&s->bcPP); free_bc(&s->bcT); free_bc(&s->bcC);
+    coeffs* cs[5] = { &s->cu, &s->cv, &s->cpp, &s->ct, &s->cc };
+    for (int i = 0; i < 5; i++) { free(cs[i]->AC); free(cs[i]->b); free(cs[i]->invAC); free(cs[i]->AF); }
+    double* sc[] = { s->T, s->C, s->TTemp, s->CTemp, s->TOld, s->COld, s->TOld2, s->COld2, s->gradTZ, s->gradTR,
+                     s->gradCZ, s->gradCR, s->resT, s->resCc, s->scaleT, s->scaleCc, s->cw, s->ocrWall };
+    for (size_t i = 0; i < sizeof(sc) / sizeof(sc[0]); i++) free(sc[i]);
     free(s->u); free(s->v); free(s->p); free(s->pp); free(s->uTemp); free(s->vTemp); free(s->ppTemp);
     free(s->DU); free(s->DV); free(s->gradPZ); free(s->gradPR); free(s->gradUZ); free(s->gradUR);
     free(s->gradVZ); free(s->gradVR); free(s->uOld); free(s->vOld); free(s->uOld2); free(s->vOld2);

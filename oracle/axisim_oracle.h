@@ -59,6 +59,16 @@ typedef struct orc_bc_field {
     const uint8_t* pulsatileByGroup;
     const double* amplitudeByGroup;
     const double* frequencyByGroup;
+    /* Michaelis-Menten / Hill wall kinetics per group (BoundaryFieldHost
+     * vmax..Rtot, solver_struct.h:469-475, filled by memory_manger.cpp:110-145);
+     * NULL = the defaults vmax = km = k2 = v2 = Rtot = 0, n = m = 1. */
+    const double* vmaxByGroup;
+    const double* kmByGroup;
+    const double* nByGroup;
+    const double* mByGroup;
+    const double* k2ByGroup;
+    const double* v2ByGroup;
+    const double* RtotByGroup;
 } orc_bc_field;
 
 /* Flattened ConfigSolver / ConfigSimple / ConfigMultigrid / ConfigResidual /
@@ -97,6 +107,20 @@ typedef struct orc_config {
     int resScale[3];
     int resEnabled[3];
     double resTol[3];
+    /* scalar transport: SolverFieldOption (solver_struct.h:9-12), the
+     * FluidPropertyConfig cp, k, D (setting.cuh:61-71) and the ConfigResidual
+     * entries "Temperature", "Concentration" (index 0 T, 1 C) */
+    int solveEnergy;
+    int solveConcentration;
+    double cp;
+    double k;
+    double D;
+    int scalarResNorm[2];
+    int scalarResScale[2];
+    int scalarResEnabled[2];
+    double scalarResTol[2];
+    /* Mesh::currentMeshType == Structured (boundary_struct.h:382-385) */
+    int structuredMesh;
 } orc_config;
 
 typedef struct orc_solver orc_solver;
@@ -128,16 +152,26 @@ void orc_mb_free(orc_packed* p);
 orc_solver* orc_create(const orc_mesh* mesh, const orc_bc_field* bcU,
                        const orc_bc_field* bcV, const orc_bc_field* bcP,
                        const orc_config* cfg);
+/* The same with the temperature and concentration boundary fields (each may be
+ * NULL when cfg does not solve that field). */
+orc_solver* orc_create_ex(const orc_mesh* mesh, const orc_bc_field* bcU,
+                          const orc_bc_field* bcV, const orc_bc_field* bcP,
+                          const orc_bc_field* bcT, const orc_bc_field* bcC,
+                          const orc_config* cfg);
 /* Runs Solver::runSimple's time + SIMPLE loops (solver.cpp:1034-1298).
  * Returns the SIMPLE iterations executed; *converged set if the residual test
  * passed. continueRun keeps currentIteration / continuity scale / time offset. */
 int orc_run(orc_solver* s, int continueRun, int* converged);
 /* Fields: u v p pp mDot DU DV gradPZ gradPR gradUZ gradUR gradVZ gradVR
- *         AC_u b_u AF_u invAC_u (and _v, _pp) res_U res_V res_Continuity */
+ *         AC_u b_u AF_u invAC_u (and _v, _pp) res_U res_V res_Continuity
+ *         T C gradTZ gradTR gradCZ gradCR AC_T b_T AF_T invAC_T (and _C)
+ *         TOld COld TOld2 COld2 res_T res_C cw ocrWall (per face) */
 int orc_get(const orc_solver* s, const char* name, double* out, size_t n);
 int orc_set(orc_solver* s, const char* name, const double* in, size_t n);
 /* residual history: resVal for U, V, Continuity of the last check */
 void orc_last_residuals(const orc_solver* s, double out[3]);
+/* resVal of the Temperature and Concentration entries of the last check */
+void orc_scalar_residuals(const orc_solver* s, double out[2]);
 int orc_iterations(const orc_solver* s);
 /* multigrid hierarchy description: level count and cells per level */
 int orc_mg_levels(const orc_solver* s, int32_t* cellsPerLevel, int maxLevels);

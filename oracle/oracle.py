@@ -32,7 +32,9 @@ class OrcBC(C.Structure):
     _fields_ = [("nGroups", C.c_int32), ("typeByGroup", _u8p), ("boundaryTypeByGroup", _u8p),
                 ("valueByGroup", _f64p), ("lengthByGroup", _f64p),
                 ("pulsatileByGroup", _u8p), ("amplitudeByGroup", _f64p),
-                ("frequencyByGroup", _f64p)]
+                ("frequencyByGroup", _f64p), ("vmaxByGroup", _f64p), ("kmByGroup", _f64p),
+                ("nByGroup", _f64p), ("mByGroup", _f64p), ("k2ByGroup", _f64p), ("v2ByGroup", _f64p),
+                ("RtotByGroup", _f64p)]
 
 
 class OrcConfig(C.Structure):
@@ -43,7 +45,11 @@ class OrcConfig(C.Structure):
                 ("mgMaxIter", C.c_int), ("mgWeight", C.c_double), ("mgLinearSweep", C.c_int),
                 ("mgPreSweep", C.c_int), ("mgPostSweep", C.c_int), ("rho", C.c_double), ("mu", C.c_double),
                 ("alphaU", C.c_double), ("alphaP", C.c_double), ("resNorm", C.c_int * 3),
-                ("resScale", C.c_int * 3), ("resEnabled", C.c_int * 3), ("resTol", C.c_double * 3)]
+                ("resScale", C.c_int * 3), ("resEnabled", C.c_int * 3), ("resTol", C.c_double * 3),
+                ("solveEnergy", C.c_int), ("solveConcentration", C.c_int), ("cp", C.c_double),
+                ("k", C.c_double), ("D", C.c_double), ("scalarResNorm", C.c_int * 2),
+                ("scalarResScale", C.c_int * 2), ("scalarResEnabled", C.c_int * 2),
+                ("scalarResTol", C.c_double * 2), ("structuredMesh", C.c_int)]
 
 
 class OrcBlock(C.Structure):
@@ -76,6 +82,9 @@ def lib():
         L.orc_create.restype = C.c_void_p
         L.orc_create.argtypes = [C.POINTER(OrcMesh), C.POINTER(OrcBC), C.POINTER(OrcBC),
                                  C.POINTER(OrcBC), C.POINTER(OrcConfig)]
+        L.orc_create_ex.restype = C.c_void_p
+        L.orc_create_ex.argtypes = [C.POINTER(OrcMesh)] + [C.POINTER(OrcBC)] * 5 + [C.POINTER(OrcConfig)]
+        L.orc_scalar_residuals.argtypes = [C.c_void_p, _f64p]
         L.orc_run.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
         L.orc_get.argtypes = [C.c_void_p, C.c_char_p, _f64p, C.c_size_t]
         L.orc_set.argtypes = [C.c_void_p, C.c_char_p, _f64p, C.c_size_t]
@@ -122,6 +131,7 @@ def multiblock(blocks, tol=1e-9, default_group=-1):
     L.orc_mb_copy(h, *[m[k].ctypes.data_as(C.c_void_p) for k in keys])
     L.orc_mb_free(h)
     m["status"] = st.value
+    m["meshType"] = 0  # MeshType::Structured
     return m
 
 
@@ -140,8 +150,12 @@ def mesh_struct(m):
     return s, keep
 
 
+KINETICS_KEYS = ("vmax", "km", "n", "m", "k2", "v2", "Rtot")
+
+
 def bc_struct(bc):
-    """bc: dict type(u8[G]) btype(u8[G]) value(f64[G]) length(f64[G]) [puls amp freq]"""
+    """bc: dict type(u8[G]) btype(u8[G]) value(f64[G]) length(f64[G]) [puls amp freq]
+    [vmax km n m k2 v2 Rtot] (the wall-kinetics arrays of a scalar field)"""
     keep = []
 
     def P(k, t, dt):
@@ -153,7 +167,7 @@ def bc_struct(bc):
     G = len(bc["type"])
     s = OrcBC(G, P("type", _u8p, np.uint8), P("btype", _u8p, np.uint8), P("value", _f64p, np.float64),
               P("length", _f64p, np.float64), P("puls", _u8p, np.uint8), P("amp", _f64p, np.float64),
-              P("freq", _f64p, np.float64))
+              P("freq", _f64p, np.float64), *[P(k, _f64p, np.float64) for k in KINETICS_KEYS])
     return s, keep
 
 
@@ -164,6 +178,10 @@ def config_struct(cfg):
             setattr(c, k, (C.c_int * 3)(*v))
         elif k == "resTol":
             setattr(c, k, (C.c_double * 3)(*v))
+        elif k in ("scalarResNorm", "scalarResScale", "scalarResEnabled"):
+            setattr(c, k, (C.c_int * 2)(*v))
+        elif k == "scalarResTol":
+            setattr(c, k, (C.c_double * 2)(*v))
         else:
             setattr(c, k, v)
     return c
@@ -177,11 +195,12 @@ class Oracle:
         if threads:
             L.orc_set_threads(threads)
         self._ms, self._mk = mesh_struct(mesh)
-        self._b = [bc_struct(bcs[k]) for k in ("u", "v", "p")]
-        self._cfg = config_struct(cfg)
+        self._b = [bc_struct(bcs[k]) if k in bcs else None for k in ("u", "v", "p", "T", "C")]
+        # Mesh::currentMeshType: multiblock meshes are structured
+        self._cfg = config_struct(dict(cfg, structuredMesh=int(mesh.get("meshType", 1) == 0)))
         self.mesh = mesh
-        self.h = L.orc_create(C.byref(self._ms), C.byref(self._b[0][0]), C.byref(self._b[1][0]),
-                              C.byref(self._b[2][0]), C.byref(self._cfg))
+        ref = [C.byref(b[0]) if b is not None else None for b in self._b]
+        self.h = L.orc_create_ex(C.byref(self._ms), *ref, C.byref(self._cfg))
         if not self.h:
             raise RuntimeError("orc_create failed")
 
@@ -208,6 +227,11 @@ class Oracle:
     def residuals(self):
         out = np.zeros(3)
         lib().orc_last_residuals(self.h, out.ctypes.data_as(_f64p))
+        return out
+
+    def scalar_residuals(self):
+        out = np.zeros(2)
+        lib().orc_scalar_residuals(self.h, out.ctypes.data_as(_f64p))
         return out
 
     def iterations(self):

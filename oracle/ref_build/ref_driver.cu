@@ -26,7 +26,8 @@
 #include "solver_struct.h"
 
 void ResidualPlot::add(int currentIteration, const std::unordered_map<std::string, ConfigResidual>& cfg) {
-    Row r{currentIteration, *cfg.at("U").resVal, *cfg.at("V").resVal, *cfg.at("Continuity").resVal};
+    Row r{currentIteration, *cfg.at("U").resVal, *cfg.at("V").resVal, *cfg.at("Continuity").resVal,
+          *cfg.at("Temperature").resVal, *cfg.at("Concentration").resVal};
     rows.push_back(r);
 }
 
@@ -54,7 +55,15 @@ BoundaryCondition makeBC(int type, double value, double amp, double freq) {
 BoundaryVariable varOf(const std::string& v) {
     if (v == "u") return BoundaryVariable::UVelocity;
     if (v == "v") return BoundaryVariable::VVelocity;
+    if (v == "T") return BoundaryVariable::StaticTemperature;
+    if (v == "C") return BoundaryVariable::Concentration;
     return BoundaryVariable::Pressure;
+}
+
+BoundarySegmentGroup* groupOf(Mesh& mesh, int id) {
+    for (BoundarySegmentGroup& g : mesh.boundaryGroups)
+        if (g.id == id) return &g;
+    return nullptr;
 }
 
 }  // namespace
@@ -104,6 +113,37 @@ int main(int argc, char** argv) {
                 g.bcs[varOf(var)] = makeBC(type, value, amp, freq);
             }
             mesh.boundaryGroups.push_back(g);
+        } else if (key == "kin") {
+            // kin <group> <var> <3 MM | 4 Hill> <Vmax> <Km> <n> <inhibition> <m> <K2> <V2>
+            int id, type, inhib;
+            std::string var;
+            double vmax, km, n, m, k2, v2;
+            in >> id >> var >> type >> vmax >> km >> n >> inhib >> m >> k2 >> v2;
+            BoundarySegmentGroup* g = groupOf(mesh, id);
+            if (!g) return 2;
+            BoundaryCondition bc{};
+            if (type == 3) {
+                MichaelisMentenParams p;
+                p.Vmax = vmax; p.Km = km; p.inhibition = inhib != 0; p.m = m; p.K2 = k2; p.V2 = v2;
+                bc.params = p;
+            } else {
+                HillParams p;
+                p.Vmax = vmax; p.Km = km; p.n = n; p.inhibition = inhib != 0; p.m = m; p.K2 = k2; p.V2 = v2;
+                bc.params = p;
+            }
+            g->bcs[varOf(var)] = bc;
+        } else if (key == "layer") {
+            // layer <group> <var> <k> <d>
+            int id;
+            std::string var;
+            double k, d;
+            in >> id >> var >> k >> d;
+            BoundarySegmentGroup* g = groupOf(mesh, id);
+            if (!g) return 2;
+            Layer l{};
+            l.k = k;
+            l.d = d;
+            g->layers[varOf(var)].push_back(l);
         } else if (key == "set") {
             std::string name;
             double value;
@@ -168,11 +208,16 @@ int main(int argc, char** argv) {
         else if (name == "mgPostSweep") solver.configMultigrid.linearPostSweep = (int)v;
         else if (name == "rho") solver.f.rho = v;
         else if (name == "mu") solver.f.mu = v;
+        else if (name == "cp") solver.f.cp = v;
+        else if (name == "k") solver.f.k = v;
+        else if (name == "D") solver.f.D = v;
+        else if (name == "solveEnergy") solver.fieldOption.solveEnergy = v != 0;
+        else if (name == "solveConcentration") solver.fieldOption.solveConcentration = v != 0;
         else if (name == "alphaU") solver.simple.momentumRelaxation = v;
         else if (name == "alphaP") solver.simple.pressureRelaxation = v;
         else {
-            const char* names[3] = {"U", "V", "Continuity"};
-            for (int i = 0; i < 3; i++) {
+            const char* names[5] = {"U", "V", "Continuity", "Temperature", "Concentration"};
+            for (int i = 0; i < 5; i++) {
                 ConfigResidual& r = solver.cfg.at(names[i]);
                 const std::string sfx = std::to_string(i);
                 if (name == "resNorm" + sfx) r.normType = (ResidualNormType)(int)v;
@@ -206,8 +251,20 @@ int main(int argc, char** argv) {
         std::fwrite(f.data(), sizeof(double), (size_t)N, out);
     }
     for (const ResidualPlot::Row& r : plot.rows) {
-        const double row[4] = {(double)r.iteration, r.u, r.v, r.continuity};
-        std::fwrite(row, sizeof(double), 4, out);
+        const double row[6] = {(double)r.iteration, r.u, r.v, r.continuity, r.temperature, r.concentration};
+        std::fwrite(row, sizeof(double), 6, out);
+    }
+    // scalar fields of the solved scalars (flags, then each field's value and gradients)
+    const int32_t flags[2] = {solver.fieldOption.solveEnergy ? 1 : 0, solver.fieldOption.solveConcentration ? 1 : 0};
+    std::fwrite(flags, sizeof(int32_t), 2, out);
+    const char* tFields[] = {"Temperature", "dT/dz", "dT/dr"};
+    const char* cFields[] = {"Concentration", "dC/dz", "dC/dr"};
+    for (int sIdx = 0; sIdx < 2; sIdx++) {
+        if (!flags[sIdx]) continue;
+        for (const char* name : (sIdx == 0 ? tFields : cFields)) {
+            const std::vector<double>& f = solver.solutions.at(name).field;
+            std::fwrite(f.data(), sizeof(double), (size_t)N, out);
+        }
     }
     std::fclose(out);
     std::printf("reference solver: %d cells, %d iterations, converged %d, %.3f ms\n", N, iterations, converged,

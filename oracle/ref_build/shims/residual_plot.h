@@ -11,7 +11,7 @@ class ResidualPlot {
 public:
     struct Row {
         int iteration;
-        double u, v, continuity;
+        double u, v, continuity, temperature, concentration;
     };
     std::vector<Row> rows;
     void resetState() { rows.clear(); }

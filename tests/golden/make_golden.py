@@ -21,7 +21,7 @@ sys.path.insert(0, os.path.join(ROOT, "axisim-software_b200"))
 from axisim import cases  # noqa: E402
 
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "axisim_ref")
-VAR_NAMES = {cases.U: "u", cases.V: "v", cases.P: "p"}
+VAR_NAMES = {cases.U: "u", cases.V: "v", cases.P: "p", cases.TEMP: "T", cases.CONC: "C"}
 
 
 def fixture_cases():
@@ -43,6 +43,33 @@ def fixture_cases():
     out.append(("pulsatile864_bdf2_3x3", c))
     c = cases.pipe(max_iter=50000, tol=1e-6)
     out.append(("pipe40x200_config1_converged", c))
+    out += scalar_fixture_cases()
+    return out
+
+
+def scalar_fixture_cases():
+    """Energy + concentration transport: Michaelis-Menten wall behind a layer
+    (GS sweeps, upwind), Hill wall with substrate inhibition (Jacobi, SOU,
+    non-integer exponents; the corrector flag is set and, on this structured
+    mesh, cleared by runCheck), a BDF2 pulsatile run with both scalars, and a
+    run to convergence."""
+    out = []
+    c = cases.with_scalars(cases.pipe(nr=10, nz=50, max_iter=10, tol=1e-30), wall_c=cases.michaelis_menten(1e-3, 0.2),
+                           wall_layers=[(1e-6, 1e-4)], D=1e-6)
+    c.settings.update(scalarResEnabled=[1, 1], scalarResTol=[1e-30, 1e-30])
+    out.append(("pipe10x50_scalars_mm_10it", c))
+    c = cases.with_scalars(cases.expansion(scale=1 / 32, max_iter=6, tol=1e-30),
+                           wall_c=cases.hill(2e-3, 0.4, 2.5, inhibition=(2.0, 0.5, 0.3)), t_wall=None, D=2e-6,
+                           k=0.6e2)
+    c.settings.update(scalarResEnabled=[1, 0], scalarResNorm=[1, 0], useNonOrthCorrector=1)
+    out.append(("expansion864_scalars_hill_sou_6it", c))
+    c = cases.with_scalars(cases.pulsatile_expansion(scale=1 / 32, dt=1e-3, steps=3, max_iter=3, tol=1e-30),
+                           wall_c=cases.michaelis_menten(1e-3, 0.2), D=1e-6)
+    out.append(("pulsatile864_bdf2_scalars_3x3", c))
+    c = cases.with_scalars(cases.pipe(nr=10, nz=50, max_iter=5000, tol=1e-6), wall_c=cases.michaelis_menten(1e-3, 0.2),
+                           wall_layers=[(1e-6, 1e-4)], D=1e-6)
+    c.settings.update(scalarResEnabled=[1, 1], scalarResTol=[1e-6, 1e-6])
+    out.append(("pipe10x50_scalars_mm_converged", c))
     return out
 
 
@@ -57,18 +84,35 @@ def write_spec(case, path, tol=1e-9):
             items = []
             for var, bc in g.bcs.items():
                 t, val = bc[0], bc[1]
+                if t in (cases.MICHAELIS_MENTEN, cases.HILL):
+                    val = 0.0  # parameters follow on a kin line
                 amp, freq = (bc[2], bc[3]) if len(bc) > 2 else (0.0, 0.0)
                 items.append(f"{VAR_NAMES[var]} {t} {val!r} {amp!r} {freq!r}")
             f.write(f"group {g.id} {g.btype} {float(np.float32(g.total_length))!r} {len(items)} {' '.join(items)}\n")
+        for g in case.groups:
+            for var, bc in g.bcs.items():
+                if bc[0] in (cases.MICHAELIS_MENTEN, cases.HILL):
+                    k = bc[1]
+                    inh = k.get("inhibition")
+                    m, k2, v2 = inh if inh else (1.0, 0.0, 0.0)
+                    f.write(f"kin {g.id} {VAR_NAMES[var]} {bc[0]} {k['Vmax']!r} {k['Km']!r} {k['n']!r} "
+                            f"{1 if inh else 0} {m!r} {k2!r} {v2!r}\n")
+            for var, layers in g.layers.items():
+                for (kl, dl) in layers:
+                    f.write(f"layer {g.id} {VAR_NAMES[var]} {kl!r} {dl!r}\n")
         s = case.settings
         for k in ("convectionScheme", "gradientScheme", "linearType", "timeScheme", "linearMaxIter", "useMultigrid",
                   "addConvectionTerm", "transient", "useNonOrthCorrector", "dt", "tEnd", "maxIter", "checkConv",
                   "mgMaxIter", "mgWeight", "mgLinearSweep", "mgPreSweep", "mgPostSweep", "rho", "mu", "alphaU",
-                  "alphaP"):
+                  "alphaP", "cp", "k", "D", "solveEnergy", "solveConcentration"):
             f.write(f"set {k} {float(s[k])!r}\n")
         for i in range(3):
             f.write(f"set resNorm{i} {s['resNorm'][i]}\nset resScale{i} {s['resScale'][i]}\n"
                     f"set resEnabled{i} {s['resEnabled'][i]}\nset resTol{i} {s['resTol'][i]!r}\n")
+        for j in range(2):
+            i = 3 + j
+            f.write(f"set resNorm{i} {s['scalarResNorm'][j]}\nset resScale{i} {s['scalarResScale'][j]}\n"
+                    f"set resEnabled{i} {s['scalarResEnabled'][j]}\nset resTol{i} {s['scalarResTol'][j]!r}\n")
 
 
 FIELDS = ["u", "v", "p", "continuity", "gradPZ", "gradPR", "gradUZ", "gradUR", "gradVZ", "gradVR"]
@@ -82,7 +126,17 @@ def read_out(path):
     for name in FIELDS:
         out[name] = np.frombuffer(raw[off:off + 8 * N], dtype=np.float64).copy()
         off += 8 * N
-    out["residual_history"] = np.frombuffer(raw[off:off + 32 * rows], dtype=np.float64).reshape(rows, 4).copy()
+    # iteration, U, V, Continuity, Temperature, Concentration
+    out["residual_history"] = np.frombuffer(raw[off:off + 48 * rows], dtype=np.float64).reshape(rows, 6).copy()
+    off += 48 * rows
+    flags = np.frombuffer(raw[off:off + 8], dtype=np.int32)
+    off += 8
+    for on, names in zip(flags, (("T", "gradTZ", "gradTR"), ("C", "gradCZ", "gradCR"))):
+        if not on:
+            continue
+        for name in names:
+            out[name] = np.frombuffer(raw[off:off + 8 * N], dtype=np.float64).copy()
+            off += 8 * N
     return out
 
 
@@ -98,8 +152,11 @@ def run_reference(case):
         return res
 
 
-def main(outdir=HERE):
+def main(outdir=HERE, only=""):
+    """Regenerates every fixture whose name contains `only`."""
     for name, case in fixture_cases():
+        if only not in name:
+            continue
         res = run_reference(case)
         keep = {k: v for k, v in res.items() if k not in ("log",)}
         if name.startswith("pipe40x200"):

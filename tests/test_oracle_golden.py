@@ -5,7 +5,10 @@ reference's solver translation units compiled unchanged from their sources
 (oracle/ref_build) on a B200. The reference sums its multigrid Galerkin and
 restriction with atomicAdd and contracts a*b+c into FMA, so agreement is to
 rounding: 1e-10 relative L2 on u, v, p and the gradients, and the same
-iteration count (also to convergence at 1e-6).
+iteration count (also to convergence at 1e-6). The scalar-transport fixtures
+add temperature and concentration with their gradients; the reference's Hill
+and inhibition laws call CUDA's pow where the oracle calls the C library's,
+so those agree to rounding as well.
 """
 import os
 
@@ -22,7 +25,8 @@ import make_golden  # noqa: E402
 
 CASES = make_golden.fixture_cases()
 ORACLE_NAMES = {"u": "u", "v": "v", "p": "p", "gradPZ": "gradPZ", "gradPR": "gradPR", "gradUZ": "gradUZ",
-                "gradUR": "gradUR", "gradVZ": "gradVZ", "gradVR": "gradVR"}
+                "gradUR": "gradUR", "gradVZ": "gradVZ", "gradVR": "gradVR", "T": "T", "gradTZ": "gradTZ",
+                "gradTR": "gradTR", "C": "C", "gradCZ": "gradCZ", "gradCR": "gradCR"}
 TOL = 1e-10
 
 
@@ -41,10 +45,17 @@ def test_oracle_matches_reference_solver(name, case):
         # per-cell mass imbalance after the last iteration (Solver::getMassImbalance)
         scale = np.abs(o.get("mDot")).max()
         assert np.max(np.abs(o.get("res_Continuity") - g["continuity"])) <= 1e-9 * scale
-    # the monitored residual history (U, V, Continuity) of the reference
+    # the monitored residual history (U, V, Continuity[, Temperature, Concentration]) of the reference
     hist = g["residual_history"]
     assert hist.shape[0] == it
-    np.testing.assert_allclose(o.residuals(), hist[-1, 1:], rtol=1e-6)
+    np.testing.assert_allclose(o.residuals(), hist[-1, 1:4], rtol=1e-6)
+    if hist.shape[1] == 6:
+        s = case.settings
+        solved = (s["solveEnergy"], s["solveConcentration"])
+        for e in range(2):
+            if s["scalarResEnabled"][e] and solved[e]:
+                # scaled residuals at rounding level (1e-16) carry no digits to compare
+                np.testing.assert_allclose(o.scalar_residuals()[e], hist[-1, 4 + e], rtol=1e-6, atol=1e-12)
 
 
 def test_fixture_cases_are_small():
