@@ -38,7 +38,11 @@ EXPORTS = [
     "axisim_learned_harvest", "axisim_learned_sample_count", "axisim_learned_add_sample",
     "axisim_learned_get_sample", "axisim_learned_init", "axisim_learned_params", "axisim_learned_grad",
     "axisim_learned_train", "axisim_learned_enable", "axisim_learned_stats", "axisim_learned_predict",
+    "axisim_set_kinetics", "axisim_set_scalars", "axisim_scalar_residuals", "axisim_set_mesh_type",
 ]
+VAR_U, VAR_V, VAR_P, VAR_T, VAR_C = range(5)
+VAR_INDEX = {"u": VAR_U, "v": VAR_V, "p": VAR_P, "T": VAR_T, "C": VAR_C}
+MESH_STRUCTURED, MESH_UNSTRUCTURED = 0, 1
 
 
 class MeshPacked(C.Structure):
@@ -56,6 +60,11 @@ class BCField(C.Structure):
     _fields_ = [("nGroups", C.c_int32), ("typeByGroup", _u8p), ("boundaryTypeByGroup", _u8p),
                 ("valueByGroup", _f64p), ("lengthByGroup", _f64p), ("pulsatileByGroup", _u8p),
                 ("amplitudeByGroup", _f64p), ("frequencyByGroup", _f64p)]
+
+
+class Kinetics(C.Structure):
+    _fields_ = [("nGroups", C.c_int32), ("vmaxByGroup", _f64p), ("kmByGroup", _f64p), ("nByGroup", _f64p),
+                ("mByGroup", _f64p), ("k2ByGroup", _f64p), ("v2ByGroup", _f64p), ("RtotByGroup", _f64p)]
 
 
 class ConfigSolver(C.Structure):
@@ -135,6 +144,10 @@ def lib():
                                             C.POINTER(ConfigMultigrid), C.POINTER(ConfigResidual),
                                             C.c_double, C.c_double]),
             "axisim_set_fluid": (C.c_int, [vp, C.POINTER(Fluid)]),
+            "axisim_set_kinetics": (C.c_int, [vp, C.c_int32, C.POINTER(Kinetics)]),
+            "axisim_set_scalars": (C.c_int, [vp, C.c_int32, C.c_int32, C.POINTER(ConfigResidual)]),
+            "axisim_scalar_residuals": (C.c_int, [vp, _f64p]),
+            "axisim_set_mesh_type": (C.c_int, [vp, C.c_int32]),
             "axisim_set_precision": (C.c_int, [vp, C.c_int32]),
             "axisim_set_pressure_solver": (C.c_int, [vp, C.c_int32, C.c_double, C.c_double]),
             "axisim_pressure_stats": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
@@ -210,7 +223,7 @@ def multiblock(blocks, tol=1e-9, default_group=-1):
     L.axisim_mesh_view(h, C.byref(v))
     n, f = v.nCells, v.nFaces
     r = v.cellFaceStart[n]
-    m = {"nCells": n, "nFaces": f, "status": seam.value}
+    m = {"nCells": n, "nFaces": f, "status": seam.value, "meshType": MESH_STRUCTURED}
     sizes = dict(faceOwner=f, faceNeighbor=f, faceNormalZ=f, faceNormalR=f, faceCenterZ=f, faceCenterR=f,
                  faceArea=f, faceBoundaryGroupID=f, cellCenterZ=n, cellCenterR=n, cellArea2D=n, cellVolume=n,
                  cellFaceStart=n + 1, cellFaceIDs=r)
@@ -266,6 +279,24 @@ def bc_struct(bc):
     return s, keep
 
 
+KINETICS_KEYS = ("vmax", "km", "n", "m", "k2", "v2", "Rtot")
+
+
+def kinetics_struct(bc):
+    """The wall-kinetics arrays of a scalar's boundary field (None when it has none)."""
+    if not any(k in bc for k in KINETICS_KEYS):
+        return None, []
+    keep = []
+
+    def P(k):
+        if k not in bc or bc[k] is None:
+            return None
+        a = np.ascontiguousarray(bc[k], dtype=np.float64)
+        keep.append(a)
+        return a.ctypes.data_as(_f64p)
+    return Kinetics(len(bc["type"]), *[P(k) for k in KINETICS_KEYS]), keep
+
+
 def settings_structs(s):
     cs = ConfigSolver()
     cs.velocitySolver = 0
@@ -286,8 +317,20 @@ def settings_structs(s):
     res = (ConfigResidual * 3)()
     for i in range(3):
         res[i] = ConfigResidual(0, s["resNorm"][i], s["resScale"][i], s["resEnabled"][i], s["resTol"][i])
-    fluid = Fluid(s["rho"], s["mu"], 4180.0, 0.6, 3.0277e-9)
+    fluid = Fluid(s["rho"], s["mu"], s.get("cp", 4180.0), s.get("k", 0.6), s.get("D", 3.0277e-9))
     return cs, sim, mg, res, fluid
+
+
+def scalar_residual_structs(s):
+    """The Temperature / Concentration ConfigResidual entries of a settings dict."""
+    res = (ConfigResidual * 2)()
+    norm = s.get("scalarResNorm", [0, 0])
+    scale = s.get("scalarResScale", [3, 3])
+    en = s.get("scalarResEnabled", [0, 0])
+    tol = s.get("scalarResTol", [1e-3, 1e-3])
+    for i in range(2):
+        res[i] = ConfigResidual(0, norm[i], scale[i], en[i], tol[i])
+    return res
 
 
 class Solver:
@@ -306,11 +349,22 @@ class Solver:
         self._residual_log = []
         ms, keep = mesh_struct(mesh)
         self._check(L.axisim_set_mesh(self.h, C.byref(ms)))
-        for var, key in enumerate(("u", "v", "p")):
+        # Mesh::currentMeshType (a packed mesh without the key counts as unstructured)
+        self._check(L.axisim_set_mesh_type(self.h, int(mesh.get("meshType", MESH_UNSTRUCTURED))))
+        for key in ("u", "v", "p", "T", "C"):
+            if key not in bcs:
+                continue
             b, keep2 = bc_struct(bcs[key])
-            self._check(L.axisim_set_bc(self.h, var, C.byref(b)))
+            self._check(L.axisim_set_bc(self.h, VAR_INDEX[key], C.byref(b)))
+            kin, keep3 = kinetics_struct(bcs[key])
+            if kin is not None:
+                self._check(L.axisim_set_kinetics(self.h, VAR_INDEX[key], C.byref(kin)))
         self._check(L.axisim_set_config(self.h, C.byref(cs), C.byref(sim), C.byref(mg), res,
                                         settings["alphaU"], settings["alphaP"]))
+        if settings.get("solveEnergy") or settings.get("solveConcentration"):
+            self._check(L.axisim_set_scalars(self.h, int(bool(settings.get("solveEnergy"))),
+                                             int(bool(settings.get("solveConcentration"))),
+                                             scalar_residual_structs(settings)))
         if precision != PREC_FP64:
             self._check(L.axisim_set_precision(self.h, precision))
         if pressure_solver != PSOLVE_VCYCLES:
@@ -328,6 +382,12 @@ class Solver:
             self._check(st)
         return dict(status=st, iterations=r.iterations, total=r.totalIterations, converged=bool(r.converged),
                     steps=r.timeSteps, residual=list(r.residual), ms=r.solveMs)
+
+    def scalar_residuals(self):
+        """Temperature and Concentration residuals of the last check."""
+        out = np.zeros(2)
+        self._check(lib().axisim_scalar_residuals(self.h, out.ctypes.data_as(_f64p)))
+        return out
 
     def get(self, name):
         n = max(self.mesh["nCells"], self.mesh["nFaces"], len(self.mesh["cellFaceIDs"]))
@@ -383,8 +443,10 @@ class Solver:
         triangles: (points, tris) of an unstructured one."""
         from . import export
         s = self.settings
-        fluid = {"rho": s["rho"], "mu": s["mu"], "cp": 4180.0, "k": 0.6, "D": 3.0277e-9}
-        sols = export.solutions_from(self.get, self.mesh, fluid)
+        fluid = {"rho": s["rho"], "mu": s["mu"], "cp": s.get("cp", 4180.0), "k": s.get("k", 0.6),
+                 "D": s.get("D", 3.0277e-9)}
+        sols = export.solutions_from(self.get, self.mesh, fluid, energy=bool(s.get("solveEnergy")),
+                                     concentration=bool(s.get("solveConcentration")))
         kw.setdefault("transient", bool(s.get("transient", 0)))
         kw.setdefault("dt", s.get("dt", 0.0))
         q = export.quad_corners(self.mesh) if quads and triangles is None else None

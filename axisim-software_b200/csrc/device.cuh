@@ -82,6 +82,9 @@ struct BCDev {
     const uint8_t* type = nullptr;
     const double* value = nullptr;
     const double* length = nullptr;
+    // wall kinetics of a transported scalar, [9][nGroups]: Vmax, Km, n, m, K2,
+    // V2, Rtot, Km^n, K2^m (null for u, v, p)
+    const double* kin = nullptr;
 };
 
 // Control block: one per solver, in device memory. Kernels of an iteration
@@ -106,7 +109,7 @@ struct Ctl {
     int resScale[3];
     int resEnabled[3];
     int histCount;        // entries written since the host last drained
-    double hist[kMaxHist][4];  // iteration, U, V, Continuity
+    double hist[kMaxHist][6];  // iteration, U, V, Continuity, Temperature, Concentration
     // batch of independent cases packed into one mesh (nCases = 0: one case)
     int nCases;
     int casesConverged;
@@ -117,6 +120,39 @@ struct Ctl {
     int ppPad;
     long long ppSolves;      // Krylov solves started
     long long ppIterations;  // Krylov iterations completed
+    // monitored residuals of the transported scalars (0 Temperature, 1 Concentration)
+    double resValS[2];
+    double scaleValS[2];
+    double tolS[2];
+    int resNormS[2];
+    int resScaleS[2];
+    int resEnabledS[2];
+    int solvedS[2];       // the scalar is solved (an unsolved one has an all-zero system)
+};
+
+// One transported scalar (energy or concentration) in the fused assembly.
+struct ScalarDev {
+    BCDev bc;
+    const double* phi;
+    const double* gZ;
+    const double* gR;
+    const double* old;
+    const double* old2;
+    double* AF;  // [W][N]
+    double* AC;
+    double* b;
+    double* inv;
+    double gamma;  // kinematic diffusivity
+    double alpha;  // under-relaxation factor
+};
+
+struct ScalarArgs {
+    ScalarDev s[2];
+    const double* mDot;
+    double* cw;    // wall concentration per face
+    double* ocr;   // wall consumption per face
+    double fluxScale, dt;
+    int conv, scheme, nonOrtho, transient;
 };
 
 // The learned first Krylov step: which p' solves use it, and the running means

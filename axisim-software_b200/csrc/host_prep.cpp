@@ -399,7 +399,9 @@ int greedyColoring(const GridLevel& g, std::vector<int32_t>& color) {
 }
 
 uint8_t defaultBCType(int boundaryType, int variable) {
-    // BCType: 0 DIRICHLET 1 NEUMANN 5 NONE; variables 0 u 1 v 2 p.
+    // BCType: 0 DIRICHLET 1 NEUMANN 5 NONE; variables 0 u 1 v 2 p 3 T 4 C.
+    // The scalars are Dirichlet at a velocity inlet, zero-gradient elsewhere.
+    if (variable == 3 || variable == 4) return (boundaryType == 1) ? 0 : (boundaryType >= 0 && boundaryType <= 4) ? 1 : 5;
     switch (boundaryType) {
         case 1:  // VELOCITY_INLET
             return variable == 2 ? 1 : 0;
@@ -417,12 +419,13 @@ uint8_t defaultBCType(int boundaryType, int variable) {
 }
 
 bool variableEditable(int variable, int boundaryType) {
+    const bool scalar = variable == 3 || variable == 4;
     switch (boundaryType) {
-        case 0: return variable == 0 || variable == 1;
+        case 0: return variable == 0 || variable == 1 || scalar;
         case 3: return false;
         case 4: return variable == 0 || variable == 1;
-        case 1: return variable == 0 || variable == 1;
-        case 2: return variable == 2;
+        case 1: return variable == 0 || variable == 1 || scalar;
+        case 2: return variable == 2 || scalar;
         default: return false;
     }
 }

@@ -59,7 +59,7 @@ void launchBuildEll(int N, int W, const int32_t* cfs, const int32_t* cfi, const 
 
 // ---- one SIMPLE iteration ----
 void launchIterBegin(Ctl* ctl, const volatile int* hostStop, cudaStream_t s);
-// gradients of up to three fields (u, v, p) with their boundary fields
+// gradients of up to five fields (u, v, p, T, C) with their boundary fields
 void launchGradient(const MeshDev& m, const Ctl* ctl, int nFields, const double* const* phi, const BCDev* bc,
                     double* const* gZ, double* const* gR, int scheme, cudaStream_t s);
 void launchMomentum(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, const BCDev& bcV,
@@ -91,11 +91,23 @@ void launchResiduals(const MeshDev& m, const Ctl* ctl, const double* AF, const d
                      const double* bu, const double* bv, const double* u, const double* v, const double* mDot,
                      double* resU, double* resV, double* resC, double* scaleU, double* scaleV, double* partial,
                      int* nBlocksOut, cudaStream_t s);
-void launchIterEnd(Ctl* ctl, const double* partial, int nBlocks, int N, cudaStream_t s);
+// partialS: per block {stat_T, |diag_T|, stat_C, |diag_C|} of the scalar
+// residual pass (null when no scalar residual is monitored)
+void launchIterEnd(Ctl* ctl, const double* partial, const double* partialS, int nBlocks, int N, cudaStream_t s);
 // batch: per-case reduction of the per-cell residual arrays, then per-case norms + convergence
 void launchBatchIterEnd(Ctl* ctl, const BatchDev& b, const double* resU, const double* resV, const double* resC,
                         const double* scaleU, const double* scaleV, cudaStream_t s);
 void launchCopy(const Ctl* ctl, double* dst, const double* src, int n, cudaStream_t s);
+
+// ---- transported scalars (scalar.cu) ----
+// assembly of ns = 1 or 2 scalars (a.s[0..ns)) after the corrections
+void launchScalarAssembly(const MeshDev& m, const Ctl* ctl, int ns, const ScalarArgs& a, cudaStream_t s);
+// residualRaw of ns solved scalars, the first of monitoring entry `first`
+// (0 Temperature, 1 Concentration), and the first reduction pass into
+// partial[4 per block]
+void launchScalarResidual(const MeshDev& m, const Ctl* ctl, int ns, int first, const double* const* AF,
+                          const double* const* AC, const double* const* b, const double* const* x,
+                          double* const* res, double* const* scale, double* partial, cudaStream_t s);
 
 // ---- multigrid (mg.cu), T = double or float ----
 // Galerkin P^T A P from a fine level of type TF into a coarse level of type TC

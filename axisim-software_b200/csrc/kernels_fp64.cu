@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstdio>
 
+#include "face.cuh"
 #include "kernels.hpp"
 
 namespace axisim {
@@ -27,8 +28,6 @@ namespace {
 
 constexpr double kPi = 3.14159265358979323846;
 constexpr int kThreads = 256;
-constexpr uint8_t BC_DIRICHLET = 0, BC_NEUMANN = 1, BC_FULLY_DEVELOPED = 2;
-constexpr int CONV_UPWIND = 0, CONV_CENTRAL = 1, CONV_SOU = 2;
 
 inline int blocksFor(int n, int t = kThreads) { return (n + t - 1) / t; }
 
@@ -48,48 +47,6 @@ __device__ __forceinline__ double interpCorr(const MeshDev& m, const double* DU,
     const double DN = normalCorr(DU, DV, nz, nr, o);
     const double w = (own == c) ? m.wP[f] : 1.0 - m.wP[f];
     return w * DP + (1.0 - w) * DN;
-}
-
-// prescribedBoundaryFaceValue (solver_util.cuh:223-238)
-__device__ __forceinline__ double prescribed(const MeshDev& m, int f, uint8_t type, double value, double len) {
-    if (type != BC_FULLY_DEVELOPED) return value;
-    const double nz = m.nZ[f], nr = m.nR[f];
-    const double along = m.fcR[f] * nz * nz + m.fcZ[f] * nr * nr;
-    const double x = along / len;
-    return value * (1.0 - x * x);
-}
-
-// interpolateFieldToFace, boundary branch (solver_util.cuh:264-296)
-__device__ __forceinline__ double boundaryFaceValue(const MeshDev& m, int f, const BCDev& bc, double phiP) {
-    const int g = m.group[f];
-    if (g < 0 || g >= bc.nGroups) return phiP;
-    const uint8_t t = bc.type[g];
-    const double val = bc.value[g];
-    if (t == BC_DIRICHLET || t == BC_FULLY_DEVELOPED) return prescribed(m, f, t, val, bc.length[g]);
-    if (t == BC_NEUMANN) return phiP + val * m.dPB[f];
-    return phiP;
-}
-
-// nonOrthoScalarDiffusionFlux (solver_util.cuh:383-430)
-__device__ __forceinline__ double nonOrthoFlux(const MeshDev& m, int c, int f, int own, int nb, const double* gZ,
-                                               const double* gR, double gamma) {
-    if (nb < 0) return 0.0;
-    const int o = (own == c) ? nb : own;
-    double nz = m.nZ[f], nr = m.nR[f];
-    if (nb == c) {
-        nz = -nz;
-        nr = -nr;
-    }
-    const double a = m.area[f];
-    const double dz = m.ccZ[o] - m.ccZ[c];
-    const double dr = m.ccR[o] - m.ccR[c];
-    const double aOverNd = a * m.invDPN[f];
-    const double Tz = a * nz - aOverNd * dz;
-    const double Tr = a * nr - aOverNd * dr;
-    const double w = (own == c) ? m.wP[f] : 1.0 - m.wP[f];
-    const double gfz = w * gZ[c] + (1.0 - w) * gZ[o];
-    const double gfr = w * gR[c] + (1.0 - w) * gR[o];
-    return gamma * (Tz * gfz + Tr * gfr);
 }
 
 // ---------------- set-up kernels ----------------
@@ -191,10 +148,10 @@ __global__ void k_iter_begin(Ctl* ctl, const volatile int* hostStop) {
 
 // ---------------- gradients (solver_util.cu:146-169, cuh:458-588) ----------------
 struct GradArgs {
-    const double* phi[3];
-    BCDev bc[3];
-    double* gZ[3];
-    double* gR[3];
+    const double* phi[5];
+    BCDev bc[5];
+    double* gZ[5];
+    double* gR[5];
 };
 
 template <int NF>
@@ -287,25 +244,6 @@ __global__ void k_gradient(MeshDev m, const Ctl* ctl, GradArgs a, int scheme) {
 }
 
 // ---------------- momentum assembly ----------------
-// Higher-order face value of the deferred correction (solver_util.cuh:724-768)
-__device__ __forceinline__ double higherOrder(const MeshDev& m, int n, int o, int f, int scheme, double F, double phiUD,
-                                              const double* phi, const double* gZ, const double* gR) {
-    if (scheme == CONV_CENTRAL) {
-        const double w = (m.owner[f] == n) ? m.wP[f] : 1.0 - m.wP[f];
-        return w * phi[n] + (1.0 - w) * phi[o];
-    }
-    if (scheme == CONV_SOU) {
-        const int up = (F > 0.0) ? n : o;
-        const double dz = m.fcZ[f] - m.ccZ[up];
-        const double dr = m.fcR[f] - m.ccR[up];
-        const double ho = phi[up] + gZ[up] * dz + gR[up] * dr;
-        const double lo = fmin(phi[n], phi[o]);
-        const double hi = fmax(phi[n], phi[o]);
-        return fmin(fmax(ho, lo), hi);
-    }
-    return phiUD;
-}
-
 // Boundary face of one momentum component: diffusion BC (solver_util.cu:355-413)
 // and first-order convection (solver_util.cuh:817-864).
 __device__ __forceinline__ void momentumBoundary(const MeshDev& m, int n, int f, double area, double F, double mu,
@@ -840,21 +778,30 @@ __global__ void __launch_bounds__(kThreads) k_residual(MeshDev m, const Ctl* ctl
 
 // Second reduction pass + residualAllHost's host arithmetic + convergence test
 // + iteration counters, all on the device (no host synchronisation).
-__global__ void __launch_bounds__(kThreads) k_iter_end(Ctl* ctl, const double* partial, int nBlocks, int N) {
+constexpr int kResS = 4;  // stat_T, |diag_T|, stat_C, |diag_C|
+
+__global__ void __launch_bounds__(kThreads) k_iter_end(Ctl* ctl, const double* partial, const double* partialS,
+                                                       int nBlocks, int N) {
     pdlEnter();
     if (ctl->done) return;
-    __shared__ double sh[kThreads][kResQ];
+    constexpr int NQ = kResQ + kResS;
+    __shared__ double sh[kThreads][NQ];
     if (ctl->checked) {
-        const int isMax[kResQ] = {ctl->resNorm[0] == 2, 0, ctl->resNorm[1] == 2, 0, 0};
-        double acc[kResQ];
-        for (int q = 0; q < kResQ; q++) acc[q] = isMax[q] ? -INFINITY : 0.0;
-        for (int i = threadIdx.x; i < nBlocks; i += blockDim.x)
+        const int isMax[NQ] = {ctl->resNorm[0] == 2, 0, ctl->resNorm[1] == 2, 0, 0,
+                               ctl->resNormS[0] == 2, 0, ctl->resNormS[1] == 2, 0};
+        double acc[NQ];
+        for (int q = 0; q < NQ; q++) acc[q] = isMax[q] ? -INFINITY : 0.0;
+        for (int i = threadIdx.x; i < nBlocks; i += blockDim.x) {
             for (int q = 0; q < kResQ; q++) acc[q] = combine(acc[q], partial[(size_t)i * kResQ + q], isMax[q]);
-        for (int q = 0; q < kResQ; q++) sh[threadIdx.x][q] = acc[q];
+            if (partialS)
+                for (int q = 0; q < kResS; q++)
+                    acc[kResQ + q] = combine(acc[kResQ + q], partialS[(size_t)i * kResS + q], isMax[kResQ + q]);
+        }
+        for (int q = 0; q < NQ; q++) sh[threadIdx.x][q] = acc[q];
         __syncthreads();
         for (int st = blockDim.x / 2; st > 0; st >>= 1) {
             if ((int)threadIdx.x < st)
-                for (int q = 0; q < kResQ; q++)
+                for (int q = 0; q < NQ; q++)
                     sh[threadIdx.x][q] = combine(sh[threadIdx.x][q], sh[threadIdx.x + st][q], isMax[q]);
             __syncthreads();
         }
@@ -885,6 +832,23 @@ __global__ void __launch_bounds__(kThreads) k_iter_end(Ctl* ctl, const double* p
             if (ctl->resNorm[i] == 1) ctl->resVal[i] = sqrt(ctl->resVal[i]);
             ctl->resVal[i] /= ctl->scaleVal[i];
         }
+        // Temperature and Concentration entries (an unsolved scalar's system is all zero)
+        for (int e = 0; e < 2; e++) {
+            if (!ctl->resEnabledS[e]) continue;
+            const double raw = ctl->solvedS[e] ? sh[0][kResQ + 2 * e] : 0.0;
+            const double diag = ctl->solvedS[e] ? sh[0][kResQ + 2 * e + 1] : 0.0;
+            ctl->resValS[e] = raw;
+            switch (ctl->resScaleS[e]) {
+                case 0: ctl->scaleValS[e] = 1.0; break;
+                case 1: ctl->scaleValS[e] = (double)N; break;
+                case 2: ctl->scaleValS[e] = sqrt((double)N); break;
+                case 3: ctl->scaleValS[e] = diag; break;
+                default: break;
+            }
+            if (ctl->scaleValS[e] == 0.0) continue;
+            if (ctl->resNormS[e] == 1) ctl->resValS[e] = sqrt(ctl->resValS[e]);
+            ctl->resValS[e] /= ctl->scaleValS[e];
+        }
         bool any = false, conv = true;
         for (int i = 0; i < 3; i++) {
             if (!ctl->resEnabled[i]) continue;
@@ -892,12 +856,20 @@ __global__ void __launch_bounds__(kThreads) k_iter_end(Ctl* ctl, const double* p
             if (!(ctl->resVal[i] <= ctl->tol[i])) conv = false;
             if (!isfinite(ctl->resVal[i])) finite = false;
         }
+        for (int e = 0; e < 2; e++) {
+            if (!ctl->resEnabledS[e]) continue;
+            any = true;
+            if (!(ctl->resValS[e] <= ctl->tolS[e])) conv = false;
+            if (!isfinite(ctl->resValS[e])) finite = false;
+        }
         ctl->converged = any && conv;
         const int h = ctl->histCount % kMaxHist;
         ctl->hist[h][0] = (double)ctl->currentIteration;
         ctl->hist[h][1] = ctl->resVal[0];
         ctl->hist[h][2] = ctl->resVal[1];
         ctl->hist[h][3] = ctl->resVal[2];
+        ctl->hist[h][4] = ctl->resValS[0];
+        ctl->hist[h][5] = ctl->resValS[1];
         ctl->histCount++;
         if (ctl->converged) ctl->done = 1;
         else if (!finite) ctl->done = 4;
@@ -993,6 +965,8 @@ __global__ void __launch_bounds__(kThreads) k_batch_iter_end(Ctl* ctl, BatchDev 
         ctl->hist[h][1] = b.resVal[0];
         ctl->hist[h][2] = b.resVal[1];
         ctl->hist[h][3] = b.resVal[2];
+        ctl->hist[h][4] = 0.0;
+        ctl->hist[h][5] = 0.0;
         ctl->histCount++;
         if (ctl->converged) ctl->done = 1;
         else if (nBad) ctl->done = 4;
@@ -1045,7 +1019,9 @@ void launchGradient(const MeshDev& m, const Ctl* ctl, int nFields, const double*
     const int b = blocksFor(m.N);
     if (nFields == 1) launchPDL(k_gradient<1>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme);
     else if (nFields == 2) launchPDL(k_gradient<2>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme);
-    else launchPDL(k_gradient<3>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme);
+    else if (nFields == 3) launchPDL(k_gradient<3>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme);
+    else if (nFields == 4) launchPDL(k_gradient<4>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme);
+    else launchPDL(k_gradient<5>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme);
 }
 
 void launchMomentum(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, const BCDev& bcV, const MomentumArgs& a,
@@ -1109,8 +1085,8 @@ void launchResiduals(const MeshDev& m, const Ctl* ctl, const double* AF, const d
                                       partial);
 }
 
-void launchIterEnd(Ctl* ctl, const double* partial, int nBlocks, int N, cudaStream_t s) {
-    launchPDL(k_iter_end, dim3(1), dim3(kThreads), 0, s, ctl, partial, nBlocks, N);
+void launchIterEnd(Ctl* ctl, const double* partial, const double* partialS, int nBlocks, int N, cudaStream_t s) {
+    launchPDL(k_iter_end, dim3(1), dim3(kThreads), 0, s, ctl, partial, partialS, nBlocks, N);
 }
 
 void launchBatchIterEnd(Ctl* ctl, const BatchDev& b, const double* resU, const double* resV, const double* resC,

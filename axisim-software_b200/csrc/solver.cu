@@ -130,6 +130,7 @@ public:
         csim_ = axisim_config_simple{50, 1, 1e-8, 1e-5};
         cmg_ = axisim_config_multigrid{3, 0.6, 30, 1, 1};
         for (int i = 0; i < 3; i++) cres_[i] = axisim_config_residual{0, 0, 3, 1, 1e-3};
+        for (int i = 0; i < 2; i++) sres_[i] = axisim_config_residual{0, 0, 3, 0, 1e-3};
         alphaU_ = 0.7;
         alphaP_ = 0.3;
     }
@@ -389,7 +390,9 @@ public:
         hier_.clear();
         haveHierarchy_ = false;
         colorN_ = 0;
+        releaseScalarBuffers();
         meshArena_.release();
+        meshType_ = AXISIM_MESH_UNSTRUCTURED;
         N_ = N;
         F_ = F;
         S_ = S;
@@ -503,7 +506,7 @@ public:
     }
 
     void setBC(int var, const axisim_bc_field& b) {
-        if (var < 0 || var > 2) throw StatusError(AXISIM_E_ARG, "variable must be 0 (u), 1 (v) or 2 (p)");
+        if (var < 0 || var > 4) throw StatusError(AXISIM_E_ARG, "variable must be 0 (u), 1 (v), 2 (p), 3 (T) or 4 (C)");
         if (b.nGroups < 0 || (b.nGroups > 0 && (!b.typeByGroup || !b.valueByGroup)))
             throw StatusError(AXISIM_E_ARG, "bc arrays are null");
         HostBC h;
@@ -519,16 +522,71 @@ public:
         h.amp.assign((size_t)G, 0.0);
         h.freq.assign((size_t)G, 0.0);
         for (int g = 0; g < G; g++) {
-            if (h.type[(size_t)g] == AXISIM_BC_PULSATILE) h.type[(size_t)g] = AXISIM_BC_DIRICHLET;
-            if (b.pulsatileByGroup && b.pulsatileByGroup[g]) {
+            const uint8_t t = h.type[(size_t)g];
+            if (var < 3 && (t == AXISIM_BC_MICHAELIS_MENTEN || t == AXISIM_BC_HILL))
+                throw StatusError(AXISIM_E_CONFIG, "Michaelis-Menten and Hill conditions apply to T and C only");
+            if (t == AXISIM_BC_PULSATILE) h.type[(size_t)g] = AXISIM_BC_DIRICHLET;
+            // only u and v follow the pulsatile law in time (solver.cpp:1038-1055)
+            if (var < 2 && b.pulsatileByGroup && b.pulsatileByGroup[g]) {
                 h.puls[(size_t)g] = 1;
                 h.amp[(size_t)g] = b.amplitudeByGroup ? b.amplitudeByGroup[g] : 0.0;
                 h.freq[(size_t)g] = b.frequencyByGroup ? b.frequencyByGroup[g] : 0.0;
             }
         }
-        hbc_[var] = h;
-        haveBC_[var] = true;
+        if (var < 3) {
+            hbc_[var] = h;
+            haveBC_[var] = true;
+        } else {
+            hbcS_[var - 3] = h;
+            haveBCS_[var - 3] = true;
+        }
         bcDirty_ = true;
+    }
+
+    void setMeshType(int t) {
+        if (t != AXISIM_MESH_STRUCTURED && t != AXISIM_MESH_UNSTRUCTURED)
+            throw StatusError(AXISIM_E_ARG, "mesh type must be 0 (structured) or 1 (unstructured)");
+        meshType_ = t;
+    }
+
+    // Wall kinetics of T (var 3) or C (var 4); null restores the defaults.
+    void setKinetics(int var, const axisim_kinetics* k) {
+        if (var != 3 && var != 4) throw StatusError(AXISIM_E_ARG, "kinetics apply to variable 3 (T) or 4 (C)");
+        std::vector<double>& kin = hkin_[var - 3];
+        kin.clear();
+        if (k) {
+            if (k->nGroups < 0) throw StatusError(AXISIM_E_ARG, "kinetics nGroups < 0");
+            const int G = k->nGroups;
+            const double* src[7] = {k->vmaxByGroup, k->kmByGroup, k->nByGroup, k->mByGroup,
+                                    k->k2ByGroup, k->v2ByGroup, k->RtotByGroup};
+            const double dflt[7] = {0.0, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0};
+            kin.assign((size_t)7 * G, 0.0);
+            for (int j = 0; j < 7; j++)
+                for (int g = 0; g < G; g++) kin[(size_t)j * G + g] = src[j] ? src[j][g] : dflt[j];
+            hkinG_[var - 3] = G;
+        } else {
+            hkinG_[var - 3] = 0;
+        }
+        bcDirty_ = true;
+    }
+
+    // SolverFieldOption and the Temperature / Concentration residual entries.
+    void setScalars(int energy, int concentration, const axisim_config_residual* r2) {
+        const int next[2] = {energy ? 1 : 0, concentration ? 1 : 0};
+        bool baked = next[0] != solveS_[0] || next[1] != solveS_[1];
+        if (r2)
+            for (int q = 0; q < 2; q++) {
+                baked |= r2[q].enabled != sres_[q].enabled;
+                sres_[q] = r2[q];
+            }
+        solveS_[0] = next[0];
+        solveS_[1] = next[1];
+        if (baked) destroyGraph();
+    }
+
+    void scalarResiduals(double* out) const {
+        out[0] = lastResS_[0];
+        out[1] = lastResS_[1];
     }
 
     void setConfig(const axisim_config_solver* s, const axisim_config_simple* sim, const axisim_config_multigrid* mg,
@@ -562,6 +620,9 @@ public:
         if (running_) return why("Solver is already running.");
         if (!isReady_) return why("Run the solver once before continuing.");
         if (!haveMesh_) return why("Generate a valid mesh first.");
+        // solver.cpp:485-493
+        if (solveS_[0] != ranS_[0]) return why("Energy field selection changed.");
+        if (solveS_[1] != ranS_[1]) return why("Concentration field selection changed.");
         return true;
     }
 
@@ -605,6 +666,34 @@ private:
     axisim_config_multigrid cmg_;
     axisim_config_residual cres_[3];
     double alphaU_ = 0.7, alphaP_ = 0.3;
+    int meshType_ = AXISIM_MESH_UNSTRUCTURED;  // Mesh::currentMeshType
+    // transported scalars, index 0 temperature, 1 concentration: which are
+    // solved (and were in the last run), their residual entries, boundary
+    // fields, user kinetics [7][G] (Vmax Km n m K2 V2 Rtot), device buffers
+    int solveS_[2] = {0, 0};
+    int ranS_[2] = {0, 0};
+    axisim_config_residual sres_[2];
+    double lastResS_[2] = {0.0, 0.0};
+    HostBC hbcS_[2];
+    bool haveBCS_[2] = {false, false};
+    std::vector<double> hkin_[2];
+    int hkinG_[2] = {0, 0};
+    BCDev bcS_[2];
+    // lvl[0], lvl[1] are the reference's simple.tempOld / tempOld2 buffers as
+    // first allocated; `swapped` says the BDF2 shift has exchanged the two
+    // names an odd number of times (simple.tempOld is then lvl[1]).
+    struct ScalarBuf {
+        double *phi = nullptr, *tmp = nullptr, *lvl[2] = {nullptr, nullptr}, *gZ = nullptr, *gR = nullptr;
+        double *AF = nullptr, *AC = nullptr, *b = nullptr, *inv = nullptr, *res = nullptr, *scale = nullptr;
+        int swapped = 0;
+        double* old() const { return lvl[swapped]; }       // simple.tempOld
+        double* old2() const { return lvl[1 - swapped]; }  // simple.tempOld2
+    } sb_[2];
+    // the `swapped` state at the start of the run the graph was captured for:
+    // the scalar step reads the levels through the names as they stood then
+    int graphSwapS_[2] = {0, 0};
+    Arena scalarArena_;
+    double *cw_ = nullptr, *ocr_ = nullptr, *partialS_ = nullptr;
     int precision_ = AXISIM_PREC_FP64;
     int psolve_ = AXISIM_PSOLVE_VCYCLES;
     double psolveTol_ = 0.0;
@@ -729,12 +818,64 @@ private:
         std::vector<double> zeros((size_t)std::max(hbc_[2].nGroups, 1), 0.0);
         pp.value = bcArena_.upload(zeros.data(), zeros.size());
         bc_[3] = pp;
+        // T and C: kinetics [9][G] = Vmax Km n m K2 V2 Rtot, then Km^n and K2^m
+        // precomputed on the host (memory_manger.cpp:72-83, 110-136)
+        for (int q = 0; q < 2; q++) {
+            const HostBC& h = hbcS_[q];
+            BCDev d;
+            d.nGroups = h.nGroups;
+            if (h.nGroups > 0) {
+                const int G = h.nGroups;
+                d.type = bcArena_.upload(h.type.data(), h.type.size());
+                d.value = bcArena_.upload(h.value.data(), h.value.size());
+                d.length = bcArena_.upload(h.length.data(), h.length.size());
+                std::vector<double> kin((size_t)9 * G, 0.0);
+                const double dflt[7] = {0.0, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0};
+                for (int j = 0; j < 7; j++)
+                    for (int g = 0; g < G; g++)
+                        kin[(size_t)j * G + g] = g < hkinG_[q] ? hkin_[q][(size_t)j * hkinG_[q] + g] : dflt[j];
+                for (int g = 0; g < G; g++) {
+                    kin[(size_t)7 * G + g] = std::pow(kin[(size_t)1 * G + g], kin[(size_t)2 * G + g]);
+                    kin[(size_t)8 * G + g] = std::pow(kin[(size_t)4 * G + g], kin[(size_t)3 * G + g]);
+                }
+                d.kin = bcArena_.upload(kin.data(), kin.size());
+            }
+            bcS_[q] = d;
+        }
         int maxG = std::max(hbc_[0].nGroups, hbc_[1].nGroups);
         if (hostBCStage_) cudaFreeHost(hostBCStage_);
         hostBCStage_ = nullptr;
         CK(cudaHostAlloc((void**)&hostBCStage_, sizeof(double) * 2 * (size_t)std::max(maxG, 1), cudaHostAllocDefault));
         bcDirty_ = false;
         destroyGraph();
+    }
+
+    // Buffers of the solved scalars (zeroed on allocation, as allocateSimple
+    // zero-fills temp / conc, memory_manger.cpp:740-772).
+    void ensureScalarBuffers() {
+        const size_t N = (size_t)N_, WN = (size_t)W_ * N_;
+        for (int q = 0; q < 2; q++) {
+            if (!solveS_[q] || sb_[q].phi) continue;
+            ScalarBuf& b = sb_[q];
+            Arena& A = scalarArena_;
+            b.phi = A.alloc<double>(N); b.tmp = A.alloc<double>(N); b.lvl[0] = A.alloc<double>(N);
+            b.lvl[1] = A.alloc<double>(N); b.gZ = A.alloc<double>(N); b.gR = A.alloc<double>(N);
+            b.AF = A.alloc<double>(WN); b.AC = A.alloc<double>(N); b.b = A.alloc<double>(N);
+            b.inv = A.alloc<double>(N); b.res = A.alloc<double>(N); b.scale = A.alloc<double>(N);
+            b.swapped = 0;
+        }
+        if ((solveS_[0] || solveS_[1]) && !cw_) {
+            cw_ = scalarArena_.alloc<double>((size_t)F_);
+            ocr_ = scalarArena_.alloc<double>((size_t)F_);
+            partialS_ = scalarArena_.alloc<double>((size_t)((N_ + 255) / 256) * 4 + 4);
+        }
+    }
+    void releaseScalarBuffers() {
+        scalarArena_.release();
+        sb_[0] = ScalarBuf{};
+        sb_[1] = ScalarBuf{};
+        cw_ = ocr_ = partialS_ = nullptr;
+        ranS_[0] = ranS_[1] = 0;
     }
 
     void ensureHierarchy() {
@@ -1190,18 +1331,26 @@ private:
         const int grad = cs_.gradientScheme;
         launchIterBegin(ctl_, hostStopDev_, stream_);
         mark("iter_begin", 0.0);
-        // gradients of u, v (when SOU / non-orthogonal) and p in one pass
+        // gradients of u, v (when SOU / non-orthogonal) and p in one pass; the
+        // solved scalars' gradients join it: the reference takes them just
+        // before each scalar's assembly (solver.cpp:1224-1226), and nothing
+        // writes T or C between the start of the iteration and that point
         {
-            const double* phi[3];
-            BCDev bc[3];
-            double* gz[3];
-            double* gr[3];
+            const double* phi[5];
+            BCDev bc[5];
+            double* gz[5];
+            double* gr[5];
             int nf = 0;
             if (nonOrtho || convNeedsGrad) {
                 phi[nf] = u_; bc[nf] = bc_[0]; gz[nf] = gUZ_; gr[nf] = gUR_; nf++;
                 phi[nf] = v_; bc[nf] = bc_[1]; gz[nf] = gVZ_; gr[nf] = gVR_; nf++;
             }
             phi[nf] = p_; bc[nf] = bc_[2]; gz[nf] = gPZ_; gr[nf] = gPR_; nf++;
+            if (nonOrtho || convNeedsGrad)
+                for (int q = 0; q < 2; q++)
+                    if (solveS_[q]) {
+                        phi[nf] = sb_[q].phi; bc[nf] = bcS_[q]; gz[nf] = sb_[q].gZ; gr[nf] = sb_[q].gR; nf++;
+                    }
             launchGradient(mesh_, ctl_, nf, phi, bc, gz, gr, grad, stream_);
             mark("gradient", gradBytes(nf, grad));
         }
@@ -1295,14 +1444,76 @@ private:
         launchCorrect(mesh_, ctl_, bc_[2], fluid_.rho, alphaP_, nonOrtho, pp_, gPZ_, gPR_, DU_, DV_, u_, v_, p_, mDot_,
                       stream_);
         mark("correct_massflux", 64.0 * F_ + (88.0 + 4.0 * W_) * N_);
+        // energy and concentration (solver.cpp:1218-1238): both assembled in one
+        // pass (each system depends only on its own field, mDot and the mesh),
+        // then each solved with the momentum linear solver
+        int ns = 0, firstS = -1;
+        for (int q = 0; q < 2; q++)
+            if (solveS_[q]) {
+                if (firstS < 0) firstS = q;
+                ns++;
+            }
+        if (ns > 0) {
+            ScalarArgs sa{};
+            int k = 0;
+            for (int q = 0; q < 2; q++) {
+                if (!solveS_[q]) continue;
+                ScalarDev& d = sa.s[k++];
+                const ScalarBuf& b = sb_[q];
+                d.bc = bcS_[q];
+                // the names simple.tempOld / tempOld2 as they stood when the run
+                // started (solver.cpp:985-1009 caches them before the time loop)
+                d.phi = b.phi; d.gZ = b.gZ; d.gR = b.gR;
+                d.old = b.lvl[graphSwapS_[q]];
+                d.old2 = b.lvl[1 - graphSwapS_[q]];
+                d.AF = b.AF; d.AC = b.AC; d.b = b.b; d.inv = b.inv;
+                d.gamma = q == 0 ? fluid_.k / (fluid_.rho * fluid_.cp) : fluid_.D;
+                d.alpha = q == 0 ? alphaU_ : 1.0;
+            }
+            sa.mDot = mDot_;
+            sa.cw = cw_;
+            sa.ocr = ocr_;
+            sa.fluxScale = 1.0 / fluid_.rho;
+            sa.dt = cs_.dt;
+            sa.conv = conv;
+            sa.scheme = (scheme == 3) ? 0 : scheme;
+            sa.nonOrtho = nonOrtho;
+            sa.transient = cs_.transient ? 1 : 0;
+            launchScalarAssembly(mesh_, ctl_, ns, sa, stream_);
+            {
+                double face = 32.0 + (scheme == 1 ? 8.0 : scheme == 2 ? 16.0 : 0.0);
+                double cell = 4.0 * W_ + 16.0 + ns * (8.0 * W_ + 8.0 + 24.0 + (cs_.transient ? 16.0 : 0.0));
+                mark("scalar", face * F_ + cell * N_);
+            }
+            for (int q = 0; q < 2; q++)
+                if (solveS_[q]) enqueueLinear(sb_[q].phi, sb_[q].tmp, sb_[q].AF, sb_[q].b, sb_[q].inv);
+        }
         launchResiduals(mesh_, ctl_, AFm_, ACu_, ACv_, bu_, bv_, u_, v_, mDot_, resU_, resV_, resC_, scU_, scV_,
                         partial_, &residualBlocks_, stream_);
         mark("residual", 16.0 * F_ + (16.0 * W_ + 88.0) * N_);
+        const bool monitorS = (solveS_[0] && sres_[0].enabled) || (solveS_[1] && sres_[1].enabled);
+        if (monitorS) {
+            const double* AF[2];
+            const double* AC[2];
+            const double* bb[2];
+            const double* x[2];
+            double* res[2];
+            double* sc[2];
+            int k = 0;
+            for (int q = 0; q < 2; q++) {
+                if (!solveS_[q]) continue;
+                AF[k] = sb_[q].AF; AC[k] = sb_[q].AC; bb[k] = sb_[q].b; x[k] = sb_[q].phi;
+                res[k] = sb_[q].res; sc[k] = sb_[q].scale;
+                k++;
+            }
+            launchScalarResidual(mesh_, ctl_, ns, firstS, AF, AC, bb, x, res, sc, partialS_, stream_);
+            mark("scalar_residual", ns * (8.0 * W_ + 48.0) * N_ + 4.0 * W_ * N_);
+        }
         if (batch_.nCases > 0) {
             launchBatchIterEnd(ctl_, batch_, resU_, resV_, resC_, scU_, scV_, stream_);
             mark("batch_iter_end", 40.0 * N_);
         } else {
-            launchIterEnd(ctl_, partial_, residualBlocks_, N_, stream_);
+            launchIterEnd(ctl_, partial_, monitorS ? partialS_ : nullptr, residualBlocks_, N_, stream_);
             mark("iter_end", 40.0 * residualBlocks_);
         }
     }
@@ -1334,6 +1545,13 @@ public:
             h.resNorm[i] = cres_[i].normType;
             h.resScale[i] = cres_[i].scaleType;
             h.resEnabled[i] = cres_[i].enabled;
+        }
+        for (int q = 0; q < 2; q++) {
+            h.tolS[q] = -1.0;
+            h.resNormS[q] = sres_[q].normType;
+            h.resScaleS[q] = sres_[q].scaleType;
+            h.resEnabledS[q] = sres_[q].enabled;
+            h.solvedS[q] = solveS_[q];
         }
         CK(cudaMemcpyAsync(ctl_, &h, sizeof(Ctl), cudaMemcpyHostToDevice, stream_));
         CK(cudaStreamSynchronize(stream_));
@@ -1385,6 +1603,7 @@ public:
 private:
     void buildGraph() {
         if (exec_) return;
+        ensureScalarBuffers();
         if (cs_.useMultigrid) ensureDeviceLevels();
         ensureMixedBuffers();
         if (cs_.useMultigrid && psolve_ == AXISIM_PSOLVE_FCG) ensureNetStats();
@@ -1408,6 +1627,17 @@ private:
         double* fields[] = {u_, v_, p_, pp_, uT_, vT_, ppT_, DU_, DV_, gPZ_, gPR_, gUZ_, gUR_, gVZ_, gVR_,
                             uOld_, vOld_, uOld2_, vOld2_};
         for (double* f : fields) CK(cudaMemsetAsync(f, 0, N * sizeof(double), stream_));
+        for (int q = 0; q < 2; q++) {
+            ScalarBuf& b = sb_[q];
+            double* sf[] = {b.phi, b.tmp, b.lvl[0], b.lvl[1], b.gZ, b.gR};
+            for (double* f : sf)
+                if (f) CK(cudaMemsetAsync(f, 0, N * sizeof(double), stream_));
+            b.swapped = 0;  // allocateSimple hands out fresh tempOld / tempOld2
+        }
+        if (cw_) {
+            CK(cudaMemsetAsync(cw_, 0, (size_t)F_ * sizeof(double), stream_));
+            CK(cudaMemsetAsync(ocr_, 0, (size_t)F_ * sizeof(double), stream_));
+        }
         CK(cudaMemsetAsync(mDot_, 0, (size_t)F_ * sizeof(double), stream_));
         CK(cudaMemsetAsync(ctl_, 0, sizeof(Ctl), stream_));
     }
@@ -1419,12 +1649,23 @@ int Solver::solve(int continueRun, axisim_result* res) {
     if (!haveMesh_) throw StatusError(AXISIM_E_STATE, "set a mesh before solving");
     for (int v = 0; v < 3; v++)
         if (!haveBC_[v]) throw StatusError(AXISIM_E_STATE, "set boundary conditions for u, v and p before solving");
+    for (int q = 0; q < 2; q++)
+        if (solveS_[q] && !haveBCS_[q])
+            throw StatusError(AXISIM_E_STATE, q == 0 ? "set boundary conditions for T before solving energy"
+                                                     : "set boundary conditions for C before solving concentration");
+    if (batch_.nCases > 0 && ((solveS_[0] && sres_[0].enabled) || (solveS_[1] && sres_[1].enabled)))
+        throw StatusError(AXISIM_E_CONFIG, "a batch monitors U, V and Continuity only; disable the scalar residuals");
     // Solver::runCheck (solver.cpp:530-661)
     if (running_) throw StatusError(AXISIM_E_STATE, "Solver still running");
     if (csim_.maxIter < 1) csim_.maxIter = 50;
     if (csim_.checkConv < 1) csim_.checkConv = 1;
     if (cs_.linearMaxIter < 1) cs_.linearMaxIter = 20;
     if (cs_.saveKeyFrameIter < 1) cs_.saveKeyFrameIter = 1;
+    // a structured mesh is orthogonal by construction: no corrector (solver.cpp:548-555)
+    if (meshType_ == AXISIM_MESH_STRUCTURED && cs_.useNonOrthCorrector) {
+        cs_.useNonOrthCorrector = 0;
+        destroyGraph();
+    }
     const bool transient = cs_.transient != 0;
     if (transient) {
         if (!std::isfinite(cs_.dt) || cs_.dt <= 0.0) throw StatusError(AXISIM_E_CONFIG, "Transient run needs a positive time step.");
@@ -1444,6 +1685,10 @@ int Solver::solve(int continueRun, axisim_result* res) {
     if (anyPuls && !transient) throw StatusError(AXISIM_E_CONFIG, "Pulsatile inlet requires Transient Solver to be enabled.");
     if (!std::isfinite(fluid_.rho) || !std::isfinite(fluid_.mu) || fluid_.rho <= 0.0 || fluid_.mu <= 0.0)
         throw StatusError(AXISIM_E_CONFIG, "Solver needs positive density and viscosity.");
+    if (solveS_[0] && !(std::isfinite(fluid_.cp) && std::isfinite(fluid_.k) && fluid_.cp > 0.0 && fluid_.k >= 0.0))
+        throw StatusError(AXISIM_E_CONFIG, "Energy equation needs a positive heat capacity and a conductivity >= 0.");
+    if (solveS_[1] && !(std::isfinite(fluid_.D) && fluid_.D >= 0.0))
+        throw StatusError(AXISIM_E_CONFIG, "Concentration equation needs a mass diffusivity >= 0.");
     bool cont = continueRun != 0;
     if (cont) {
         std::string why;
@@ -1453,6 +1698,7 @@ int Solver::solve(int continueRun, axisim_result* res) {
         }
     }
     uploadBC();
+    ensureScalarBuffers();
     running_ = true;
     struct Guard {
         std::atomic<bool>& r;
@@ -1470,6 +1716,15 @@ int Solver::solve(int continueRun, axisim_result* res) {
             CK(cudaStreamSynchronize(stream_));
         }
     }
+    // the scalar step reads the time levels through the names tempOld /
+    // tempOld2 as they stand at the start of the run (solver.cpp:985-1009)
+    bool regraph = false;
+    for (int q = 0; q < 2; q++)
+        if (graphSwapS_[q] != sb_[q].swapped) {
+            graphSwapS_[q] = sb_[q].swapped;
+            regraph = true;
+        }
+    if (regraph) destroyGraph();
     buildGraph();
     // control block: settings for this run
     Ctl h;
@@ -1484,6 +1739,13 @@ int Solver::solve(int continueRun, axisim_result* res) {
         h.resNorm[i] = cres_[i].normType;
         h.resScale[i] = cres_[i].scaleType;
         h.resEnabled[i] = cres_[i].enabled;
+    }
+    for (int q = 0; q < 2; q++) {
+        h.tolS[q] = sres_[q].tol;
+        h.resNormS[q] = sres_[q].normType;
+        h.resScaleS[q] = sres_[q].scaleType;
+        h.resEnabledS[q] = sres_[q].enabled;
+        h.solvedS[q] = solveS_[q];
     }
     const double timeOffset = (transient && cont) ? simTime_ : 0.0;
     const int numSteps = transient ? (int)std::ceil(cs_.tEnd / cs_.dt) : 1;
@@ -1521,6 +1783,12 @@ int Solver::solve(int continueRun, axisim_result* res) {
             }
             CK(cudaMemcpyAsync(uOld_, u_, (size_t)N_ * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
             CK(cudaMemcpyAsync(vOld_, v_, (size_t)N_ * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+            for (int q = 0; q < 2; q++) {  // solver.cpp:1076-1095: swap the names, copy into tempOld
+                if (!solveS_[q]) continue;
+                ScalarBuf& b = sb_[q];
+                if (bdf2) b.swapped ^= 1;
+                CK(cudaMemcpyAsync(b.old(), b.phi, (size_t)N_ * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+            }
         }
         h.done = 0;
         h.k = 0;
@@ -1541,7 +1809,7 @@ int Solver::solve(int continueRun, axisim_result* res) {
             if (resFn) {
                 for (int q = drained; q < h.histCount; q++) {
                     const double* e = h.hist[q % kMaxHist];
-                    resFn(cbCtx, (int32_t)e[0], e + 1);
+                    resFn(cbCtx, (int32_t)e[0], e + 1);  // U, V, Continuity, Temperature, Concentration
                 }
             }
             drained = h.histCount;
@@ -1570,6 +1838,18 @@ int Solver::solve(int continueRun, axisim_result* res) {
         BCDev bc[3] = {bc_[0], bc_[1], bc_[2]};
         launchGradient(mesh_, nullptr, 3, phi, bc, gz, gr, cs_.gradientScheme, stream_);
     }
+    // and of the solved scalars (solver.cpp:1334-1336)
+    for (int q = 0; q < 2; q++) {
+        if (!solveS_[q]) continue;
+        const double* phi[1] = {sb_[q].phi};
+        double* gz[1] = {sb_[q].gZ};
+        double* gr[1] = {sb_[q].gR};
+        launchGradient(mesh_, nullptr, 1, phi, &bcS_[q], gz, gr, cs_.gradientScheme, stream_);
+    }
+    ranS_[0] = solveS_[0];
+    ranS_[1] = solveS_[1];
+    lastResS_[0] = h.resValS[0];
+    lastResS_[1] = h.resValS[1];
     CK(cudaStreamSynchronize(stream_));
     CK(cudaGetLastError());
     float ms = 0.f;
@@ -1611,6 +1891,14 @@ int64_t Solver::getField(const std::string& name, double* out, size_t n) const {
         {"length2D", mesh_.length2D, F, 0}, {"lsqWZ", mesh_.lsqWZ, F, 0}, {"lsqWR", mesh_.lsqWR, F, 0},
         {"invA2D", mesh_.invA2D, N, 0}, {"lsqInvZZ", mesh_.lsqIZZ, N, 0}, {"lsqInvZR", mesh_.lsqIZR, N, 0},
         {"lsqInvRR", mesh_.lsqIRR, N, 0},
+        // transported scalars (null until the scalar is solved)
+        {"T", sb_[0].phi, N, 0}, {"gradTZ", sb_[0].gZ, N, 0}, {"gradTR", sb_[0].gR, N, 0},
+        {"AC_T", sb_[0].AC, N, 0}, {"b_T", sb_[0].b, N, 0}, {"AF_T", sb_[0].AF, S, 1}, {"invAC_T", sb_[0].inv, N, 0},
+        {"TOld", sb_[0].old(), N, 0}, {"TOld2", sb_[0].old2(), N, 0}, {"res_T", sb_[0].res, N, 0},
+        {"C", sb_[1].phi, N, 0}, {"gradCZ", sb_[1].gZ, N, 0}, {"gradCR", sb_[1].gR, N, 0},
+        {"AC_C", sb_[1].AC, N, 0}, {"b_C", sb_[1].b, N, 0}, {"AF_C", sb_[1].AF, S, 1}, {"invAC_C", sb_[1].inv, N, 0},
+        {"COld", sb_[1].old(), N, 0}, {"COld2", sb_[1].old2(), N, 0}, {"res_C", sb_[1].res, N, 0},
+        {"cw", cw_, F, 0}, {"ocrWall", ocr_, F, 0},
     };
     if (name == "continuity") {
         // Solver::getMassImbalance (solver.cpp:298-331): per-cell net outflow
@@ -1632,6 +1920,7 @@ int64_t Solver::getField(const std::string& name, double* out, size_t n) const {
     }
     for (const E& e : tab) {
         if (name != e.n) continue;
+        if (!e.p) throw StatusError(AXISIM_E_STATE, name + " is not available: its scalar is not solved");
         if (!out || n < e.len) throw StatusError(AXISIM_E_ARG, "output buffer too small for " + name);
         CK(cudaStreamSynchronize(stream_));
         if (!e.ell) {
@@ -1656,10 +1945,14 @@ int64_t Solver::setField(const std::string& name, const double* in, size_t n) {
         double* p;
         size_t len;
     };
+    if (solveS_[0] || solveS_[1]) ensureScalarBuffers();
     const E tab[] = {{"u", u_, N}, {"v", v_, N}, {"p", p_, N}, {"mDot", mDot_, F}, {"uOld", uOld_, N},
-                     {"vOld", vOld_, N}, {"uOld2", uOld2_, N}, {"vOld2", vOld2_, N}};
+                     {"vOld", vOld_, N}, {"uOld2", uOld2_, N}, {"vOld2", vOld2_, N},
+                     {"T", sb_[0].phi, N}, {"TOld", sb_[0].old(), N}, {"TOld2", sb_[0].old2(), N},
+                     {"C", sb_[1].phi, N}, {"COld", sb_[1].old(), N}, {"COld2", sb_[1].old2(), N}};
     for (const E& e : tab) {
         if (name != e.n) continue;
+        if (!e.p) throw StatusError(AXISIM_E_STATE, name + " is not available: its scalar is not solved");
         if (!in || n < e.len) throw StatusError(AXISIM_E_ARG, "input buffer too small for " + name);
         CK(cudaStreamSynchronize(stream_));
         CK(cudaMemcpy(e.p, in, e.len * sizeof(double), cudaMemcpyHostToDevice));
@@ -1765,6 +2058,34 @@ int axisim_set_bc(axisim_handle* h, int32_t variable, const axisim_bc_field* bc)
         h->s->setBC(variable, *bc);
         return AXISIM_OK;
     });
+}
+
+int axisim_set_mesh_type(axisim_handle* h, int32_t meshType) {
+    return guarded(h, [&] {
+        h->s->setMeshType(meshType);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_set_kinetics(axisim_handle* h, int32_t variable, const axisim_kinetics* kin) {
+    return guarded(h, [&] {
+        h->s->setKinetics(variable, kin);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_set_scalars(axisim_handle* h, int32_t solveEnergy, int32_t solveConcentration,
+                       const axisim_config_residual* res2) {
+    return guarded(h, [&] {
+        h->s->setScalars(solveEnergy, solveConcentration, res2);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_scalar_residuals(const axisim_handle* h, double* out2) {
+    if (!h || !out2) return AXISIM_E_ARG;
+    h->s->scalarResiduals(out2);
+    return AXISIM_OK;
 }
 
 int axisim_set_config(axisim_handle* h, const axisim_config_solver* solver, const axisim_config_simple* simple,
@@ -2054,7 +2375,7 @@ int axisim_mesh_free(axisim_mesh* m) {
 
 int axisim_resolve_bc(int32_t boundaryType, int32_t variable, int32_t hasUser, int32_t userType, double userValue,
                       uint8_t* typeOut, double* valueOut, uint8_t* pulsatileOut) {
-    if (!typeOut || !valueOut || variable < 0 || variable > 2) return AXISIM_E_ARG;
+    if (!typeOut || !valueOut || variable < 0 || variable > 4) return AXISIM_E_ARG;
     int t;
     double v;
     if (hasUser && axisim::variableEditable(variable, boundaryType)) {

@@ -42,8 +42,11 @@ enum { AXISIM_BC_DIRICHLET = 0, AXISIM_BC_NEUMANN = 1, AXISIM_BC_FULLY_DEVELOPED
 /* BoundaryType (structs/boundary_struct.h:342-348) */
 enum { AXISIM_WALL = 0, AXISIM_VELOCITY_INLET = 1, AXISIM_PRESSURE_OUTLET = 2, AXISIM_SYMMETRY = 3,
        AXISIM_FAR_FIELD = 4 };
-/* BoundaryVariable (structs/boundary_struct.h:48-57) */
-enum { AXISIM_VAR_U = 0, AXISIM_VAR_V = 1, AXISIM_VAR_P = 2 };
+/* BoundaryVariable (structs/boundary_struct.h:44-53): StaticTemperature and
+ * Concentration are the transported scalars */
+enum { AXISIM_VAR_U = 0, AXISIM_VAR_V = 1, AXISIM_VAR_P = 2, AXISIM_VAR_T = 3, AXISIM_VAR_C = 4 };
+/* MeshType (structs/boundary_struct.h:382-385) */
+enum { AXISIM_MESH_STRUCTURED = 0, AXISIM_MESH_UNSTRUCTURED = 1 };
 /* Precision of the pressure-correction multigrid (new; no reference counterpart) */
 enum { AXISIM_PREC_FP64 = 0, AXISIM_PREC_MIXED = 1 };
 /* Method of the pressure-correction solve (new; no reference counterpart) */
@@ -154,8 +157,9 @@ typedef struct axisim_result {
 typedef struct axisim_handle axisim_handle;
 
 /* Per-iteration residual callback, replacing ResidualPlot::add / Console line
- * (solver.cpp:1267-1268). Called after each check with U, V, Continuity. */
-typedef void (*axisim_residual_fn)(void* ctx, int32_t iteration, const double* residuals3);
+ * (solver.cpp:1267-1268). Called after each check with five values: U, V,
+ * Continuity, Temperature, Concentration (the last two 0 unless monitored). */
+typedef void (*axisim_residual_fn)(void* ctx, int32_t iteration, const double* residuals);
 typedef void (*axisim_log_fn)(void* ctx, const char* line);
 
 /* ---- lifetime ---- */
@@ -174,8 +178,50 @@ int axisim_set_log(axisim_handle* h, axisim_log_fn log, axisim_residual_fn resid
 /* Mesh::getFVMesh + createFVMeshDevice (solver.cpp:774-785, memory_manger.cpp:679-689):
  * copies the packed mesh to the device and precomputes the geometry on the GPU. */
 int axisim_set_mesh(axisim_handle* h, const axisim_mesh_packed* mesh);
-/* createBoundarySolverDevice (memory_manger.cpp:191-237) for one variable. */
+/* Mesh::currentMeshType of the handle's mesh (AXISIM_MESH_*), which
+ * Solver::runCheck reads (solver.cpp:548-555): a solve on a STRUCTURED mesh
+ * clears configSolver.useNonOrthCorrector (and it stays cleared), as the
+ * reference does. axisim_set_mesh resets it to UNSTRUCTURED. */
+int axisim_set_mesh_type(axisim_handle* h, int32_t meshType);
+/* createBoundarySolverDevice (memory_manger.cpp:191-237) for one variable
+ * (AXISIM_VAR_*). MICHAELIS_MENTEN and HILL are accepted for T and C only; a
+ * PULSATILE T or C group is a Dirichlet value at its mean (only u and v are
+ * updated per time step, solver.cpp:1038-1055). */
 int axisim_set_bc(axisim_handle* h, int32_t variable, const axisim_bc_field* bc);
+/* Wall kinetics of a scalar's MICHAELIS_MENTEN / HILL groups: the vmax, km,
+ * n, m, k2, v2 and Rtot arrays of BoundaryFieldHost (solver_struct.h:469-475)
+ * as createBoundaryFieldHost fills them (memory_manger.cpp:110-145): rate
+ * J(c) = Vmax c / (Km + c) or Vmax c^n / (Km^n + c^n), times
+ * 1 - V2 c^m / (K2^m + c^m) when V2 != 0, through the series wall
+ * resistance Rtot. Any array may be NULL (defaults Vmax = Km = K2 = V2 =
+ * Rtot = 0, n = m = 1); groups at or past nGroups take the defaults. */
+typedef struct axisim_kinetics {
+    int32_t nGroups;
+    const double* vmaxByGroup;
+    const double* kmByGroup;
+    const double* nByGroup;
+    const double* mByGroup;
+    const double* k2ByGroup;
+    const double* v2ByGroup;
+    const double* RtotByGroup;
+} axisim_kinetics;
+/* variable is AXISIM_VAR_T or AXISIM_VAR_C; kin = NULL restores the defaults. */
+int axisim_set_kinetics(axisim_handle* h, int32_t variable, const axisim_kinetics* kin);
+/* SolverFieldOption (solver_struct.h:9-12) and the "Temperature" /
+ * "Concentration" ConfigResidual entries (res2[0], res2[1]; NULL keeps them;
+ * the reference creates both disabled, solver.cpp:88-100). A solved scalar is
+ * assembled and solved after the velocity / pressure corrections of every
+ * SIMPLE iteration (solver.cpp:1218-1238): energy with the diffusivity
+ * k / (rho cp) and the momentum relaxation factor, concentration with D,
+ * unrelaxed; both convect with mDot / rho. Both start from zero, like the
+ * reference's fields. An enabled entry joins the convergence test. With BDF2
+ * the scalar step reads the time levels as the reference does: through the
+ * names tempOld / tempOld2 as they stood when the run started, which the
+ * per-step shift keeps exchanging (solver.cpp:985-1009, 1066-1095). */
+int axisim_set_scalars(axisim_handle* h, int32_t solveEnergy, int32_t solveConcentration,
+                       const axisim_config_residual* res2);
+/* Temperature and Concentration residuals of the last check (out2[2]). */
+int axisim_scalar_residuals(const axisim_handle* h, double* out2);
 /* Solver's public config members configSolver / configSimple / configMultigrid /
  * cfg / simple.{momentum,pressure}Relaxation (solver.h:83-133). res[3] = U, V,
  * Continuity. */
@@ -276,9 +322,14 @@ int axisim_request_stop(axisim_handle* h);
  * reference's CSR slot order) "res_U" "res_V" "res_Continuity" "continuity"
  * (per-cell mass imbalance, Solver::getMassImbalance) and the geometry
  * "invDPN" "wP" "dPB" "length2D" "lsqWZ" "lsqWR" "invA2D" "lsqInvZZ"
- * "lsqInvZR" "lsqInvRR". Returns the element count written, or -status. */
+ * "lsqInvZR" "lsqInvRR"; with a solved scalar "T" / "C", "gradTZ" "gradTR"
+ * "gradCZ" "gradCR", "AC_T" "b_T" "AF_T" "invAC_T" (and _C), "TOld" "TOld2"
+ * "COld" "COld2", "res_T" "res_C", and per face the wall concentration "cw"
+ * and wall consumption "ocrWall" of reactive walls (mesh.faces.cw / ocrWall).
+ * Returns the element count written, or -status. */
 int64_t axisim_get_field(const axisim_handle* h, const char* name, double* out, size_t n);
-/* Initial state for u v p mDot (and uOld vOld for a transient restart). */
+/* Initial state for u v p mDot (and uOld vOld for a transient restart; T C
+ * TOld COld TOld2 COld2 for a solved scalar). */
 int64_t axisim_set_field(axisim_handle* h, const char* name, const double* in, size_t n);
 
 /* ---- batches (new: the reference solves one case per Solver, solver.h:18-185) ---- */

@@ -7,8 +7,9 @@
 //   Solver::requestStop()      -> requestStop()                   (solver.cpp:175-184)
 //   Solver::shutdown()         -> shutdown(): join the worker      (solver.cpp:663-667)
 //   Solver::canContinue(...)   -> canContinue(reason)              (solver.cpp:469-528)
-//   continueSolver, configSolver, configSimple, configMultigrid, relaxation,
-//   solutions (solver.h:37-133)
+//   continueSolver, fieldOption, configSolver, configSimple, configMultigrid,
+//   relaxation, cfg (U, V, Continuity, Temperature, Concentration), solutions
+//   (solver.h:37-133)
 // The case (packed mesh + per-variable boundary fields) is handed over with
 // setCase(); the reference derives both from its Mesh (mesh.cpp, memory_manger.cpp).
 #pragma once
@@ -39,6 +40,7 @@ public:
         configSimple = axisim_config_simple{50, 1, 1e-8, 1e-5};
         configMultigrid = axisim_config_multigrid{3, 0.6, 30, 1, 1};
         for (auto& r : cfg) r = axisim_config_residual{0, 0, 3, 1, 1e-3};
+        cfg[3].enabled = cfg[4].enabled = 0;  // solver.cpp:88-100
     }
     ~Solver() {
         shutdown();
@@ -52,7 +54,11 @@ public:
     axisim_config_solver configSolver;
     axisim_config_simple configSimple;
     axisim_config_multigrid configMultigrid;
-    axisim_config_residual cfg[3];  // U, V, Continuity
+    axisim_config_residual cfg[5];  // U, V, Continuity, Temperature, Concentration
+    struct FieldOption {            // SolverFieldOption (solver_struct.h:9-12)
+        bool solveEnergy = false;
+        bool solveConcentration = false;
+    } fieldOption;
     double momentumRelaxation = 0.7;
     double pressureRelaxation = 0.3;
     bool continueSolver = false;
@@ -62,13 +68,22 @@ public:
     int lastStatus = AXISIM_OK;
 
     // Mesh + boundary fields (what Mesh / createBoundarySolverDevice provide).
+    // meshType: Mesh::currentMeshType (AXISIM_MESH_*)
     int setCase(const axisim_mesh_packed& mesh, const axisim_bc_field& u, const axisim_bc_field& v,
-                const axisim_bc_field& p) {
+                const axisim_bc_field& p, int meshType = AXISIM_MESH_UNSTRUCTURED) {
         int st = axisim_set_mesh(h_, &mesh);
+        if (st == AXISIM_OK) st = axisim_set_mesh_type(h_, meshType);
         if (st == AXISIM_OK) st = axisim_set_bc(h_, AXISIM_VAR_U, &u);
         if (st == AXISIM_OK) st = axisim_set_bc(h_, AXISIM_VAR_V, &v);
         if (st == AXISIM_OK) st = axisim_set_bc(h_, AXISIM_VAR_P, &p);
         nCells_ = mesh.nCells;
+        return st;
+    }
+    // Temperature / concentration boundary fields and their wall kinetics
+    // (kin may be null); variable AXISIM_VAR_T or AXISIM_VAR_C.
+    int setScalarBC(int variable, const axisim_bc_field& bc, const axisim_kinetics* kin = nullptr) {
+        int st = axisim_set_bc(h_, variable, &bc);
+        if (st == AXISIM_OK) st = axisim_set_kinetics(h_, variable, kin);
         return st;
     }
 
@@ -84,6 +99,7 @@ public:
         axisim_set_fluid(h_, &f);
         axisim_set_config(h_, &configSolver, &configSimple, &configMultigrid, cfg, momentumRelaxation,
                           pressureRelaxation);
+        axisim_set_scalars(h_, fieldOption.solveEnergy ? 1 : 0, fieldOption.solveConcentration ? 1 : 0, cfg + 3);
         lastStatus = axisim_solve(h_, continueSolver ? 1 : 0, &lastResult);
         if (lastStatus == AXISIM_OK || lastStatus == AXISIM_E_STOPPED) createSolutions();
         return lastStatus;
@@ -122,6 +138,18 @@ private:
         for (const auto& [label, field] : names) {
             std::vector<double> v((size_t)nCells_);
             if (axisim_get_field(h_, field, v.data(), v.size()) >= 0) solutions[label] = std::move(v);
+        }
+        const std::pair<const char*, const char*> tNames[] = {
+            {"Temperature", "T"}, {"dT/dz", "gradTZ"}, {"dT/dr", "gradTR"}};
+        const std::pair<const char*, const char*> cNames[] = {
+            {"Concentration", "C"}, {"dC/dz", "gradCZ"}, {"dC/dr", "gradCR"}};
+        for (int q = 0; q < 2; q++) {
+            if (!(q == 0 ? fieldOption.solveEnergy : fieldOption.solveConcentration)) continue;
+            const auto* list = q == 0 ? tNames : cNames;
+            for (int i = 0; i < 3; i++) {
+                std::vector<double> v((size_t)nCells_);
+                if (axisim_get_field(h_, list[i].second, v.data(), v.size()) >= 0) solutions[list[i].first] = std::move(v);
+            }
         }
     }
 };

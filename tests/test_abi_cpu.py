@@ -85,7 +85,7 @@ def test_nonconformal_seam_drops_interfaces(lib):
 def test_resolve_bc_matches_boundary_defaults(lib):
     # (boundaryType, variable) -> default BCType, boundary_func.cpp:117-201
     for bt in range(5):
-        for var, key in enumerate(("u", "v", "p")):
+        for var, key in enumerate(("u", "v", "p", "T", "C")):
             t, v, p = abi.resolve_bc(bt, var)
             assert t == cases.default_bc_type(bt, key), (bt, var)
             assert v == 0.0 and p == 0
