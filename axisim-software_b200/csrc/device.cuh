@@ -142,6 +142,7 @@ struct ScalarDev {
     double* AC;
     double* b;
     double* inv;
+    double* wall;  // per face: c_w of this scalar's reactive wall faces
     double gamma;  // kinematic diffusivity
     double alpha;  // under-relaxation factor
 };

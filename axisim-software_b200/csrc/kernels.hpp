@@ -100,8 +100,12 @@ void launchBatchIterEnd(Ctl* ctl, const BatchDev& b, const double* resU, const d
 void launchCopy(const Ctl* ctl, double* dst, const double* src, int n, cudaStream_t s);
 
 // ---- transported scalars (scalar.cu) ----
+// wall concentration of the reactive boundary faces faces[0..nFaces) (before the assembly)
+void launchScalarWall(const MeshDev& m, const Ctl* ctl, int ns, const ScalarArgs& a, const int32_t* faces,
+                      int nFaces, cudaStream_t s);
 // assembly of ns = 1 or 2 scalars (a.s[0..ns)) after the corrections
 void launchScalarAssembly(const MeshDev& m, const Ctl* ctl, int ns, const ScalarArgs& a, cudaStream_t s);
+
 // residualRaw of ns solved scalars, the first of monitoring entry `first`
 // (0 Temperature, 1 Concentration), and the first reduction pass into
 // partial[4 per block]

@@ -285,7 +285,7 @@ __device__ __forceinline__ void momentumBoundary(const MeshDev& m, int n, int f,
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_momentum(MeshDev m, const Ctl* ctl, BCDev bcU, BCDev bcV,
+__global__ void __launch_bounds__(kThreads, 4) k_momentum(MeshDev m, const Ctl* ctl, BCDev bcU, BCDev bcV,
                                                        MomentumArgs a) {
     pdlEnter();
     if (ctl->done) return;

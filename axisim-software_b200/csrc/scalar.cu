@@ -11,11 +11,16 @@
 // (concentration_equation.cu:6-160) and the wall enters the row as the
 // conductance A h with source A h c_w (solver_util.cu:388-411).
 //
-// k_scalar fuses, for up to two scalars in one pass over the cells' slots,
-// clearAllCoefficients + addTransportCoefficients + addTransientCoefficient
-// + underRelaxEquation + buildInverseDiagonal, each row's arithmetic in the
-// reference's order. k_scalar_residual is residualRaw for the scalars plus
-// the first reduction pass of their monitored residuals.
+// k_scalar_wall solves the wall concentration of every reactive boundary
+// face (one thread per face of a host-built list, before the assembly). k_scalar fuses, for up to
+// two scalars in one pass over the cells' slots, clearAllCoefficients +
+// addTransportCoefficients + addTransientCoefficient + underRelaxEquation +
+// buildInverseDiagonal, each row's arithmetic in the reference's order; a
+// reactive face enters it through the c_w k_scalar_wall stored. Keeping the
+// Newton iteration (and pow) out of the assembly keeps its register count,
+// and so its occupancy, at the level of the momentum assembly.
+// k_scalar_residual is residualRaw for the scalars plus the first reduction
+// pass of their monitored residuals.
 #include <cmath>
 
 #include "face.cuh"
@@ -71,10 +76,8 @@ __device__ __forceinline__ double kinDHill(const Kin& k, double c) {
 
 // wallConcentrationMichaelisMenten / wallConcentrationHill
 // (concentration_equation.cu:90-160): Newton from c_w = c_P, clipped at zero,
-// mixed step tolerance, at most 100 steps. Kept out of line: only reactive
-// wall faces call it, and inlined it would raise the register count of the
-// whole assembly.
-__device__ __noinline__ double wallConcentration(const Kin& k, bool hill, double cp, double h) {
+// mixed step tolerance, at most 100 steps.
+__device__ double wallConcentration(const Kin& k, bool hill, double cp, double h) {
     double cw = cp;
     const double relTol = 1e-10, absTol = 1e-14;
 #pragma unroll 1
@@ -98,8 +101,7 @@ __device__ __noinline__ double wallConcentration(const Kin& k, bool hill, double
 // (solver_util.cu:355-413), reactive walls included, then first-order
 // convection (solver_util.cuh:817-864).
 __device__ __forceinline__ void scalarBoundary(const MeshDev& m, int n, int f, double area, double F,
-                                               const ScalarDev& q, double& AC, double& b, double* cwOut,
-                                               double* ocrOut) {
+                                               const ScalarDev& q, double& AC, double& b) {
     const BCDev& bc = q.bc;
     const int g = m.group[f];
     const bool valid = g >= 0 && g < bc.nGroups;
@@ -118,13 +120,10 @@ __device__ __forceinline__ void scalarBoundary(const MeshDev& m, int n, int f, d
             AC += K;
             b += K * prescribed(m, f, t, val, bc.length[g]);
         } else if (t == BC_MICHAELIS_MENTEN || t == BC_HILL) {
-            const bool hill = t == BC_HILL;
-            const Kin k = kinOf(bc, g);
-            const double Rtot = (dPF / q.gamma) + k.Rtot;
+            // c_w from k_scalar_wall, which used the same h
+            const double Rtot = (dPF / q.gamma) + bc.kin[6 * bc.nGroups + g];
             const double h = 1 / Rtot;
-            const double cw = wallConcentration(k, hill, q.phi[n], h);
-            cwOut[f] = cw;
-            ocrOut[f] = area * (hill ? kinHill(k, cw) : kinMM(k, cw)) * kinInhib(k, cw);
+            const double cw = q.wall[f];
             AC += area * h;
             b += area * h * cw;
         }
@@ -148,8 +147,43 @@ __device__ __forceinline__ void scalarBoundary(const MeshDev& m, int n, int f, d
     }
 }
 
+// Reactive wall faces (solver_util.cu:388-411 with the wall solves of
+// concentration_equation.cu:90-160): c_w from the owner cell's current value,
+// the wall consumption A J(c_w), and c_w kept per scalar for the assembly.
+// A face reactive for both scalars leaves the second one's c_w and consumption
+// in cw / ocr, as the reference's shared mesh.faces arrays do.
 template <int NS>
-__global__ void __launch_bounds__(kThreads) k_scalar(MeshDev m, const Ctl* ctl, ScalarArgs a) {
+__global__ void __launch_bounds__(kThreads) k_scalar_wall(MeshDev m, const Ctl* ctl, ScalarArgs a,
+                                                          const int32_t* __restrict__ faces, int nFaces) {
+    pdlEnter();
+    if (ctl->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nFaces) return;
+    const int f = faces[i];
+    const int g = m.group[f];
+    const int n = m.owner[f];
+#pragma unroll
+    for (int q = 0; q < NS; q++) {
+        const ScalarDev& sc = a.s[q];
+        const BCDev& bc = sc.bc;
+        if (g < 0 || g >= bc.nGroups) continue;
+        const uint8_t t = bc.type[g];
+        if (t != BC_MICHAELIS_MENTEN && t != BC_HILL) continue;
+        const bool hill = t == BC_HILL;
+        const double nz = m.nZ[f], nr = m.nR[f];
+        const double dPF = fabs((m.fcZ[f] - m.ccZ[n]) * nz + (m.fcR[f] - m.ccR[n]) * nr);
+        const Kin k = kinOf(bc, g);
+        const double Rtot = (dPF / sc.gamma) + k.Rtot;
+        const double h = 1 / Rtot;
+        const double cw = wallConcentration(k, hill, sc.phi[n], h);
+        sc.wall[f] = cw;
+        a.cw[f] = cw;
+        a.ocr[f] = m.area[f] * (hill ? kinHill(k, cw) : kinMM(k, cw)) * kinInhib(k, cw);
+    }
+}
+
+template <int NS>
+__global__ void __launch_bounds__(kThreads, 4) k_scalar(MeshDev m, const Ctl* ctl, ScalarArgs a) {
     pdlEnter();
     if (ctl->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -197,7 +231,7 @@ __global__ void __launch_bounds__(kThreads) k_scalar(MeshDev m, const Ctl* ctl, 
 #pragma unroll
             for (int q = 0; q < NS; q++) {
                 a.s[q].AF[s] = 0.0;
-                scalarBoundary(m, n, f, area, F, a.s[q], AC[q], b[q], a.cw, a.ocr);
+                scalarBoundary(m, n, f, area, F, a.s[q], AC[q], b[q]);
             }
         }
     }
@@ -297,6 +331,13 @@ __global__ void __launch_bounds__(kThreads) k_scalar_residual(int N, int W, cons
 }
 
 }  // namespace
+
+void launchScalarWall(const MeshDev& m, const Ctl* ctl, int ns, const ScalarArgs& a, const int32_t* faces,
+                      int nFaces, cudaStream_t s) {
+    if (nFaces <= 0) return;
+    if (ns == 2) launchPDL(k_scalar_wall<2>, dim3(blocksFor(nFaces)), dim3(kThreads), 0, s, m, ctl, a, faces, nFaces);
+    else launchPDL(k_scalar_wall<1>, dim3(blocksFor(nFaces)), dim3(kThreads), 0, s, m, ctl, a, faces, nFaces);
+}
 
 void launchScalarAssembly(const MeshDev& m, const Ctl* ctl, int ns, const ScalarArgs& a, cudaStream_t s) {
     if (ns == 2) launchPDL(k_scalar<2>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, a);

@@ -581,7 +581,10 @@ public:
             }
         solveS_[0] = next[0];
         solveS_[1] = next[1];
-        if (baked) destroyGraph();
+        if (baked) {
+            wallFacesReady_ = false;
+            destroyGraph();
+        }
     }
 
     void scalarResiduals(double* out) const {
@@ -685,6 +688,7 @@ private:
     struct ScalarBuf {
         double *phi = nullptr, *tmp = nullptr, *lvl[2] = {nullptr, nullptr}, *gZ = nullptr, *gR = nullptr;
         double *AF = nullptr, *AC = nullptr, *b = nullptr, *inv = nullptr, *res = nullptr, *scale = nullptr;
+        double* wall = nullptr;  // per face: c_w of this scalar's reactive faces
         int swapped = 0;
         double* old() const { return lvl[swapped]; }       // simple.tempOld
         double* old2() const { return lvl[1 - swapped]; }  // simple.tempOld2
@@ -694,6 +698,10 @@ private:
     int graphSwapS_[2] = {0, 0};
     Arena scalarArena_;
     double *cw_ = nullptr, *ocr_ = nullptr, *partialS_ = nullptr;
+    Arena wallArena_;
+    int32_t* wallFaces_ = nullptr;  // reactive boundary faces of the solved scalars
+    int nWallFaces_ = 0;
+    bool wallFacesReady_ = false;
     int precision_ = AXISIM_PREC_FP64;
     int psolve_ = AXISIM_PSOLVE_VCYCLES;
     double psolveTol_ = 0.0;
@@ -803,6 +811,7 @@ private:
     void uploadBC() {
         if (!bcDirty_) return;
         bcArena_.release();
+        wallFacesReady_ = false;
         for (int var = 0; var < 3; var++) {
             const HostBC& h = hbc_[var];
             BCDev d;
@@ -862,6 +871,7 @@ private:
             b.lvl[1] = A.alloc<double>(N); b.gZ = A.alloc<double>(N); b.gR = A.alloc<double>(N);
             b.AF = A.alloc<double>(WN); b.AC = A.alloc<double>(N); b.b = A.alloc<double>(N);
             b.inv = A.alloc<double>(N); b.res = A.alloc<double>(N); b.scale = A.alloc<double>(N);
+            b.wall = A.alloc<double>((size_t)F_);
             b.swapped = 0;
         }
         if ((solveS_[0] || solveS_[1]) && !cw_) {
@@ -875,6 +885,9 @@ private:
         sb_[0] = ScalarBuf{};
         sb_[1] = ScalarBuf{};
         cw_ = ocr_ = partialS_ = nullptr;
+        wallFaces_ = nullptr;
+        nWallFaces_ = 0;
+        wallFacesReady_ = false;
         ranS_[0] = ranS_[1] = 0;
     }
 
@@ -1298,7 +1311,10 @@ private:
         }
     }
 
-    void enqueueLinear(double* x, double* xT, const double* AF, const double* b, const double* inv) {
+    // The linear solver of one system (LinearSolver::run); `tag` names its
+    // launches in the profile ("pp" or the scalar's).
+    void enqueueLinear(double* x, double* xT, const double* AF, const double* b, const double* inv,
+                       const char* tag = "pp") {
         const int iters = cs_.linearMaxIter;
         if (cs_.type == 1 && colorN_ > 0) {
             for (int k = 0; k < iters; k++)
@@ -1306,7 +1322,7 @@ private:
                     const int b0 = hColorStart_[(size_t)c], cnt = hColorStart_[(size_t)c + 1] - b0;
                     if (cnt > 0) {
                         launchGaussSeidel1(mesh_, ctl_, AF, b, inv, x, dCellOrder_, b0, cnt, stream_);
-                        mark("gs_pp", (double)cnt * (12.0 * W_ + 28.0));
+                        mark((std::string("gs_") + tag).c_str(), (double)cnt * (12.0 * W_ + 28.0));
                     }
                 }
             return;
@@ -1314,13 +1330,37 @@ private:
         double *live = x, *spare = xT;
         for (int k = 0; k < iters; k++) {
             launchJacobi1(mesh_, ctl_, AF, b, inv, live, spare, stream_);
-            mark("jacobi_pp", (double)N_ * (12.0 * W_ + 32.0));
+            mark((std::string("jacobi_") + tag).c_str(), (double)N_ * (12.0 * W_ + 32.0));
             std::swap(live, spare);
         }
         if (live != x) {
             launchCopy(ctl_, x, live, N_, stream_);
             mark("copy", 16.0 * N_);
         }
+    }
+
+    // Boundary faces in a Michaelis-Menten or Hill group of a solved scalar,
+    // ascending (uploaded with the scalar buffers; rebuilt when those are).
+    void ensureWallFaces() {
+        if (wallFacesReady_) return;
+        std::vector<int32_t> list;
+        std::vector<int32_t> grp((size_t)F_);
+        CK(cudaMemcpy(grp.data(), mesh_.group, (size_t)F_ * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        for (int f = 0; f < F_; f++) {
+            if (hNeighbor_[(size_t)f] >= 0) continue;
+            const int g = grp[(size_t)f];
+            bool reactive = false;
+            for (int q = 0; q < 2; q++) {
+                if (!solveS_[q] || g < 0 || g >= hbcS_[q].nGroups) continue;
+                const uint8_t t = hbcS_[q].type[(size_t)g];
+                reactive |= t == AXISIM_BC_MICHAELIS_MENTEN || t == AXISIM_BC_HILL;
+            }
+            if (reactive) list.push_back(f);
+        }
+        wallArena_.release();
+        nWallFaces_ = (int)list.size();
+        wallFaces_ = nWallFaces_ ? wallArena_.upload(list.data(), list.size()) : nullptr;
+        wallFacesReady_ = true;
     }
 
     void enqueueIteration() {
@@ -1466,7 +1506,7 @@ private:
                 d.phi = b.phi; d.gZ = b.gZ; d.gR = b.gR;
                 d.old = b.lvl[graphSwapS_[q]];
                 d.old2 = b.lvl[1 - graphSwapS_[q]];
-                d.AF = b.AF; d.AC = b.AC; d.b = b.b; d.inv = b.inv;
+                d.AF = b.AF; d.AC = b.AC; d.b = b.b; d.inv = b.inv; d.wall = b.wall;
                 d.gamma = q == 0 ? fluid_.k / (fluid_.rho * fluid_.cp) : fluid_.D;
                 d.alpha = q == 0 ? alphaU_ : 1.0;
             }
@@ -1479,14 +1519,20 @@ private:
             sa.scheme = (scheme == 3) ? 0 : scheme;
             sa.nonOrtho = nonOrtho;
             sa.transient = cs_.transient ? 1 : 0;
+            if (nWallFaces_ > 0) {
+                launchScalarWall(mesh_, ctl_, ns, sa, wallFaces_, nWallFaces_, stream_);
+                mark("scalar_wall", 100.0 * nWallFaces_);
+            }
             launchScalarAssembly(mesh_, ctl_, ns, sa, stream_);
             {
                 double face = 32.0 + (scheme == 1 ? 8.0 : scheme == 2 ? 16.0 : 0.0);
                 double cell = 4.0 * W_ + 16.0 + ns * (8.0 * W_ + 8.0 + 24.0 + (cs_.transient ? 16.0 : 0.0));
                 mark("scalar", face * F_ + cell * N_);
             }
+            // temperature's sweeps, then concentration's: each system's working
+            // set stays in L2 across its own consecutive sweeps
             for (int q = 0; q < 2; q++)
-                if (solveS_[q]) enqueueLinear(sb_[q].phi, sb_[q].tmp, sb_[q].AF, sb_[q].b, sb_[q].inv);
+                if (solveS_[q]) enqueueLinear(sb_[q].phi, sb_[q].tmp, sb_[q].AF, sb_[q].b, sb_[q].inv, q == 0 ? "T" : "C");
         }
         launchResiduals(mesh_, ctl_, AFm_, ACu_, ACv_, bu_, bv_, u_, v_, mDot_, resU_, resV_, resC_, scU_, scV_,
                         partial_, &residualBlocks_, stream_);
@@ -1604,6 +1650,7 @@ private:
     void buildGraph() {
         if (exec_) return;
         ensureScalarBuffers();
+        if (solveS_[0] || solveS_[1]) ensureWallFaces();  // host copies: before the capture
         if (cs_.useMultigrid) ensureDeviceLevels();
         ensureMixedBuffers();
         if (cs_.useMultigrid && psolve_ == AXISIM_PSOLVE_FCG) ensureNetStats();

@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip cpu baseline / e2e / time-to-residual legs")
     ap.add_argument("--network-only", action="store_true",
                     help="time the learned p' network alone (inference and training steps, 2M-cell mesh)")
+    ap.add_argument("--scalars-only", action="store_true",
+                    help="energy + concentration transport on the workload mesh: cost per SIMPLE iteration with "
+                         "and without the scalars, and the scalar kernels' achieved bandwidth (--steps iterations)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="mixed: FP32 inner solves inside FP64 refinement (the workload's setting); fp64: plain")
     return ap.parse_args()
@@ -451,6 +454,40 @@ def network_leg(abi, local, scale=1.512, infer=5, train=5):
             "note": "predict includes the host copies of r, A_C, deficit and the result"}
 
 
+def scalars_leg(abi, local, scale=1.0, iters=20):
+    """Energy + concentration (Michaelis-Menten wall behind a layer) on the
+    workload mesh, FP64 SIMPLE iterations: device time per iteration with and
+    without the scalars (CUDA events over `iters` iterations after a warm run
+    of the same length), and the per-kernel profile of the scalar step
+    (algorithmic bytes / CUDA-event time, eager replay)."""
+    from axisim import cases
+    hbm, src = peaks()
+    flow = workload(scale)
+    flow.settings.update(maxIter=iters)
+    both = cases.with_scalars(workload(scale), wall_c=cases.michaelis_menten(1e-3, 0.2),
+                              wall_layers=[(1e-6, 1e-4)], D=1e-6)
+    both.settings.update(maxIter=iters)
+    mesh = abi.multiblock(flow.blocks)
+    out = {"cells": int(mesh["nCells"]), "iterations": iters, "peak_gbs": hbm, "peak_source": src}
+    for name, case in (("flow", flow), ("flow_T_C", both)):
+        s = abi.Solver(mesh, case.bc_fields(), case.settings, device=local)
+        s.solve()
+        r = s.solve(cont=True)
+        out[name + "_ms_per_iter"] = r["ms"] / max(1, r["iterations"])
+        if name == "flow_T_C":
+            prof = {}
+            for k in s.profile(3):
+                if k["name"] in ("scalar", "scalar_wall", "jacobi_TC", "gs_TC", "jacobi_T", "jacobi_C", "gs_T", "gs_C",
+                                 "scalar_residual", "momentum"):
+                    gbs = k["bytes"] / (k["ms"] * 1e-3) / 1e9 if k["ms"] > 0 else 0.0
+                    prof[k["name"]] = {"launches": k["launches"], "ms_per_launch": k["ms"] / k["launches"],
+                                       "GBps": gbs, "frac_of_peak": gbs / hbm}
+            out["kernels"] = prof
+        s.close()
+    out["scalar_overhead"] = out["flow_T_C_ms_per_iter"] / out["flow_ms_per_iter"] - 1.0
+    return out
+
+
 def run_b200(args):
     world, rank, local, dist = dist_setup(args.gpus)
     import numpy as np
@@ -461,6 +498,11 @@ def run_b200(args):
     if args.network_only:
         if rank == 0:
             print(json.dumps(network_leg(abi, local, scale=1.512 * args.scale), default=_json_scalar), flush=True)
+        return
+    if args.scalars_only:
+        if rank == 0:
+            print(json.dumps(scalars_leg(abi, local, scale=args.scale, iters=max(1, args.steps)),
+                             default=_json_scalar), flush=True)
         return
     case = workload(args.scale)
     mesh = abi.multiblock(case.blocks)
