@@ -154,8 +154,11 @@ struct GradArgs {
     double* gR[5];
 };
 
+// Bounded to 4 resident CTAs per SM up to three fields (64 registers, no
+// spills); the four- and five-field forms of the scalar runs keep 3.
 template <int NF>
-__global__ void k_gradient(MeshDev m, const Ctl* ctl, GradArgs a, int scheme) {
+__global__ void __launch_bounds__(kThreads, NF <= 3 ? 4 : 3) k_gradient(MeshDev m, const Ctl* ctl, GradArgs a,
+                                                                       int scheme) {
     pdlEnter();
     if (ctl && ctl->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
