@@ -39,6 +39,7 @@ EXPORTS = [
     "axisim_learned_get_sample", "axisim_learned_init", "axisim_learned_params", "axisim_learned_grad",
     "axisim_learned_train", "axisim_learned_enable", "axisim_learned_stats", "axisim_learned_predict",
     "axisim_set_kinetics", "axisim_set_scalars", "axisim_scalar_residuals", "axisim_set_mesh_type",
+    "axisim_trellis_build", "axisim_triangle_mesh_build", "axisim_classify_boundary_faces",
 ]
 VAR_U, VAR_V, VAR_P, VAR_T, VAR_C = range(5)
 VAR_INDEX = {"u": VAR_U, "v": VAR_V, "p": VAR_P, "T": VAR_T, "C": VAR_C}
@@ -65,6 +66,11 @@ class BCField(C.Structure):
 class Kinetics(C.Structure):
     _fields_ = [("nGroups", C.c_int32), ("vmaxByGroup", _f64p), ("kmByGroup", _f64p), ("nByGroup", _f64p),
                 ("mByGroup", _f64p), ("k2ByGroup", _f64p), ("v2ByGroup", _f64p), ("RtotByGroup", _f64p)]
+
+
+class OutlineC(C.Structure):
+    _fields_ = [("nVertices", C.c_int32), ("vertexZ", _f64p), ("vertexR", _f64p), ("nEdges", C.c_int32),
+                ("edgeV0", _i32p), ("edgeV1", _i32p), ("edgeGroup", _i32p)]
 
 
 class ConfigSolver(C.Structure):
@@ -181,6 +187,13 @@ def lib():
             "axisim_mesh_free": (C.c_int, [vp]),
             "axisim_resolve_bc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, _u8p,
                                             _f64p, _u8p]),
+            "axisim_trellis_build": (C.c_int, [C.c_int32, _f64p, C.c_int32, _f64p, _i32p, _i32p,
+                                               C.POINTER(OutlineC), C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                               C.POINTER(vp), _i32p]),
+            "axisim_triangle_mesh_build": (C.c_int, [C.c_int32, _f64p, _f64p, C.c_int32, _i32p,
+                                                     C.POINTER(OutlineC), C.c_double, C.c_double, C.POINTER(vp)]),
+            "axisim_classify_boundary_faces": (C.c_int, [C.c_int32, _i32p, _f64p, _f64p, C.POINTER(OutlineC),
+                                                         C.c_double, C.c_double, _i32p]),
             "axisim_profile_iteration": (C.c_int, [vp, C.c_int32, C.POINTER(KernelStat), C.c_int32, _i32p]),
             "axisim_set_batch": (C.c_int, [vp, C.c_int32, _i32p]),
             "axisim_batch_status": (C.c_int, [vp, _i32p, _f64p, C.c_int32]),
@@ -219,11 +232,17 @@ def multiblock(blocks, tol=1e-9, default_group=-1):
     st = L.axisim_multiblock_build(len(blocks), arr, tol, default_group, C.byref(h), C.byref(seam))
     if st != OK:
         raise AxisimError(st, "multiblock build failed")
+    return _take_mesh(h, seam.value, MESH_STRUCTURED)
+
+
+def _take_mesh(h, status, mesh_type):
+    """Copies a library-built mesh into numpy arrays and frees it."""
+    L = lib()
     v = MeshPacked()
     L.axisim_mesh_view(h, C.byref(v))
     n, f = v.nCells, v.nFaces
     r = v.cellFaceStart[n]
-    m = {"nCells": n, "nFaces": f, "status": seam.value, "meshType": MESH_STRUCTURED}
+    m = {"nCells": n, "nFaces": f, "status": status, "meshType": mesh_type}
     sizes = dict(faceOwner=f, faceNeighbor=f, faceNormalZ=f, faceNormalR=f, faceCenterZ=f, faceCenterR=f,
                  faceArea=f, faceBoundaryGroupID=f, cellCenterZ=n, cellCenterR=n, cellArea2D=n, cellVolume=n,
                  cellFaceStart=n + 1, cellFaceIDs=r)
@@ -232,6 +251,67 @@ def multiblock(blocks, tol=1e-9, default_group=-1):
         m[k] = np.ctypeslib.as_array(ptr, shape=(sizes[k],)).copy()
     L.axisim_mesh_free(h)
     return m
+
+
+def outline_struct(vertices, edges, groups):
+    """vertices (V, 2) as (z, r); edges (E, 2) vertex ids; groups (E,) boundary
+    group per edge (-1 = none). Returns (struct, arrays kept alive)."""
+    v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 2)
+    e = np.ascontiguousarray(edges, dtype=np.int32).reshape(-1, 2)
+    keep = [np.ascontiguousarray(v[:, 0]), np.ascontiguousarray(v[:, 1]), np.ascontiguousarray(e[:, 0]),
+            np.ascontiguousarray(e[:, 1]), np.ascontiguousarray(groups, dtype=np.int32)]
+    s = OutlineC(len(v), keep[0].ctypes.data_as(_f64p), keep[1].ctypes.data_as(_f64p), len(e),
+                 keep[2].ctypes.data_as(_i32p), keep[3].ctypes.data_as(_i32p), keep[4].ctypes.data_as(_i32p))
+    return s, keep
+
+
+def trellis(z_lines, r_lines, z_cells, r_cells, outline, L, R, nz=1, nr=1):
+    """Mesh::buildStructuredMultiBlock through the library: a uniform block per
+    trellis cell inside `outline` ((vertices, edges, groups)), external faces
+    classified by the nearest outline edge. Returns the packed-mesh dict."""
+    z = np.ascontiguousarray(z_lines, dtype=np.float64)
+    r = np.ascontiguousarray(r_lines, dtype=np.float64)
+    zc = np.ascontiguousarray(z_cells, dtype=np.int32)
+    rc = np.ascontiguousarray(r_cells, dtype=np.int32)
+    o, keep = outline_struct(*outline)
+    h = C.c_void_p()
+    seam = C.c_int32(0)
+    st = lib().axisim_trellis_build(len(z), z.ctypes.data_as(_f64p), len(r), r.ctypes.data_as(_f64p),
+                                    zc.ctypes.data_as(_i32p), rc.ctypes.data_as(_i32p), C.byref(o), L, R, nz, nr,
+                                    C.byref(h), C.byref(seam))
+    if st != OK:
+        raise AxisimError(st, "trellis build failed")
+    return _take_mesh(h, seam.value, MESH_STRUCTURED)
+
+
+def triangle_mesh(points, tris, outline, L, R):
+    """Mesh::createUnstructuredMesh through the library, external faces
+    classified by the nearest edge of `outline`."""
+    p = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 2)
+    pz, pr = np.ascontiguousarray(p[:, 0]), np.ascontiguousarray(p[:, 1])
+    t = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1, 3)
+    o, keep = outline_struct(*outline)
+    h = C.c_void_p()
+    st = lib().axisim_triangle_mesh_build(len(p), pz.ctypes.data_as(_f64p), pr.ctypes.data_as(_f64p), len(t),
+                                          t.ctypes.data_as(_i32p), C.byref(o), L, R, C.byref(h))
+    if st != OK:
+        raise AxisimError(st, "triangle mesh build failed")
+    return _take_mesh(h, 0, MESH_UNSTRUCTURED)
+
+
+def classify_boundary_faces(mesh, outline, L, R):
+    """Mesh::classifyBoundaryFaces on a packed-mesh dict (in place)."""
+    o, keep = outline_struct(*outline)
+    nb = np.ascontiguousarray(mesh["faceNeighbor"], dtype=np.int32)
+    fz = np.ascontiguousarray(mesh["faceCenterZ"], dtype=np.float64)
+    fr = np.ascontiguousarray(mesh["faceCenterR"], dtype=np.float64)
+    g = np.ascontiguousarray(mesh["faceBoundaryGroupID"], dtype=np.int32).copy()
+    st = lib().axisim_classify_boundary_faces(len(nb), nb.ctypes.data_as(_i32p), fz.ctypes.data_as(_f64p),
+                                              fr.ctypes.data_as(_f64p), C.byref(o), L, R, g.ctypes.data_as(_i32p))
+    if st != OK:
+        raise AxisimError(st, "classification failed")
+    mesh["faceBoundaryGroupID"] = g
+    return mesh
 
 
 def resolve_bc(boundary_type, variable, user=None):

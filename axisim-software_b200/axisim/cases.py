@@ -313,6 +313,23 @@ def with_scalars(case, energy=True, concentration=True, t_in=310.0, t_wall=300.0
     return case
 
 
+def polygon_outline(points, groups):
+    """A closed outline loop: points [(z, r), ...] in order, groups[i] the
+    boundary group of the edge from point i to point i + 1 (the last edge
+    closes the loop). Returns (vertices, edges, groups) as the mesh builders
+    take them."""
+    n = len(points)
+    edges = [(i, (i + 1) % n) for i in range(n)]
+    return np.asarray(points, np.float64), np.asarray(edges, np.int32), np.asarray(groups, np.int32)
+
+
+def expansion_outline(r_in=0.002, r_out=0.006, l_in=0.04, l_out=0.12, g_in=0, g_out=1, g_wall=2, g_axis=3):
+    """The sudden expansion's outline with the groups expansion() uses."""
+    L = l_in + l_out
+    pts = [(0.0, 0.0), (L, 0.0), (L, r_out), (l_in, r_out), (l_in, r_in), (0.0, r_in)]
+    return polygon_outline(pts, [g_axis, g_out, g_wall, g_wall, g_wall, g_in])
+
+
 def cell_count(case):
     return sum(int(b["axial"][1]) * int(b["radial"][1]) for b in case.blocks)
 

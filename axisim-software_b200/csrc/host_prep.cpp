@@ -1,11 +1,14 @@
-// host_prep.cpp -- multiblock packer, agglomeration hierarchy, colouring and
-// boundary defaults (host side, once per solve). Behaviour follows the
-// reference files cited per routine; the code is this project's own.
+// host_prep.cpp -- multiblock packer, trellis / triangle mesh builders with
+// boundary classification, agglomeration hierarchy, colouring and boundary
+// defaults (host side, once per solve). Behaviour follows the reference
+// files cited per routine; the code is this project's own.
 #include "host_prep.hpp"
 
 #include <algorithm>
 #include <cmath>
 #include <numeric>
+#include <stdexcept>
+#include <unordered_map>
 
 namespace axisim {
 
@@ -240,6 +243,173 @@ PackedMesh buildMultiblock(const std::vector<BlockSpec>& spec, double tol, int d
     m.cellFaceIDs.reserve((size_t)m.cellFaceStart[(size_t)total]);
     for (int c = 0; c < total; c++)
         m.cellFaceIDs.insert(m.cellFaceIDs.end(), cellFaces[(size_t)c].begin(), cellFaces[(size_t)c].end());
+    return m;
+}
+
+// ---------------- domain outline, trellis and triangle meshes ----------------
+
+bool pointInsideDomain(const Outline& o, double z, double r) {
+    bool inside = false;
+    const int nv = (int)o.vz.size();
+    for (size_t e = 0; e < o.e0.size(); e++) {
+        const int v0 = o.e0[e], v1 = o.e1[e];
+        if (v0 < 0 || v1 < 0 || v0 >= nv || v1 >= nv) continue;
+        const double az = o.vz[(size_t)v0], ar = o.vr[(size_t)v0];
+        const double bz = o.vz[(size_t)v1], br = o.vr[(size_t)v1];
+        const bool straddles = (ar > r) != (br > r);
+        if (!straddles) continue;
+        const double zCross = az + (r - ar) * (bz - az) / (br - ar);
+        if (z < zCross) inside = !inside;
+    }
+    return inside;
+}
+
+int groupAtPoint(const Outline& o, double z, double r, double tol) {
+    int best = -1;
+    double bestDist = tol;
+    const int nv = (int)o.vz.size();
+    for (size_t e = 0; e < o.e0.size(); e++) {
+        if (o.group[e] < 0) continue;
+        const int v0 = o.e0[e], v1 = o.e1[e];
+        if (v0 < 0 || v1 < 0 || v0 >= nv || v1 >= nv) continue;
+        // closestPointOnSegment + distance (math_func.cpp:75-80, 152-169)
+        const double az = o.vz[(size_t)v0], ar = o.vr[(size_t)v0];
+        const double abZ = o.vz[(size_t)v1] - az, abR = o.vr[(size_t)v1] - ar;
+        const double apZ = z - az, apR = r - ar;
+        const double ab2 = abZ * abZ + abR * abR;
+        double qz = az, qr = ar;
+        if (!(ab2 <= 1e-30)) {
+            double t = (apZ * abZ + apR * abR) / ab2;
+            t = std::clamp(t, 0.0, 1.0);
+            qz = az + t * abZ;
+            qr = ar + t * abR;
+        }
+        const double dz = qz - z, dr = qr - r;
+        const double dist = std::sqrt(dz * dz + dr * dr);
+        if (dist < bestDist) {
+            bestDist = dist;
+            best = o.group[e];
+        }
+    }
+    return best;
+}
+
+void classifyBoundaryFaces(PackedMesh& m, const Outline& o, double L, double R) {
+    const double matchTol = 1e-4 * std::max(std::max(L, R), 1.0);
+    for (int f = 0; f < m.nFaces; f++) {
+        if (m.faceNeighbor[(size_t)f] >= 0) continue;
+        m.faceBoundaryGroupID[(size_t)f] = groupAtPoint(o, m.faceCenterZ[(size_t)f], m.faceCenterR[(size_t)f], matchTol);
+    }
+}
+
+PackedMesh buildTrellis(const std::vector<double>& zL, const std::vector<double>& rL, const std::vector<int>& zCells,
+                        const std::vector<int>& rCells, const Outline& o, double L, double R, int nz, int nr,
+                        int& seamStatus) {
+    std::vector<BlockSpec> blocks;
+    if (zL.size() >= 2 && rL.size() >= 2) {
+        for (size_t i = 0; i + 1 < zL.size(); i++)
+            for (size_t j = 0; j + 1 < rL.size(); j++) {
+                const double cz = 0.5 * (zL[i] + zL[i + 1]), cr = 0.5 * (rL[j] + rL[j + 1]);
+                if (!pointInsideDomain(o, cz, cr)) continue;
+                BlockSpec b;
+                b.z0 = zL[i];
+                b.r0 = rL[j];
+                b.axialLength = zL[i + 1] - zL[i];
+                b.axialCells = std::max(zCells[i], 1);
+                b.radialLength = rL[j + 1] - rL[j];
+                b.radialCells = std::max(rCells[j], 1);
+                blocks.push_back(b);
+            }
+    }
+    if (blocks.empty()) {
+        BlockSpec b;
+        b.axialLength = L;
+        b.axialCells = std::max(nz, 1);
+        b.radialLength = R;
+        b.radialCells = std::max(nr, 1);
+        blocks.push_back(b);
+    }
+    // trellis blocks share full edges: every seam is conformal
+    PackedMesh m = buildMultiblock(blocks, std::max(L, R) * 1e-6, -1, seamStatus);
+    classifyBoundaryFaces(m, o, L, R);
+    return m;
+}
+
+PackedMesh buildTriangleMesh(const std::vector<double>& pz, const std::vector<double>& pr,
+                             const std::vector<int32_t>& tri, const Outline& o, double L, double R) {
+    constexpr double kPi = 3.14159265358979323846;
+    const int T = (int)(tri.size() / 3);
+    const int P = (int)pz.size();
+    PackedMesh m;
+    m.nCells = T;
+    m.cellCenterZ.resize((size_t)T);
+    m.cellCenterR.resize((size_t)T);
+    m.cellArea2D.resize((size_t)T);
+    m.cellVolume.resize((size_t)T);
+    for (int c = 0; c < T; c++) {
+        const int v[3] = {tri[3 * (size_t)c], tri[3 * (size_t)c + 1], tri[3 * (size_t)c + 2]};
+        for (int k = 0; k < 3; k++)
+            if (v[k] < 0 || v[k] >= P) throw std::runtime_error("triangle vertex out of range");
+        const double az = pz[(size_t)v[0]], ar = pr[(size_t)v[0]];
+        const double bz = pz[(size_t)v[1]], br = pr[(size_t)v[1]];
+        const double dz_ = pz[(size_t)v[2]], dr_ = pr[(size_t)v[2]];
+        m.cellCenterZ[(size_t)c] = (az + bz + dz_) / 3.0;   // triangleCentroid (mesh.cpp:1549-1554)
+        m.cellCenterR[(size_t)c] = (ar + br + dr_) / 3.0;
+        const double dz1 = bz - az, dr1 = br - ar, dz2 = dz_ - az, dr2 = dr_ - ar;
+        m.cellArea2D[(size_t)c] = 0.5 * std::abs(dz1 * dr2 - dr1 * dz2);  // triangleArea2D
+        m.cellVolume[(size_t)c] = 2.0 * kPi * m.cellCenterR[(size_t)c] * m.cellArea2D[(size_t)c];
+    }
+    std::unordered_map<int64_t, int32_t> edgeToFace;
+    edgeToFace.reserve((size_t)T * 2);
+    std::vector<int32_t> uses;
+    m.cellFaceStart.assign((size_t)T + 1, 0);
+    m.cellFaceIDs.reserve((size_t)T * 3);
+    auto addEdge = [&](int c, int v0, int v1) {
+        const int64_t key = (int64_t)std::min(v0, v1) * P + std::max(v0, v1);
+        auto it = edgeToFace.find(key);
+        if (it == edgeToFace.end()) {
+            const double p0z = pz[(size_t)v0], p0r = pr[(size_t)v0], p1z = pz[(size_t)v1], p1r = pr[(size_t)v1];
+            const double fz = 0.5 * (p0z + p1z), fr = 0.5 * (p0r + p1r);
+            const double dz = p1z - p0z, dr = p1r - p0r;
+            const double len = std::sqrt(dz * dz + dr * dr);
+            double nzv = dr, nrv = -dz;
+            const double mag = std::sqrt(nzv * nzv + nrv * nrv);
+            if (mag > 1e-30) {
+                nzv /= mag;
+                nrv /= mag;
+            }
+            const double tz = fz - m.cellCenterZ[(size_t)c], tr = fr - m.cellCenterR[(size_t)c];
+            if (nzv * tz + nrv * tr < 0.0) {
+                nzv *= -1.0;
+                nrv *= -1.0;
+            }
+            const int32_t id = m.nFaces++;
+            m.faceOwner.push_back(c);
+            m.faceNeighbor.push_back(-1);
+            m.faceBoundaryGroupID.push_back(-1);
+            m.faceCenterZ.push_back(fz);
+            m.faceCenterR.push_back(fr);
+            m.faceArea.push_back(2.0 * kPi * fr * len);
+            m.faceNormalZ.push_back(nzv);
+            m.faceNormalR.push_back(nrv);
+            uses.push_back(1);
+            edgeToFace.emplace(key, id);
+            m.cellFaceIDs.push_back(id);
+        } else {
+            const int32_t id = it->second;
+            if (++uses[(size_t)id] > 2) throw std::runtime_error("an edge is shared by more than two triangles");
+            m.faceNeighbor[(size_t)id] = c;
+            m.cellFaceIDs.push_back(id);
+        }
+    };
+    for (int c = 0; c < T; c++) {
+        const int v0 = tri[3 * (size_t)c], v1 = tri[3 * (size_t)c + 1], v2 = tri[3 * (size_t)c + 2];
+        addEdge(c, v0, v1);
+        addEdge(c, v1, v2);
+        addEdge(c, v2, v0);
+        m.cellFaceStart[(size_t)c + 1] = (int32_t)m.cellFaceIDs.size();
+    }
+    classifyBoundaryFaces(m, o, L, R);
     return m;
 }
 

@@ -1,7 +1,9 @@
 // host_prep.hpp -- host-side case preparation for the B200 SIMPLE solver.
 //
 // Pieces of the reference that run once per solve on the CPU: the multiblock
-// packer (structs/multiblock.h), the agglomeration hierarchy
+// packer (structs/multiblock.h), the trellis builder and boundary-face
+// classification of Mesh (solver/source/mesh.cpp), the triangle-mesh builder,
+// the agglomeration hierarchy
 // (solver/source/multigrid.cu:79-325), the greedy colouring
 // (manager/source/memory_manger.cpp:325-409) and the boundary defaults
 // (manager/source/boundary_func.cpp:104-201, 333-378).
@@ -34,6 +36,35 @@ struct BlockSpec {
 // seamStatus = 1 when a non-conformal seam made every interface drop.
 PackedMesh buildMultiblock(const std::vector<BlockSpec>& blocks, double tol, int defaultGroup,
                            int& seamStatus);
+
+// Domain outline as Mesh keeps it (BoundaryVertex / BoundaryEdge,
+// structs/boundary_struct.h:408-490): vertex positions and edges between
+// them, each edge with its boundary group (-1 = unassigned).
+struct Outline {
+    std::vector<double> vz, vr;
+    std::vector<int32_t> e0, e1, group;
+};
+
+// Mesh::pointInsideDomain (mesh.cpp:1177-1205): even-odd ray cast along +z
+// against every edge, so obstacle loops make holes.
+bool pointInsideDomain(const Outline& o, double z, double r);
+// groupAtPoint (manager/source/math_func.cpp:175-196): the group of the
+// nearest grouped edge closer than tol, else -1.
+int groupAtPoint(const Outline& o, double z, double r, double tol);
+// Mesh::classifyBoundaryFaces (mesh.cpp:1835-1846): every external face takes
+// the group of the nearest outline edge, tolerance 1e-4 max(L, R, 1).
+void classifyBoundaryFaces(PackedMesh& m, const Outline& o, double L, double R);
+// Mesh::buildStructuredMultiBlock (mesh.cpp:2717-2762) from trellis lines and
+// band cell counts (a uniform block per trellis cell whose centre lies inside
+// the outline; one nz x nr block over [0, L] x [0, R] when none does), packed,
+// then classified as createMultiBlockFVMesh does (mesh.cpp:2458-2460).
+PackedMesh buildTrellis(const std::vector<double>& zLines, const std::vector<double>& rLines,
+                        const std::vector<int>& zCells, const std::vector<int>& rCells, const Outline& o, double L,
+                        double R, int nz, int nr, int& seamStatus);
+// Mesh::createUnstructuredMesh (mesh.cpp:1848-2002): triangles (3 vertex ids
+// each) over shared points, faces in triangle-edge order, then classified.
+PackedMesh buildTriangleMesh(const std::vector<double>& pz, const std::vector<double>& pr,
+                             const std::vector<int32_t>& tri, const Outline& o, double L, double R);
 
 // One multigrid level's graph, CSR exactly as GridLevel (multigrid.cuh:29-68).
 struct GridLevel {

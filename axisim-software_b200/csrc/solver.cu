@@ -2385,6 +2385,83 @@ int axisim_multiblock_build(int32_t nBlocks, const axisim_block_spec* blocks, do
     }
 }
 
+namespace {
+// Copies and checks an outline; false when an array it needs is missing.
+bool outlineFrom(const axisim_outline* o, axisim::Outline& d) {
+    if (!o || o->nVertices < 0 || o->nEdges < 0) return false;
+    if (o->nVertices > 0 && (!o->vertexZ || !o->vertexR)) return false;
+    if (o->nEdges > 0 && (!o->edgeV0 || !o->edgeV1 || !o->edgeGroup)) return false;
+    d.vz.assign(o->vertexZ, o->vertexZ + o->nVertices);
+    d.vr.assign(o->vertexR, o->vertexR + o->nVertices);
+    d.e0.assign(o->edgeV0, o->edgeV0 + o->nEdges);
+    d.e1.assign(o->edgeV1, o->edgeV1 + o->nEdges);
+    d.group.assign(o->edgeGroup, o->edgeGroup + o->nEdges);
+    return true;
+}
+}  // namespace
+
+int axisim_trellis_build(int32_t nZLines, const double* zLines, int32_t nRLines, const double* rLines,
+                         const int32_t* zBandCells, const int32_t* rBandCells, const axisim_outline* outline,
+                         double L, double R, int32_t nz, int32_t nr, axisim_mesh** out, int32_t* seamStatus) {
+    if (!out || nZLines < 0 || nRLines < 0) return AXISIM_E_ARG;
+    if ((nZLines > 0 && (!zLines || !zBandCells)) || (nRLines > 0 && (!rLines || !rBandCells))) return AXISIM_E_ARG;
+    axisim::Outline o;
+    if (!outlineFrom(outline, o)) return AXISIM_E_ARG;
+    for (int i = 0; i + 1 < nZLines; i++)
+        if (!(zLines[i + 1] > zLines[i])) return AXISIM_E_ARG;
+    for (int j = 0; j + 1 < nRLines; j++)
+        if (!(rLines[j + 1] > rLines[j])) return AXISIM_E_ARG;
+    try {
+        std::vector<double> zL(zLines, zLines + nZLines), rL(rLines, rLines + nRLines);
+        std::vector<int> zc(zBandCells, zBandCells + std::max(nZLines - 1, 0));
+        std::vector<int> rc(rBandCells, rBandCells + std::max(nRLines - 1, 0));
+        int seam = 0;
+        auto* m = new axisim_mesh;
+        m->m = axisim::buildTrellis(zL, rL, zc, rc, o, L, R, nz, nr, seam);
+        if (seamStatus) *seamStatus = seam;
+        *out = m;
+        return AXISIM_OK;
+    } catch (...) {
+        return AXISIM_E_MESH;
+    }
+}
+
+int axisim_triangle_mesh_build(int32_t nPoints, const double* pointZ, const double* pointR, int32_t nTriangles,
+                               const int32_t* triangles, const axisim_outline* outline, double L, double R,
+                               axisim_mesh** out) {
+    if (!out || nPoints <= 0 || nTriangles <= 0 || !pointZ || !pointR || !triangles) return AXISIM_E_ARG;
+    axisim::Outline o;
+    if (!outlineFrom(outline, o)) return AXISIM_E_ARG;
+    try {
+        std::vector<double> pz(pointZ, pointZ + nPoints), pr(pointR, pointR + nPoints);
+        std::vector<int32_t> tri(triangles, triangles + 3 * (size_t)nTriangles);
+        auto* m = new axisim_mesh;
+        try {
+            m->m = axisim::buildTriangleMesh(pz, pr, tri, o, L, R);
+        } catch (...) {
+            delete m;
+            throw;
+        }
+        *out = m;
+        return AXISIM_OK;
+    } catch (...) {
+        return AXISIM_E_MESH;
+    }
+}
+
+int axisim_classify_boundary_faces(int32_t nFaces, const int32_t* faceNeighbor, const double* faceCenterZ,
+                                   const double* faceCenterR, const axisim_outline* outline, double L, double R,
+                                   int32_t* faceBoundaryGroupID) {
+    if (nFaces < 0 || (nFaces > 0 && (!faceNeighbor || !faceCenterZ || !faceCenterR || !faceBoundaryGroupID)))
+        return AXISIM_E_ARG;
+    axisim::Outline o;
+    if (!outlineFrom(outline, o)) return AXISIM_E_ARG;
+    const double tol = 1e-4 * std::max(std::max(L, R), 1.0);
+    for (int f = 0; f < nFaces; f++)
+        if (faceNeighbor[f] < 0) faceBoundaryGroupID[f] = axisim::groupAtPoint(o, faceCenterZ[f], faceCenterR[f], tol);
+    return AXISIM_OK;
+}
+
 int axisim_mesh_sizes(const axisim_mesh* m, int32_t* nCells, int32_t* nFaces, int32_t* nRefs) {
     if (!m) return AXISIM_E_ARG;
     if (nCells) *nCells = m->m.nCells;

@@ -419,6 +419,46 @@ int axisim_mesh_sizes(const axisim_mesh* m, int32_t* nCells, int32_t* nFaces, in
 int axisim_mesh_view(const axisim_mesh* m, axisim_mesh_packed* view);
 int axisim_mesh_free(axisim_mesh* m);
 
+/* The domain outline as Mesh keeps it (BoundaryVertex / BoundaryEdge,
+ * structs/boundary_struct.h:408-490): vertex positions and the edges between
+ * them, each with its boundary group (-1 = unassigned). Obstacle loops are
+ * more edges of the same outline. */
+typedef struct axisim_outline {
+    int32_t nVertices;
+    const double* vertexZ;
+    const double* vertexR;
+    int32_t nEdges;
+    const int32_t* edgeV0;
+    const int32_t* edgeV1;
+    const int32_t* edgeGroup;
+} axisim_outline;
+/* Mesh::buildStructuredMultiBlock + createMultiBlockFVMesh (mesh.cpp:2717-2762,
+ * 2364-2462): trellis lines zLines[nZLines] and rLines[nRLines] (ascending)
+ * cut the domain into cells; each trellis cell whose centre lies inside the
+ * outline (even-odd ray cast, Mesh::pointInsideDomain, mesh.cpp:1177-1205)
+ * becomes a uniform block of zBandCells[i] x rBandCells[j] cells; with none
+ * inside, one nz x nr block covers [0, L] x [0, R]. Blocks are joined and
+ * packed as axisim_multiblock_build does, then every external face takes the
+ * group of the nearest grouped outline edge within 1e-4 max(L, R, 1)
+ * (Mesh::classifyBoundaryFaces, mesh.cpp:1835-1846). */
+int axisim_trellis_build(int32_t nZLines, const double* zLines, int32_t nRLines, const double* rLines,
+                         const int32_t* zBandCells, const int32_t* rBandCells, const axisim_outline* outline,
+                         double L, double R, int32_t nz, int32_t nr, axisim_mesh** out, int32_t* seamStatus);
+/* Mesh::createUnstructuredMesh (mesh.cpp:1848-2002): nTriangles triangles
+ * (3 point ids each) over nPoints shared points; cell centre the vertex mean,
+ * volume 2 pi r_c A; faces created per triangle in edge order (v0 v1),
+ * (v1 v2), (v2 v0), owned by the first triangle to reach them, normal away
+ * from the owner, area 2 pi r_f L; external faces classified as above.
+ * An edge shared by more than two triangles is rejected (AXISIM_E_MESH). */
+int axisim_triangle_mesh_build(int32_t nPoints, const double* pointZ, const double* pointR, int32_t nTriangles,
+                               const int32_t* triangles, const axisim_outline* outline, double L, double R,
+                               axisim_mesh** out);
+/* Mesh::classifyBoundaryFaces on a packed mesh the caller holds: rewrites
+ * faceBoundaryGroupID[f] for every face with faceNeighbor[f] < 0. */
+int axisim_classify_boundary_faces(int32_t nFaces, const int32_t* faceNeighbor, const double* faceCenterZ,
+                                   const double* faceCenterR, const axisim_outline* outline, double L, double R,
+                                   int32_t* faceBoundaryGroupID);
+
 /* BoundaryDefaults::getEffectiveBC + createBoundaryFieldHost for one group and
  * one variable (boundary_func.cpp:104-201, 333-378; memory_manger.cpp:96-109):
  * given the group's BoundaryType and the user's BC (hasUser = 0 for none),
