@@ -83,6 +83,7 @@ class Group:
     bcs: dict = field(default_factory=dict)
     total_length: float = 0.0
     layers: dict = field(default_factory=dict)
+    name: str = ""   # BoundarySegmentGroup::name (the OpenFOAM export derives patch names from it)
 
 
 def effective_bc(group, var):
