@@ -32,6 +32,12 @@ __device__ __forceinline__ void pdlEnter() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// Set on the host thread before a launch whose predecessor in the captured
+// graph is not a kernel (the first kernel of a conditional node's body, the
+// first kernel after that node): the next launchPDL then goes without the
+// programmatic attribute, and clears the flag.
+inline thread_local bool tNextLaunchPlain = false;
+
 template <typename... KArgs, typename... Args>
 inline cudaError_t launchPDL(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
                              Args&&... args) {
@@ -44,7 +50,8 @@ inline cudaError_t launchPDL(void (*kernel)(KArgs...), dim3 grid, dim3 block, si
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = tNextLaunchPlain ? 0 : 1;
+    tNextLaunchPlain = false;
     return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 

@@ -172,10 +172,16 @@ void launchFcgDots(const Ctl* ctl, int N, const float* e, const double* r, const
                    cudaStream_t s);
 void launchFcgSpmv(const Ctl* ctl, const LevelDev& L0, const float* e, const double* pOld, double* pNew, double* q,
                    int first, int pqOld, int pqNew, FcgScratch& f, cudaStream_t s);
-// next: 0 = x only, 1 = also r and (r, r), 2 = also the first sweep
+// next: 0 = x only, 1 = also r and (r, r), 2 = also the first sweep; the
+// solve stops (Ctl::ppSkip) at relTol or after maxIt iterations
 void launchFcgUpdate(Ctl* ctl, const LevelDev& L0, double* x, double* r, const double* p, const double* q,
                      FcgScratch& f, int pqSlot, float* r32, float* eFirst, double w, int next, double relTol,
-                     cudaStream_t s);
+                     int maxIt, cudaStream_t s);
+// condition of the conditional WHILE node that repeats the Krylov iterations
+// in a captured graph: head (before the node) resets the body count, tail
+// (last kernel of the body) counts one; both set run = solve not stopped and
+// fewer than maxBodies bodies run
+void launchFcgLoop(Ctl* ctl, FcgScratch& f, cudaGraphConditionalHandle h, int head, int maxBodies, cudaStream_t s);
 // per-solve choice between the learned first preconditioner and the V-cycle;
 // the learned one is z = alpha y + V-cycle(r - alpha A y), y the network's
 // output and alpha = (y, r) / (y, A y) its best scale (scalars [8..10])

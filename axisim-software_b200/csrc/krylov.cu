@@ -14,9 +14,13 @@
 //   V-cycle(r) -> e ; dots (r,e),(e,q) ; p = e + beta p, q = A p, (p,q) ;
 //   x += alpha p, r -= alpha q (and r in FP32 for the next V-cycle)
 // with no host round trip, inside the captured SIMPLE iteration. The solve
-// stops early once ||r||_2 <= relTol ||b||_2: the kernel that finds it sets
-// Ctl::ppSkip, every later kernel of the solve (the V-cycle's included) returns
-// at entry, and k_fcg_end clears the flag.
+// stops early once ||r||_2 <= relTol ||b||_2, or at its iteration cap: the
+// kernel that finds it sets Ctl::ppSkip, every later kernel of the solve (the
+// V-cycle's included) returns at entry, and k_fcg_end clears the flag. In a
+// captured graph the iterations after the first are the body of a conditional
+// WHILE node (two iterations per body), so a solve that stops early launches
+// at most one iteration's kernels past that point instead of running every
+// remaining iteration's kernels up to the cap as early returns.
 #include <cmath>
 
 #include "kernels.hpp"
@@ -183,8 +187,8 @@ __global__ void __launch_bounds__(kThreads) k_fcg_update(Ctl* ctl, LevelDev L, d
                                                          double* __restrict__ r, const double* __restrict__ p,
                                                          const double* __restrict__ q, double* s, int pqSlot,
                                                          float* __restrict__ r32, float* __restrict__ eFirst, double w,
-                                                         int next, double relTol, double* __restrict__ partial,
-                                                         unsigned int* counter) {
+                                                         int next, double relTol, int maxIt,
+                                                         double* __restrict__ partial, unsigned int* counter) {
     pdlEnter();
     if (ctl->done || ctl->ppSkip) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -205,13 +209,26 @@ __global__ void __launch_bounds__(kThreads) k_fcg_update(Ctl* ctl, LevelDev L, d
         }
     }
     if (!next) {
-        if (n == 0) ctl->ppIterations++;
+        if (n == 0) {
+            ctl->ppIterations++;
+            if (ctl->ppIterations - (long long)s[6] >= maxIt) ctl->ppSkip = 1;
+        }
         return;
     }
     if (gridSum<1>(acc, partial, counter, s + 5)) {
         ctl->ppIterations++;
-        if (s[5] <= relTol * relTol * s[4]) ctl->ppSkip = 1;
+        if (s[5] <= relTol * relTol * s[4] || ctl->ppIterations - (long long)s[6] >= maxIt) ctl->ppSkip = 1;
     }
+}
+
+// Condition of the WHILE node over the Krylov iterations; s[15] counts the
+// bodies run in this solve, so the loop ends after maxBodies bodies even if
+// the iteration cap in k_fcg_update were never reached.
+__global__ void k_fcg_loop(const Ctl* ctl, double* s, cudaGraphConditionalHandle h, int head, int maxBodies) {
+    pdlEnter();
+    s[15] = head ? 0.0 : s[15] + 1.0;
+    const bool run = !ctl->done && !ctl->ppSkip && s[15] < (double)maxBodies;
+    cudaGraphSetConditional(h, run ? 1u : 0u);
 }
 
 // Chooses, for this solve, between the learned first preconditioner and the
@@ -337,9 +354,13 @@ void launchFcgSpmv(const Ctl* ctl, const LevelDev& L0, const float* e, const dou
 
 void launchFcgUpdate(Ctl* ctl, const LevelDev& L0, double* x, double* r, const double* p, const double* q,
                      FcgScratch& f, int pqSlot, float* r32, float* eFirst, double w, int next, double relTol,
-                     cudaStream_t s) {
+                     int maxIt, cudaStream_t s) {
     launchPDL(k_fcg_update, dim3(blocksFor(L0.N)), dim3(kThreads), 0, s, ctl, L0, x, r, p, q, f.scalars, pqSlot, r32,
-              eFirst, w, next, relTol, f.partial, f.counter + 1);
+              eFirst, w, next, relTol, maxIt, f.partial, f.counter + 1);
+}
+
+void launchFcgLoop(Ctl* ctl, FcgScratch& f, cudaGraphConditionalHandle h, int head, int maxBodies, cudaStream_t s) {
+    launchPDL(k_fcg_loop, dim3(1), dim3(1), 0, s, (const Ctl*)ctl, f.scalars, h, head, maxBodies);
 }
 
 void launchFcgGate(Ctl* ctl, NetStats* ns, int always, cudaStream_t s) {

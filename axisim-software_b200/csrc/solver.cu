@@ -106,6 +106,7 @@ public:
         if (ev0_) cudaEventDestroy(ev0_);
         if (ev1_) cudaEventDestroy(ev1_);
         if (stream_) cudaStreamDestroy(stream_);
+        if (loopStream_) cudaStreamDestroy(loopStream_);
     }
 
     // Every entry point makes the handle's device current on the calling thread.
@@ -709,6 +710,7 @@ private:
     double curProlong_ = 1.0;    // scale of the cycle being captured
 
     cudaStream_t stream_ = nullptr;
+    cudaStream_t loopStream_ = nullptr;  // captures the body of the Krylov loop's WHILE node
     volatile int* hostStop_ = nullptr;
     int* hostStopDev_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
@@ -1226,59 +1228,112 @@ private:
     }
 
     // Flexible CG on the FP64 p' system with one FP32 V-cycle (from zero) as the
-    // preconditioner of each iteration; cmg_.maxIter iterations.
+    // preconditioner of each iteration; at most cmg_.maxIter iterations. Inside a
+    // stream capture of a solve with a tolerance, iterations 1.. are the body of
+    // a conditional WHILE node (two iterations per body, so the direction
+    // buffers keep their parity), and the kernels of iterations past the
+    // stopping point are never launched.
     void enqueuePressureFcg() {
         enqueueGalerkin32();
         curProlong_ = prolongScale_;
         const bool firstSweep = (hier_[0].isCoarsest() ? cmg_.linearSweep : cmg_.linearPreSweep) >= 1;
-        const int L = (int)levels_.size();
         const int iters = cmg_.maxIter > 1 ? cmg_.maxIter : 1;
+        const int nextSweep = firstSweep ? 2 : 1;
         const double vb = 4.0;
         launchFcgInit(ctl_, levels_[0], pp_, fcgR_, r32pp_, levels32_[0].x, cmg_.weight, firstSweep ? 1 : 0,
                       psolveTol_, fcg_, stream_);
         mark("fcg_init", (double)N_ * (12.0 * W_ + 8.0 + 8.0 + 8.0 + 8.0 + vb + (firstSweep ? vb : 0.0)));
         const bool useNet = learnedMode_ != AXISIM_LEARNED_OFF && net_.ready();
-        for (int it = 0; it < iters; it++) {
-            std::vector<float*> cur((size_t)L), alt((size_t)L);
-            for (int l = 0; l < L; l++) {
-                cur[(size_t)l] = levels32_[(size_t)l].x;
-                alt[(size_t)l] = levels32_[(size_t)l].xNew;
+        fcgIteration(0, iters > 1 ? nextSweep : 1, iters, firstSweep, useNet);
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        CK(cudaStreamIsCapturing(stream_, &cap));
+        // the loop pays (two kernels per body, one edge without overlap) only
+        // where a solve can stop before its cap: a tolerance and a cap of 8 or more
+        if (iters >= 8 && psolveTol_ > 0.0 && cap == cudaStreamCaptureStatusActive) {
+            cudaGraph_t g = nullptr;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t nDeps = 0;
+            cudaGraphConditionalHandle h;
+            CK(cudaStreamGetCaptureInfo(stream_, &cap, nullptr, &g, &deps, &nDeps));
+            CK(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+            const int maxBodies = iters / 2;  // iterations 1 .. iters-1, two per body
+            launchFcgLoop(ctl_, fcg_, h, 1, maxBodies, stream_);
+            CK(cudaStreamGetCaptureInfo(stream_, &cap, nullptr, &g, &deps, &nDeps));
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            CK(cudaGraphAddNode(&node, g, deps, nDeps, &cp));
+            CK(cudaStreamUpdateCaptureDependencies(stream_, &node, 1, cudaStreamSetCaptureDependencies));
+            if (!loopStream_) CK(cudaStreamCreateWithFlags(&loopStream_, cudaStreamNonBlocking));
+            CK(cudaStreamBeginCaptureToGraph(loopStream_, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeThreadLocal));
+            std::swap(stream_, loopStream_);
+            try {
+                tNextLaunchPlain = true;
+                fcgIteration(1, nextSweep, iters, firstSweep, false);
+                fcgIteration(2, nextSweep, iters, firstSweep, false);
+                launchFcgLoop(ctl_, fcg_, h, 0, maxBodies, stream_);
+            } catch (...) {
+                std::swap(stream_, loopStream_);
+                cudaGraph_t body = nullptr;
+                cudaStreamEndCapture(loopStream_, &body);
+                tNextLaunchPlain = false;
+                throw;
             }
-            const bool netStep = useNet && it == 0;
-            // first iteration with the network: the gate picks the learned
-            // preconditioner z = alpha y + V-cycle(r - alpha A y), y =
-            // network(r), whose kernels run while ppSkip == 2, or the plain
-            // V-cycle
-            if (netStep) {
-                launchFcgGate(ctl_, netStats_, learnedMode_ == AXISIM_LEARNED_ALWAYS ? 1 : 0, stream_);
-                net_.infer(ctl_, 1, fcgR_, ACpp_, AFpp_, mesh_.snb, W_, nnY_, stream_);
-                mark("nn_infer", 0.0);
-                launchNnResidual(ctl_, levels_[0], fcgR_, nnY_, nnAy_, fcg_, r32pp_, levels32_[0].x, cmg_.weight,
-                                 firstSweep ? 1 : 0, stream_);
-                mark("nn_residual", (double)N_ * (12.0 * W_ + 8.0 + 4.0 * W_ + 8.0 + 8.0 + 8.0 + 8.0 + 4.0 + 4.0));
-                launchFcgUngate(ctl_, stream_);
-            }
-            vcycleT<float>(levels32_, 0, cur, alt, firstSweep);
-            const float* e = cur[0];
-            if (netStep) {
-                launchNnCombine(ctl_, netStats_, N_, nnY_, fcg_, cur[0], stream_);
-                mark("nn_combine", 12.0 * N_);
-            }
-            launchFcgDots(ctl_, N_, e, fcgR_, fcgQ_, it > 0 ? 1 : 0, fcg_, stream_);
-            mark("fcg_dots", (double)N_ * (vb + 8.0 + (it > 0 ? 8.0 : 0.0)));
-            double* pOld = fcgP_[(it + 1) & 1];
-            double* pNew = fcgP_[it & 1];
-            const int pqOld = 2 + ((it + 1) & 1), pqNew = 2 + (it & 1);
-            launchFcgSpmv(ctl_, levels_[0], e, pOld, pNew, fcgQ_, it == 0 ? 1 : 0, pqOld, pqNew, fcg_, stream_);
-            mark("fcg_spmv", (double)N_ * (12.0 * W_ + 8.0 + vb + (it > 0 ? 8.0 : 0.0) + 16.0));
-            const int next = it + 1 < iters ? (firstSweep ? 2 : 1) : 1;
-            launchFcgUpdate(ctl_, levels_[0], pp_, fcgR_, pNew, fcgQ_, fcg_, pqNew, r32pp_, levels32_[0].x,
-                            cmg_.weight, next, psolveTol_, stream_);
-            mark("fcg_update", (double)N_ * (24.0 + 24.0 + vb + (next > 1 ? 8.0 + vb : 0.0)));
+            std::swap(stream_, loopStream_);
+            cudaGraph_t body = nullptr;
+            CK(cudaStreamEndCapture(loopStream_, &body));
+            tNextLaunchPlain = true;
+        } else {
+            for (int it = 1; it < iters; it++) fcgIteration(it, it + 1 < iters ? nextSweep : 1, iters, firstSweep, false);
         }
         launchFcgEnd(ctl_, fcg_, useNet ? netStats_ : nullptr, stream_);
         mark("fcg_end", 0.0);
         curProlong_ = 1.0;
+    }
+
+    // Krylov iteration `it` (its parity picks the direction buffers; 0 starts
+    // the directions and, with netStep, may take the learned step): V-cycle(r),
+    // dots, direction and A p, update of x and r.
+    void fcgIteration(int it, int next, int iters, bool firstSweep, bool netStep) {
+        const int L = (int)levels_.size();
+        const double vb = 4.0;
+        std::vector<float*> cur((size_t)L), alt((size_t)L);
+        for (int l = 0; l < L; l++) {
+            cur[(size_t)l] = levels32_[(size_t)l].x;
+            alt[(size_t)l] = levels32_[(size_t)l].xNew;
+        }
+        // with the network, the gate picks the learned preconditioner
+        // z = alpha y + V-cycle(r - alpha A y), y = network(r), whose kernels run
+        // while ppSkip == 2, or the plain V-cycle
+        if (netStep) {
+            launchFcgGate(ctl_, netStats_, learnedMode_ == AXISIM_LEARNED_ALWAYS ? 1 : 0, stream_);
+            net_.infer(ctl_, 1, fcgR_, ACpp_, AFpp_, mesh_.snb, W_, nnY_, stream_);
+            mark("nn_infer", 0.0);
+            launchNnResidual(ctl_, levels_[0], fcgR_, nnY_, nnAy_, fcg_, r32pp_, levels32_[0].x, cmg_.weight,
+                             firstSweep ? 1 : 0, stream_);
+            mark("nn_residual", (double)N_ * (12.0 * W_ + 8.0 + 4.0 * W_ + 8.0 + 8.0 + 8.0 + 8.0 + 4.0 + 4.0));
+            launchFcgUngate(ctl_, stream_);
+        }
+        vcycleT<float>(levels32_, 0, cur, alt, firstSweep);
+        const float* e = cur[0];
+        if (netStep) {
+            launchNnCombine(ctl_, netStats_, N_, nnY_, fcg_, cur[0], stream_);
+            mark("nn_combine", 12.0 * N_);
+        }
+        launchFcgDots(ctl_, N_, e, fcgR_, fcgQ_, it > 0 ? 1 : 0, fcg_, stream_);
+        mark("fcg_dots", (double)N_ * (vb + 8.0 + (it > 0 ? 8.0 : 0.0)));
+        double* pOld = fcgP_[(it + 1) & 1];
+        double* pNew = fcgP_[it & 1];
+        const int pqOld = 2 + ((it + 1) & 1), pqNew = 2 + (it & 1);
+        launchFcgSpmv(ctl_, levels_[0], e, pOld, pNew, fcgQ_, it == 0 ? 1 : 0, pqOld, pqNew, fcg_, stream_);
+        mark("fcg_spmv", (double)N_ * (12.0 * W_ + 8.0 + vb + (it > 0 ? 8.0 : 0.0) + 16.0));
+        launchFcgUpdate(ctl_, levels_[0], pp_, fcgR_, pNew, fcgQ_, fcg_, pqNew, r32pp_, levels32_[0].x, cmg_.weight,
+                        next, psolveTol_, iters, stream_);
+        mark("fcg_update", (double)N_ * (24.0 + 24.0 + vb + (next > 1 ? 8.0 + vb : 0.0)));
     }
 
     void enqueueMultigrid() {

@@ -73,6 +73,28 @@ def test_fcg_relative_tolerance_stops_early_and_keeps_the_solution():
     assert abi.lib().axisim_set_pressure_solver(early.h, abi.PSOLVE_FCG, 0.1, 0.0) == abi.E_ARG
 
 
+@pytest.mark.parametrize("cap", [9, 10])
+def test_fcg_conditional_loop_matches_unrolled_iterations_and_keeps_the_cap(cap):
+    """With a tolerance the captured solve repeats its Krylov iterations in a
+    conditional WHILE node (two per body); without one they are unrolled. A
+    tolerance no solve reaches runs every solve to the cap either way, so both
+    graphs compute the same iterations: same fields bit for bit, and exactly
+    cap iterations per solve for an odd and an even number of loop iterations."""
+    import numpy as np
+    case = cases.expansion(scale=1 / 8, max_iter=6, tol=1e-30)
+    mesh = abi.multiblock(case.blocks)
+    st = dict(case.settings, mgMaxIter=cap)
+    for prec in (abi.PREC_FP64, abi.PREC_MIXED):
+        loop = abi.Solver(mesh, case.bc_fields(), st, precision=prec, pressure_solver=abi.PSOLVE_FCG,
+                          pressure_tol=1e-300)
+        unrolled = abi.Solver(mesh, case.bc_fields(), st, precision=prec, pressure_solver=abi.PSOLVE_FCG)
+        ra, rb = loop.solve(), unrolled.solve()
+        assert ra["iterations"] == rb["iterations"] == 6
+        assert loop.pressure_stats() == unrolled.pressure_stats() == (6, 6 * cap)
+        for f in ("u", "v", "p"):
+            assert np.array_equal(loop.get(f), unrolled.get(f)), (prec, f)
+
+
 def test_fcg_over_corrected_preconditioner_converges_to_the_same_solution():
     case = cases.expansion(scale=1 / 16, max_iter=40000, tol=1e-8)
     mesh = abi.multiblock(case.blocks)
