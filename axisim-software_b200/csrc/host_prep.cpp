@@ -490,40 +490,58 @@ int aggregate(const GridLevel& fine, std::vector<int32_t>& c2c) {
     return next;
 }
 
-// Coarse CSR + fine slot -> coarse slot map (multigrid.cu:196-287).
+// Coarse CSR + fine slot -> coarse slot map (multigrid.cu:196-287): every
+// distinct (coarse cell, coarse neighbour) pair met across an aggregate
+// boundary, in ascending order of cell then neighbour, and for each fine slot
+// the coarse slot of its pair. Each aggregate's members (a counting sort of
+// the fine cells) give its boundary slots, a few dozen, which are sorted by
+// neighbour in place, so the cost is linear in the slots; the order of equal
+// pairs does not change the result.
 GridLevel coarsen(GridLevel& fine) {
     GridLevel coarse;
     const int nC = aggregate(fine, fine.cellToCoarse);
     coarse.nCells = nC;
-    struct Ref {
-        int cc, cn, slot;
-    };
-    std::vector<Ref> refs;
-    refs.reserve((size_t)fine.nFaceRefs());
-    for (int n = 0; n < fine.nCells; n++) {
-        const int cn = fine.cellToCoarse[(size_t)n];
-        for (int k = fine.faceStart[(size_t)n]; k < fine.faceStart[(size_t)n + 1]; k++) {
-            const int nb = fine.faceNeighbor[(size_t)k];
-            if (nb < 0) continue;
-            const int cb = fine.cellToCoarse[(size_t)nb];
-            if (cb != cn) refs.push_back(Ref{cn, cb, k});
-        }
+    const int N = fine.nCells;
+    const std::vector<int32_t>& c2c = fine.cellToCoarse;
+    std::vector<int32_t> mStart((size_t)nC + 1, 0), mList((size_t)N);
+    for (int n = 0; n < N; n++) mStart[(size_t)c2c[(size_t)n] + 1]++;
+    for (int c = 0; c < nC; c++) mStart[(size_t)c + 1] += mStart[(size_t)c];
+    {
+        std::vector<int32_t> fill(mStart.begin(), mStart.end() - 1);
+        for (int n = 0; n < N; n++) mList[(size_t)fill[(size_t)c2c[(size_t)n]]++] = n;
     }
-    std::sort(refs.begin(), refs.end(), [](const Ref& a, const Ref& b) {
-        return a.cc != b.cc ? a.cc < b.cc : a.cn < b.cn;
-    });
+    struct Ref {
+        int32_t cn, slot;
+    };
+    std::vector<Ref> buf;
     fine.fineSlotToCoarseSlot.assign((size_t)fine.nFaceRefs(), -1);
     coarse.faceStart.assign((size_t)nC + 1, 0);
-    coarse.faceNeighbor.reserve(refs.size());
-    for (size_t i = 0; i < refs.size(); i++) {
-        const bool fresh = i == 0 || refs[i].cc != refs[i - 1].cc || refs[i].cn != refs[i - 1].cn;
-        if (fresh) {
-            coarse.faceNeighbor.push_back(refs[i].cn);
-            coarse.faceStart[(size_t)refs[i].cc + 1]++;
+    coarse.faceNeighbor.reserve((size_t)fine.nFaceRefs() / 2);
+    for (int c = 0; c < nC; c++) {
+        buf.clear();
+        for (int q = mStart[(size_t)c]; q < mStart[(size_t)c + 1]; q++) {
+            const int n = mList[(size_t)q];
+            for (int k = fine.faceStart[(size_t)n]; k < fine.faceStart[(size_t)n + 1]; k++) {
+                const int nb = fine.faceNeighbor[(size_t)k];
+                if (nb < 0) continue;
+                const int cb = c2c[(size_t)nb];
+                if (cb != c) buf.push_back(Ref{cb, k});
+            }
         }
-        fine.fineSlotToCoarseSlot[(size_t)refs[i].slot] = (int)coarse.faceNeighbor.size() - 1;
+        Ref* b = buf.data();
+        Ref* e = b + buf.size();
+        if (e - b > 32)
+            std::sort(b, e, [](const Ref& x, const Ref& y) { return x.cn < y.cn; });
+        else
+            for (Ref* i = b + 1; i < e; i++)  // insertion sort by neighbour
+                for (Ref* j = i; j > b && (j - 1)->cn > j->cn; j--) std::swap(*(j - 1), *j);
+        for (Ref* i = b; i < e; i++) {
+            if (i == b || i->cn != (i - 1)->cn) coarse.faceNeighbor.push_back(i->cn);
+            fine.fineSlotToCoarseSlot[(size_t)i->slot] = (int)coarse.faceNeighbor.size() - 1;
+        }
+        coarse.faceStart[(size_t)c + 1] = (int)coarse.faceNeighbor.size();
     }
-    for (int c = 0; c < nC; c++) coarse.faceStart[(size_t)c + 1] += coarse.faceStart[(size_t)c];
+    coarse.faceNeighbor.shrink_to_fit();
     return coarse;
 }
 
