@@ -17,10 +17,12 @@
 // stops early once ||r||_2 <= relTol ||b||_2, or at its iteration cap: the
 // kernel that finds it sets Ctl::ppSkip, every later kernel of the solve (the
 // V-cycle's included) returns at entry, and k_fcg_end clears the flag. In a
-// captured graph the iterations after the first are the body of a conditional
-// WHILE node (two iterations per body), so a solve that stops early launches
-// at most one iteration's kernels past that point instead of running every
-// remaining iteration's kernels up to the cap as early returns.
+// captured graph of a solve with a tolerance and a cap of 8 or more, the
+// iterations after the first are the body of a conditional WHILE node (two
+// iterations per body), so a solve that stops early launches at most one
+// iteration's kernels past that point instead of running every remaining
+// iteration's kernels up to the cap as early returns; a solve without a
+// tolerance always runs to its cap and keeps its iterations unrolled.
 #include <cmath>
 
 #include "kernels.hpp"
