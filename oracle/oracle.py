@@ -1,7 +1,7 @@
 """ctypes binding of the CPU oracle (oracle/liborc.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
-cpu_baseline leg of bench.py as the checker. The product path never imports it.
+cpu_baseline leg of bench.py, to compare against. The product path never imports it.
 """
 import ctypes as C
 import os
