@@ -40,6 +40,7 @@ EXPORTS = [
     "axisim_learned_train", "axisim_learned_enable", "axisim_learned_stats", "axisim_learned_predict",
     "axisim_set_kinetics", "axisim_set_scalars", "axisim_scalar_residuals", "axisim_set_mesh_type",
     "axisim_trellis_build", "axisim_triangle_mesh_build", "axisim_classify_boundary_faces",
+    "axisim_mg_levels_host", "axisim_mg_level_maps_host", "axisim_coloring_host",
 ]
 VAR_U, VAR_V, VAR_P, VAR_T, VAR_C = range(5)
 VAR_INDEX = {"u": VAR_U, "v": VAR_V, "p": VAR_P, "T": VAR_T, "C": VAR_C}
@@ -194,6 +195,9 @@ def lib():
                                                      C.POINTER(OutlineC), C.c_double, C.c_double, C.POINTER(vp)]),
             "axisim_classify_boundary_faces": (C.c_int, [C.c_int32, _i32p, _f64p, _f64p, C.POINTER(OutlineC),
                                                          C.c_double, C.c_double, _i32p]),
+            "axisim_mg_levels_host": (C.c_int, [C.POINTER(MeshPacked), _i32p, C.c_int32]),
+            "axisim_mg_level_maps_host": (C.c_int64, [C.POINTER(MeshPacked), C.c_int32, vp, vp, vp, vp]),
+            "axisim_coloring_host": (C.c_int, [C.POINTER(MeshPacked), _i32p, C.c_size_t]),
             "axisim_profile_iteration": (C.c_int, [vp, C.c_int32, C.POINTER(KernelStat), C.c_int32, _i32p]),
             "axisim_set_batch": (C.c_int, [vp, C.c_int32, _i32p]),
             "axisim_batch_status": (C.c_int, [vp, _i32p, _f64p, C.c_int32]),
@@ -325,6 +329,47 @@ def resolve_bc(boundary_type, variable, user=None):
     if st != OK:
         raise AxisimError(st, "resolve_bc failed")
     return t.value, v.value, p.value
+
+
+def mg_levels_host(mesh):
+    """Cells per multigrid level of `mesh`, built on the host without a device
+    (the hierarchy a handle holding this mesh reports)."""
+    s, keep = mesh_struct(mesh)
+    cells = np.zeros(64, np.int32)
+    n = lib().axisim_mg_levels_host(C.byref(s), cells.ctypes.data_as(_i32p), 64)
+    if n < 0:
+        raise AxisimError(-n, "mg_levels_host failed")
+    return cells[:n].copy()
+
+
+def mg_level_maps_host(mesh, level):
+    """(cellToCoarse, fineSlotToCoarseSlot, coarseFaceStart, coarseFaceNeighbor)
+    of `level`, built on the host without a device."""
+    s, keep = mesh_struct(mesh)
+    cells = mg_levels_host(mesh)
+    if not 0 <= level < len(cells) - 1:
+        raise AxisimError(E_ARG, "level out of range")
+    f = lib().axisim_mg_level_maps_host
+    S = len(mesh["cellFaceIDs"]) if level == 0 else int(f(C.byref(s), level - 1, None, None, None, None))
+    Sc = int(f(C.byref(s), level, None, None, None, None))
+    if S < 0 or Sc < 0:
+        raise AxisimError(-min(S, Sc), "mg_level_maps_host failed")
+    out = (np.zeros(cells[level], np.int32), np.zeros(S, np.int32), np.zeros(cells[level + 1] + 1, np.int32),
+           np.zeros(max(Sc, 1), np.int32))
+    r = f(C.byref(s), level, *(a.ctypes.data_as(C.c_void_p) for a in out))
+    if r < 0:
+        raise AxisimError(-r, "mg_level_maps_host failed")
+    return out[0], out[1], out[2], out[3][:Sc]
+
+
+def coloring_host(mesh):
+    """(colour per cell, number of colours) of `mesh`, on the host."""
+    s, keep = mesh_struct(mesh)
+    out = np.zeros(mesh["nCells"], np.int32)
+    nc = lib().axisim_coloring_host(C.byref(s), out.ctypes.data_as(_i32p), out.size)
+    if nc < 0:
+        raise AxisimError(-nc, "coloring_host failed")
+    return out, nc
 
 
 def mesh_struct(m):

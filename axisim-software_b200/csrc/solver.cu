@@ -2386,6 +2386,77 @@ int axisim_coloring(const axisim_handle* h, int32_t* colorOut, size_t n) {
     return st == AXISIM_OK ? r : -st;
 }
 
+namespace {
+// The connectivity checks of axisim_set_mesh: false for a mesh whose indices
+// would read outside its arrays.
+bool connectivityOk(const axisim_mesh_packed* pm) {
+    if (!pm || pm->nCells <= 0 || pm->nFaces <= 0 || !pm->cellFaceStart || !pm->cellFaceIDs || !pm->faceOwner ||
+        !pm->faceNeighbor || pm->cellFaceStart[0] != 0)
+        return false;
+    const int N = pm->nCells, F = pm->nFaces;
+    for (int c = 0; c < N; c++) {
+        const int d = pm->cellFaceStart[c + 1] - pm->cellFaceStart[c];
+        if (d < 0 || d > 32) return false;
+    }
+    for (int k = 0; k < pm->cellFaceStart[N]; k++)
+        if (pm->cellFaceIDs[k] < 0 || pm->cellFaceIDs[k] >= F) return false;
+    for (int f = 0; f < F; f++)
+        if (pm->faceOwner[f] < 0 || pm->faceOwner[f] >= N || pm->faceNeighbor[f] >= N) return false;
+    return true;
+}
+
+axisim::GridLevel hostFinest(const axisim_mesh_packed* pm) {
+    return axisim::finestLevel(pm->nCells, pm->nFaces, pm->cellFaceStart, pm->cellFaceIDs, pm->faceOwner,
+                               pm->faceNeighbor);
+}
+}  // namespace
+
+int axisim_mg_levels_host(const axisim_mesh_packed* mesh, int32_t* cellsPerLevel, int32_t maxLevels) {
+    if (maxLevels < 0 || (maxLevels > 0 && !cellsPerLevel)) return -AXISIM_E_ARG;
+    if (!connectivityOk(mesh)) return -AXISIM_E_MESH;
+    try {
+        const std::vector<axisim::GridLevel> h = axisim::buildHierarchy(hostFinest(mesh));
+        for (int l = 0; l < (int)h.size() && l < maxLevels; l++) cellsPerLevel[l] = h[(size_t)l].nCells;
+        return (int)h.size();
+    } catch (...) {
+        return -AXISIM_E_MESH;
+    }
+}
+
+int64_t axisim_mg_level_maps_host(const axisim_mesh_packed* mesh, int32_t level, int32_t* cellToCoarse,
+                                  int32_t* fineSlotToCoarseSlot, int32_t* coarseFaceStart,
+                                  int32_t* coarseFaceNeighbor) {
+    if (!connectivityOk(mesh)) return -AXISIM_E_MESH;
+    try {
+        const std::vector<axisim::GridLevel> h = axisim::buildHierarchy(hostFinest(mesh));
+        if (level < 0 || level + 1 >= (int)h.size()) return -AXISIM_E_ARG;
+        const axisim::GridLevel& f = h[(size_t)level];
+        const axisim::GridLevel& c = h[(size_t)level + 1];
+        if (cellToCoarse) std::copy(f.cellToCoarse.begin(), f.cellToCoarse.end(), cellToCoarse);
+        if (fineSlotToCoarseSlot)
+            std::copy(f.fineSlotToCoarseSlot.begin(), f.fineSlotToCoarseSlot.end(), fineSlotToCoarseSlot);
+        if (coarseFaceStart) std::copy(c.faceStart.begin(), c.faceStart.end(), coarseFaceStart);
+        if (coarseFaceNeighbor) std::copy(c.faceNeighbor.begin(), c.faceNeighbor.end(), coarseFaceNeighbor);
+        return c.nFaceRefs();
+    } catch (...) {
+        return -AXISIM_E_MESH;
+    }
+}
+
+int axisim_coloring_host(const axisim_mesh_packed* mesh, int32_t* colorOut, size_t n) {
+    if (!colorOut) return -AXISIM_E_ARG;
+    if (!connectivityOk(mesh)) return -AXISIM_E_MESH;
+    if (n < (size_t)mesh->nCells) return -AXISIM_E_ARG;
+    try {
+        std::vector<int32_t> color;
+        const int nc = axisim::greedyColoring(hostFinest(mesh), color);
+        std::copy(color.begin(), color.end(), colorOut);
+        return nc;
+    } catch (...) {
+        return -AXISIM_E_MESH;
+    }
+}
+
 int axisim_profile_iteration(axisim_handle* h, int32_t iterations, axisim_kernel_stat* out, int32_t maxOut,
                              int32_t* nOut) {
     if (!h) return AXISIM_E_ARG;

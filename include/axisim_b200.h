@@ -353,6 +353,17 @@ int64_t axisim_mg_level_maps(const axisim_handle* h, int32_t level, int32_t* cel
                              int32_t* coarseFaceNeighbor);
 /* MeshColoring (solver_struct.h:122-154): colour per cell; returns nColors. */
 int axisim_coloring(const axisim_handle* h, int32_t* colorOut, size_t n);
+/* The same hierarchy and colouring computed on the host from a packed mesh,
+ * with no handle and no device (MultigridSolver::buildLevels,
+ * multigrid.cu:298-325; buildMeshColoring, memory_manger.cpp:334-409): the
+ * results of the three calls above for a handle holding that mesh. Each call
+ * rebuilds what it reports. A mesh whose connectivity fails axisim_set_mesh's
+ * checks gives -AXISIM_E_MESH. */
+int axisim_mg_levels_host(const axisim_mesh_packed* mesh, int32_t* cellsPerLevel, int32_t maxLevels);
+int64_t axisim_mg_level_maps_host(const axisim_mesh_packed* mesh, int32_t level, int32_t* cellToCoarse,
+                                  int32_t* fineSlotToCoarseSlot, int32_t* coarseFaceStart,
+                                  int32_t* coarseFaceNeighbor);
+int axisim_coloring_host(const axisim_mesh_packed* mesh, int32_t* colorOut, size_t n);
 
 /* ---- measurement ---- */
 /* Per-kernel statistics of the profiled iterations: launches, summed CUDA-event

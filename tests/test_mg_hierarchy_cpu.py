@@ -1,0 +1,69 @@
+"""Agglomeration hierarchy and cell colouring built by the library on the host
+(axisim_mg_levels_host, axisim_mg_level_maps_host, axisim_coloring_host) against
+the oracle's restatement of buildAgglomerationMap / coarsenGrid / buildLevels
+(multigrid.cu:79-325) and buildMeshColoring (memory_manger.cpp:334-409):
+identical level sizes, fine-to-coarse maps, coarse CSR and colours on a
+structured pipe, a graded multiblock expansion, a jittered triangle mesh and a
+packed batch of uneven cases. No device is needed.
+"""
+import numpy as np
+import pytest
+
+import axisim.abi as abi
+from axisim import batch, cases
+import oracle
+
+
+def _pipe():
+    c = cases.pipe(max_iter=1)
+    return oracle.multiblock(c.blocks), c.bc_fields(), c.settings
+
+
+def _expansion():
+    c = cases.expansion(scale=1 / 16, max_iter=1)
+    return oracle.multiblock(c.blocks), c.bc_fields(), c.settings
+
+
+def _bullet():
+    c = cases.bullet(scale=0.05, max_iter=1)
+    return c.mesh, c.bc_fields(), c.settings
+
+
+def _batch():
+    cs = batch.random_cases(5, seed=3, lo=2_000, hi=12_000)
+    union, _, bcs = batch.pack_union([oracle.multiblock(c.blocks) for c in cs], [c.groups for c in cs])
+    return union, bcs, cs[0].settings
+
+
+@pytest.mark.parametrize("make", [_pipe, _expansion, _bullet, _batch], ids=["pipe", "expansion", "bullet", "batch"])
+def test_host_hierarchy_and_coloring_match_oracle(make):
+    mesh, bcs, settings = make()
+    # the oracle colours the cells only for the red-black Gauss-Seidel smoother
+    orc = oracle.Oracle(mesh, bcs, dict(settings, linearType=cases.LINEAR_GS_RB))
+    levels = abi.mg_levels_host(mesh)
+    np.testing.assert_array_equal(levels, orc.mg_levels())
+    assert len(levels) >= 3
+    for lvl in range(len(levels) - 1):
+        for a, b in zip(abi.mg_level_maps_host(mesh, lvl), orc.mg_level_maps(lvl)):
+            np.testing.assert_array_equal(a, b)
+    colors, nc = abi.coloring_host(mesh)
+    oc, onc = orc.coloring()
+    assert nc == onc
+    np.testing.assert_array_equal(colors, oc)
+
+
+def test_host_hierarchy_rejects_bad_connectivity_and_levels():
+    mesh, _, _ = _pipe()
+    with pytest.raises(abi.AxisimError) as e:
+        abi.mg_level_maps_host(mesh, len(abi.mg_levels_host(mesh)) - 1)
+    assert e.value.status == abi.E_ARG
+    bad = dict(mesh)
+    ids = np.array(mesh["cellFaceIDs"], dtype=np.int32)
+    ids[5] = mesh["nFaces"]  # a face id past the last face
+    bad["cellFaceIDs"] = ids
+    with pytest.raises(abi.AxisimError) as e:
+        abi.mg_levels_host(bad)
+    assert e.value.status == abi.E_MESH
+    with pytest.raises(abi.AxisimError) as e:
+        abi.coloring_host(bad)
+    assert e.value.status == abi.E_MESH
