@@ -52,6 +52,26 @@ def test_host_hierarchy_and_coloring_match_oracle(make):
     np.testing.assert_array_equal(colors, oc)
 
 
+@pytest.mark.parametrize("nr,nz", [(2, 4), (8, 8), (3, 50), (1, 200)])
+def test_host_hierarchy_small_and_thin_meshes_match_oracle(nr, nz):
+    # 8 and 64 cells stay one level (coarsening stops at 64 cells); a one-cell
+    # thick strip aggregates along its length only
+    c = cases.pipe(nr=nr, nz=nz, max_iter=1)
+    mesh = oracle.multiblock(c.blocks)
+    orc = oracle.Oracle(mesh, c.bc_fields(), dict(c.settings, linearType=cases.LINEAR_GS_RB))
+    levels = abi.mg_levels_host(mesh)
+    np.testing.assert_array_equal(levels, orc.mg_levels())
+    if nr * nz <= 64:
+        assert len(levels) == 1
+    for lvl in range(len(levels) - 1):
+        for a, b in zip(abi.mg_level_maps_host(mesh, lvl), orc.mg_level_maps(lvl)):
+            np.testing.assert_array_equal(a, b)
+    colors, nc = abi.coloring_host(mesh)
+    oc, onc = orc.coloring()
+    assert nc == onc
+    np.testing.assert_array_equal(colors, oc)
+
+
 def test_host_hierarchy_rejects_bad_connectivity_and_levels():
     mesh, _, _ = _pipe()
     with pytest.raises(abi.AxisimError) as e:
