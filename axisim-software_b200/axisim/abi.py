@@ -41,6 +41,7 @@ EXPORTS = [
     "axisim_set_kinetics", "axisim_set_scalars", "axisim_scalar_residuals", "axisim_set_mesh_type",
     "axisim_trellis_build", "axisim_triangle_mesh_build", "axisim_classify_boundary_faces",
     "axisim_mg_levels_host", "axisim_mg_level_maps_host", "axisim_coloring_host",
+    "axisim_set_autotune", "axisim_autotune_report",
 ]
 VAR_U, VAR_V, VAR_P, VAR_T, VAR_C = range(5)
 VAR_INDEX = {"u": VAR_U, "v": VAR_V, "p": VAR_P, "T": VAR_T, "C": VAR_C}
@@ -157,6 +158,8 @@ def lib():
             "axisim_set_mesh_type": (C.c_int, [vp, C.c_int32]),
             "axisim_set_precision": (C.c_int, [vp, C.c_int32]),
             "axisim_set_pressure_solver": (C.c_int, [vp, C.c_int32, C.c_double, C.c_double]),
+            "axisim_set_autotune": (C.c_int, [vp, C.c_int32]),
+            "axisim_autotune_report": (C.c_int, [vp, _i32p, _f64p, C.c_int32]),
             "axisim_pressure_stats": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
             "axisim_learned_harvest": (C.c_int, [vp, C.c_int32, C.c_int32]),
             "axisim_learned_sample_count": (C.c_int, [vp, C.POINTER(C.c_int32)]),
@@ -462,7 +465,7 @@ class Solver:
     """One solver handle (Solver in the reference): case in, fields out."""
 
     def __init__(self, mesh, bcs, settings, precision=PREC_FP64, device=0, pressure_solver=PSOLVE_VCYCLES,
-                 pressure_tol=0.0, prolong_scale=1.0):
+                 pressure_tol=0.0, prolong_scale=1.0, autotune=False):
         L = lib()
         cs, sim, mg, res, fluid = settings_structs(settings)
         self.h = C.c_void_p()
@@ -494,6 +497,8 @@ class Solver:
             self._check(L.axisim_set_precision(self.h, precision))
         if pressure_solver != PSOLVE_VCYCLES:
             self._check(L.axisim_set_pressure_solver(self.h, pressure_solver, pressure_tol, prolong_scale))
+        if autotune:
+            self._check(L.axisim_set_autotune(self.h, 1))
 
     def _check(self, st):
         if st != OK:
@@ -641,6 +646,19 @@ class Solver:
         a, f, sn, sv = C.c_int64(), C.c_int64(), C.c_double(), C.c_double()
         self._check(lib().axisim_learned_stats(self.h, C.byref(a), C.byref(f), C.byref(sn), C.byref(sv)))
         return dict(applied=a.value, fallbacks=f.value, score_net=sn.value, score_vcycle=sv.value)
+
+    def set_autotune(self, on=True):
+        """Tune the multigrid levels' launch shapes before the next solve captures its graph."""
+        self._check(lib().axisim_set_autotune(self.h, 1 if on else 0))
+
+    def autotune_report(self):
+        """(block size per level, sweep microseconds per level and candidate 64/128/256)."""
+        blocks = np.zeros(64, np.int32)
+        us = np.zeros(64 * 3)
+        n = lib().axisim_autotune_report(self.h, blocks.ctypes.data_as(_i32p), us.ctypes.data_as(_f64p), 64)
+        if n < 0:
+            self._check(-n)
+        return blocks[:n].copy(), us[:3 * n].reshape(n, 3).copy()
 
     def pressure_stats(self):
         """(Krylov p' solves started, Krylov iterations completed)."""

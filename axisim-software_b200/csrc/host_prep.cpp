@@ -565,6 +565,17 @@ std::vector<GridLevel> buildHierarchy(GridLevel fine) {
     return levels;
 }
 
+int pickBlock(const std::vector<int>& candidates, const std::vector<double>& timeUs, int defaultIndex, double tol) {
+    const int n = (int)std::min(candidates.size(), timeUs.size());
+    auto ok = [&](int i) { return i >= 0 && i < n && std::isfinite(timeUs[(size_t)i]) && timeUs[(size_t)i] > 0.0; };
+    int best = -1;
+    for (int i = 0; i < n; i++)
+        if (ok(i) && (best < 0 || timeUs[(size_t)i] < timeUs[(size_t)best])) best = i;
+    if (best < 0) return (defaultIndex >= 0 && defaultIndex < n) ? defaultIndex : 0;  // nothing measured
+    if (ok(defaultIndex) && timeUs[(size_t)defaultIndex] <= (1.0 + tol) * timeUs[(size_t)best]) return defaultIndex;
+    return best;
+}
+
 int greedyColoring(const GridLevel& g, std::vector<int32_t>& color) {
     const int N = g.nCells;
     color.assign((size_t)N, -1);

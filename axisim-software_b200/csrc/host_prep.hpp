@@ -88,6 +88,13 @@ std::vector<GridLevel> buildHierarchy(GridLevel finest);
 // buildMeshColoring (memory_manger.cpp:334-409): greedy colour per cell.
 int greedyColoring(const GridLevel& g, std::vector<int32_t>& color);
 
+// Launch-shape autotuning: the index of the candidate block size to use for a
+// level, given each candidate's measured time. The default candidate is kept
+// unless the fastest one beats it by more than the relative tolerance tol, so
+// timing noise does not move a level off the default shape; a candidate with a
+// non-finite or non-positive time is never picked.
+int pickBlock(const std::vector<int>& candidates, const std::vector<double>& timeUs, int defaultIndex, double tol);
+
 // Boundary defaults: effective BC for a group type and variable.
 uint8_t defaultBCType(int boundaryType, int variable);
 bool variableEditable(int variable, int boundaryType);

@@ -32,6 +32,7 @@ struct LevelT {
     int32_t* gStart = nullptr;  // [totalSlots+1] fine slots feeding each coarse slot
     int32_t* gList = nullptr;   // fine slot positions, ascending fine cell then slot
     uint32_t* internalMask = nullptr;  // on the FINE level: slots folding into the coarse diagonal
+    int block = 0;  // threads per CTA of this level's smoothing, residual and transfer kernels (0: 256)
 };
 using LevelDev = LevelT<double>;
 using LevelF = LevelT<float>;

@@ -29,6 +29,12 @@ constexpr int kTailThreads = 1024;  // tail levels hold at most this many cells:
 constexpr int kRegW = 16;
 
 inline int blocksFor(long long n, int t = kThreads) { return (int)((n + t - 1) / t); }
+// Threads per CTA for a level's kernels: its tuned block size, else kThreads
+// (the kernels' launch bound).
+template <class T>
+inline int tpb(const LevelT<T>& L) {
+    return (L.block >= 32 && L.block <= kThreads && L.block % 32 == 0) ? L.block : kThreads;
+}
 
 template <class T>
 __device__ __forceinline__ T tiny();
@@ -437,9 +443,10 @@ void launchGalerkin(const Ctl* ctl, const LevelT<TF>& fine, const LevelT<TC>& co
 
 template <class T>
 void launchMGSmooth(const Ctl* ctl, const LevelT<T>& L, const T* x, T* y, T w, cudaStream_t s) {
-    if (!L.sliceOff && L.W == 4) launchPDL(k_mg_smooth_ell<T, 4>, dim3(blocksFor(L.N)), dim3(kThreads), 0, s, ctl, L, x, y, w);
-    else if (!L.sliceOff && L.W == 3) launchPDL(k_mg_smooth_ell<T, 3>, dim3(blocksFor(L.N)), dim3(kThreads), 0, s, ctl, L, x, y, w);
-    else launchPDL(k_mg_smooth<T>, dim3(blocksFor(L.N)), dim3(kThreads), 0, s, ctl, L, x, y, w);
+    const int t = tpb(L);
+    if (!L.sliceOff && L.W == 4) launchPDL(k_mg_smooth_ell<T, 4>, dim3(blocksFor(L.N, t)), dim3(t), 0, s, ctl, L, x, y, w);
+    else if (!L.sliceOff && L.W == 3) launchPDL(k_mg_smooth_ell<T, 3>, dim3(blocksFor(L.N, t)), dim3(t), 0, s, ctl, L, x, y, w);
+    else launchPDL(k_mg_smooth<T>, dim3(blocksFor(L.N, t)), dim3(t), 0, s, ctl, L, x, y, w);
 }
 
 template <class T>
@@ -455,20 +462,23 @@ void launchMGSmoothBlock(const Ctl* ctl, const LevelT<T>& L, T* x, T w, int swee
 
 template <class T>
 void launchMGResidual(const Ctl* ctl, const LevelT<T>& L, const T* x, cudaStream_t s) {
-    if (!L.sliceOff && L.W == 4) launchPDL(k_mg_residual_ell<T, 4>, dim3(blocksFor(L.N)), dim3(kThreads), 0, s, ctl, L, x);
-    else if (!L.sliceOff && L.W == 3) launchPDL(k_mg_residual_ell<T, 3>, dim3(blocksFor(L.N)), dim3(kThreads), 0, s, ctl, L, x);
-    else launchPDL(k_mg_residual<T>, dim3(blocksFor(L.N)), dim3(kThreads), 0, s, ctl, L, x);
+    const int t = tpb(L);
+    if (!L.sliceOff && L.W == 4) launchPDL(k_mg_residual_ell<T, 4>, dim3(blocksFor(L.N, t)), dim3(t), 0, s, ctl, L, x);
+    else if (!L.sliceOff && L.W == 3) launchPDL(k_mg_residual_ell<T, 3>, dim3(blocksFor(L.N, t)), dim3(t), 0, s, ctl, L, x);
+    else launchPDL(k_mg_residual<T>, dim3(blocksFor(L.N, t)), dim3(t), 0, s, ctl, L, x);
 }
 
 template <class T>
 void launchMGGather(const Ctl* ctl, const LevelT<T>& fine, const LevelT<T>& coarse, T* xCur, T* xAlt, int firstSweep,
                     T w, cudaStream_t s) {
-    launchPDL(k_mg_gather<T>, dim3(blocksFor(coarse.N)), dim3(kThreads), 0, s, ctl, fine.res, coarse, xCur, xAlt, firstSweep, w);
+    const int t = tpb(coarse);
+    launchPDL(k_mg_gather<T>, dim3(blocksFor(coarse.N, t)), dim3(t), 0, s, ctl, fine.res, coarse, xCur, xAlt, firstSweep, w);
 }
 
 template <class T>
 void launchMGProlong(const Ctl* ctl, const LevelT<T>& fine, T* xFine, const T* xCoarse, T scale, cudaStream_t s) {
-    launchPDL(k_mg_prolong<T>, dim3(blocksFor(fine.N)), dim3(kThreads), 0, s, ctl, fine.N, fine.c2c, xFine, xCoarse,
+    const int t = tpb(fine);
+    launchPDL(k_mg_prolong<T>, dim3(blocksFor(fine.N, t)), dim3(t), 0, s, ctl, fine.N, fine.c2c, xFine, xCoarse,
               scale);
 }
 
@@ -476,11 +486,12 @@ template <class T>
 bool launchMGProlongSmooth(const Ctl* ctl, const LevelT<T>& fine, const T* xFine, const T* xCoarse, T* y, T w,
                            T scale, cudaStream_t s) {
     if (fine.sliceOff || !fine.c2c) return false;
+    const int t = tpb(fine);
     if (fine.W == 4)
-        launchPDL(k_mg_prolong_smooth_ell<T, 4>, dim3(blocksFor(fine.N)), dim3(kThreads), 0, s, ctl, fine, xFine,
+        launchPDL(k_mg_prolong_smooth_ell<T, 4>, dim3(blocksFor(fine.N, t)), dim3(t), 0, s, ctl, fine, xFine,
                   xCoarse, y, w, scale);
     else if (fine.W == 3)
-        launchPDL(k_mg_prolong_smooth_ell<T, 3>, dim3(blocksFor(fine.N)), dim3(kThreads), 0, s, ctl, fine, xFine,
+        launchPDL(k_mg_prolong_smooth_ell<T, 3>, dim3(blocksFor(fine.N, t)), dim3(t), 0, s, ctl, fine, xFine,
                   xCoarse, y, w, scale);
     else
         return false;

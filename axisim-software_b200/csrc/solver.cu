@@ -743,6 +743,8 @@ private:
     // multigrid / colouring
     std::vector<GridLevel> hier_;
     bool haveHierarchy_ = false;
+    int autotune_ = 0;             // tune the level launch shapes before capturing the graph
+    std::vector<double> tuneUs_;   // measured sweep time per level and candidate (us)
     std::vector<LevelDev> levels_;
     // mixed precision: FP32 copies of the hierarchy and the inner-solve vectors
     Arena mixArena_;
@@ -1702,6 +1704,88 @@ public:
     }
 
 private:
+    // Launch-shape autotuner: for every level the V-cycle launches kernels on
+    // (the tail's levels run inside one CTA and are skipped), time the weighted
+    // Jacobi sweep at each candidate block size and keep pickBlock's choice in
+    // LevelT::block, which the level's smoothing, residual, restriction and
+    // prolongation launches use. The sweeps run on scratch inputs (unit
+    // diagonal, zero right-hand side and iterate, a zeroed control block), so
+    // the solution and the level's own vectors are untouched; only the sparsity
+    // pattern and coefficient storage are the level's.
+    static constexpr int kTuneCandidates[3] = {64, 128, 256};
+    template <class T>
+    void tuneLevels(std::vector<LevelT<T>>& lv) {
+        const int L = (int)lv.size();
+        const int upto = tailStart_ > 0 ? std::min(tailStart_, L) : L;
+        int nMax = 1;
+        for (int l = 0; l < upto; l++) nMax = std::max(nMax, lv[(size_t)l].N);
+        Arena scratch;
+        Ctl* ctl = scratch.alloc<Ctl>(1);
+        const std::vector<T> ones((size_t)nMax, T(1));
+        T* ac = scratch.upload(ones.data(), ones.size());
+        T* b = scratch.alloc<T>((size_t)nMax);
+        T* x = scratch.alloc<T>((size_t)nMax);
+        T* y = scratch.alloc<T>((size_t)nMax);
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        const std::vector<int> cand(std::begin(kTuneCandidates), std::end(kTuneCandidates));
+        const int nc = (int)cand.size(), def = nc - 1, reps = 8;
+        tuneUs_.assign((size_t)L * nc, 0.0);
+        try {
+            for (int l = 0; l < upto; l++) {
+                LevelT<T> t = lv[(size_t)l];
+                t.AC = ac;
+                t.b = b;
+                std::vector<double> us((size_t)nc, 0.0);
+                for (int c = 0; c < nc; c++) {
+                    t.block = cand[(size_t)c];
+                    for (int r = 0; r < 2; r++) launchMGSmooth<T>(ctl, t, x, y, (T)cmg_.weight, stream_);
+                    CK(cudaEventRecord(e0, stream_));
+                    for (int r = 0; r < reps; r++) launchMGSmooth<T>(ctl, t, x, y, (T)cmg_.weight, stream_);
+                    CK(cudaEventRecord(e1, stream_));
+                    CK(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    CK(cudaEventElapsedTime(&ms, e0, e1));
+                    us[(size_t)c] = 1e3 * (double)ms / reps;
+                    tuneUs_[(size_t)l * nc + c] = us[(size_t)c];
+                }
+                lv[(size_t)l].block = cand[(size_t)pickBlock(cand, us, def, 0.03)];
+            }
+            CK(cudaGetLastError());
+        } catch (...) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            for (auto& v : lv) v.block = 0;
+            throw;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+
+public:
+    void setAutotune(int on) {
+        autotune_ = on ? 1 : 0;
+        destroyGraph();
+        for (auto& v : levels_) v.block = 0;
+        for (auto& v : levels32_) v.block = 0;
+        tuneUs_.clear();
+    }
+    // Block size per level of the set the V-cycle uses (0: not tuned, or a
+    // tail level) and, with us, the measured sweep time per candidate.
+    int autotuneReport(int32_t* blocks, double* us, int maxL) const {
+        const bool f32 = fp32PressureCycle();
+        const int L = f32 ? (int)levels32_.size() : (int)levels_.size();
+        const int nc = (int)(sizeof(kTuneCandidates) / sizeof(int));
+        for (int l = 0; l < L && l < maxL; l++) {
+            if (blocks) blocks[l] = f32 ? levels32_[(size_t)l].block : levels_[(size_t)l].block;
+            for (int c = 0; c < nc && us; c++)
+                us[(size_t)l * nc + c] = (size_t)l * nc + c < tuneUs_.size() ? tuneUs_[(size_t)l * nc + c] : 0.0;
+        }
+        return L;
+    }
+
+private:
     void buildGraph() {
         if (exec_) return;
         ensureScalarBuffers();
@@ -1710,6 +1794,13 @@ private:
         ensureMixedBuffers();
         if (cs_.useMultigrid && psolve_ == AXISIM_PSOLVE_FCG) ensureNetStats();
         if (cs_.type == 1) ensureColoring();
+        if (autotune_ && cs_.useMultigrid) {  // launch shapes are fixed in the graph: tune first
+            if (fp32PressureCycle()) {
+                if (!levels32_.empty() && levels32_[0].block == 0) tuneLevels(levels32_);
+            } else if (!levels_.empty() && levels_[0].block == 0) {
+                tuneLevels(levels_);
+            }
+        }
         CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
         try {
             enqueueIteration();
@@ -2219,6 +2310,27 @@ int axisim_set_pressure_solver(axisim_handle* h, int32_t mode, double relTol, do
         h->s->setPressureSolver(mode, relTol, prolongScale);
         return AXISIM_OK;
     });
+}
+
+int axisim_set_autotune(axisim_handle* h, int32_t enable) {
+    if (!h) return AXISIM_E_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    return guarded(h, [&] {
+        h->s->setAutotune(enable);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_autotune_report(const axisim_handle* h, int32_t* blockPerLevel, double* usPerCandidate,
+                           int32_t maxLevels) {
+    auto* hh = const_cast<axisim_handle*>(h);
+    if (maxLevels < 0) return -AXISIM_E_ARG;
+    int r = 0;
+    const int st = guarded(hh, [&] {
+        r = hh->s->autotuneReport(blockPerLevel, usPerCandidate, maxLevels);
+        return AXISIM_OK;
+    });
+    return st == AXISIM_OK ? r : -st;
 }
 
 int axisim_learned_harvest(axisim_handle* h, int32_t every, int32_t capacity) {

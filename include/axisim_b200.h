@@ -244,6 +244,20 @@ int axisim_set_pressure_solver(axisim_handle* h, int32_t mode, double relTol, do
 /* New: Krylov p' solves started and iterations completed since the handle's
  * mesh was set. */
 int axisim_pressure_stats(axisim_handle* h, int64_t* solves, int64_t* iterations);
+/* New (no reference counterpart; the reference launches every multigrid kernel
+ * with fixed shapes): enable = 1 tunes, before the next solve captures its
+ * graph, the threads per CTA (64, 128 or 256) of each multigrid level's
+ * smoothing, residual, restriction and prolongation kernels by timing that
+ * level's Jacobi sweep at each size on scratch inputs, keeping 256 unless
+ * another size is more than 3 % faster. Results are unchanged (every cell's
+ * arithmetic is the same at any shape). enable = 0 returns to 256. */
+int axisim_set_autotune(axisim_handle* h, int32_t enable);
+/* The tuned block size per level (0: not tuned, or a level solved inside the
+ * one-CTA tail) and, with usPerCandidate, the measured sweep time in
+ * microseconds per level and candidate (3 per level: 64, 128, 256 threads).
+ * Returns the level count. */
+int axisim_autotune_report(const axisim_handle* h, int32_t* blockPerLevel, double* usPerCandidate,
+                           int32_t maxLevels);
 
 /* ---- learned p' preconditioner (new; no reference counterpart) ----
  * A U-Net over the multigrid's agglomeration hierarchy maps a p' residual r to
