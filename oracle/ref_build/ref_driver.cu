@@ -4,7 +4,9 @@
 // translation units compiled unchanged from their sources (see Makefile) and
 // drives Solver::run exactly as SolverGUI does (solver_gui.cpp:898-933):
 //   mesh  : the reference's multiblock packer (structs/multiblock.h) turned into
-//           an FVMesh the way Mesh::createMultiBlockFVMesh does (mesh.cpp:2366-2393)
+//           an FVMesh the way Mesh::createMultiBlockFVMesh does (mesh.cpp:2366-2393),
+//           or (spec key `packed <file>`) packed arrays of an unstructured mesh read
+//           from a file in FVMeshHostPacked order, with MeshType::Unstructured
 //   groups: BoundarySegmentGroup with per-variable BoundaryCondition
 //   run   : Solver::run + Solver::shutdown (joins the worker thread)
 // and writes the solution fields and the residual history to a binary file.
@@ -60,6 +62,42 @@ BoundaryVariable varOf(const std::string& v) {
     return BoundaryVariable::Pressure;
 }
 
+// Packed mesh file: int32 nCells, nFaces, nRefs, then the FVMeshHostPacked
+// arrays in declaration order (int32 or float64 as declared).
+bool readPacked(const std::string& path, FVMeshHostPacked& p) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) return false;
+    int32_t h[3];
+    if (!f.read(reinterpret_cast<char*>(h), sizeof(h)) || h[0] <= 0 || h[1] <= 0 || h[2] < 0) return false;
+    p.nCells = h[0];
+    p.nFaces = h[1];
+    const size_t N = (size_t)h[0], F = (size_t)h[1], S = (size_t)h[2];
+    auto ints = [&](std::vector<int>& v, size_t n) {
+        std::vector<int32_t> t(n);
+        f.read(reinterpret_cast<char*>(t.data()), (std::streamsize)(n * sizeof(int32_t)));
+        v.assign(t.begin(), t.end());
+    };
+    auto reals = [&](std::vector<double>& v, size_t n) {
+        v.resize(n);
+        f.read(reinterpret_cast<char*>(v.data()), (std::streamsize)(n * sizeof(double)));
+    };
+    ints(p.faceOwner, F);
+    ints(p.faceNeighbor, F);
+    reals(p.faceNormalZ, F);
+    reals(p.faceNormalR, F);
+    reals(p.faceCenterZ, F);
+    reals(p.faceCenterR, F);
+    reals(p.faceArea, F);
+    ints(p.faceBoundaryGroupID, F);
+    reals(p.cellCenterZ, N);
+    reals(p.cellCenterR, N);
+    reals(p.cellArea2D, N);
+    reals(p.cellVolume, N);
+    ints(p.cellFaceStart, N + 1);
+    ints(p.cellFaceIDs, S);
+    return (bool)f && p.cellFaceStart[0] == 0 && (size_t)p.cellFaceStart[N] == S;
+}
+
 BoundarySegmentGroup* groupOf(Mesh& mesh, int id) {
     for (BoundarySegmentGroup& g : mesh.boundaryGroups)
         if (g.id == id) return &g;
@@ -84,10 +122,20 @@ int main(int argc, char** argv) {
     Config config{};
     Solver* solverPtr = nullptr;
     std::vector<std::pair<std::string, double>> settings;
+    FVMeshHostPacked packed{};
+    bool fromFile = false;
     std::string key;
     while (in >> key) {
         if (key == "tol") {
             in >> tol;
+        } else if (key == "packed") {
+            std::string path;
+            in >> path;
+            if (!readPacked(path, packed)) {
+                std::fprintf(stderr, "cannot read packed mesh %s\n", path.c_str());
+                return 2;
+            }
+            fromFile = true;
         } else if (key == "block") {
             double z0, r0, axL, axC, rdL, rdC;
             int axN, axG, rdN, rdG, e[4];
@@ -151,11 +199,12 @@ int main(int argc, char** argv) {
             settings.emplace_back(name, value);
         }
     }
-    std::string reason;
-    if (!autoDetectInterfaces(mb, reason, tol)) mb.interfaces.clear();
-    mb.assignGlobalNumbering();
-    FVMeshHostPacked packed{};
-    toPackedMesh(mb, packed);
+    if (!fromFile) {
+        std::string reason;
+        if (!autoDetectInterfaces(mb, reason, tol)) mb.interfaces.clear();
+        mb.assignGlobalNumbering();
+        toPackedMesh(mb, packed);
+    }
     // FVMesh from the packed arrays, as Mesh::createMultiBlockFVMesh does
     FVMesh& fv = mesh.fvMesh;
     fv.cells.resize((size_t)packed.nCells);
@@ -178,7 +227,7 @@ int main(int argc, char** argv) {
         face.boundaryGroupID = packed.faceBoundaryGroupID[(size_t)f];
     }
     mesh.isReady = true;
-    mesh.currentMeshType = MeshType::Structured;
+    mesh.currentMeshType = fromFile ? MeshType::Unstructured : MeshType::Structured;
 
     Console console;
     ResidualPlot plot;

@@ -43,6 +43,11 @@ def fixture_cases():
     out.append(("pulsatile864_bdf2_3x3", c))
     c = cases.pipe(max_iter=50000, tol=1e-6)
     out.append(("pipe40x200_config1_converged", c))
+    # triangles (the bullet body, jittered): least-squares gradients with the
+    # non-orthogonal corrector on an unstructured mesh, packed by this
+    # project's createUnstructuredMesh restatement and handed to the reference
+    # solver as packed arrays
+    out.append(("bullet1205_lsq_nonortho_6it", cases.bullet(scale=0.05, max_iter=6, tol=1e-30)))
     out += scalar_fixture_cases()
     return out
 
@@ -73,9 +78,29 @@ def scalar_fixture_cases():
     return out
 
 
+PACKED_ORDER = [("faceOwner", np.int32), ("faceNeighbor", np.int32), ("faceNormalZ", np.float64),
+                ("faceNormalR", np.float64), ("faceCenterZ", np.float64), ("faceCenterR", np.float64),
+                ("faceArea", np.float64), ("faceBoundaryGroupID", np.int32), ("cellCenterZ", np.float64),
+                ("cellCenterR", np.float64), ("cellArea2D", np.float64), ("cellVolume", np.float64),
+                ("cellFaceStart", np.int32), ("cellFaceIDs", np.int32)]
+
+
+def write_packed(mesh, path):
+    """The driver's packed-mesh file: int32 nCells, nFaces, nRefs, then the
+    FVMeshHostPacked arrays in declaration order."""
+    with open(path, "wb") as f:
+        np.array([mesh["nCells"], mesh["nFaces"], len(mesh["cellFaceIDs"])], np.int32).tofile(f)
+        for k, dt in PACKED_ORDER:
+            np.ascontiguousarray(mesh[k], dtype=dt).tofile(f)
+
+
 def write_spec(case, path, tol=1e-9):
     with open(path, "w") as f:
         f.write(f"tol {tol!r}\n")
+        if case.mesh is not None:
+            mesh_path = os.path.join(os.path.dirname(path), "mesh.bin")
+            write_packed(case.mesh, mesh_path)
+            f.write(f"packed {mesh_path}\n")
         for b in case.blocks:
             ax, rd = b["axial"], b["radial"]
             f.write("block %r %r %r %d %d %r %r %d %d %r %d %d %d %d\n" % (

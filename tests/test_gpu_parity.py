@@ -162,7 +162,7 @@ def test_cuda_path_matches_reference_solver(name):
     import make_golden
     case = dict(make_golden.fixture_cases())[name]
     g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", name + ".npz"))
-    mesh = abi.multiblock(case.blocks)
+    mesh = case.packed(abi.multiblock)
     gpu = abi.Solver(mesh, case.bc_fields(), case.settings)
     r = gpu.solve()
     assert r["iterations"] == int(g["iterations"]) and r["converged"] == bool(g["converged"])

@@ -33,7 +33,7 @@ TOL = 1e-10
 @pytest.mark.parametrize("name,case", CASES, ids=[n for n, _ in CASES])
 def test_oracle_matches_reference_solver(name, case):
     g = np.load(os.path.join(HERE, "golden", name + ".npz"))
-    mesh = oracle.multiblock(case.blocks)
+    mesh = case.packed(oracle.multiblock)
     o = oracle.Oracle(mesh, case.bc_fields(), case.settings)
     it, conv = o.run()
     assert it == int(g["iterations"])
