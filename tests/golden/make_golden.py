@@ -18,6 +18,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "axisim-software_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
 from axisim import cases  # noqa: E402
 
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "axisim_ref")
@@ -48,8 +49,23 @@ def fixture_cases():
     # project's createUnstructuredMesh restatement and handed to the reference
     # solver as packed arrays
     out.append(("bullet1205_lsq_nonortho_6it", cases.bullet(scale=0.05, max_iter=6, tol=1e-30)))
+    out.append(("batch4_union6316_5it", batch_union()[0]))
     out += scalar_fixture_cases()
     return out
+
+
+def batch_union(n=4, seed=7, scale=0.02, iters=5):
+    """Four random cases of the batch mix packed into one mesh (cell, face and
+    group ids offset per case), as a Case the reference solves as one mesh;
+    returns (case, caseCellStart). With the tolerance out of reach every case
+    runs the same iterations, so a batched solve must give these fields."""
+    from axisim import batch
+    import oracle
+    cs = batch.random_cases(n, seed=seed, scale=scale, max_iter=iters, tol=1e-30)
+    union, start, _ = batch.pack_union([oracle.multiblock(c.blocks) for c in cs], [c.groups for c in cs])
+    groups = [cases.Group(g.id + batch.GROUPS_PER_CASE * i, g.btype, dict(g.bcs), g.total_length)
+              for i, c in enumerate(cs) for g in c.groups]
+    return cases.Case(f"batch{n}_union{union['nCells']}", [], groups, dict(cs[0].settings), mesh=union), start
 
 
 def scalar_fixture_cases():
@@ -184,7 +200,7 @@ def main(outdir=HERE, only=""):
             continue
         res = run_reference(case)
         keep = {k: v for k, v in res.items() if k not in ("log",)}
-        if name.startswith("pipe40x200"):
+        if name.startswith("pipe40x200") or name.startswith("batch"):
             keep = {k: keep[k] for k in ("u", "v", "p", "iterations", "converged", "residual_history")}
         np.savez_compressed(os.path.join(outdir, name + ".npz"), **keep)
         print(name, res["iterations"], res["converged"], res["log"].strip().splitlines()[0])

@@ -65,3 +65,19 @@ def test_batch_layout_is_validated():
         g.set_batch([0, 10, union["nCells"]])   # a face crosses the boundary at cell 10
     with pytest.raises(abi.AxisimError):
         g.set_batch([0, union["nCells"] - 1])   # does not cover the mesh
+
+
+def test_batched_solve_matches_reference_solver_on_the_union():
+    # the reference solves the packed union of four cases as one mesh; batch
+    # mode only adds per-case monitoring, so with the tolerance out of reach the
+    # batched fields equal the reference's to rounding (its atomicAdd order)
+    import os
+    import make_golden
+    case, start = make_golden.batch_union()
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", case.name + "_5it.npz"))
+    s = abi.Solver(case.mesh, case.bc_fields(), case.settings)
+    s.set_batch(start)
+    r = s.solve()
+    assert r["iterations"] == int(g["iterations"]) == 5
+    for f in ("u", "v", "p"):
+        assert rel_l2(s.get(f), g[f]) <= 1e-10, (f, rel_l2(s.get(f), g[f]))
