@@ -246,11 +246,13 @@ int axisim_set_pressure_solver(axisim_handle* h, int32_t mode, double relTol, do
 int axisim_pressure_stats(axisim_handle* h, int64_t* solves, int64_t* iterations);
 /* New (no reference counterpart; the reference launches every multigrid kernel
  * with fixed shapes): enable = 1 tunes, before the next solve captures its
- * graph, the threads per CTA (64, 128 or 256) of each multigrid level's
- * smoothing, residual, restriction and prolongation kernels by timing that
- * level's Jacobi sweep at each size on scratch inputs, keeping 256 unless
- * another size is more than 3 % faster. Results are unchanged (every cell's
- * arithmetic is the same at any shape). enable = 0 returns to 256. */
+ * graph, the threads per CTA (64, 128 or 256) of the smoothing, residual,
+ * restriction and prolongation kernels of each multigrid level the V-cycle
+ * launches kernels on (the levels solved inside the one-CTA tail are not
+ * tuned), by timing that level's Jacobi sweep at each size on scratch inputs
+ * and keeping 256 unless another size is more than 3 % faster. Results are
+ * unchanged (every cell's arithmetic is the same at any shape). enable = 0
+ * returns to 256. */
 int axisim_set_autotune(axisim_handle* h, int32_t enable);
 /* The tuned block size per level (0: not tuned, or a level solved inside the
  * one-CTA tail) and, with usPerCandidate, the measured sweep time in
