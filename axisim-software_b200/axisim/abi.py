@@ -41,7 +41,7 @@ EXPORTS = [
     "axisim_set_kinetics", "axisim_set_scalars", "axisim_scalar_residuals", "axisim_set_mesh_type",
     "axisim_trellis_build", "axisim_triangle_mesh_build", "axisim_classify_boundary_faces",
     "axisim_mg_levels_host", "axisim_mg_level_maps_host", "axisim_coloring_host",
-    "axisim_set_autotune", "axisim_autotune_report",
+    "axisim_set_autotune", "axisim_autotune_report", "axisim_setup_profile", "axisim_profile_levels",
 ]
 VAR_U, VAR_V, VAR_P, VAR_T, VAR_C = range(5)
 VAR_INDEX = {"u": VAR_U, "v": VAR_V, "p": VAR_P, "T": VAR_T, "C": VAR_C}
@@ -202,6 +202,8 @@ def lib():
             "axisim_mg_level_maps_host": (C.c_int64, [C.POINTER(MeshPacked), C.c_int32, vp, vp, vp, vp]),
             "axisim_coloring_host": (C.c_int, [C.POINTER(MeshPacked), _i32p, C.c_size_t]),
             "axisim_profile_iteration": (C.c_int, [vp, C.c_int32, C.POINTER(KernelStat), C.c_int32, _i32p]),
+            "axisim_setup_profile": (C.c_int, [vp, C.POINTER(KernelStat), C.c_int32, _i32p, C.c_int32]),
+            "axisim_profile_levels": (C.c_int, [vp, C.c_int32, C.POINTER(KernelStat), C.c_int32, _i32p]),
             "axisim_set_batch": (C.c_int, [vp, C.c_int32, _i32p]),
             "axisim_batch_status": (C.c_int, [vp, _i32p, _f64p, C.c_int32]),
         }
@@ -543,14 +545,23 @@ class Solver:
         self._check(lib().axisim_set_config(self.h, C.byref(cs), C.byref(sim), C.byref(mg), res,
                                             self.settings["alphaU"], self.settings["alphaP"]))
 
-    def profile(self, iterations=1):
+    def profile(self, iterations=1, by_level=False):
         """Per-kernel launches / CUDA-event ms / algorithmic bytes over `iterations`
-        eagerly replayed SIMPLE iterations (advances the solution)."""
+        eagerly replayed SIMPLE iterations (advances the solution). by_level:
+        multigrid launches are named "<kernel>@<level>"."""
+        out = (KernelStat * 256)()
+        n = C.c_int32(0)
+        fn = lib().axisim_profile_levels if by_level else lib().axisim_profile_iteration
+        self._check(fn(self.h, iterations, out, 256, C.byref(n)))
+        return [dict(name=out[i].name.decode(), launches=out[i].launches, ms=out[i].ms, bytes=out[i].bytes)
+                for i in range(min(n.value, 256))]
+
+    def setup_profile(self, reset=False):
+        """Host-clock ms and call count of each set-up stage since creation (or the last reset)."""
         out = (KernelStat * 64)()
         n = C.c_int32(0)
-        self._check(lib().axisim_profile_iteration(self.h, iterations, out, 64, C.byref(n)))
-        return [dict(name=out[i].name.decode(), launches=out[i].launches, ms=out[i].ms, bytes=out[i].bytes)
-                for i in range(min(n.value, 64))]
+        self._check(lib().axisim_setup_profile(self.h, out, 64, C.byref(n), 1 if reset else 0))
+        return {out[i].name.decode(): dict(calls=out[i].launches, ms=out[i].ms) for i in range(min(n.value, 64))}
 
     def set_batch(self, case_cell_start):
         cs = np.ascontiguousarray(case_cell_start, dtype=np.int32)

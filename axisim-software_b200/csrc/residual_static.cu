@@ -154,13 +154,17 @@ void setError(char* err, size_t errLen, const char* msg) {
     std::snprintf(err, errLen, "%s", msg);
 }
 
-bool isDevicePointer(const void* p) {
+// Device memory of device `dev`, or managed memory (reachable from any device).
+// A pointer into another GPU's memory is rejected: without peer access the
+// kernel would fault on it.
+bool isDevicePointerOn(const void* p, int dev) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type == cudaMemoryTypeManaged) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
 }  // namespace
@@ -187,18 +191,32 @@ extern "C" int axisim_residual_static(int32_t nCells, int32_t nFaces, int32_t nS
         setError(err, errLen, "norm type must be 0 (L1), 1 (L2) or 2 (LINF)");
         return AXISIM_E_ARG;
     }
-    const void* ptrs[] = {cellFaceStart, cellFaceIDs, faceOwner, faceNeighbor, AF, ACu, ACv, bu, bv, u, v, mDot,
-                          resU, resV, resC, sums};
-    for (const void* p : ptrs)
-        if (!p || !isDevicePointer(p)) {
-            setError(err, errLen, "every array must be a device pointer on the current device");
-            return AXISIM_E_ARG;
-        }
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         setError(err, errLen, "no current CUDA device");
         return AXISIM_E_CUDA;
+    }
+    const void* ptrs[] = {cellFaceStart, cellFaceIDs, faceOwner, faceNeighbor, AF, ACu, ACv, bu, bv, u, v, mDot,
+                          resU, resV, resC, sums};
+    for (const void* p : ptrs)
+        if (!p || !isDevicePointerOn(p, dev)) {
+            setError(err, errLen, "every array must be a device pointer on the current device");
+            return AXISIM_E_ARG;
+        }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // every call ends with a blocking read-back of the bad-index count, which
+    // a capturing stream cannot do: refuse before touching the stream
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess) {
+        std::snprintf(msg, sizeof msg, "cudaStreamIsCapturing: %s", cudaGetErrorString(e));
+        setError(err, errLen, msg);
+        return AXISIM_E_CUDA;
+    }
+    if (cap != cudaStreamCaptureStatusNone) {
+        setError(err, errLen, "cannot be called while the stream is being captured (it reads its status back)");
+        return AXISIM_E_ARG;
     }
     double* scratch = nullptr;
     {
@@ -214,7 +232,6 @@ extern "C" int axisim_residual_static(int32_t nCells, int32_t nFaces, int32_t nS
         }
         scratch = g_scratchPtr[dev];
     }
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     unsigned int* words = reinterpret_cast<unsigned int*>(scratch + kPartialDoubles);
     // the arrival ticket and the bad-index count must start at zero
     e = cudaMemsetAsync(words, 0, kWordDoubles * sizeof(double), s);

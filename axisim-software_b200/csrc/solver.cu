@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -352,6 +353,7 @@ public:
 
     // ---------------- mesh ----------------
     void setMesh(const axisim_mesh_packed& pm) {
+        std::unique_ptr<PhaseTimer> ph(new PhaseTimer(*this, "mesh_validate"));
         const int N = pm.nCells, F = pm.nFaces;
         if (N <= 0 || F <= 0) throw StatusError(AXISIM_E_MESH, "mesh needs cells and faces");
         const void* req[] = {pm.faceOwner, pm.faceNeighbor, pm.faceNormalZ, pm.faceNormalR, pm.faceCenterZ,
@@ -402,6 +404,7 @@ public:
         hCfi_.assign(pm.cellFaceIDs, pm.cellFaceIDs + S);
         hOwner_.assign(pm.faceOwner, pm.faceOwner + F);
         hNeighbor_.assign(pm.faceNeighbor, pm.faceNeighbor + F);
+        ph.reset(new PhaseTimer(*this, "mesh_upload"));
         Arena& A = meshArena_;
         MeshDev& m = mesh_;
         m.N = N;
@@ -436,9 +439,12 @@ public:
         m.snb = snb;
         double* tz = A.alloc<double>(F);
         double* tr = A.alloc<double>(F);
+        ph.reset(new PhaseTimer(*this, "mesh_precompute_ell"));
         launchPrecompute(m, dCfs, dCfi, tz, tr, stream_);
         launchBuildEll(N, W, dCfs, dCfi, m.owner, m.neighbor, sface, snb, stream_);
         CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(stream_));
+        ph.reset(new PhaseTimer(*this, "fields_alloc"));
         // fields and coefficient systems (allocateSimple / allocateCoefficients)
         const size_t WN = (size_t)W * N;
         u_ = A.alloc<double>(N); v_ = A.alloc<double>(N); p_ = A.alloc<double>(N); pp_ = A.alloc<double>(N);
@@ -782,7 +788,13 @@ private:
         double bytes;
     };
     bool profiling_ = false;
+    bool profileByLevel_ = false;  // multigrid marks carry "@<level>"
     std::vector<Mark> marks_;
+    // a multigrid launch on `level`
+    void markL(const std::string& name, int level, double bytes) {
+        if (!profiling_) return;
+        mark(profileByLevel_ ? (name + "@" + std::to_string(level)).c_str() : name.c_str(), bytes);
+    }
     void mark(const char* name, double bytes) {
         if (!profiling_) return;
         Mark m{name, nullptr, bytes};
@@ -791,6 +803,50 @@ private:
         marks_.push_back(m);
     }
 
+    // host-clock cost of each set-up stage (set_mesh, hierarchy, graph
+    // capture, ...), summed per stage name since the handle was created
+    struct Phase {
+        std::string name;
+        int calls;
+        double ms;
+    };
+    std::vector<Phase> phases_;
+    struct PhaseTimer {
+        Solver& s;
+        const char* name;
+        std::chrono::steady_clock::time_point t0;
+        PhaseTimer(Solver& so, const char* n) : s(so), name(n), t0(std::chrono::steady_clock::now()) {}
+        ~PhaseTimer() {
+            const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            s.addPhase(name, ms);
+        }
+    };
+    void addPhase(const char* name, double ms) {
+        for (Phase& p : phases_)
+            if (p.name == name) {
+                p.calls++;
+                p.ms += ms;
+                return;
+            }
+        phases_.push_back(Phase{name, 1, ms});
+    }
+
+public:
+    int setupProfile(axisim_kernel_stat* out, int maxOut, int reset) {
+        const int n = (int)phases_.size();
+        for (int i = 0; i < n && i < maxOut; i++) {
+            axisim_kernel_stat st{};
+            std::snprintf(st.name, sizeof(st.name), "%s", phases_[(size_t)i].name.c_str());
+            st.launches = phases_[(size_t)i].calls;
+            st.ms = phases_[(size_t)i].ms;
+            st.bytes = 0.0;
+            out[i] = st;
+        }
+        if (reset) phases_.clear();
+        return n;
+    }
+
+private:
     // batch of independent cases packed into one mesh
     Arena batchArena_;
     BatchDev batch_;
@@ -814,6 +870,7 @@ private:
 
     void uploadBC() {
         if (!bcDirty_) return;
+        PhaseTimer ph(*this, "bc_upload");
         bcArena_.release();
         wallFacesReady_ = false;
         for (int var = 0; var < 3; var++) {
@@ -898,6 +955,7 @@ private:
     void ensureHierarchy() {
         if (haveHierarchy_) return;
         if (!haveMesh_) throw StatusError(AXISIM_E_STATE, "no mesh");
+        PhaseTimer ph(*this, "hierarchy_host");
         hier_ = buildHierarchy(finestLevel(N_, F_, hCfs_.data(), hCfi_.data(), hOwner_.data(), hNeighbor_.data()));
         haveHierarchy_ = true;
         levels_.clear();
@@ -907,6 +965,7 @@ private:
 
     void ensureColoring() {
         if (colorN_ > 0) return;
+        PhaseTimer ph(*this, "coloring_host");
         GridLevel g = finestLevel(N_, F_, hCfs_.data(), hCfi_.data(), hOwner_.data(), hNeighbor_.data());
         colorN_ = greedyColoring(g, hColor_);
         hColorStart_.assign((size_t)colorN_ + 1, 0);
@@ -924,6 +983,7 @@ private:
     void ensureDeviceLevels() {
         ensureHierarchy();
         if (!levels_.empty()) return;
+        PhaseTimer ph(*this, "levels_build_upload");
         const int L = (int)hier_.size();
         levels_.resize((size_t)L);
         std::vector<std::vector<int32_t>> sliceOffH((size_t)L);
@@ -1044,6 +1104,7 @@ private:
 
     void ensureMixedBuffers() {
         if (precision_ != AXISIM_PREC_MIXED && !fp32PressureCycle()) return;
+        PhaseTimer ph(*this, "mixed_buffers");
         if (psolve_ == AXISIM_PSOLVE_FCG && !fcgR_) {
             const size_t N = (size_t)N_;
             Arena& A = mixArena_;
@@ -1116,12 +1177,12 @@ private:
         const char* tag = sizeof(T) == 8 ? "" : "32";
         if (sweeps > 1 && L.N <= 4096) {
             launchMGSmoothBlock<T>(ctl_, L, cur[(size_t)l], w, sweeps, stream_);
-            mark((std::string("mg_smooth_block") + tag).c_str(), (double)L.N * ((4.0 + 2 * sizeof(T)) * L.W + 4.0 * sizeof(T)));
+            markL(std::string("mg_smooth_block") + tag, l, (double)L.N * ((4.0 + 2 * sizeof(T)) * L.W + 4.0 * sizeof(T)));
             return;
         }
         for (int i = 0; i < sweeps; i++) {
             launchMGSmooth<T>(ctl_, L, cur[(size_t)l], alt[(size_t)l], w, stream_);
-            mark((std::string(l == 0 ? "mg_smooth_l0" : "mg_smooth") + tag).c_str(),
+            markL(std::string(l == 0 ? "mg_smooth_l0" : "mg_smooth") + tag, l,
                  (double)L.N * ((4.0 + sizeof(T)) * L.W + 4.0 * sizeof(T)));
             std::swap(cur[(size_t)l], alt[(size_t)l]);
         }
@@ -1146,7 +1207,7 @@ private:
         LevelT<T>& F = lv[(size_t)l];
         LevelT<T>& C = lv[(size_t)l + 1];
         launchMGResidual<T>(ctl_, F, cur[(size_t)l], stream_);
-        mark((std::string("mg_residual") + tag).c_str(), (double)F.N * ((4.0 + vb) * F.W + 4.0 * vb));
+        markL(std::string("mg_residual") + tag, l, (double)F.N * ((4.0 + vb) * F.W + 4.0 * vb));
         if (l + 1 == tailStart_) {
             TailArgsT<T> a;
             a.first = l + 1;
@@ -1167,13 +1228,13 @@ private:
             launchMGTail<T>(ctl_, a, stream_);
             double tb = 0.0;
             for (int i = 0; i < a.count; i++) tb += (double)a.lv[i].N * ((4.0 + vb) * a.lv[i].W + 4.0 * vb);
-            mark((std::string("mg_tail") + tag).c_str(), tb);
+            markL(std::string("mg_tail") + tag, l + 1, tb);
         } else {
             const bool coarseIsCoarsest = hier_[(size_t)l + 1].isCoarsest();
             const int sweepsBelow = coarseIsCoarsest ? cmg_.linearSweep : cmg_.linearPreSweep;
             const bool fuse = sweepsBelow >= 1;
             launchMGGather<T>(ctl_, F, C, cur[(size_t)l + 1], alt[(size_t)l + 1], fuse ? 1 : 0, w, stream_);
-            mark((std::string("mg_gather") + tag).c_str(), (4.0 + vb) * F.N + 4.0 * vb * C.N);
+            markL(std::string("mg_gather") + tag, l + 1, (4.0 + vb) * F.N + 4.0 * vb * C.N);
             if (fuse) std::swap(cur[(size_t)l + 1], alt[(size_t)l + 1]);
             vcycleT<T>(lv, l + 1, cur, alt, fuse);
         }
@@ -1182,13 +1243,13 @@ private:
         if (post >= 1 && !blockSmoother &&
             launchMGProlongSmooth<T>(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], alt[(size_t)l], w,
                                      (T)curProlong_, stream_)) {
-            mark((std::string("mg_prolong_smooth") + tag).c_str(),
+            markL(std::string("mg_prolong_smooth") + tag, l,
                  (double)F.N * ((4.0 + vb) * F.W + 4.0 + 4.0 * vb) + vb * C.N);
             std::swap(cur[(size_t)l], alt[(size_t)l]);
             smoothT<T>(lv, l, post - 1, cur, alt);
         } else {
             launchMGProlong<T>(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], (T)curProlong_, stream_);
-            mark((std::string("mg_prolong") + tag).c_str(), (4.0 + 2 * vb) * F.N + vb * C.N);
+            markL(std::string("mg_prolong") + tag, l, (4.0 + 2 * vb) * F.N + vb * C.N);
             smoothT<T>(lv, l, post, cur, alt);
         }
     }
@@ -1199,11 +1260,11 @@ private:
         const int L = (int)levels_.size();
         if (L > 1) {
             launchGalerkin<double, float>(ctl_, levels_[0], levels32_[1], stream_);
-            mark("mg_galerkin", (double)levels_[0].N * (20.0 + 8.0 * levels_[0].W) + 12.0 * levels32_[1].totalSlots);
+            markL("mg_galerkin", 1, (double)levels_[0].N * (20.0 + 8.0 * levels_[0].W) + 12.0 * levels32_[1].totalSlots);
         }
         for (int l = 2; l < L; l++) {
             launchGalerkin<float, float>(ctl_, levels32_[(size_t)l - 1], levels32_[(size_t)l], stream_);
-            mark("mg_galerkin32", (double)levels32_[(size_t)l - 1].N * (12.0 + 4.0 * levels32_[(size_t)l - 1].W) +
+            markL("mg_galerkin32", l, (double)levels32_[(size_t)l - 1].N * (12.0 + 4.0 * levels32_[(size_t)l - 1].W) +
                                       8.0 * levels32_[(size_t)l].totalSlots);
         }
     }
@@ -1352,7 +1413,7 @@ private:
             const LevelDev& f = levels_[(size_t)l - 1];
             const LevelDev& c = levels_[(size_t)l];
             launchGalerkin(ctl_, f, c, stream_);
-            mark("mg_galerkin", (double)f.N * (20.0 + 8.0 * std::max(1, f.W / 2)) + (double)c.totalSlots * 8.0 +
+            markL("mg_galerkin", l, (double)f.N * (20.0 + 8.0 * std::max(1, f.W / 2)) + (double)c.totalSlots * 8.0 +
                                     (double)c.N * 16.0);
         }
         std::vector<double*> cur((size_t)L), alt((size_t)L);
@@ -1631,7 +1692,7 @@ private:
 public:
     // Runs `iters` SIMPLE iterations eagerly from the current state with an
     // event after every launch; returns per-kernel launches, time and bytes.
-    int profile(int iters, axisim_kernel_stat* out, int maxOut) {
+    int profile(int iters, axisim_kernel_stat* out, int maxOut, bool byLevel = false) {
         if (!haveMesh_) throw StatusError(AXISIM_E_STATE, "no mesh");
         uploadBC();
         buildGraph();
@@ -1659,6 +1720,7 @@ public:
         CK(cudaMemcpyAsync(ctl_, &h, sizeof(Ctl), cudaMemcpyHostToDevice, stream_));
         CK(cudaStreamSynchronize(stream_));
         profiling_ = true;
+        profileByLevel_ = byLevel;
         marks_.clear();
         cudaEvent_t start;
         CK(cudaEventCreate(&start));
@@ -1667,9 +1729,11 @@ public:
             for (int i = 0; i < iters; i++) enqueueIteration();
         } catch (...) {
             profiling_ = false;
+            profileByLevel_ = false;
             throw;
         }
         profiling_ = false;
+        profileByLevel_ = false;
         CK(cudaStreamSynchronize(stream_));
         std::vector<axisim_kernel_stat> acc;
         cudaEvent_t prev = start;
@@ -1801,6 +1865,7 @@ private:
                 tuneLevels(levels_);
             }
         }
+        std::unique_ptr<PhaseTimer> ph(new PhaseTimer(*this, "graph_capture"));
         CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
         try {
             enqueueIteration();
@@ -1811,8 +1876,11 @@ private:
             throw;
         }
         CK(cudaStreamEndCapture(stream_, &graph_));
+        ph.reset(new PhaseTimer(*this, "graph_instantiate"));
         CK(cudaGraphInstantiate(&exec_, graph_, 0));
+        ph.reset(new PhaseTimer(*this, "graph_upload"));
         CK(cudaGraphUpload(exec_, stream_));
+        CK(cudaStreamSynchronize(stream_));
     }
 
     void zeroState() {
@@ -1899,6 +1967,7 @@ int Solver::solve(int continueRun, axisim_result* res) {
     } guard{running_};
     *hostStop_ = 0;
     if (!cont) {
+        PhaseTimer ph(*this, "zero_state");
         zeroState();
         simTime_ = 0.0;
         if (batch_.nCases > 0) {
@@ -1943,6 +2012,7 @@ int Solver::solve(int continueRun, axisim_result* res) {
     const double timeOffset = (transient && cont) ? simTime_ : 0.0;
     const int numSteps = transient ? (int)std::ceil(cs_.tEnd / cs_.dt) : 1;
     const bool bdf2 = transient && cs_.timeScheme == 1;
+    std::unique_ptr<PhaseTimer> ph(new PhaseTimer(*this, "solve_iterations"));
     CK(cudaEventRecord(ev0_, stream_));
     int stepsDone = 0;
     int status = AXISIM_OK;
@@ -2023,6 +2093,7 @@ int Solver::solve(int continueRun, axisim_result* res) {
         }
     }
     CK(cudaEventRecord(ev1_, stream_));
+    ph.reset(new PhaseTimer(*this, "solve_final_gradients"));
     // final gradients of u, v, p for the solution fields (solver.cpp:1330-1332)
     {
         const double* phi[3] = {u_, v_, p_};
@@ -2576,6 +2647,29 @@ int axisim_profile_iteration(axisim_handle* h, int32_t iterations, axisim_kernel
     return guarded(h, [&] {
         if (iterations < 1 || !out || maxOut < 1) throw StatusError(AXISIM_E_ARG, "bad profile arguments");
         const int n = h->s->profile(iterations, out, maxOut);
+        if (nOut) *nOut = n;
+        return AXISIM_OK;
+    });
+}
+
+int axisim_profile_levels(axisim_handle* h, int32_t iterations, axisim_kernel_stat* out, int32_t maxOut,
+                          int32_t* nOut) {
+    if (!h) return AXISIM_E_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    return guarded(h, [&] {
+        if (iterations < 1 || !out || maxOut < 1) throw StatusError(AXISIM_E_ARG, "bad profile arguments");
+        const int n = h->s->profile(iterations, out, maxOut, true);
+        if (nOut) *nOut = n;
+        return AXISIM_OK;
+    });
+}
+
+int axisim_setup_profile(axisim_handle* h, axisim_kernel_stat* out, int32_t maxOut, int32_t* nOut, int32_t reset) {
+    if (!h) return AXISIM_E_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    return guarded(h, [&] {
+        if (!out || maxOut < 1) throw StatusError(AXISIM_E_ARG, "bad setup profile arguments");
+        const int n = h->s->setupProfile(out, maxOut, reset);
         if (nOut) *nOut = n;
         return AXISIM_OK;
     });

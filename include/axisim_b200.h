@@ -396,6 +396,18 @@ typedef struct axisim_kernel_stat {
  * event recorded after every kernel on the solver's stream. */
 int axisim_profile_iteration(axisim_handle* h, int32_t iterations, axisim_kernel_stat* out, int32_t maxOut,
                              int32_t* nOut);
+/* As axisim_profile_iteration, with every multigrid launch (smoothing,
+ * residual, restriction, prolongation, Galerkin, the one-CTA tail) named
+ * "<kernel>@<level>" for a per-level breakdown of the V-cycle. */
+int axisim_profile_levels(axisim_handle* h, int32_t iterations, axisim_kernel_stat* out, int32_t maxOut,
+                          int32_t* nOut);
+/* New (the reference logs no set-up timings): host-clock cost of the handle's
+ * set-up stages (mesh validation, upload, GPU precompute, multigrid hierarchy,
+ * level build, graph capture / instantiate / upload, state reset, the solve's
+ * iteration loop), summed per stage since creation or the last reset. Each
+ * entry reuses axisim_kernel_stat: `launches` counts the stage's calls, `ms`
+ * is their total, `bytes` is 0. reset != 0 clears the record after reading. */
+int axisim_setup_profile(axisim_handle* h, axisim_kernel_stat* out, int32_t maxOut, int32_t* nOut, int32_t reset);
 
 /* New; no counterpart in the reference. The SIMPLE residuals of caller-owned
  * device arrays, computed with the same arithmetic as a solve's residual step
@@ -412,12 +424,17 @@ int axisim_profile_iteration(axisim_handle* h, int32_t iterations, axisim_kernel
  * Outputs: resU/resV = |b - A x| and resC = the signed mass imbalance per cell,
  * sums[5] = the U statistic (sum, sum of squares or max by norm), sum |AC_u u|,
  * the V statistic, sum |AC_v v| and sum |imbalance| -- the values before
- * residualAllHost's scaling. Runs on the calling thread's current device, on
- * `stream` (a cudaStream_t; NULL = default stream), and returns once the results
- * are written. Out-of-range indices are skipped and reported as AXISIM_E_MESH.
- * The first call on each device looks up the scratch address, so make it before
- * any stream capture. All calls share the scratch: calls that overlap in time
- * (other threads, or other streams still running) race and give wrong sums.
+ * residualAllHost's scaling. The per-cell arrays equal a solve's bit for bit;
+ * the sums are deterministic but reduced in a different order (256-cell block
+ * partials, then a 256-wide tree), so they agree with the solve's to rounding,
+ * not bit for bit. Runs on the calling thread's current device, on `stream` (a
+ * cudaStream_t; NULL = default stream), and returns once the results are
+ * written: every call ends with a blocking read-back, so NO call may be made
+ * while `stream` is being captured into a CUDA graph (AXISIM_E_ARG). Pointers
+ * into another GPU's memory are rejected (AXISIM_E_ARG). Out-of-range indices
+ * are skipped and reported as AXISIM_E_MESH with their count. All calls share
+ * the scratch: calls that overlap in time (other threads, or other streams
+ * still running) race and give wrong sums.
  * Messages go to err[errLen] (may be NULL). */
 #define AXISIM_STATIC_MAX_CELLS 4194304
 int axisim_residual_static(int32_t nCells, int32_t nFaces, int32_t nSlots, const int32_t* cellFaceStart,

@@ -5,6 +5,13 @@ from axisim import cases
 import axisim.abi as abi
 import oracle
 
+# intermediate state compared bit for bit between the FP64 CUDA path and the oracle
+FIELDS = ["u", "v", "p", "pp", "mDot", "DU", "DV", "gradPZ", "gradPR", "gradUZ", "gradUR", "gradVZ", "gradVR",
+          "AC_u", "b_u", "AF_u", "invAC_u", "AC_v", "b_v", "AF_v", "invAC_v", "AC_pp", "b_pp", "AF_pp",
+          "invAC_pp", "res_U", "res_V", "res_Continuity"]
+# the geometry precompute (memory_manger.cpp:512-617)
+GEOM = ["invDPN", "wP", "dPB", "length2D", "lsqWZ", "lsqWR", "invA2D", "lsqInvZZ", "lsqInvZR", "lsqInvRR"]
+
 
 def oracle_case(case, mesh=None):
     m = mesh if mesh is not None else oracle.multiblock(case.blocks)

@@ -12,14 +12,9 @@ import pytest
 from axisim import cases
 import axisim.abi as abi
 import oracle
-from helpers import rel_l2
+from helpers import FIELDS, GEOM, rel_l2
 
 pytestmark = pytest.mark.gpu
-
-FIELDS = ["u", "v", "p", "pp", "mDot", "DU", "DV", "gradPZ", "gradPR", "gradUZ", "gradUR", "gradVZ", "gradVR",
-          "AC_u", "b_u", "AF_u", "invAC_u", "AC_v", "b_v", "AF_v", "invAC_v", "AC_pp", "b_pp", "AF_pp",
-          "invAC_pp", "res_U", "res_V", "res_Continuity"]
-GEOM = ["invDPN", "wP", "dPB", "length2D", "lsqWZ", "lsqWR", "invA2D", "lsqInvZZ", "lsqInvZR", "lsqInvRR"]
 
 
 def _variants():
