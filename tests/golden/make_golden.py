@@ -50,8 +50,61 @@ def fixture_cases():
     # solver as packed arrays
     out.append(("bullet1205_lsq_nonortho_6it", cases.bullet(scale=0.05, max_iter=6, tol=1e-30)))
     out.append(("batch4_union6316_5it", batch_union()[0]))
+    # the same four cases, each solved alone by the reference: a batched solve
+    # coarsens every case on its own, so each case of it must give these
+    for i, c in enumerate(batch_cases()):
+        out.append((f"batch4_case{i}_{c.name.split('_')[-1]}_5it", c))
     out += scalar_fixture_cases()
     return out
+
+
+def fullsize_fixture_cases():
+    """Workloads at their own sizes. Their fields do not fit a small fixture, so
+    compact() keeps a strided sample of cells, per-block sums and the norms."""
+    return [("expansion874496_sou_5it", cases.expansion(scale=1.0, max_iter=5, tol=1e-30))]
+
+
+SAMPLE_STRIDE = 211   # every 211th cell (4,145 of 874,496)
+BLOCK = 4096          # consecutive cells per block sum
+COMPACT_FIELDS = ("u", "v", "p", "gradPZ", "gradPR")
+
+
+def compact(res):
+    """The size-independent summary of a full-size run: for each field a
+    strided sample, the sum and the sum of magnitudes over every block of
+    BLOCK consecutive cells (so every cell contributes), and the L2 norm."""
+    out = {k: res[k] for k in ("iterations", "converged", "residual_history")}
+    for k in COMPACT_FIELDS:
+        a = np.asarray(res[k], dtype=np.float64)
+        starts = np.arange(0, a.size, BLOCK)
+        out[k + "_sample"] = a[::SAMPLE_STRIDE].copy()
+        out[k + "_blocksum"] = np.add.reduceat(a, starts)
+        out[k + "_blockabs"] = np.add.reduceat(np.abs(a), starts)
+        out[k + "_norm"] = np.array(np.linalg.norm(a))
+    out["nCells"] = np.array(len(res["u"]))
+    return out
+
+
+def compact_mismatch(fields, g):
+    """Largest relative disagreement between full fields and a compact fixture:
+    samples and norms by relative L2 / relative difference, block sums against
+    the block's sum of magnitudes (sums of signed values may cancel)."""
+    worst = {}
+    for k in COMPACT_FIELDS:
+        a = np.asarray(fields[k], dtype=np.float64)
+        starts = np.arange(0, a.size, BLOCK)
+        smp = a[::SAMPLE_STRIDE]
+        e_s = np.linalg.norm(smp - g[k + "_sample"]) / max(np.linalg.norm(g[k + "_sample"]), 1e-300)
+        e_b = np.max(np.abs(np.add.reduceat(a, starts) - g[k + "_blocksum"]) / np.maximum(g[k + "_blockabs"], 1e-300))
+        e_n = abs(np.linalg.norm(a) - float(g[k + "_norm"])) / max(float(g[k + "_norm"]), 1e-300)
+        worst[k] = max(e_s, e_b, e_n)
+    return worst
+
+
+def batch_cases(n=4, seed=7, scale=0.02, iters=5):
+    """The random cases of batch_union, each as a case of its own."""
+    from axisim import batch
+    return batch.random_cases(n, seed=seed, scale=scale, max_iter=iters, tol=1e-30)
 
 
 def batch_union(n=4, seed=7, scale=0.02, iters=5):
@@ -194,13 +247,20 @@ def run_reference(case):
 
 
 def main(outdir=HERE, only=""):
-    """Regenerates every fixture whose name contains `only`."""
+    """Regenerates every fixture whose name contains `only` (the full-size
+    ones only when `only` names them)."""
+    for name, case in fullsize_fixture_cases():
+        if not only or only not in name:
+            continue
+        res = run_reference(case)
+        np.savez_compressed(os.path.join(outdir, name + ".npz"), **compact(res))
+        print(name, res["iterations"], res["converged"], res["log"].strip().splitlines()[0])
     for name, case in fixture_cases():
         if only not in name:
             continue
         res = run_reference(case)
         keep = {k: v for k, v in res.items() if k not in ("log",)}
-        if name.startswith("pipe40x200") or name.startswith("batch"):
+        if name.startswith("pipe40x200") or name.startswith("batch4_union"):
             keep = {k: keep[k] for k in ("u", "v", "p", "iterations", "converged", "residual_history")}
         np.savez_compressed(os.path.join(outdir, name + ".npz"), **keep)
         print(name, res["iterations"], res["converged"], res["log"].strip().splitlines()[0])

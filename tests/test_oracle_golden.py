@@ -58,6 +58,25 @@ def test_oracle_matches_reference_solver(name, case):
                 np.testing.assert_allclose(o.scalar_residuals()[e], hist[-1, 4 + e], rtol=1e-6, atol=1e-12)
 
 
+FULLSIZE = make_golden.fullsize_fixture_cases()
+
+
+@pytest.mark.parametrize("name,case", FULLSIZE, ids=[n for n, _ in FULLSIZE])
+def test_oracle_matches_reference_solver_at_full_size(name, case):
+    """874,496 cells, 5 iterations: strided samples, block sums and norms of u,
+    v, p and grad p (compact fixture) to 1e-10, the same iteration count."""
+    g = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    mesh = oracle.multiblock(case.blocks)
+    assert mesh["nCells"] == int(g["nCells"])
+    o = oracle.Oracle(mesh, case.bc_fields(), case.settings)
+    it, conv = o.run()
+    assert it == int(g["iterations"]) and conv == bool(g["converged"])
+    worst = make_golden.compact_mismatch({k: o.get(k) for k in make_golden.COMPACT_FIELDS}, g)
+    assert max(worst.values()) <= TOL, worst
+    np.testing.assert_allclose(o.residuals(), g["residual_history"][-1, 1:4], rtol=1e-6)
+    o.close()
+
+
 def test_fixture_cases_are_small():
-    for name, _ in CASES:
+    for name, _ in CASES + FULLSIZE:
         assert os.path.getsize(os.path.join(HERE, "golden", name + ".npz")) < 400_000
