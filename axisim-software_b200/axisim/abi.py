@@ -42,6 +42,7 @@ EXPORTS = [
     "axisim_trellis_build", "axisim_triangle_mesh_build", "axisim_classify_boundary_faces",
     "axisim_mg_levels_host", "axisim_mg_level_maps_host", "axisim_coloring_host",
     "axisim_set_autotune", "axisim_autotune_report", "axisim_setup_profile", "axisim_profile_levels",
+    "axisim_mg_batch_levels_host",
 ]
 VAR_U, VAR_V, VAR_P, VAR_T, VAR_C = range(5)
 VAR_INDEX = {"u": VAR_U, "v": VAR_V, "p": VAR_P, "T": VAR_T, "C": VAR_C}
@@ -199,6 +200,8 @@ def lib():
             "axisim_classify_boundary_faces": (C.c_int, [C.c_int32, _i32p, _f64p, _f64p, C.POINTER(OutlineC),
                                                          C.c_double, C.c_double, _i32p]),
             "axisim_mg_levels_host": (C.c_int, [C.POINTER(MeshPacked), _i32p, C.c_int32]),
+            "axisim_mg_batch_levels_host": (C.c_int, [C.POINTER(MeshPacked), C.c_int32, _i32p, _i32p, _i32p,
+                                                      C.c_int32]),
             "axisim_mg_level_maps_host": (C.c_int64, [C.POINTER(MeshPacked), C.c_int32, vp, vp, vp, vp]),
             "axisim_coloring_host": (C.c_int, [C.POINTER(MeshPacked), _i32p, C.c_size_t]),
             "axisim_profile_iteration": (C.c_int, [vp, C.c_int32, C.POINTER(KernelStat), C.c_int32, _i32p]),
@@ -345,6 +348,19 @@ def mg_levels_host(mesh):
     if n < 0:
         raise AxisimError(-n, "mg_levels_host failed")
     return cells[:n].copy()
+
+
+def mg_batch_levels_host(mesh, case_cell_start):
+    """(cells per level, terminal cells per level) of the per-case hierarchy a batch solve builds."""
+    s, keep = mesh_struct(mesh)
+    cs = np.ascontiguousarray(case_cell_start, dtype=np.int32)
+    cells = np.zeros(64, np.int32)
+    term = np.zeros(64, np.int32)
+    n = lib().axisim_mg_batch_levels_host(C.byref(s), len(cs) - 1, cs.ctypes.data_as(_i32p),
+                                          cells.ctypes.data_as(_i32p), term.ctypes.data_as(_i32p), 64)
+    if n < 0:
+        raise AxisimError(-n, "mg_batch_levels_host failed")
+    return cells[:n].copy(), term[:n].copy()
 
 
 def mg_level_maps_host(mesh, level):

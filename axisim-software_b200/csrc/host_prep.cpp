@@ -5,6 +5,7 @@
 #include "host_prep.hpp"
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <numeric>
 #include <stdexcept>
@@ -563,6 +564,78 @@ std::vector<GridLevel> buildHierarchy(GridLevel fine) {
     }
     levels.push_back(std::move(fine));
     return levels;
+}
+
+std::vector<GridLevel> buildBatchHierarchy(const GridLevel& finest, const std::vector<int32_t>& caseStart,
+                                           std::vector<std::vector<int32_t>>& terminal) {
+    const int nCases = (int)caseStart.size() - 1;
+    std::vector<std::vector<GridLevel>> per((size_t)nCases);
+    size_t depth = 0;
+    for (int c = 0; c < nCases; c++) {
+        const int s = caseStart[(size_t)c], e = caseStart[(size_t)c + 1];
+        GridLevel g;
+        g.nCells = e - s;
+        const int k0 = finest.faceStart[(size_t)s], k1 = finest.faceStart[(size_t)e];
+        g.faceStart.resize((size_t)g.nCells + 1);
+        for (int n = 0; n <= g.nCells; n++) g.faceStart[(size_t)n] = finest.faceStart[(size_t)(s + n)] - k0;
+        g.faceNeighbor.resize((size_t)(k1 - k0));
+        for (int k = k0; k < k1; k++) {
+            const int nb = finest.faceNeighbor[(size_t)k];
+            if (nb >= 0 && (nb < s || nb >= e)) throw std::runtime_error("a face connects two cases");
+            g.faceNeighbor[(size_t)(k - k0)] = nb >= 0 ? nb - s : -1;
+        }
+        per[(size_t)c] = buildHierarchy(std::move(g));
+        depth = std::max(depth, per[(size_t)c].size());
+    }
+    const int L = (int)depth;
+    // cell and slot offsets of each case on each level (cases without the level add nothing)
+    std::vector<std::vector<int64_t>> cellOff((size_t)L, std::vector<int64_t>((size_t)nCases + 1, 0));
+    std::vector<std::vector<int64_t>> slotOff((size_t)L, std::vector<int64_t>((size_t)nCases + 1, 0));
+    for (int l = 0; l < L; l++)
+        for (int c = 0; c < nCases; c++) {
+            const bool has = (int)per[(size_t)c].size() > l;
+            const GridLevel* g = has ? &per[(size_t)c][(size_t)l] : nullptr;
+            cellOff[(size_t)l][(size_t)c + 1] = cellOff[(size_t)l][(size_t)c] + (has ? g->nCells : 0);
+            slotOff[(size_t)l][(size_t)c + 1] = slotOff[(size_t)l][(size_t)c] + (has ? g->nFaceRefs() : 0);
+        }
+    std::vector<GridLevel> out((size_t)L);
+    terminal.assign((size_t)L, {});
+    for (int l = 0; l < L; l++) {
+        GridLevel& u = out[(size_t)l];
+        if (cellOff[(size_t)l][(size_t)nCases] > INT32_MAX || slotOff[(size_t)l][(size_t)nCases] > INT32_MAX)
+            throw std::runtime_error("batch too large");
+        u.nCells = (int)cellOff[(size_t)l][(size_t)nCases];
+        u.faceStart.assign((size_t)u.nCells + 1, 0);
+        u.faceNeighbor.resize((size_t)slotOff[(size_t)l][(size_t)nCases]);
+        const bool deepest = l == L - 1;
+        if (!deepest) {
+            u.cellToCoarse.assign((size_t)u.nCells, -1);
+            u.fineSlotToCoarseSlot.assign(u.faceNeighbor.size(), -1);
+        }
+        for (int c = 0; c < nCases; c++) {
+            if ((int)per[(size_t)c].size() <= l) continue;
+            const GridLevel& g = per[(size_t)c][(size_t)l];
+            const int co = (int)cellOff[(size_t)l][(size_t)c], so = (int)slotOff[(size_t)l][(size_t)c];
+            for (int n = 0; n < g.nCells; n++) u.faceStart[(size_t)(co + n) + 1] = so + g.faceStart[(size_t)n + 1];
+            for (int k = 0; k < g.nFaceRefs(); k++) {
+                const int nb = g.faceNeighbor[(size_t)k];
+                u.faceNeighbor[(size_t)(so + k)] = nb >= 0 ? nb + co : -1;
+            }
+            if (deepest) continue;
+            if (g.isCoarsest()) {  // this case ends here: terminal cells, no coarse parent
+                terminal[(size_t)l].push_back(co);
+                terminal[(size_t)l].push_back(co + g.nCells);
+                continue;
+            }
+            const int cco = (int)cellOff[(size_t)l + 1][(size_t)c], cso = (int)slotOff[(size_t)l + 1][(size_t)c];
+            for (int n = 0; n < g.nCells; n++) u.cellToCoarse[(size_t)(co + n)] = g.cellToCoarse[(size_t)n] + cco;
+            for (int k = 0; k < g.nFaceRefs(); k++) {
+                const int t = g.fineSlotToCoarseSlot[(size_t)k];
+                u.fineSlotToCoarseSlot[(size_t)(so + k)] = t >= 0 ? t + cso : -1;
+            }
+        }
+    }
+    return out;
 }
 
 int pickBlock(const std::vector<int>& candidates, const std::vector<double>& timeUs, int defaultIndex, double tol) {

@@ -85,6 +85,17 @@ GridLevel finestLevel(int nCells, int nFaces, const int32_t* cellFaceStart, cons
 // shrinks by less than 0.8.
 std::vector<GridLevel> buildHierarchy(GridLevel finest);
 
+// A batch of independent cases packed into one mesh (cells
+// [caseStart[c], caseStart[c+1]) of case c, no face between cases): each
+// case's hierarchy built alone with buildHierarchy, then merged level by level
+// (level l holds, in case order, the level-l cells of every case that has a
+// level l). A case whose coarsest level is l < the deepest level has
+// cellToCoarse = fineSlotToCoarseSlot = -1 there; its cells are that level's
+// terminal cells, listed per level as [begin, end) pairs in terminal[l].
+// Every level of every case is then exactly its standalone level.
+std::vector<GridLevel> buildBatchHierarchy(const GridLevel& finest, const std::vector<int32_t>& caseStart,
+                                           std::vector<std::vector<int32_t>>& terminal);
+
 // buildMeshColoring (memory_manger.cpp:334-409): greedy colour per cell.
 int greedyColoring(const GridLevel& g, std::vector<int32_t>& color);
 

@@ -33,6 +33,13 @@ struct LevelT {
     int32_t* gList = nullptr;   // fine slot positions, ascending fine cell then slot
     uint32_t* internalMask = nullptr;  // on the FINE level: slots folding into the coarse diagonal
     int block = 0;  // threads per CTA of this level's smoothing, residual and transfer kernels (0: 256)
+    // batch with per-case hierarchies: the cases whose coarsest level this is
+    // (not the deepest level), as [begin, end) cell ranges; their cells have
+    // c2c = -1, keep their values through the level's sweeps and transfers,
+    // and are solved by the coarsest-level sweeps of launchMGTerminal
+    int nTerm = 0;
+    int termMax = 0;                // cells of the largest terminal range
+    const int32_t* term = nullptr;  // [2 nTerm]
 };
 using LevelDev = LevelT<double>;
 using LevelF = LevelT<float>;
@@ -136,6 +143,10 @@ void launchMGProlong(const Ctl* ctl, const LevelT<T>& fine, T* xFine, const T* x
 template <class T>
 bool launchMGProlongSmooth(const Ctl* ctl, const LevelT<T>& fine, const T* xFine, const T* xCoarse, T* y, T w,
                            T scale, cudaStream_t s);
+// the coarsest-level solve of each terminal case of a level: `sweeps` Jacobi
+// sweeps from zero, one CTA per case, written to x (cells of other cases untouched)
+template <class T>
+void launchMGTerminal(const Ctl* ctl, const LevelT<T>& L, T* x, T w, int sweeps, cudaStream_t s);
 template <class T>
 size_t tailSharedBytes(const TailArgsT<T>& a);
 template <class T>

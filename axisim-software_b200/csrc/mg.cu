@@ -211,6 +211,12 @@ __global__ void __launch_bounds__(kThreads) k_mg_residual_ell(const Ctl* ctl, Le
     L.res[n] = L.b[n] - ellAx<T, WC>(L, n, x, false);
 }
 
+// A terminal cell of a batch level (its case's coarsest level) keeps its value.
+template <class T>
+__device__ __forceinline__ bool frozen(const LevelT<T>& L, int n) {
+    return L.nTerm > 0 && L.c2c[n] < 0;
+}
+
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_mg_smooth(const Ctl* ctl, LevelT<T> L, const T* __restrict__ x,
                                                         T* __restrict__ y, T w) {
@@ -218,7 +224,69 @@ __global__ void __launch_bounds__(kThreads) k_mg_smooth(const Ctl* ctl, LevelT<T
     if (ctl->done || ctl->ppSkip) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= L.N) return;
-    y[n] = jacobiRow(L, n, x, w, L.b[n]);
+    y[n] = frozen(L, n) ? x[n] : jacobiRow(L, n, x, w, L.b[n]);
+}
+
+// Coarsest-level sweeps of the terminal cases of a batch level, one CTA per
+// case: from zero, `sweeps` weighted-Jacobi sweeps (jacobiRow's arithmetic)
+// with both iterates in shared memory, as the case's standalone coarsest
+// level runs them. A case's neighbours all lie inside its range.
+template <class T>
+__device__ __forceinline__ void terminalBody(const LevelT<T>& L, T* x, T w, int sweeps, int r, unsigned char* smraw) {
+    const int s0 = L.term[2 * r], n1 = L.term[2 * r + 1];
+    const int m = n1 - s0;
+    T* xo = reinterpret_cast<T*>(smraw);
+    T* xn = xo + m;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) xo[i] = T(0);
+    __syncthreads();
+    for (int it = 0; it < sweeps; it++) {
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            const int n = s0 + i;
+            const T ac = L.AC[n];
+            if (fabs(ac) < tiny<T>()) {
+                xn[i] = xo[i];
+                continue;
+            }
+            T Ax = ac * xo[i];
+            const Slots sl = slotsOf(L, n);
+            for (int j = 0; j < sl.width; j++) {
+                const int p = sl.base + j * sl.stride;
+                const int k = L.nb[p];
+                if (k != -1) Ax += L.AF[p] * xo[k - s0];
+            }
+            xn[i] = xo[i] + w * (L.b[n] - Ax) / ac;
+        }
+        __syncthreads();
+        T* t = xo;
+        xo = xn;
+        xn = t;
+    }
+    for (int i = threadIdx.x; i < m; i += blockDim.x) x[s0 + i] = xo[i];
+}
+
+template <class T>
+__global__ void k_mg_terminal(const Ctl* ctl, LevelT<T> L, T* x, T w, int sweeps) {
+    pdlEnter();
+    if (ctl->done || ctl->ppSkip) return;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    terminalBody(L, x, w, sweeps, (int)blockIdx.x, smraw);
+}
+
+// `sweeps` sweeps of a whole level inside one CTA, both iterates in shared memory.
+template <class T>
+__device__ __forceinline__ void smoothBlockBody(const LevelT<T>& L, T* x, T w, int sweeps, unsigned char* smraw) {
+    T* xo = reinterpret_cast<T*>(smraw);
+    T* xn = xo + L.N;
+    for (int n = threadIdx.x; n < L.N; n += blockDim.x) xo[n] = x[n];
+    __syncthreads();
+    for (int it = 0; it < sweeps; it++) {
+        for (int n = threadIdx.x; n < L.N; n += blockDim.x) xn[n] = frozen(L, n) ? xo[n] : jacobiRow(L, n, xo, w, L.b[n]);
+        __syncthreads();
+        T* t = xo;
+        xo = xn;
+        xn = t;
+    }
+    for (int n = threadIdx.x; n < L.N; n += blockDim.x) x[n] = xo[n];
 }
 
 template <class T>
@@ -226,18 +294,7 @@ __global__ void k_mg_smooth_block(const Ctl* ctl, LevelT<T> L, T* x, T w, int sw
     pdlEnter();
     if (ctl->done || ctl->ppSkip) return;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* xo = reinterpret_cast<T*>(smraw);
-    T* xn = xo + L.N;
-    for (int n = threadIdx.x; n < L.N; n += blockDim.x) xo[n] = x[n];
-    __syncthreads();
-    for (int it = 0; it < sweeps; it++) {
-        for (int n = threadIdx.x; n < L.N; n += blockDim.x) xn[n] = jacobiRow(L, n, xo, w, L.b[n]);
-        __syncthreads();
-        T* t = xo;
-        xo = xn;
-        xn = t;
-    }
-    for (int n = threadIdx.x; n < L.N; n += blockDim.x) x[n] = xo[n];
+    smoothBlockBody(L, x, w, sweeps, smraw);
 }
 
 template <class T>
@@ -276,7 +333,8 @@ __global__ void __launch_bounds__(kThreads) k_mg_prolong(const Ctl* ctl, int N, 
     if (ctl->done || ctl->ppSkip) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
-    x[n] += scale * xc[c2c[n]];
+    const int c = c2c[n];
+    if (c >= 0) x[n] += scale * xc[c];  // a batch's terminal cells have no coarse parent
 }
 
 // Galerkin, step 1 (coalesced over fine cells): each row's contribution to
@@ -499,6 +557,19 @@ bool launchMGProlongSmooth(const Ctl* ctl, const LevelT<T>& fine, const T* xFine
 }
 
 template <class T>
+void launchMGTerminal(const Ctl* ctl, const LevelT<T>& L, T* x, T w, int sweeps, cudaStream_t s) {
+    if (L.nTerm <= 0) return;
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_mg_terminal<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        configured = true;
+    }
+    const int threads = L.termMax < 256 ? ((L.termMax + 31) / 32) * 32 : 256;
+    launchPDL(k_mg_terminal<T>, dim3(L.nTerm), dim3(threads), 2 * (size_t)L.termMax * sizeof(T), s, ctl, L, x, w,
+              sweeps);
+}
+
+template <class T>
 size_t tailSharedBytes(const TailArgsT<T>& a) {
     size_t d = 0;
     for (int i = 0; i < a.count; i++) d += 4 * (size_t)a.lv[i].N;
@@ -527,6 +598,7 @@ template void launchGalerkin<float, float>(const Ctl*, const LevelT<float>&, con
     template void launchMGGather<T>(const Ctl*, const LevelT<T>&, const LevelT<T>&, T*, T*, int, T, cudaStream_t); \
     template void launchMGProlong<T>(const Ctl*, const LevelT<T>&, T*, const T*, T, cudaStream_t);                 \
     template bool launchMGProlongSmooth<T>(const Ctl*, const LevelT<T>&, const T*, const T*, T*, T, T, cudaStream_t); \
+    template void launchMGTerminal<T>(const Ctl*, const LevelT<T>&, T*, T, int, cudaStream_t);                  \
     template size_t tailSharedBytes<T>(const TailArgsT<T>&);                                                   \
     template void launchMGTail<T>(const Ctl*, const TailArgsT<T>&, cudaStream_t);
 AXISIM_MG_INSTANTIATE(double)

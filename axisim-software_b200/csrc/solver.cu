@@ -251,6 +251,9 @@ public:
         if (!haveMesh_) throw StatusError(AXISIM_E_STATE, "no mesh");
         if (precision < 0 || precision > 2) throw StatusError(AXISIM_E_ARG, "unknown network precision");
         ensureHierarchy();
+        if (!termRanges_.empty())
+            throw StatusError(AXISIM_E_CONFIG, "the learned preconditioner needs one hierarchy over the whole mesh "
+                                               "(not a batch of per-case hierarchies)");
         net_.init(hier_, mesh_.snb, W_, precision, seed, stream_);
         adamT_ = 0;
         destroyGraph();
@@ -488,6 +491,23 @@ public:
         destroyGraph();
         batchArena_.release();
         batch_ = BatchDev{};
+        // the multigrid hierarchy depends on the case layout (one per case)
+        if (haveHierarchy_ && (nCases > 0 || !termRanges_.empty())) {
+            mixArena_.release();
+            levels32_.clear();
+            AF32m_ = nullptr;
+            fcgR_ = nullptr;
+            netArena_.release();
+            netStats_ = nullptr;
+            nnY_ = nullptr;
+            nnAy_ = nullptr;
+            resetLearned();
+            mgArena_.release();
+            levels_.clear();
+            hier_.clear();
+            termRanges_.clear();
+            haveHierarchy_ = false;
+        }
         hCaseStart_.clear();
         if (nCases == 0) return;
         hCaseStart_.assign(caseStart, caseStart + nCases + 1);
@@ -748,6 +768,10 @@ private:
 
     // multigrid / colouring
     std::vector<GridLevel> hier_;
+    // batch with per-case hierarchies: per level, the [begin, end) ranges of
+    // the cases whose coarsest level it is (empty: one joint hierarchy)
+    std::vector<std::vector<int32_t>> termRanges_;
+    static constexpr int kMaxTerminalCells = 12 * 1024;  // a terminal case's shared-memory sweeps
     bool haveHierarchy_ = false;
     int autotune_ = 0;             // tune the level launch shapes before capturing the graph
     std::vector<double> tuneUs_;   // measured sweep time per level and candidate (us)
@@ -956,7 +980,28 @@ private:
         if (haveHierarchy_) return;
         if (!haveMesh_) throw StatusError(AXISIM_E_STATE, "no mesh");
         PhaseTimer ph(*this, "hierarchy_host");
-        hier_ = buildHierarchy(finestLevel(N_, F_, hCfs_.data(), hCfi_.data(), hOwner_.data(), hNeighbor_.data()));
+        GridLevel fine = finestLevel(N_, F_, hCfs_.data(), hCfi_.data(), hOwner_.data(), hNeighbor_.data());
+        termRanges_.clear();
+        if (hCaseStart_.size() > 2) {
+            // each case coarsened alone; a case with one level only would be
+            // terminal on the finest level, which the fine-level kernels do
+            // not support: such a batch keeps one joint hierarchy
+            std::vector<std::vector<int32_t>> term;
+            std::vector<GridLevel> h = buildBatchHierarchy(fine, hCaseStart_, term);
+            size_t biggest = 0;
+            for (const auto& t : term)
+                for (size_t i = 0; i + 1 < t.size(); i += 2) biggest = std::max(biggest, (size_t)(t[i + 1] - t[i]));
+            if (term.empty() || !term[0].empty() || biggest > kMaxTerminalCells) {
+                log("batch: a case has a single multigrid level or a coarsest level above " +
+                    std::to_string(kMaxTerminalCells) + " cells; the batch shares one hierarchy\n");
+                hier_ = buildHierarchy(std::move(fine));
+            } else {
+                hier_ = std::move(h);
+                termRanges_ = std::move(term);
+            }
+        } else {
+            hier_ = buildHierarchy(std::move(fine));
+        }
         haveHierarchy_ = true;
         levels_.clear();
         levels32_.clear();
@@ -1040,12 +1085,16 @@ private:
             const GridLevel& c = hier_[(size_t)l];
             LevelDev& fd = levels_[(size_t)l - 1];
             LevelDev& cd = levels_[(size_t)l];
-            std::vector<int32_t> mStart((size_t)c.nCells + 1, 0), mList((size_t)f.nCells);
-            for (int n = 0; n < f.nCells; n++) mStart[(size_t)f.cellToCoarse[(size_t)n] + 1]++;
+            // members of each coarse cell (a batch's terminal cells have no coarse cell)
+            std::vector<int32_t> mStart((size_t)c.nCells + 1, 0), mList;
+            for (int n = 0; n < f.nCells; n++)
+                if (f.cellToCoarse[(size_t)n] >= 0) mStart[(size_t)f.cellToCoarse[(size_t)n] + 1]++;
             for (int k = 0; k < c.nCells; k++) mStart[(size_t)k + 1] += mStart[(size_t)k];
+            mList.resize((size_t)std::max(mStart[(size_t)c.nCells], 1));
             {
                 std::vector<int32_t> fill(mStart);
-                for (int n = 0; n < f.nCells; n++) mList[(size_t)fill[(size_t)f.cellToCoarse[(size_t)n]]++] = n;
+                for (int n = 0; n < f.nCells; n++)
+                    if (f.cellToCoarse[(size_t)n] >= 0) mList[(size_t)fill[(size_t)f.cellToCoarse[(size_t)n]]++] = n;
             }
             std::vector<int32_t> coarsePos((size_t)std::max(c.nFaceRefs(), 1));
             for (int cc = 0; cc < c.nCells; cc++)
@@ -1078,9 +1127,20 @@ private:
             cd.gList = mgArena_.upload(gList.data(), gList.size());
             fd.internalMask = mgArena_.upload(mask.data(), mask.size());
         }
+        int lastTerminal = -1;
+        for (int l = 0; l < (int)termRanges_.size() && l < L; l++) {
+            const std::vector<int32_t>& t = termRanges_[(size_t)l];
+            if (t.empty()) continue;
+            LevelDev& d = levels_[(size_t)l];
+            d.nTerm = (int)t.size() / 2;
+            d.termMax = 0;
+            for (size_t i = 0; i + 1 < t.size(); i += 2) d.termMax = std::max(d.termMax, t[i + 1] - t[i]);
+            d.term = mgArena_.upload(t.data(), t.size());
+            lastTerminal = l;
+        }
         // V-cycle tail: the deepest levels that all fit one CTA's shared memory
         tailStart_ = -1;
-        for (int t = 1; t < L; t++) {
+        for (int t = std::max(1, lastTerminal + 1); t < L; t++) {
             if (L - t > kMaxTail) continue;
             bool fits = true;
             size_t bytes = 0;
@@ -1150,6 +1210,9 @@ private:
             f.gStart = d.gStart;
             f.gList = d.gList;
             f.internalMask = d.internalMask;
+            f.nTerm = d.nTerm;
+            f.termMax = d.termMax;
+            f.term = d.term;
             if (l == 0) {
                 f.AF = AF32pp_;
                 f.AC = AC32pp_;
@@ -1236,6 +1299,10 @@ private:
             launchMGGather<T>(ctl_, F, C, cur[(size_t)l + 1], alt[(size_t)l + 1], fuse ? 1 : 0, w, stream_);
             markL(std::string("mg_gather") + tag, l + 1, (4.0 + vb) * F.N + 4.0 * vb * C.N);
             if (fuse) std::swap(cur[(size_t)l + 1], alt[(size_t)l + 1]);
+            if (C.nTerm > 0) {  // the cases whose coarsest level this is: their coarsest-level sweeps
+                launchMGTerminal<T>(ctl_, C, cur[(size_t)l + 1], w, cmg_.linearSweep, stream_);
+                markL(std::string("mg_terminal") + tag, l + 1, (double)C.N * ((4.0 + vb) * C.W + 3.0 * vb));
+            }
             vcycleT<T>(lv, l + 1, cur, alt, fuse);
         }
         const int post = cmg_.linearPostSweep;
@@ -2600,6 +2667,30 @@ int axisim_mg_levels_host(const axisim_mesh_packed* mesh, int32_t* cellsPerLevel
     try {
         const std::vector<axisim::GridLevel> h = axisim::buildHierarchy(hostFinest(mesh));
         for (int l = 0; l < (int)h.size() && l < maxLevels; l++) cellsPerLevel[l] = h[(size_t)l].nCells;
+        return (int)h.size();
+    } catch (...) {
+        return -AXISIM_E_MESH;
+    }
+}
+
+int axisim_mg_batch_levels_host(const axisim_mesh_packed* mesh, int32_t nCases, const int32_t* caseCellStart,
+                                int32_t* cellsPerLevel, int32_t* terminalCellsPerLevel, int32_t maxLevels) {
+    if (maxLevels < 0 || (maxLevels > 0 && (!cellsPerLevel || !terminalCellsPerLevel))) return -AXISIM_E_ARG;
+    if (nCases < 1 || !caseCellStart) return -AXISIM_E_ARG;
+    if (!connectivityOk(mesh)) return -AXISIM_E_MESH;
+    if (caseCellStart[0] != 0 || caseCellStart[nCases] != mesh->nCells) return -AXISIM_E_ARG;
+    for (int c = 0; c < nCases; c++)
+        if (caseCellStart[c + 1] <= caseCellStart[c]) return -AXISIM_E_ARG;
+    try {
+        std::vector<std::vector<int32_t>> term;
+        const std::vector<int32_t> start(caseCellStart, caseCellStart + nCases + 1);
+        const std::vector<axisim::GridLevel> h = axisim::buildBatchHierarchy(hostFinest(mesh), start, term);
+        for (int l = 0; l < (int)h.size() && l < maxLevels; l++) {
+            cellsPerLevel[l] = h[(size_t)l].nCells;
+            int t = 0;
+            for (size_t i = 0; i + 1 < term[(size_t)l].size(); i += 2) t += term[(size_t)l][i + 1] - term[(size_t)l][i];
+            terminalCellsPerLevel[l] = t;
+        }
         return (int)h.size();
     } catch (...) {
         return -AXISIM_E_MESH;

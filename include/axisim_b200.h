@@ -376,6 +376,13 @@ int axisim_coloring(const axisim_handle* h, int32_t* colorOut, size_t n);
  * rebuilds what it reports. A mesh whose connectivity fails axisim_set_mesh's
  * checks gives -AXISIM_E_MESH. */
 int axisim_mg_levels_host(const axisim_mesh_packed* mesh, int32_t* cellsPerLevel, int32_t maxLevels);
+/* New: the hierarchy a batch solve uses (axisim_set_batch with these case
+ * ranges): each case coarsened alone as MultigridSolver::buildLevels does for
+ * a mesh of its own (multigrid.cu:298-325), merged level by level. Per level,
+ * the cells of all cases and the cells of the cases whose coarsest level it is
+ * (0 on the deepest level). Returns the number of levels or -status. */
+int axisim_mg_batch_levels_host(const axisim_mesh_packed* mesh, int32_t nCases, const int32_t* caseCellStart,
+                                int32_t* cellsPerLevel, int32_t* terminalCellsPerLevel, int32_t maxLevels);
 int64_t axisim_mg_level_maps_host(const axisim_mesh_packed* mesh, int32_t level, int32_t* cellToCoarse,
                                   int32_t* fineSlotToCoarseSlot, int32_t* coarseFaceStart,
                                   int32_t* coarseFaceNeighbor);

@@ -87,3 +87,25 @@ def test_host_hierarchy_rejects_bad_connectivity_and_levels():
     with pytest.raises(abi.AxisimError) as e:
         abi.coloring_host(bad)
     assert e.value.status == abi.E_MESH
+
+
+def test_batch_hierarchy_is_each_case_coarsened_alone():
+    """A batch solve coarsens every case on its own (multigrid.cu:298-325 per
+    case) and merges the levels: each level holds the cells of every case that
+    reaches it, and a case's coarsest level is terminal there."""
+    cs = batch.random_cases(6, seed=5, lo=2_000, hi=40_000)
+    meshes = [oracle.multiblock(c.blocks) for c in cs]
+    union, start, _ = batch.pack_union(meshes, [c.groups for c in cs])
+    cells, term = abi.mg_batch_levels_host(union, start)
+    alone = [abi.mg_levels_host(m) for m in meshes]
+    depth = max(len(a) for a in alone)
+    assert len(cells) == depth
+    assert len({len(a) for a in alone}) > 1, "the draw should hold cases of different depths"
+    for lvl in range(depth):
+        assert cells[lvl] == sum(int(a[lvl]) for a in alone if len(a) > lvl)
+        want = sum(int(a[lvl]) for a in alone if len(a) == lvl + 1) if lvl < depth - 1 else 0
+        assert term[lvl] == want, lvl
+    # a one-case batch is the case's own hierarchy
+    c1, t1 = abi.mg_batch_levels_host(meshes[0], [0, meshes[0]["nCells"]])
+    np.testing.assert_array_equal(c1, alone[0])
+    assert not t1.any()
