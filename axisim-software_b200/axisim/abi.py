@@ -22,6 +22,7 @@ OK, E_ARG, E_CONFIG, E_MESH, E_CUDA, E_DIVERGED, E_STOPPED, E_STATE, E_TIMEOUT =
 STATUS_NAMES = {0: "OK", 1: "E_ARG", 2: "E_CONFIG", 3: "E_MESH", 4: "E_CUDA", 5: "E_DIVERGED",
                 6: "E_STOPPED", 7: "E_STATE", 8: "E_TIMEOUT"}
 PREC_FP64, PREC_MIXED = 0, 1
+VCYCLE_PER_PHASE, VCYCLE_RESIDENT = 0, 1
 PSOLVE_VCYCLES, PSOLVE_FCG = 0, 1
 LEARNED_OFF, LEARNED_FIRST_STEP, LEARNED_ALWAYS = 0, 1, 2
 NET_FP32, NET_BF16, NET_BF16_WEIGHTS = 0, 1, 2
@@ -42,7 +43,7 @@ EXPORTS = [
     "axisim_trellis_build", "axisim_triangle_mesh_build", "axisim_classify_boundary_faces",
     "axisim_mg_levels_host", "axisim_mg_level_maps_host", "axisim_coloring_host",
     "axisim_set_autotune", "axisim_autotune_report", "axisim_setup_profile", "axisim_profile_levels",
-    "axisim_mg_batch_levels_host",
+    "axisim_mg_batch_levels_host", "axisim_set_vcycle_kernel", "axisim_test_barrier_timeout",
 ]
 VAR_U, VAR_V, VAR_P, VAR_T, VAR_C = range(5)
 VAR_INDEX = {"u": VAR_U, "v": VAR_V, "p": VAR_P, "T": VAR_T, "C": VAR_C}
@@ -160,6 +161,8 @@ def lib():
             "axisim_set_precision": (C.c_int, [vp, C.c_int32]),
             "axisim_set_pressure_solver": (C.c_int, [vp, C.c_int32, C.c_double, C.c_double]),
             "axisim_set_autotune": (C.c_int, [vp, C.c_int32]),
+            "axisim_set_vcycle_kernel": (C.c_int, [vp, C.c_int32]),
+            "axisim_test_barrier_timeout": (C.c_int, [vp, C.c_int32]),
             "axisim_autotune_report": (C.c_int, [vp, _i32p, _f64p, C.c_int32]),
             "axisim_pressure_stats": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
             "axisim_learned_harvest": (C.c_int, [vp, C.c_int32, C.c_int32]),
@@ -673,6 +676,11 @@ class Solver:
         a, f, sn, sv = C.c_int64(), C.c_int64(), C.c_double(), C.c_double()
         self._check(lib().axisim_learned_stats(self.h, C.byref(a), C.byref(f), C.byref(sn), C.byref(sv)))
         return dict(applied=a.value, fallbacks=f.value, score_net=sn.value, score_vcycle=sv.value)
+
+    def set_vcycle_kernel(self, mode):
+        """VCYCLE_RESIDENT (default): the coarser levels' V-cycle in one cooperative kernel;
+        VCYCLE_PER_PHASE: one launch per phase."""
+        self._check(lib().axisim_set_vcycle_kernel(self.h, mode))
 
     def set_autotune(self, on=True):
         """Tune the multigrid levels' launch shapes before the next solve captures its graph."""

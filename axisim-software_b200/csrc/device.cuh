@@ -98,7 +98,8 @@ struct BCDev {
 // return at entry once `done` is set, so a captured iteration graph can be
 // replayed past convergence without changing the result.
 struct Ctl {
-    int done;             // 0 running, 1 converged, 2 stopped, 3 iteration budget, 4 non-finite residual
+    int done;             // 0 running, 1 converged, 2 stopped, 3 iteration budget, 4 non-finite residual,
+                          // 5 a grid barrier of the resident V-cycle gave up
     int k;                // SIMPLE iteration within the current time step
     int currentIteration; // run-global iteration counter (continues across continue runs)
     int maxIter;
@@ -135,6 +136,13 @@ struct Ctl {
     int resScaleS[2];
     int resEnabledS[2];
     int solvedS[2];       // the scalar is solved (an unsolved one has an all-zero system)
+    // grid-wide barrier of the resident V-cycle kernel: arrivals, generation;
+    // mgErr is set when a wait gives up (the next iteration then ends the run);
+    // mgPhantom extra arrivals are expected per barrier (0; 1 in a test that
+    // makes a wait run out)
+    unsigned int mgBar[2];
+    int mgErr;
+    int mgPhantom;
 };
 
 // One transported scalar (energy or concentration) in the fused assembly.

@@ -59,6 +59,37 @@ struct TailArgsT {
 };
 using TailArgs = TailArgsT<double>;
 
+// The V-cycle below the finest level run as ONE resident (cooperative) kernel:
+// the phases the per-phase launches would run, recorded in order at capture
+// time, each followed by a grid-wide barrier. Every phase keeps the per-cell
+// arithmetic of its separate kernel, so results are the same bit for bit.
+enum MgOpType : int {
+    kOpSmooth = 1,      // y = sweep(x) on the level              p0 = x, p1 = y
+    kOpSmoothBlock,     // ival sweeps of the level in one CTA    p0 = x (in place)
+    kOpResidual,        // res = b - A x                          p0 = x
+    kOpGather,          // b = restricted finer residual; x = 0 or first sweep (ival) p0 = xCur, p1 = xAlt
+    kOpTerminal,        // terminal cases' coarsest sweeps (ival) p0 = x
+    kOpProlong,         // x += scale * P xc                      p0 = x (fine), p1 = xc
+    kOpTail,            // the one-CTA tail (ResidentArgsT::tail)
+};
+struct MgOp {
+    int type = 0, level = 0, ival = 0, pad = 0;
+    void* p0 = nullptr;
+    void* p1 = nullptr;
+    double scale = 0.0;
+};
+constexpr int kMaxResidentLevels = 12;
+constexpr int kMaxResidentOps = 64;
+template <class T>
+struct ResidentArgsT {
+    int nOps = 0, first = 0, nLevels = 0;
+    T w = T(0);
+    LevelT<T> lv[kMaxResidentLevels];  // levels first .. first + nLevels - 1
+    MgOp ops[kMaxResidentOps];
+    TailArgsT<T> tail;
+    size_t smem = 0;  // dynamic shared memory the phases need
+};
+
 // ---- setup ----
 void launchPrecompute(const MeshDev& m, const int32_t* cfs, const int32_t* cfi, double* lsqDZ, double* lsqDR,
                       cudaStream_t s);
@@ -147,6 +178,11 @@ bool launchMGProlongSmooth(const Ctl* ctl, const LevelT<T>& fine, const T* xFine
 // sweeps from zero, one CTA per case, written to x (cells of other cases untouched)
 template <class T>
 void launchMGTerminal(const Ctl* ctl, const LevelT<T>& L, T* x, T w, int sweeps, cudaStream_t s);
+// the resident V-cycle kernel: one CTA of 1024 threads per SM (cooperative
+// launch, no programmatic serialisation on either side); false when the
+// device cannot hold the grid or the program does not fit
+template <class T>
+bool launchMGResident(Ctl* ctl, const ResidentArgsT<T>& a, cudaStream_t s);
 template <class T>
 size_t tailSharedBytes(const TailArgsT<T>& a);
 template <class T>

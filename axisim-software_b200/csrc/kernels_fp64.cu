@@ -139,6 +139,10 @@ __global__ void k_iter_begin(Ctl* ctl, const volatile int* hostStop) {
         ctl->done = 2;
         return;
     }
+    if (ctl->mgErr) {  // a grid barrier of the resident V-cycle gave up
+        ctl->done = 5;
+        return;
+    }
     if (ctl->k >= ctl->maxIter) {
         ctl->done = 3;
         return;

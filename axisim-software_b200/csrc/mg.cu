@@ -309,12 +309,8 @@ __global__ void __launch_bounds__(kThreads) k_mg_residual(const Ctl* ctl, LevelT
 // Restriction (multigrid.cu:398-410) as a gather; optionally the coarse
 // level's first Jacobi sweep from x = 0: x1 = 0 + w (b - A 0) / AC.
 template <class T>
-__global__ void __launch_bounds__(kThreads) k_mg_gather(const Ctl* ctl, const T* __restrict__ resFine, LevelT<T> C,
-                                                        T* xCur, T* xAlt, int firstSweep, T w) {
-    pdlEnter();
-    if (ctl->done || ctl->ppSkip) return;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= C.N) return;
+__device__ __forceinline__ void gatherCell(int c, const T* __restrict__ resFine, const LevelT<T>& C, T* xCur, T* xAlt,
+                                           int firstSweep, T w) {
     T sum = T(0);
     for (int q = C.mStart[c]; q < C.mStart[c + 1]; q++) sum += resFine[C.mList[q]];
     C.b[c] = sum;
@@ -324,6 +320,16 @@ __global__ void __launch_bounds__(kThreads) k_mg_gather(const Ctl* ctl, const T*
     }
     const T ac = C.AC[c];
     xAlt[c] = (fabs(ac) < tiny<T>()) ? T(0) : T(0) + w * (sum - ac * T(0)) / ac;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_mg_gather(const Ctl* ctl, const T* __restrict__ resFine, LevelT<T> C,
+                                                        T* xCur, T* xAlt, int firstSweep, T w) {
+    pdlEnter();
+    if (ctl->done || ctl->ppSkip) return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C.N) return;
+    gatherCell(c, resFine, C, xCur, xAlt, firstSweep, w);
 }
 
 template <class T>
@@ -389,9 +395,37 @@ __device__ __forceinline__ void tailSmooth(const LevelT<T>& L, T*& xo, T*& xn, c
     }
 }
 
-// Coarsest level with one row per thread held in registers.
+// Barrier of the first `threads` threads of the CTA (a multiple of 32):
+// named barrier 1, or the warp's own barrier for a single warp.
+__device__ __forceinline__ void groupSync(int threads) {
+    if (threads <= 32) __syncwarp();
+    else asm volatile("bar.sync 1, %0;" ::"r"(threads) : "memory");
+}
+
+template <class T>
+__device__ __forceinline__ void tailCoarsestGroup(const LevelT<T>& L, T*& xo, T*& xn, const T* b, T w, int sweeps,
+                                                  int group);
+
+// Coarsest level with one row per thread held in registers. Only the warps
+// that hold rows take part in the sweeps, synchronising among themselves (a
+// CTA-wide barrier per sweep would wait on every warp of the CTA); the others
+// go straight to the closing CTA barrier.
 template <class T>
 __device__ __forceinline__ void tailCoarsest(const LevelT<T>& L, T*& xo, T*& xn, const T* b, T w, int sweeps) {
+    const int n = threadIdx.x;
+    const int group = ((L.N + 31) / 32) * 32;  // threads of the warps holding rows (whole warps)
+    if (n < group) tailCoarsestGroup(L, xo, xn, b, w, sweeps, group);
+    else if (sweeps & 1) {  // the same buffer roles as the sweeping warps end with
+        T* t = xo;
+        xo = xn;
+        xn = t;
+    }
+    __syncthreads();
+}
+
+template <class T>
+__device__ __forceinline__ void tailCoarsestGroup(const LevelT<T>& L, T*& xo, T*& xn, const T* b, T w, int sweeps,
+                                                  int group) {
     const int n = threadIdx.x;
     const bool active = n < L.N;
     T af[kRegW];
@@ -426,7 +460,7 @@ __device__ __forceinline__ void tailCoarsest(const LevelT<T>& L, T*& xo, T*& xn,
                 xn[n] = xo[n] + w * (bn - Ax) / ac;
             }
         }
-        __syncthreads();
+        groupSync(group);
         T* t = xo;
         xo = xn;
         xn = t;
@@ -434,10 +468,7 @@ __device__ __forceinline__ void tailCoarsest(const LevelT<T>& L, T*& xo, T*& xn,
 }
 
 template <class T>
-__global__ void __launch_bounds__(kTailThreads) k_mg_tail(const Ctl* ctl, TailArgsT<T> a) {
-    pdlEnter();
-    if (ctl->done || ctl->ppSkip) return;
-    extern __shared__ __align__(16) unsigned char smraw[];
+__device__ __forceinline__ void tailBody(const TailArgsT<T>& a, unsigned char* smraw) {
     T* sm = reinterpret_cast<T*>(smraw);
     T* X[kMaxTail];
     T* Y[kMaxTail];
@@ -488,6 +519,109 @@ __global__ void __launch_bounds__(kTailThreads) k_mg_tail(const Ctl* ctl, TailAr
         tailSmooth(L, X[i], Y[i], B[i], a.w, a.post);
     }
     for (int n = threadIdx.x; n < a.lv[0].N; n += blockDim.x) a.xOut[n] = X[0][n];
+}
+
+template <class T>
+__global__ void __launch_bounds__(kTailThreads) k_mg_tail(const Ctl* ctl, TailArgsT<T> a) {
+    pdlEnter();
+    if (ctl->done || ctl->ppSkip) return;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    tailBody(a, smraw);
+}
+
+// ---------------- resident V-cycle (one cooperative kernel) ----------------
+__device__ __forceinline__ unsigned long long globalTimerNs() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid-wide barrier of a cooperative grid: arrivals counted in Ctl::mgBar[0],
+// the last arrival resets the count and advances the generation mgBar[1] that
+// the others wait on. A wait gives up after one second of the GPU's global
+// timer (sets Ctl::mgErr, and every later wait of the grid returns at once),
+// so a grid whose CTAs do not all arrive ends with an error instead of
+// hanging. Ctl::mgPhantom extra arrivals are expected (0; a test sets 1 to
+// make the wait run out).
+__device__ __forceinline__ void gridSync(Ctl* ctl) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int* gen = &ctl->mgBar[1];
+        volatile int* err = &ctl->mgErr;
+        const unsigned int g = *gen;
+        __threadfence();
+        if (atomicAdd(&ctl->mgBar[0], 1u) == gridDim.x - 1 + (unsigned int)ctl->mgPhantom) {
+            atomicExch(&ctl->mgBar[0], 0u);
+            __threadfence();
+            atomicAdd(&ctl->mgBar[1], 1u);
+        } else {
+            const unsigned long long t0 = globalTimerNs();
+            while (*gen == g && !*err) {
+                if (globalTimerNs() - t0 > 1000000000ull) {
+                    atomicExch(&ctl->mgErr, 1);
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+template <class T>
+__global__ void __launch_bounds__(kTailThreads, 1) k_mg_resident(Ctl* ctl, const __grid_constant__ ResidentArgsT<T> a) {
+    // launched after its predecessor completes, and never lets its successor
+    // start early: every CTA of this grid holds an SM until the last barrier
+    if (ctl->done || ctl->ppSkip || ctl->mgErr) return;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    for (int i = 0; i < a.nOps; i++) {
+        const MgOp& op = a.ops[i];
+        const LevelT<T>& L = a.lv[op.level - a.first];
+        switch (op.type) {
+            case kOpSmooth: {
+                const T* x = static_cast<const T*>(op.p0);
+                T* y = static_cast<T*>(op.p1);
+                for (int n = tid; n < L.N; n += stride) y[n] = frozen(L, n) ? x[n] : jacobiRow(L, n, x, a.w, L.b[n]);
+                break;
+            }
+            case kOpSmoothBlock:
+                if (blockIdx.x == 0) smoothBlockBody(L, static_cast<T*>(op.p0), a.w, op.ival, smraw);
+                break;
+            case kOpResidual: {
+                const T* x = static_cast<const T*>(op.p0);
+                for (int n = tid; n < L.N; n += stride) L.res[n] = residualRow(L, n, x, L.b[n]);
+                break;
+            }
+            case kOpGather: {
+                const T* resFine = a.lv[op.level - 1 - a.first].res;
+                for (int c = tid; c < L.N; c += stride)
+                    gatherCell(c, resFine, L, static_cast<T*>(op.p0), static_cast<T*>(op.p1), op.ival, a.w);
+                break;
+            }
+            case kOpTerminal:
+                for (int r = blockIdx.x; r < L.nTerm; r += gridDim.x)
+                    terminalBody(L, static_cast<T*>(op.p0), a.w, op.ival, r, smraw);
+                break;
+            case kOpProlong: {
+                T* x = static_cast<T*>(op.p0);
+                const T* xc = static_cast<const T*>(op.p1);
+                const T sc = (T)op.scale;
+                for (int n = tid; n < L.N; n += stride) {
+                    const int c = L.c2c[n];
+                    if (c >= 0) x[n] += sc * xc[c];
+                }
+                break;
+            }
+            case kOpTail:
+                if (blockIdx.x == 0) tailBody(a.tail, smraw);
+                break;
+            default:
+                break;
+        }
+        if (i + 1 < a.nOps) gridSync(ctl);
+    }
 }
 
 }  // namespace
@@ -570,6 +704,39 @@ void launchMGTerminal(const Ctl* ctl, const LevelT<T>& L, T* x, T w, int sweeps,
 }
 
 template <class T>
+bool launchMGResident(Ctl* ctl, const ResidentArgsT<T>& a, cudaStream_t s) {
+    if (a.nOps <= 0 || a.smem > 200 * 1024) return false;
+    static int grid = -1;
+    if (grid < 0) {
+        grid = 0;
+        int dev = 0, sms = 0, coop = 0, perSM = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && coop &&
+            cudaFuncSetAttribute(k_mg_resident<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) ==
+                cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_mg_resident<T>, kTailThreads, 200 * 1024) ==
+                cudaSuccess &&
+            perSM >= 1)
+            grid = sms;  // one CTA per SM: every CTA resident at once
+        cudaGetLastError();
+    }
+    if (grid <= 0) return false;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kTailThreads);
+    cfg.dynamicSmemBytes = a.smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    tNextLaunchPlain = false;
+    return cudaLaunchKernelEx(&cfg, k_mg_resident<T>, ctl, a) == cudaSuccess;
+}
+
+template <class T>
 size_t tailSharedBytes(const TailArgsT<T>& a) {
     size_t d = 0;
     for (int i = 0; i < a.count; i++) d += 4 * (size_t)a.lv[i].N;
@@ -599,6 +766,7 @@ template void launchGalerkin<float, float>(const Ctl*, const LevelT<float>&, con
     template void launchMGProlong<T>(const Ctl*, const LevelT<T>&, T*, const T*, T, cudaStream_t);                 \
     template bool launchMGProlongSmooth<T>(const Ctl*, const LevelT<T>&, const T*, const T*, T*, T, T, cudaStream_t); \
     template void launchMGTerminal<T>(const Ctl*, const LevelT<T>&, T*, T, int, cudaStream_t);                  \
+    template bool launchMGResident<T>(Ctl*, const ResidentArgsT<T>&, cudaStream_t);                              \
     template size_t tailSharedBytes<T>(const TailArgsT<T>&);                                                   \
     template void launchMGTail<T>(const Ctl*, const TailArgsT<T>&, cudaStream_t);
 AXISIM_MG_INSTANTIATE(double)

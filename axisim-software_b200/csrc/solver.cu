@@ -20,6 +20,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/axisim_b200.h"
@@ -47,16 +48,29 @@ struct StatusError : std::runtime_error {
 
 }  // namespace
 
-// Every device allocation of a solver; freed together.
+// Every device allocation of a solver; freed together. Buffers are carved,
+// 256-byte aligned and zero-filled, out of a few large chunks (one cudaMalloc
+// and one memset per chunk instead of per buffer: set-up makes about a hundred
+// buffers per mesh).
 class Arena {
 public:
     ~Arena() { release(); }
     template <class T>
     T* alloc(size_t n) {
-        void* p = nullptr;
-        CK(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
-        ptrs_.push_back(p);
-        CK(cudaMemset(p, 0, std::max<size_t>(n, 1) * sizeof(T)));
+        const size_t bytes = (std::max<size_t>(n, 1) * sizeof(T) + 255) & ~size_t(255);
+        if (chunks_.empty() || used_ + bytes > cap_) {
+            // chunks grow from 1 MiB to 64 MiB, so a small arena stays small
+            const size_t cap = std::max(bytes, next_);
+            next_ = std::min(next_ * 2, kChunkMax);
+            void* p = nullptr;
+            CK(cudaMalloc(&p, cap));
+            chunks_.push_back(p);
+            CK(cudaMemset(p, 0, cap));
+            cap_ = cap;
+            used_ = 0;
+        }
+        void* p = static_cast<char*>(chunks_.back()) + used_;
+        used_ += bytes;
         return static_cast<T*>(p);
     }
     template <class T>
@@ -66,12 +80,16 @@ public:
         return d;
     }
     void release() {
-        for (void* p : ptrs_) cudaFree(p);
-        ptrs_.clear();
+        for (void* p : chunks_) cudaFree(p);
+        chunks_.clear();
+        cap_ = used_ = 0;
+        next_ = kChunkMin;
     }
 
 private:
-    std::vector<void*> ptrs_;
+    static constexpr size_t kChunkMin = size_t(1) << 20, kChunkMax = size_t(64) << 20;
+    std::vector<void*> chunks_;
+    size_t cap_ = 0, used_ = 0, next_ = kChunkMin;
 };
 
 struct HostBC {
@@ -649,6 +667,7 @@ public:
         };
         if (running_) return why("Solver is already running.");
         if (!isReady_) return why("Run the solver once before continuing.");
+        if (timedOut_) return why("The last run ended when a multigrid barrier gave up waiting.");
         if (!haveMesh_) return why("Generate a valid mesh first.");
         // solver.cpp:485-493
         if (solveS_[0] != ranS_[0]) return why("Energy field selection changed.");
@@ -1239,16 +1258,58 @@ private:
         const T w = (T)cmg_.weight;
         const char* tag = sizeof(T) == 8 ? "" : "32";
         if (sweeps > 1 && L.N <= 4096) {
-            launchMGSmoothBlock<T>(ctl_, L, cur[(size_t)l], w, sweeps, stream_);
-            markL(std::string("mg_smooth_block") + tag, l, (double)L.N * ((4.0 + 2 * sizeof(T)) * L.W + 4.0 * sizeof(T)));
+            T* x = cur[(size_t)l];
+            emit<T>(kOpSmoothBlock, l, x, nullptr, sweeps, 0.0, 2 * (size_t)L.N * sizeof(T),
+                    std::string("mg_smooth_block") + tag,
+                    (double)L.N * ((4.0 + 2 * sizeof(T)) * L.W + 4.0 * sizeof(T)),
+                    [&] { launchMGSmoothBlock<T>(ctl_, L, x, w, sweeps, stream_); });
             return;
         }
         for (int i = 0; i < sweeps; i++) {
-            launchMGSmooth<T>(ctl_, L, cur[(size_t)l], alt[(size_t)l], w, stream_);
-            markL(std::string(l == 0 ? "mg_smooth_l0" : "mg_smooth") + tag, l,
-                 (double)L.N * ((4.0 + sizeof(T)) * L.W + 4.0 * sizeof(T)));
+            T* x = cur[(size_t)l];
+            T* y = alt[(size_t)l];
+            emit<T>(kOpSmooth, l, x, y, 0, 0.0, 0, std::string(l == 0 ? "mg_smooth_l0" : "mg_smooth") + tag,
+                    (double)L.N * ((4.0 + sizeof(T)) * L.W + 4.0 * sizeof(T)),
+                    [&] { launchMGSmooth<T>(ctl_, L, x, y, w, stream_); });
             std::swap(cur[(size_t)l], alt[(size_t)l]);
         }
+    }
+
+    // The V-cycle below the finest level as one resident kernel: while a
+    // program is being recorded, emit() appends the phase instead of
+    // launching it (the launch and its profile mark happen otherwise).
+    ResidentArgsT<double>* rec64_ = nullptr;
+    ResidentArgsT<float>* rec32_ = nullptr;
+    double recBytes_ = 0.0;
+    int residentVcycle_ = 1;
+    int barrierPhantom_ = 0;  // test hook: extra arrivals each grid barrier expects
+    bool timedOut_ = false;   // the last run ended on a barrier that gave up
+    template <class T>
+    ResidentArgsT<T>*& recSlot() {
+        if constexpr (std::is_same_v<T, double>) return rec64_;
+        else return rec32_;
+    }
+    template <class T, class Launch>
+    void emit(int type, int level, void* p0, void* p1, int ival, double scale, size_t smem, const std::string& name,
+              double bytes, Launch&& launch) {
+        ResidentArgsT<T>* r = recSlot<T>();
+        if (!r) {
+            launch();
+            markL(name, level, bytes);
+            return;
+        }
+        if (r->nOps < kMaxResidentOps) {
+            MgOp& o = r->ops[r->nOps];
+            o.type = type;
+            o.level = level;
+            o.ival = ival;
+            o.p0 = p0;
+            o.p1 = p1;
+            o.scale = scale;
+        }
+        r->nOps++;  // a count past the capacity drops the program (per-phase launches instead)
+        r->smem = std::max(r->smem, smem);
+        recBytes_ += bytes;
     }
 
     // One V-cycle from level l (multigrid.cu:607-662). firstDone: the gather
@@ -1269,8 +1330,11 @@ private:
         smoothT<T>(lv, l, cmg_.linearPreSweep - (firstDone ? 1 : 0), cur, alt);
         LevelT<T>& F = lv[(size_t)l];
         LevelT<T>& C = lv[(size_t)l + 1];
-        launchMGResidual<T>(ctl_, F, cur[(size_t)l], stream_);
-        markL(std::string("mg_residual") + tag, l, (double)F.N * ((4.0 + vb) * F.W + 4.0 * vb));
+        {
+            T* x = cur[(size_t)l];
+            emit<T>(kOpResidual, l, x, nullptr, 0, 0.0, 0, std::string("mg_residual") + tag,
+                    (double)F.N * ((4.0 + vb) * F.W + 4.0 * vb), [&] { launchMGResidual<T>(ctl_, F, x, stream_); });
+        }
         if (l + 1 == tailStart_) {
             TailArgsT<T> a;
             a.first = l + 1;
@@ -1288,35 +1352,78 @@ private:
             a.post = cmg_.linearPostSweep;
             a.coarseSweeps = cmg_.linearSweep;
             a.prolongScale = (T)curProlong_;
-            launchMGTail<T>(ctl_, a, stream_);
             double tb = 0.0;
             for (int i = 0; i < a.count; i++) tb += (double)a.lv[i].N * ((4.0 + vb) * a.lv[i].W + 4.0 * vb);
-            markL(std::string("mg_tail") + tag, l + 1, tb);
+            if (ResidentArgsT<T>* r = recSlot<T>()) r->tail = a;
+            emit<T>(kOpTail, l + 1, nullptr, nullptr, 0, 0.0, tailSharedBytes<T>(a), std::string("mg_tail") + tag, tb,
+                    [&] { launchMGTail<T>(ctl_, a, stream_); });
         } else {
             const bool coarseIsCoarsest = hier_[(size_t)l + 1].isCoarsest();
             const int sweepsBelow = coarseIsCoarsest ? cmg_.linearSweep : cmg_.linearPreSweep;
             const bool fuse = sweepsBelow >= 1;
-            launchMGGather<T>(ctl_, F, C, cur[(size_t)l + 1], alt[(size_t)l + 1], fuse ? 1 : 0, w, stream_);
-            markL(std::string("mg_gather") + tag, l + 1, (4.0 + vb) * F.N + 4.0 * vb * C.N);
+            {
+                T* xc = cur[(size_t)l + 1];
+                T* xa = alt[(size_t)l + 1];
+                emit<T>(kOpGather, l + 1, xc, xa, fuse ? 1 : 0, 0.0, 0, std::string("mg_gather") + tag,
+                        (4.0 + vb) * F.N + 4.0 * vb * C.N,
+                        [&] { launchMGGather<T>(ctl_, F, C, xc, xa, fuse ? 1 : 0, w, stream_); });
+            }
             if (fuse) std::swap(cur[(size_t)l + 1], alt[(size_t)l + 1]);
             if (C.nTerm > 0) {  // the cases whose coarsest level this is: their coarsest-level sweeps
-                launchMGTerminal<T>(ctl_, C, cur[(size_t)l + 1], w, cmg_.linearSweep, stream_);
-                markL(std::string("mg_terminal") + tag, l + 1, (double)C.N * ((4.0 + vb) * C.W + 3.0 * vb));
+                T* x = cur[(size_t)l + 1];
+                const int sw = cmg_.linearSweep;
+                emit<T>(kOpTerminal, l + 1, x, nullptr, sw, 0.0, 2 * (size_t)C.termMax * sizeof(T),
+                        std::string("mg_terminal") + tag, (double)C.N * ((4.0 + vb) * C.W + 3.0 * vb),
+                        [&] { launchMGTerminal<T>(ctl_, C, x, w, sw, stream_); });
             }
-            vcycleT<T>(lv, l + 1, cur, alt, fuse);
+            if (l == 0 && residentVcycle_ && !recSlot<T>() && L - 1 <= kMaxResidentLevels) {
+                // every level below the finest in one resident kernel; if the
+                // program does not fit or the device cannot hold the grid, the
+                // same phases are launched one by one
+                std::unique_ptr<ResidentArgsT<T>> prog(new ResidentArgsT<T>());
+                prog->first = 1;
+                prog->nLevels = L - 1;
+                prog->w = w;
+                for (int i = 1; i < L; i++) prog->lv[i - 1] = lv[(size_t)i];
+                const std::vector<T*> cur0 = cur, alt0 = alt;
+                recBytes_ = 0.0;
+                recSlot<T>() = prog.get();
+                try {
+                    vcycleT<T>(lv, l + 1, cur, alt, fuse);
+                } catch (...) {
+                    recSlot<T>() = nullptr;
+                    throw;
+                }
+                recSlot<T>() = nullptr;
+                if (prog->nOps <= kMaxResidentOps && launchMGResident<T>(ctl_, *prog, stream_)) {
+                    markL(std::string("mg_resident") + tag, 1, recBytes_);
+                } else {
+                    cur = cur0;
+                    alt = alt0;
+                    vcycleT<T>(lv, l + 1, cur, alt, fuse);
+                }
+            } else {
+                vcycleT<T>(lv, l + 1, cur, alt, fuse);
+            }
         }
         const int post = cmg_.linearPostSweep;
         const bool blockSmoother = post > 1 && F.N <= 4096;
-        if (post >= 1 && !blockSmoother &&
-            launchMGProlongSmooth<T>(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], alt[(size_t)l], w,
-                                     (T)curProlong_, stream_)) {
+        // the fused prolongation + first sweep exists for [W][N] levels with
+        // W = 3 or 4 (the finest level), which are never recorded
+        const bool fusedPost = post >= 1 && !blockSmoother && !F.sliceOff && F.c2c && (F.W == 3 || F.W == 4) &&
+                               !recSlot<T>();
+        if (fusedPost && launchMGProlongSmooth<T>(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], alt[(size_t)l], w,
+                                                  (T)curProlong_, stream_)) {
             markL(std::string("mg_prolong_smooth") + tag, l,
                  (double)F.N * ((4.0 + vb) * F.W + 4.0 + 4.0 * vb) + vb * C.N);
             std::swap(cur[(size_t)l], alt[(size_t)l]);
             smoothT<T>(lv, l, post - 1, cur, alt);
         } else {
-            launchMGProlong<T>(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], (T)curProlong_, stream_);
-            markL(std::string("mg_prolong") + tag, l, (4.0 + 2 * vb) * F.N + vb * C.N);
+            T* x = cur[(size_t)l];
+            T* xc = cur[(size_t)l + 1];
+            const T sc = (T)curProlong_;
+            emit<T>(kOpProlong, l, x, xc, 0, (double)sc, 0, std::string("mg_prolong") + tag,
+                    (4.0 + 2 * vb) * F.N + vb * C.N, [&] { launchMGProlong<T>(ctl_, F, x, xc, sc, stream_); });
             smoothT<T>(lv, l, post, cur, alt);
         }
     }
@@ -1895,6 +2002,13 @@ private:
     }
 
 public:
+    void testBarrierTimeout(int on) { barrierPhantom_ = on ? 1 : 0; }
+    void setVcycleKernel(int mode) {
+        if (mode != AXISIM_VCYCLE_PER_PHASE && mode != AXISIM_VCYCLE_RESIDENT)
+            throw StatusError(AXISIM_E_ARG, "V-cycle kernel mode must be 0 (one launch per phase) or 1 (resident)");
+        residentVcycle_ = mode;
+        destroyGraph();
+    }
     void setAutotune(int on) {
         autotune_ = on ? 1 : 0;
         destroyGraph();
@@ -2018,6 +2132,7 @@ int Solver::solve(int continueRun, axisim_result* res) {
     if (solveS_[1] && !(std::isfinite(fluid_.D) && fluid_.D >= 0.0))
         throw StatusError(AXISIM_E_CONFIG, "Concentration equation needs a mass diffusivity >= 0.");
     bool cont = continueRun != 0;
+    timedOut_ = false;
     if (cont) {
         std::string why;
         if (!canContinue(&why)) {
@@ -2063,6 +2178,7 @@ int Solver::solve(int continueRun, axisim_result* res) {
     h.checkConv = csim_.checkConv;
     h.transient = transient ? 1 : 0;
     h.itersThisCall = 0;
+    h.mgPhantom = barrierPhantom_;
     for (int i = 0; i < 3; i++) {
         h.tol[i] = cres_[i].tol;
         h.resNorm[i] = cres_[i].normType;
@@ -2158,6 +2274,11 @@ int Solver::solve(int continueRun, axisim_result* res) {
             status = AXISIM_E_DIVERGED;
             break;
         }
+        if (h.done == 5) {
+            status = AXISIM_E_TIMEOUT;
+            timedOut_ = true;
+            break;
+        }
     }
     CK(cudaEventRecord(ev1_, stream_));
     ph.reset(new PhaseTimer(*this, "solve_final_gradients"));
@@ -2195,6 +2316,7 @@ int Solver::solve(int continueRun, axisim_result* res) {
         res->solveMs = ms;
     }
     if (status == AXISIM_E_STOPPED) lastError = "Solver stopped by user";
+    if (status == AXISIM_E_TIMEOUT) lastError = "a grid-wide barrier of the resident multigrid kernel gave up waiting";
     if (status == AXISIM_E_DIVERGED) lastError = "non-finite residual: the solve diverged";
     return status;
 }
@@ -2446,6 +2568,24 @@ int axisim_set_precision(axisim_handle* h, int32_t mode) {
 int axisim_set_pressure_solver(axisim_handle* h, int32_t mode, double relTol, double prolongScale) {
     return guarded(h, [&] {
         h->s->setPressureSolver(mode, relTol, prolongScale);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_set_vcycle_kernel(axisim_handle* h, int32_t mode) {
+    if (!h) return AXISIM_E_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    return guarded(h, [&] {
+        h->s->setVcycleKernel(mode);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_test_barrier_timeout(axisim_handle* h, int32_t on) {
+    if (!h) return AXISIM_E_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    return guarded(h, [&] {
+        h->s->testBarrierTimeout(on);
         return AXISIM_OK;
     });
 }

@@ -244,6 +244,22 @@ int axisim_set_pressure_solver(axisim_handle* h, int32_t mode, double relTol, do
 /* New: Krylov p' solves started and iterations completed since the handle's
  * mesh was set. */
 int axisim_pressure_stats(axisim_handle* h, int64_t* solves, int64_t* iterations);
+/* New (the reference launches every multigrid phase as its own kernel or
+ * graph node, multigrid.cu:607-662): how the V-cycle below the finest level
+ * runs. AXISIM_VCYCLE_RESIDENT (the default): one cooperative kernel, one CTA
+ * per SM, runs every phase of the coarser levels in order with a grid-wide
+ * barrier between phases (the same per-cell arithmetic, so the same results
+ * bit for bit); a barrier that waits longer than a second ends the solve with
+ * AXISIM_E_TIMEOUT. AXISIM_VCYCLE_PER_PHASE: one launch per phase. */
+#define AXISIM_VCYCLE_PER_PHASE 0
+#define AXISIM_VCYCLE_RESIDENT 1
+int axisim_set_vcycle_kernel(axisim_handle* h, int32_t mode);
+/* Test hook for the failure path above: on = 1 makes every grid-wide barrier
+ * of the resident V-cycle expect one arrival that never comes, so its waits
+ * run out (after one second), the solve returns AXISIM_E_TIMEOUT and the
+ * handle stays usable (no continue; the next solve starts fresh). on = 0
+ * restores normal barriers. */
+int axisim_test_barrier_timeout(axisim_handle* h, int32_t on);
 /* New (no reference counterpart; the reference launches every multigrid kernel
  * with fixed shapes): enable = 1 tunes, before the next solve captures its
  * graph, the threads per CTA (64, 128 or 256) of the smoothing, residual,
