@@ -29,6 +29,7 @@
 #include <string>
 
 #include <cuda_bf16.h>
+#include <type_traits>
 
 #include "host_prep.hpp"
 #include "learned.hpp"
@@ -47,6 +48,22 @@ inline int blocksFor(size_t n, int t = kThreads) { return (int)((n + t - 1) / t)
     } while (0)
 
 using bfloat = __nv_bfloat16;
+
+// FP32 -> TF32 (round to nearest, ties away), as the tensor cores read it
+__device__ __forceinline__ uint32_t toTf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+// d += a b for one m16n8k8 block (A row-major 16 x 8, B column-major 8 x 8, FP32 accumulators)
+__device__ __forceinline__ void mmaTf32(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
 
 __device__ __forceinline__ float ldv(const float* p, size_t i) { return p[i]; }
 __device__ __forceinline__ float ldv(const bfloat* p, size_t i) { return __bfloat162float(p[i]); }
@@ -293,14 +310,28 @@ __global__ void __launch_bounds__(256) k_layer_tile(const Ctl* ctl, int gated, N
         for (int r = threadIdx.x / K; r < TR; r += rstep)
             if (row0 + r < L.N) stv(Z, (size_t)(row0 + r) * K + k, zs[r * ldz + k]);
     }
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 x 16 threads
+    // Tensor cores: the TR x COUT tile is (TR/16) x (COUT/8) mma.sync
+    // m16n8k8 TF32 blocks with FP32 accumulators, dealt round-robin to the 8
+    // warps. The FP32 activations are split into a TF32 high part and the
+    // TF32 rounding of the remainder, and both are multiplied: close to FP32
+    // accuracy. BF16 weights are exact in TF32; FP32 weights (the gradient
+    // check's mode) are split the same way, adding a third product.
+    constexpr int NRB = RPT, NCB = 2 * CPT;
+    constexpr int TPW = (NRB * NCB + 7) / 8;  // blocks per warp
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t4 = lane & 3;
     const TW* W = P + L.wOff;
-    float acc[RPT][CPT];
+    float acc[TPW][4];
 #pragma unroll
-    for (int j = 0; j < CPT; j++) {
-        const float bj = ldv(W + (size_t)K * COUT, tx + 16 * j);
-#pragma unroll
-        for (int i = 0; i < RPT; i++) acc[i][j] = bj;
+    for (int q = 0; q < TPW; q++) {
+        const int blk = warp + 8 * q;
+        const int cb = blk % NCB;
+        const float b0 = blk < NRB * NCB ? ldv(W + (size_t)K * COUT, cb * 8 + 2 * t4) : 0.f;
+        const float b1 = blk < NRB * NCB ? ldv(W + (size_t)K * COUT, cb * 8 + 2 * t4 + 1) : 0.f;
+        acc[q][0] = b0;
+        acc[q][1] = b1;
+        acc[q][2] = b0;
+        acc[q][3] = b1;
     }
     for (int k0 = 0; k0 < K; k0 += kChunk) {
         const int kn = min(kChunk, K - k0);
@@ -317,28 +348,51 @@ __global__ void __launch_bounds__(256) k_layer_tile(const Ctl* ctl, int gated, N
 #pragma unroll
         for (int u = 0; u < PER; u++) ws[threadIdx.x + 256 * u] = wv[u];
         __syncthreads();
-        for (int kk = 0; kk < kn; kk++) {
-            float z[RPT];
+        for (int kk = 0; kk < kn; kk += 8) {
+            // columns past the chunk (K below 8) read as zero, never the next row
+            const bool c0ok = kk + t4 < kn, c1ok = kk + t4 + 4 < kn;
 #pragma unroll
-            for (int i = 0; i < RPT; i++) z[i] = zs[(ty * RPT + i) * ldz + k0 + kk];
+            for (int q = 0; q < TPW; q++) {
+                const int blk = warp + 8 * q;
+                if (blk >= NRB * NCB) break;
+                const int rb = blk / NCB, cb = blk % NCB;
+                const float* zr0 = zs + (rb * 16 + g) * ldz + k0 + kk;
+                const float* zr1 = zr0 + 8 * ldz;
+                const float a[4] = {c0ok ? zr0[t4] : 0.f, c0ok ? zr1[t4] : 0.f, c1ok ? zr0[t4 + 4] : 0.f,
+                                    c1ok ? zr1[t4 + 4] : 0.f};
+                const float bw[2] = {ws[(kk + t4) * COUT + cb * 8 + g], ws[(kk + t4 + 4) * COUT + cb * 8 + g]};
+                uint32_t ahi[4], alo[4], bhi[2];
 #pragma unroll
-            for (int j = 0; j < CPT; j++) {
-                const float w = ws[kk * COUT + tx + 16 * j];
+                for (int e = 0; e < 4; e++) {
+                    ahi[e] = toTf32(a[e]);
+                    alo[e] = toTf32(a[e] - __uint_as_float(ahi[e]));
+                }
 #pragma unroll
-                for (int i = 0; i < RPT; i++) acc[i][j] = fmaf(z[i], w, acc[i][j]);
+                for (int e = 0; e < 2; e++) bhi[e] = toTf32(bw[e]);
+                if constexpr (std::is_same<TW, float>::value) {
+                    uint32_t blo[2];
+#pragma unroll
+                    for (int e = 0; e < 2; e++) blo[e] = toTf32(bw[e] - __uint_as_float(bhi[e]));
+                    mmaTf32(acc[q], ahi, blo);
+                }
+                mmaTf32(acc[q], alo, bhi);
+                mmaTf32(acc[q], ahi, bhi);
             }
         }
     }
     const TA* add = (const TA*)L.add;
     TA* Y = (TA*)L.Y;
 #pragma unroll
-    for (int i = 0; i < RPT; i++) {
-        const int n = row0 + ty * RPT + i;
-        if (n >= L.N) continue;
+    for (int q = 0; q < TPW; q++) {
+        const int blk = warp + 8 * q;
+        if (blk >= NRB * NCB) break;
+        const int rb = blk / NCB, cb = blk % NCB;
 #pragma unroll
-        for (int j = 0; j < CPT; j++) {
-            const int o = tx + 16 * j;
-            float v = acc[i][j];
+        for (int e = 0; e < 4; e++) {
+            const int n = row0 + rb * 16 + g + (e >= 2 ? 8 : 0);
+            const int o = cb * 8 + 2 * t4 + (e & 1);
+            if (n >= L.N) continue;
+            float v = acc[q][e];
             if (add) v += ldv(add, (size_t)n * COUT + o);
             if (L.relu) v = fmaxf(v, 0.f);
             stv(Y, (size_t)n * COUT + o, v);
@@ -372,13 +426,17 @@ __global__ void __launch_bounds__(256) k_layer_dz_tile(NetLayer L, const TW* __r
         gs[r * ldg + o] = v;
     }
     if (!dZ) return;
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    // tensor cores: the 64 x KD tile of dZ is 4 x (KD/8) mma.sync m16n8k8
+    // TF32 blocks dealt to the 8 warps; G split into TF32 high and low parts,
+    // W exact (BF16) or split (FP32)
+    constexpr int NCB = 2 * KPT, NBLK = 4 * NCB, TPW = (NBLK + 7) / 8;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
     const TW* W = P + L.wOff;
-    float acc[4][KPT];
+    float acc[TPW][4];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+    for (int q = 0; q < TPW; q++)
 #pragma unroll
-        for (int j = 0; j < KPT; j++) acc[i][j] = 0.f;
+        for (int e = 0; e < 4; e++) acc[q][e] = 0.f;
     for (int o0 = 0; o0 < Cout; o0 += kChunk) {
         const int on = min(kChunk, Cout - o0);
         constexpr int PER = kChunk * KD / 256;
@@ -393,24 +451,47 @@ __global__ void __launch_bounds__(256) k_layer_dz_tile(NetLayer L, const TW* __r
 #pragma unroll
         for (int u = 0; u < PER; u++) wt[threadIdx.x + 256 * u] = wv[u];
         __syncthreads();
-        for (int oo = 0; oo < on; oo++) {
-            float g[4];
+        for (int oo = 0; oo < on; oo += 8) {
+            const bool c0ok = oo + t4 < on, c1ok = oo + t4 + 4 < on;
 #pragma unroll
-            for (int i = 0; i < 4; i++) g[i] = gs[(ty * 4 + i) * ldg + o0 + oo];
+            for (int q = 0; q < TPW; q++) {
+                const int blk = warp + 8 * q;
+                if (blk >= NBLK) break;
+                const int rb = blk / NCB, cb = blk % NCB;
+                const float* g0 = gs + (rb * 16 + g) * ldg + o0 + oo;
+                const float* g1 = g0 + 8 * ldg;
+                const float a[4] = {c0ok ? g0[t4] : 0.f, c0ok ? g1[t4] : 0.f, c1ok ? g0[t4 + 4] : 0.f,
+                                    c1ok ? g1[t4 + 4] : 0.f};
+                const float bw[2] = {wt[(oo + t4) * KD + cb * 8 + g], wt[(oo + t4 + 4) * KD + cb * 8 + g]};
+                uint32_t ahi[4], alo[4], bhi[2];
 #pragma unroll
-            for (int j = 0; j < KPT; j++) {
-                const float w = wt[oo * KD + tx + 16 * j];
+                for (int e = 0; e < 4; e++) {
+                    ahi[e] = toTf32(a[e]);
+                    alo[e] = toTf32(a[e] - __uint_as_float(ahi[e]));
+                }
 #pragma unroll
-                for (int i = 0; i < 4; i++) acc[i][j] = fmaf(g[i], w, acc[i][j]);
+                for (int e = 0; e < 2; e++) bhi[e] = toTf32(bw[e]);
+                if constexpr (std::is_same<TW, float>::value) {
+                    uint32_t blo[2];
+#pragma unroll
+                    for (int e = 0; e < 2; e++) blo[e] = toTf32(bw[e] - __uint_as_float(bhi[e]));
+                    mmaTf32(acc[q], ahi, blo);
+                }
+                mmaTf32(acc[q], alo, bhi);
+                mmaTf32(acc[q], ahi, bhi);
             }
         }
     }
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int n = row0 + ty * 4 + i;
-        if (n >= L.N) continue;
+    for (int q = 0; q < TPW; q++) {
+        const int blk = warp + 8 * q;
+        if (blk >= NBLK) break;
+        const int rb = blk / NCB, cb = blk % NCB;
 #pragma unroll
-        for (int j = 0; j < KPT; j++) dZ[(size_t)n * KD + tx + 16 * j] = acc[i][j];
+        for (int e = 0; e < 4; e++) {
+            const int n = row0 + rb * 16 + g + (e >= 2 ? 8 : 0);
+            if (n < L.N) dZ[(size_t)n * KD + cb * 8 + 2 * t4 + (e & 1)] = acc[q][e];
+        }
     }
 }
 
@@ -508,10 +589,14 @@ __global__ void __launch_bounds__(kThreads) k_wgrad(int N, int K, int Cout, int 
     __shared__ float gs[64][33];
     const int tk = blockIdx.x / tilesO, to = blockIdx.x % tilesO;
     const int k0 = tk * 32, o0 = to * 32;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int split = blockIdx.y;
     const int r0 = split * rowsPerSplit;
     const int r1 = min(N, r0 + rowsPerSplit);
+    // tensor cores: the 32 x 32 tile of dW = Z^T G is 2 x 4 mma.sync m16n8k8
+    // TF32 blocks, one per warp, reduced over the rows 8 at a time; FP32
+    // operands split into TF32 high and low parts (BF16 activations are exact)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
+    const int mb = warp >> 2, nb = warp & 3;
     float acc[4] = {0.f, 0.f, 0.f, 0.f};
     float bacc = 0.f;
     for (int rc = r0; rc < r1; rc += 64) {
@@ -522,25 +607,41 @@ __global__ void __launch_bounds__(kThreads) k_wgrad(int N, int K, int Cout, int 
             gs[rr][cc] = (n < r1 && o0 + cc < Cout) ? G[(size_t)n * Cout + o0 + cc] : 0.f;
         }
         __syncthreads();
-        for (int rr = 0; rr < 64; rr++) {
-            const float g = gs[rr][tx];
+#pragma unroll 2
+        for (int kk = 0; kk < 64; kk += 8) {
+            const float a[4] = {zs[kk + t4][mb * 16 + g], zs[kk + t4][mb * 16 + g + 8], zs[kk + t4 + 4][mb * 16 + g],
+                                zs[kk + t4 + 4][mb * 16 + g + 8]};
+            const float b[2] = {gs[kk + t4][nb * 8 + g], gs[kk + t4 + 4][nb * 8 + g]};
+            uint32_t ahi[4], bhi[2], blo[2];
 #pragma unroll
-            for (int j = 0; j < 4; j++) acc[j] = fmaf(zs[rr][ty * 4 + j], g, acc[j]);
-            bacc += g;
+            for (int e = 0; e < 4; e++) ahi[e] = toTf32(a[e]);
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                bhi[e] = toTf32(b[e]);
+                blo[e] = toTf32(b[e] - __uint_as_float(bhi[e]));
+            }
+            if constexpr (std::is_same<TA, float>::value) {
+                uint32_t alo[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) alo[e] = toTf32(a[e] - __uint_as_float(ahi[e]));
+                mmaTf32(acc, alo, bhi);
+            }
+            mmaTf32(acc, ahi, blo);
+            mmaTf32(acc, ahi, bhi);
         }
+        if (warp == 0)
+            for (int rr = 0; rr < 64; rr++) bacc += gs[rr][lane];
         __syncthreads();
     }
     const size_t stride = (size_t)K * Cout + Cout;
     float* out = partial + (size_t)split * stride;
-    const int o = o0 + tx;
-    if (o < Cout) {
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int k = k0 + ty * 4 + j;
-            if (k < K) out[(size_t)k * Cout + o] = acc[j];
-        }
-        if (tk == 0 && ty == 0) out[(size_t)K * Cout + o] = bacc;
+    for (int e = 0; e < 4; e++) {
+        const int k = k0 + mb * 16 + g + (e >= 2 ? 8 : 0);
+        const int o = o0 + nb * 8 + 2 * t4 + (e & 1);
+        if (k < K && o < Cout) out[(size_t)k * Cout + o] = acc[e];
     }
+    if (tk == 0 && warp == 0 && o0 + lane < Cout) out[(size_t)K * Cout + o0 + lane] = bacc;
 }
 
 __global__ void __launch_bounds__(kThreads) k_wgrad_reduce(int entries, int splits, const float* __restrict__ partial,
