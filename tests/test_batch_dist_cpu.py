@@ -77,3 +77,32 @@ def test_two_rank_batch_equals_single_process():
     for i in range(N_CASES):
         for f in ("u", "p"):
             np.testing.assert_array_equal(np.array(merged[i][f]), ref[i][f])
+
+
+def _worker_one_rank_fails(rank, world, port, q):
+    import datetime
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    if rank == 1:
+        os._exit(3)  # a rank that dies between steps, before the gather
+    try:
+        batch.gather_results(_solve_cases([0]), world, dist)
+        q.put("no error")
+    except Exception as e:  # the peer's loss surfaces as an error, not a hang
+        q.put("raised: " + type(e).__name__)
+    os._exit(0)
+
+
+@pytest.mark.timeout(300)
+def test_a_rank_that_dies_makes_the_gather_fail_instead_of_hanging():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker_one_rank_fails, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    msg = q.get(timeout=240)
+    for p in procs:
+        p.join(timeout=60)
+    assert msg.startswith("raised"), msg
+    assert procs[1].exitcode == 3 and procs[0].exitcode == 0
