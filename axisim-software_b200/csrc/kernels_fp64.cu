@@ -292,6 +292,12 @@ __device__ __forceinline__ void momentumBoundary(const MeshDev& m, int n, int f,
     }
 }
 
+// WC > 0: the mesh's slot count, known at compile time. Every slot's face id,
+// then every face's owner, neighbour, area, 1/d_PN and mass flux are loaded
+// before the per-face arithmetic (which keeps the reference's order), so the
+// slot -> face -> value chains of the cell's faces are in flight together
+// instead of one after another. WC = 0: any slot count, loads as needed.
+template <int WC>
 __global__ void __launch_bounds__(kThreads, 4) k_momentum(MeshDev m, const Ctl* ctl, BCDev bcU, BCDev bcV,
                                                        MomentumArgs a) {
     pdlEnter();
@@ -299,16 +305,34 @@ __global__ void __launch_bounds__(kThreads, 4) k_momentum(MeshDev m, const Ctl* 
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m.N) return;
     const int N = m.N;
+    constexpr int P = WC > 0 ? WC : 1;
+    int pf[P], po[P], pn[P];
+    double pa[P], pd[P], pm[P];
+    if (WC > 0) {
+#pragma unroll
+        for (int j = 0; j < P; j++) pf[j] = m.sface[(size_t)j * N + n];
+#pragma unroll
+        for (int j = 0; j < P; j++) {
+            const int f = pf[j] >= 0 ? pf[j] : 0;
+            po[j] = m.owner[f];
+            pn[j] = m.neighbor[f];
+            pa[j] = m.area[f];
+            pd[j] = m.invDPN[f];
+            pm[j] = a.conv ? a.mDot[f] : 0.0;
+        }
+    }
     double ACu = 0.0, ACv = 0.0, bu = 0.0, bv = 0.0, netF = 0.0;
-    for (int j = 0; j < m.W; j++) {
+#pragma unroll
+    for (int j = 0; j < (WC > 0 ? WC : 32); j++) {
+        if (WC == 0 && j >= m.W) break;
         const size_t s = (size_t)j * N + n;
-        const int f = m.sface[s];
+        const int f = WC > 0 ? pf[j] : m.sface[s];
         if (f < 0) break;
-        const int own = m.owner[f], nb = m.neighbor[f];
-        const double area = m.area[f];
+        const int own = WC > 0 ? po[j] : m.owner[f], nb = WC > 0 ? pn[j] : m.neighbor[f];
+        const double area = WC > 0 ? pa[j] : m.area[f];
         double F = 0.0;
         if (a.conv) {
-            const double Fo = a.mDot[f] * 1.0;
+            const double Fo = (WC > 0 ? pm[j] : a.mDot[f]) * 1.0;
             if (own == n) F = Fo;
             else if (nb == n) F = -Fo;
             if (fabs(F) <= 1.0e-30) F = 0.0;
@@ -316,7 +340,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_momentum(MeshDev m, const Ctl* 
         }
         if (nb >= 0) {
             const int o = (own == n) ? nb : own;
-            const double K = a.mu * area * m.invDPN[f];
+            const double K = a.mu * area * (WC > 0 ? pd[j] : m.invDPN[f]);
             ACu += K;
             ACv += K;
             double af = 0.0 - K;
@@ -1033,7 +1057,9 @@ void launchGradient(const MeshDev& m, const Ctl* ctl, int nFields, const double*
 
 void launchMomentum(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, const BCDev& bcV, const MomentumArgs& a,
                     cudaStream_t s) {
-    launchPDL(k_momentum, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcU, bcV, a);
+    if (m.W == 4) launchPDL(k_momentum<4>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcU, bcV, a);
+    else if (m.W == 3) launchPDL(k_momentum<3>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcU, bcV, a);
+    else launchPDL(k_momentum<0>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcU, bcV, a);
 }
 
 void launchJacobiUV(const MeshDev& m, const Ctl* ctl, const double* AF, const double* bu, const double* bv,
