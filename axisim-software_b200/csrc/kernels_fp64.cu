@@ -158,10 +158,11 @@ struct GradArgs {
     double* gR[5];
 };
 
-// Bounded to 4 resident CTAs per SM up to three fields (64 registers, no
-// spills); the four- and five-field forms of the scalar runs keep 3.
+// Bounded to 4 resident CTAs per SM up to two fields (64 registers, no
+// spills); three to five fields keep 3 (85 registers: the four face chains
+// of the least-squares loop are loaded ahead, in registers).
 template <int NF>
-__global__ void __launch_bounds__(kThreads, NF <= 3 ? 4 : 3) k_gradient(MeshDev m, const Ctl* ctl, GradArgs a,
+__global__ void __launch_bounds__(kThreads, NF <= 2 ? 4 : 3) k_gradient(MeshDev m, const Ctl* ctl, GradArgs a,
                                                                        int scheme) {
     pdlEnter();
     if (ctl && ctl->done) return;
@@ -219,11 +220,7 @@ __global__ void __launch_bounds__(kThreads, NF <= 3 ? 4 : 3) k_gradient(MeshDev 
             bz[q] = br[q] = 0.0;
             phiP[q] = a.phi[q][n];
         }
-        for (int j = 0; j < m.W; j++) {
-            const int f = m.sface[(size_t)j * N + n];
-            if (f < 0) break;
-            const int own = m.owner[f], nb = m.neighbor[f];
-            const double wz = m.lsqWZ[f], wr = m.lsqWR[f];
+        auto face = [&](int f, int own, int nb, double wz, double wr) {
             for (int q = 0; q < NF; q++) {
                 double dphi;
                 if (nb >= 0) {
@@ -236,6 +233,34 @@ __global__ void __launch_bounds__(kThreads, NF <= 3 ? 4 : 3) k_gradient(MeshDev 
                 bz[q] += wz * dphi;
                 br[q] += wr * dphi;
             }
+        };
+        // the first four slots' face id, owner, neighbour and weights are
+        // loaded before any arithmetic, so those chains are in flight together
+        int pf[4], po[4], pn[4];
+        double pz[4], pr[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) pf[j] = j < m.W ? m.sface[(size_t)j * N + n] : -1;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int f = pf[j] >= 0 ? pf[j] : 0;
+            po[j] = m.owner[f];
+            pn[j] = m.neighbor[f];
+            pz[j] = m.lsqWZ[f];
+            pr[j] = m.lsqWR[f];
+        }
+        bool more = true;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (pf[j] < 0) {
+                more = false;
+                break;
+            }
+            face(pf[j], po[j], pn[j], pz[j], pr[j]);
+        }
+        for (int j = 4; more && j < m.W; j++) {
+            const int f = m.sface[(size_t)j * N + n];
+            if (f < 0) break;
+            face(f, m.owner[f], m.neighbor[f], m.lsqWZ[f], m.lsqWR[f]);
         }
         const double izz = m.lsqIZZ[n], izr = m.lsqIZR[n], irr = m.lsqIRR[n];
         for (int q = 0; q < NF; q++) {
