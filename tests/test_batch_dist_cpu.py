@@ -90,19 +90,32 @@ def _worker_one_rank_fails(rank, world, port, q):
         q.put("no error")
     except Exception as e:  # the peer's loss surfaces as an error, not a hang
         q.put("raised: " + type(e).__name__)
+    q.close()
+    q.join_thread()  # the message is delivered before the process ends
     os._exit(0)
 
 
 @pytest.mark.timeout(300)
 def test_a_rank_that_dies_makes_the_gather_fail_instead_of_hanging():
+    # the surviving rank either gets an exception from the gather or is ended
+    # by the communication library on the lost connection; both end the rank
+    # (what must not happen is a gather that waits for good)
+    import queue
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
     procs = [ctx.Process(target=_worker_one_rank_fails, args=(r, 2, port, q)) for r in range(2)]
     for p in procs:
         p.start()
-    msg = q.get(timeout=240)
     for p in procs:
-        p.join(timeout=60)
-    assert msg.startswith("raised"), msg
-    assert procs[1].exitcode == 3 and procs[0].exitcode == 0
+        p.join(timeout=120)
+    assert all(p.exitcode is not None for p in procs), "a rank is still waiting"
+    assert procs[1].exitcode == 3
+    try:
+        msg = q.get(timeout=5)
+    except queue.Empty:
+        msg = None
+    if procs[0].exitcode == 0:
+        assert msg is not None and msg.startswith("raised"), msg
+    else:
+        assert msg is None or msg.startswith("raised"), msg
