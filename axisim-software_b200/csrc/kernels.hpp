@@ -71,11 +71,14 @@ enum MgOpType : int {
     kOpTerminal,        // terminal cases' coarsest sweeps (ival) p0 = x
     kOpProlong,         // x += scale * P xc                      p0 = x (fine), p1 = xc
     kOpTail,            // the one-CTA tail (ResidentArgsT::tail)
+    kOpGatherRes,       // kOpGather with the finer residual formed on the fly  p2 = fine x
+    kOpProlongSmooth,   // y = sweep(x + scale * P xc)           p0 = x, p1 = xc, p2 = y
 };
 struct MgOp {
     int type = 0, level = 0, ival = 0, pad = 0;
     void* p0 = nullptr;
     void* p1 = nullptr;
+    void* p2 = nullptr;
     double scale = 0.0;
 };
 constexpr int kMaxResidentLevels = 12;
@@ -169,6 +172,14 @@ void launchMGGather(const Ctl* ctl, const LevelT<T>& fine, const LevelT<T>& coar
                     int firstSweep, T w, cudaStream_t s);
 template <class T>
 void launchMGProlong(const Ctl* ctl, const LevelT<T>& fine, T* xFine, const T* xCoarse, T scale, cudaStream_t s);
+// the restriction with the fine residual formed per member (no residual pass)
+template <class T>
+void launchMGGatherRes(const Ctl* ctl, const LevelT<T>& fine, const T* xFine, const LevelT<T>& coarse, T* xCur,
+                       T* xAlt, int firstSweep, T w, cudaStream_t s);
+// prolongation fused into the first post-smoothing sweep, any level layout
+template <class T>
+void launchMGProlongSmoothAny(const Ctl* ctl, const LevelT<T>& fine, const T* xFine, const T* xCoarse, T* y, T w,
+                              T scale, cudaStream_t s);
 // prolongation fused into the first post-smoothing sweep (ELL levels with
 // W = 3 or 4): y = smooth(x + s P e); returns false when not applicable
 template <class T>

@@ -309,10 +309,32 @@ __global__ void __launch_bounds__(kThreads) k_mg_residual(const Ctl* ctl, LevelT
 // Restriction (multigrid.cu:398-410) as a gather; optionally the coarse
 // level's first Jacobi sweep from x = 0: x1 = 0 + w (b - A 0) / AC.
 template <class T>
+__device__ __forceinline__ void gatherFinish(int c, const LevelT<T>& C, T* xCur, T* xAlt, int firstSweep, T w, T sum);
+
+template <class T>
 __device__ __forceinline__ void gatherCell(int c, const T* __restrict__ resFine, const LevelT<T>& C, T* xCur, T* xAlt,
                                            int firstSweep, T w) {
     T sum = T(0);
     for (int q = C.mStart[c]; q < C.mStart[c + 1]; q++) sum += resFine[C.mList[q]];
+    gatherFinish(c, C, xCur, xAlt, firstSweep, w, sum);
+}
+
+// The same restriction with each member's residual formed on the fly
+// (residualRow's arithmetic, summed in ascending member order), so no
+// separate residual pass over the fine level is needed.
+template <class T>
+__device__ __forceinline__ void gatherResCell(int c, const LevelT<T>& F, const T* __restrict__ xf, const LevelT<T>& C,
+                                              T* xCur, T* xAlt, int firstSweep, T w) {
+    T sum = T(0);
+    for (int q = C.mStart[c]; q < C.mStart[c + 1]; q++) {
+        const int m = C.mList[q];
+        sum += residualRow(F, m, xf, F.b[m]);
+    }
+    gatherFinish(c, C, xCur, xAlt, firstSweep, w, sum);
+}
+
+template <class T>
+__device__ __forceinline__ void gatherFinish(int c, const LevelT<T>& C, T* xCur, T* xAlt, int firstSweep, T w, T sum) {
     C.b[c] = sum;
     if (!firstSweep) {
         xCur[c] = T(0);
@@ -320,6 +342,51 @@ __device__ __forceinline__ void gatherCell(int c, const T* __restrict__ resFine,
     }
     const T ac = C.AC[c];
     xAlt[c] = (fabs(ac) < tiny<T>()) ? T(0) : T(0) + w * (sum - ac * T(0)) / ac;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_mg_gather_res(const Ctl* ctl, LevelT<T> F, const T* __restrict__ xf,
+                                                            LevelT<T> C, T* xCur, T* xAlt, int firstSweep, T w) {
+    pdlEnter();
+    if (ctl->done || ctl->ppSkip) return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C.N) return;
+    gatherResCell(c, F, xf, C, xCur, xAlt, firstSweep, w);
+}
+
+// Prolongation fused into the first post-smoothing sweep on any level layout:
+// x' = x + s P e formed on the fly for the cell and its neighbours, then the
+// weighted-Jacobi row of jacobiRow, so the result equals the separate
+// prolongation and sweep bit for bit. A batch's terminal cell keeps its value.
+template <class T>
+__device__ __forceinline__ T prolongSmoothRow(const LevelT<T>& L, int n, const T* x, const T* xc, T w, T scale) {
+    const int cn = L.c2c[n];
+    if (cn < 0) return x[n];
+    const T xn = x[n] + scale * xc[cn];
+    const T ac = L.AC[n];
+    if (fabs(ac) < tiny<T>()) return xn;
+    T Ax = ac * xn;
+    const Slots sl = slotsOf(L, n);
+    for (int j = 0; j < sl.width; j++) {
+        const int p = sl.base + j * sl.stride;
+        const int k = L.nb[p];
+        if (k != -1) {
+            const int ck = L.c2c[k];
+            Ax += L.AF[p] * (ck >= 0 ? x[k] + scale * xc[ck] : x[k]);
+        }
+    }
+    return xn + w * (L.b[n] - Ax) / ac;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_mg_prolong_smooth(const Ctl* ctl, LevelT<T> L, const T* __restrict__ x,
+                                                                const T* __restrict__ xc, T* __restrict__ y, T w,
+                                                                T scale) {
+    pdlEnter();
+    if (ctl->done || ctl->ppSkip) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L.N) return;
+    y[n] = prolongSmoothRow(L, n, x, xc, w, scale);
 }
 
 template <class T>
@@ -614,6 +681,21 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_resident(Ctl* ctl, const
                 }
                 break;
             }
+            case kOpGatherRes: {
+                const LevelT<T>& F = a.lv[op.level - 1 - a.first];
+                for (int c = tid; c < L.N; c += stride)
+                    gatherResCell(c, F, static_cast<const T*>(op.p2), L, static_cast<T*>(op.p0),
+                                  static_cast<T*>(op.p1), op.ival, a.w);
+                break;
+            }
+            case kOpProlongSmooth: {
+                const T* x = static_cast<const T*>(op.p0);
+                const T* xc = static_cast<const T*>(op.p1);
+                T* y = static_cast<T*>(op.p2);
+                const T sc = (T)op.scale;
+                for (int n = tid; n < L.N; n += stride) y[n] = prolongSmoothRow(L, n, x, xc, a.w, sc);
+                break;
+            }
             case kOpTail:
                 if (blockIdx.x == 0) tailBody(a.tail, smraw);
                 break;
@@ -665,6 +747,22 @@ void launchMGGather(const Ctl* ctl, const LevelT<T>& fine, const LevelT<T>& coar
                     T w, cudaStream_t s) {
     const int t = tpb(coarse);
     launchPDL(k_mg_gather<T>, dim3(blocksFor(coarse.N, t)), dim3(t), 0, s, ctl, fine.res, coarse, xCur, xAlt, firstSweep, w);
+}
+
+template <class T>
+void launchMGGatherRes(const Ctl* ctl, const LevelT<T>& fine, const T* xFine, const LevelT<T>& coarse, T* xCur,
+                       T* xAlt, int firstSweep, T w, cudaStream_t s) {
+    const int t = tpb(coarse);
+    launchPDL(k_mg_gather_res<T>, dim3(blocksFor(coarse.N, t)), dim3(t), 0, s, ctl, fine, xFine, coarse, xCur, xAlt,
+              firstSweep, w);
+}
+
+template <class T>
+void launchMGProlongSmoothAny(const Ctl* ctl, const LevelT<T>& fine, const T* xFine, const T* xCoarse, T* y, T w,
+                              T scale, cudaStream_t s) {
+    const int t = tpb(fine);
+    launchPDL(k_mg_prolong_smooth<T>, dim3(blocksFor(fine.N, t)), dim3(t), 0, s, ctl, fine, xFine, xCoarse, y, w,
+              scale);
 }
 
 template <class T>
@@ -767,6 +865,10 @@ template void launchGalerkin<float, float>(const Ctl*, const LevelT<float>&, con
     template bool launchMGProlongSmooth<T>(const Ctl*, const LevelT<T>&, const T*, const T*, T*, T, T, cudaStream_t); \
     template void launchMGTerminal<T>(const Ctl*, const LevelT<T>&, T*, T, int, cudaStream_t);                  \
     template bool launchMGResident<T>(Ctl*, const ResidentArgsT<T>&, cudaStream_t);                              \
+    template void launchMGGatherRes<T>(const Ctl*, const LevelT<T>&, const T*, const LevelT<T>&, T*, T*, int, T,     \
+                                       cudaStream_t);                                                            \
+    template void launchMGProlongSmoothAny<T>(const Ctl*, const LevelT<T>&, const T*, const T*, T*, T, T,          \
+                                              cudaStream_t);                                                     \
     template size_t tailSharedBytes<T>(const TailArgsT<T>&);                                                   \
     template void launchMGTail<T>(const Ctl*, const TailArgsT<T>&, cudaStream_t);
 AXISIM_MG_INSTANTIATE(double)

@@ -1291,7 +1291,7 @@ private:
     }
     template <class T, class Launch>
     void emit(int type, int level, void* p0, void* p1, int ival, double scale, size_t smem, const std::string& name,
-              double bytes, Launch&& launch) {
+              double bytes, Launch&& launch, void* p2 = nullptr) {
         ResidentArgsT<T>* r = recSlot<T>();
         if (!r) {
             launch();
@@ -1305,6 +1305,7 @@ private:
             o.ival = ival;
             o.p0 = p0;
             o.p1 = p1;
+            o.p2 = p2;
             o.scale = scale;
         }
         r->nOps++;  // a count past the capacity drops the program (per-phase launches instead)
@@ -1330,7 +1331,11 @@ private:
         smoothT<T>(lv, l, cmg_.linearPreSweep - (firstDone ? 1 : 0), cur, alt);
         LevelT<T>& F = lv[(size_t)l];
         LevelT<T>& C = lv[(size_t)l + 1];
-        {
+        // on a coarse level the restriction forms its members' residuals itself;
+        // the finest level (coalesced [W][N] rows) and the level above the tail
+        // (whose residual the tail reads) keep the separate residual pass
+        const bool gatherRes = F.sliceOff != nullptr && l + 1 != tailStart_;
+        if (!gatherRes) {
             T* x = cur[(size_t)l];
             emit<T>(kOpResidual, l, x, nullptr, 0, 0.0, 0, std::string("mg_residual") + tag,
                     (double)F.N * ((4.0 + vb) * F.W + 4.0 * vb), [&] { launchMGResidual<T>(ctl_, F, x, stream_); });
@@ -1364,9 +1369,16 @@ private:
             {
                 T* xc = cur[(size_t)l + 1];
                 T* xa = alt[(size_t)l + 1];
-                emit<T>(kOpGather, l + 1, xc, xa, fuse ? 1 : 0, 0.0, 0, std::string("mg_gather") + tag,
-                        (4.0 + vb) * F.N + 4.0 * vb * C.N,
-                        [&] { launchMGGather<T>(ctl_, F, C, xc, xa, fuse ? 1 : 0, w, stream_); });
+                if (gatherRes) {
+                    T* xf = cur[(size_t)l];
+                    emit<T>(kOpGatherRes, l + 1, xc, xa, fuse ? 1 : 0, 0.0, 0, std::string("mg_gather_res") + tag,
+                            (double)F.N * ((4.0 + vb) * F.W + 4.0 * vb) + 4.0 * F.N + 4.0 * vb * C.N,
+                            [&] { launchMGGatherRes<T>(ctl_, F, xf, C, xc, xa, fuse ? 1 : 0, w, stream_); }, xf);
+                } else {
+                    emit<T>(kOpGather, l + 1, xc, xa, fuse ? 1 : 0, 0.0, 0, std::string("mg_gather") + tag,
+                            (4.0 + vb) * F.N + 4.0 * vb * C.N,
+                            [&] { launchMGGather<T>(ctl_, F, C, xc, xa, fuse ? 1 : 0, w, stream_); });
+                }
             }
             if (fuse) std::swap(cur[(size_t)l + 1], alt[(size_t)l + 1]);
             if (C.nTerm > 0) {  // the cases whose coarsest level this is: their coarsest-level sweeps
@@ -1408,12 +1420,24 @@ private:
         }
         const int post = cmg_.linearPostSweep;
         const bool blockSmoother = post > 1 && F.N <= 4096;
-        // the fused prolongation + first sweep exists for [W][N] levels with
-        // W = 3 or 4 (the finest level), which are never recorded
-        const bool fusedPost = post >= 1 && !blockSmoother && !F.sliceOff && F.c2c && (F.W == 3 || F.W == 4) &&
-                               !recSlot<T>();
-        if (fusedPost && launchMGProlongSmooth<T>(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], alt[(size_t)l], w,
-                                                  (T)curProlong_, stream_)) {
+        // the prolongation fused into the first post-smoothing sweep: the
+        // [W][N] kernel on the finest level (W = 3 or 4; never recorded), the
+        // layout-generic one on coarse levels
+        const bool fusedEll = post >= 1 && !blockSmoother && !F.sliceOff && F.c2c && (F.W == 3 || F.W == 4) &&
+                              !recSlot<T>();
+        const bool fusedAny = post >= 1 && !blockSmoother && F.sliceOff && F.c2c;
+        if (fusedAny) {
+            T* x = cur[(size_t)l];
+            T* xc = cur[(size_t)l + 1];
+            T* y = alt[(size_t)l];
+            const T sc = (T)curProlong_;
+            emit<T>(kOpProlongSmooth, l, x, xc, 0, (double)sc, 0, std::string("mg_prolong_smooth") + tag,
+                    (double)F.N * ((4.0 + vb) * F.W + 4.0 + 4.0 * vb) + vb * C.N,
+                    [&] { launchMGProlongSmoothAny<T>(ctl_, F, x, xc, y, w, sc, stream_); }, y);
+            std::swap(cur[(size_t)l], alt[(size_t)l]);
+            smoothT<T>(lv, l, post - 1, cur, alt);
+        } else if (fusedEll && launchMGProlongSmooth<T>(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], alt[(size_t)l], w,
+                                                        (T)curProlong_, stream_)) {
             markL(std::string("mg_prolong_smooth") + tag, l,
                  (double)F.N * ((4.0 + vb) * F.W + 4.0 + 4.0 * vb) + vb * C.N);
             std::swap(cur[(size_t)l], alt[(size_t)l]);
