@@ -540,13 +540,20 @@ class Solver:
         self._check(lib().axisim_scalar_residuals(self.h, out.ctypes.data_as(_f64p)))
         return out
 
+    FACE_FIELDS = frozenset(("mDot", "invDPN", "wP", "dPB", "length2D", "lsqWZ", "lsqWR", "cw", "ocrWall"))
+
     def get(self, name):
-        n = max(self.mesh["nCells"], self.mesh["nFaces"], len(self.mesh["cellFaceIDs"]))
-        out = np.zeros(n)
+        if name.startswith("AF_"):
+            n = len(self.mesh["cellFaceIDs"])
+        elif name in self.FACE_FIELDS:
+            n = self.mesh["nFaces"]
+        else:
+            n = self.mesh["nCells"]
+        out = np.empty(n)
         k = lib().axisim_get_field(self.h, name.encode(), out.ctypes.data_as(_f64p), n)
         if k < 0:
             self._check(int(-k))
-        return out[:k].copy()
+        return out if k == n else out[:k].copy()
 
     def set(self, name, arr):
         a = np.ascontiguousarray(arr, dtype=np.float64)
