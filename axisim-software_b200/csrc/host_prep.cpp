@@ -7,7 +7,9 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <memory>
 #include <numeric>
+#include <thread>
 #include <stdexcept>
 #include <unordered_map>
 
@@ -414,22 +416,50 @@ PackedMesh buildTriangleMesh(const std::vector<double>& pz, const std::vector<do
     return m;
 }
 
+namespace {
+
+// fn(begin, end) over [0, n) split into contiguous ranges, one per host
+// thread (up to 16); small ranges run on the calling thread. Each index is
+// handled by exactly one call, so results do not depend on the split.
+template <class Fn>
+void parallelFor(int n, Fn&& fn) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nt = std::max(1, std::min({(int)(hw ? hw : 1), 16, n / 16384}));
+    if (nt <= 1) {
+        fn(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    pool.reserve((size_t)nt - 1);
+    const int chunk = (n + nt - 1) / nt;
+    for (int t = 1; t < nt; t++) {
+        const int b = t * chunk, e = std::min(n, b + chunk);
+        if (b < e) pool.emplace_back([&fn, b, e] { fn(b, e); });
+    }
+    fn(0, std::min(n, chunk));
+    for (std::thread& th : pool) th.join();
+}
+
+}  // namespace
+
 GridLevel finestLevel(int nCells, int nFaces, const int32_t* cfs, const int32_t* cfi, const int32_t* owner,
                       const int32_t* neighbor) {
     GridLevel g;
     g.nCells = nCells;
     g.faceStart.assign(cfs, cfs + nCells + 1);
     g.faceNeighbor.resize((size_t)cfs[nCells]);
-    for (int c = 0; c < nCells; c++)
-        for (int k = cfs[c]; k < cfs[c + 1]; k++) {
-            const int f = cfi[k];
-            int nb = -1;
-            if (f >= 0 && f < nFaces) {
-                if (owner[f] == c) nb = neighbor[f];
-                else if (neighbor[f] == c) nb = owner[f];
+    parallelFor(nCells, [&](int c0, int c1) {
+        for (int c = c0; c < c1; c++)
+            for (int k = cfs[c]; k < cfs[c + 1]; k++) {
+                const int f = cfi[k];
+                int nb = -1;
+                if (f >= 0 && f < nFaces) {
+                    if (owner[f] == c) nb = neighbor[f];
+                    else if (neighbor[f] == c) nb = owner[f];
+                }
+                g.faceNeighbor[(size_t)k] = nb;
             }
-            g.faceNeighbor[(size_t)k] = nb;
-        }
+    });
     return g;
 }
 
@@ -511,38 +541,71 @@ GridLevel coarsen(GridLevel& fine) {
         std::vector<int32_t> fill(mStart.begin(), mStart.end() - 1);
         for (int n = 0; n < N; n++) mList[(size_t)fill[(size_t)c2c[(size_t)n]]++] = n;
     }
+    // every aggregate's boundary slots as (coarse neighbour, fine slot) pairs,
+    // stored at the aggregate's offset among all member slots, sorted by
+    // neighbour in place; aggregates are independent, so they run in parallel
     struct Ref {
         int32_t cn, slot;
     };
-    std::vector<Ref> buf;
-    fine.fineSlotToCoarseSlot.assign((size_t)fine.nFaceRefs(), -1);
-    coarse.faceStart.assign((size_t)nC + 1, 0);
-    coarse.faceNeighbor.reserve((size_t)fine.nFaceRefs() / 2);
-    for (int c = 0; c < nC; c++) {
-        buf.clear();
-        for (int q = mStart[(size_t)c]; q < mStart[(size_t)c + 1]; q++) {
-            const int n = mList[(size_t)q];
-            for (int k = fine.faceStart[(size_t)n]; k < fine.faceStart[(size_t)n + 1]; k++) {
-                const int nb = fine.faceNeighbor[(size_t)k];
-                if (nb < 0) continue;
-                const int cb = c2c[(size_t)nb];
-                if (cb != c) buf.push_back(Ref{cb, k});
+    std::vector<int64_t> refStart((size_t)nC + 1, 0);
+    parallelFor(nC, [&](int c0, int c1) {
+        for (int c = c0; c < c1; c++) {
+            int64_t d = 0;
+            for (int q = mStart[(size_t)c]; q < mStart[(size_t)c + 1]; q++) {
+                const int n = mList[(size_t)q];
+                d += fine.faceStart[(size_t)n + 1] - fine.faceStart[(size_t)n];
+            }
+            refStart[(size_t)c + 1] = d;
+        }
+    });
+    for (int c = 0; c < nC; c++) refStart[(size_t)c + 1] += refStart[(size_t)c];
+    // scratch left uninitialised (every entry read is written first): fresh
+    // zero-filled pages of this size cost more than the pass itself
+    std::unique_ptr<Ref[]> refs(new Ref[(size_t)std::max<int64_t>(refStart[(size_t)nC], 1)]);
+    std::vector<int32_t> nRef((size_t)nC), nUnique((size_t)nC + 1, 0);
+    fine.fineSlotToCoarseSlot.resize((size_t)fine.nFaceRefs());
+    parallelFor(nC, [&](int c0, int c1) {
+        for (int c = c0; c < c1; c++) {
+            Ref* b = refs.get() + refStart[(size_t)c];
+            Ref* e = b;
+            for (int q = mStart[(size_t)c]; q < mStart[(size_t)c + 1]; q++) {
+                const int n = mList[(size_t)q];
+                for (int k = fine.faceStart[(size_t)n]; k < fine.faceStart[(size_t)n + 1]; k++) {
+                    fine.fineSlotToCoarseSlot[(size_t)k] = -1;  // internal and boundary slots stay -1
+                    const int nb = fine.faceNeighbor[(size_t)k];
+                    if (nb < 0) continue;
+                    const int cb = c2c[(size_t)nb];
+                    if (cb != c) *e++ = Ref{cb, k};
+                }
+            }
+            if (e - b > 32)
+                std::sort(b, e, [](const Ref& x, const Ref& y) { return x.cn < y.cn; });
+            else
+                for (Ref* i = b + 1; i < e; i++)  // insertion sort by neighbour
+                    for (Ref* j = i; j > b && (j - 1)->cn > j->cn; j--) std::swap(*(j - 1), *j);
+            int u = 0;
+            for (Ref* i = b; i < e; i++)
+                if (i == b || i->cn != (i - 1)->cn) u++;
+            nRef[(size_t)c] = (int32_t)(e - b);
+            nUnique[(size_t)c + 1] = u;
+        }
+    });
+    // the coarse CSR: distinct (coarse cell, coarse neighbour) pairs in
+    // ascending order of cell then neighbour, and each fine slot's coarse slot
+    for (int c = 0; c < nC; c++) nUnique[(size_t)c + 1] += nUnique[(size_t)c];
+    coarse.faceStart.assign(nUnique.begin(), nUnique.end());
+    coarse.faceNeighbor.resize((size_t)nUnique[(size_t)nC]);
+    parallelFor(nC, [&](int c0, int c1) {
+        for (int c = c0; c < c1; c++) {
+            const Ref* b = refs.get() + refStart[(size_t)c];
+            const Ref* e = b + nRef[(size_t)c];
+            int pos = nUnique[(size_t)c] - 1;
+            for (const Ref* i = b; i < e; i++) {
+                if (i == b || i->cn != (i - 1)->cn) coarse.faceNeighbor[(size_t)++pos] = i->cn;
+                fine.fineSlotToCoarseSlot[(size_t)i->slot] = pos;
             }
         }
-        Ref* b = buf.data();
-        Ref* e = b + buf.size();
-        if (e - b > 32)
-            std::sort(b, e, [](const Ref& x, const Ref& y) { return x.cn < y.cn; });
-        else
-            for (Ref* i = b + 1; i < e; i++)  // insertion sort by neighbour
-                for (Ref* j = i; j > b && (j - 1)->cn > j->cn; j--) std::swap(*(j - 1), *j);
-        for (Ref* i = b; i < e; i++) {
-            if (i == b || i->cn != (i - 1)->cn) coarse.faceNeighbor.push_back(i->cn);
-            fine.fineSlotToCoarseSlot[(size_t)i->slot] = (int)coarse.faceNeighbor.size() - 1;
-        }
-        coarse.faceStart[(size_t)c + 1] = (int)coarse.faceNeighbor.size();
-    }
-    coarse.faceNeighbor.shrink_to_fit();
+    });
     return coarse;
 }
 
