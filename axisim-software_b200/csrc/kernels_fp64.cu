@@ -736,23 +736,42 @@ struct CorrectArgs {
     double* mDot;
 };
 
+// WC > 0: the slot count at compile time; every slot's face id, owner,
+// neighbour and area are loaded before the first store.
+template <int WC>
 __global__ void __launch_bounds__(kThreads) k_correct(MeshDev m, const Ctl* ctl, BCDev bcP, CorrectArgs a) {
     pdlEnter();
     if (ctl->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m.N) return;
     const int N = m.N;
+    constexpr int P = WC > 0 ? WC : 1;
+    int pf[P], po[P], pn[P];
+    double pa[P];
+    if (WC > 0) {
+#pragma unroll
+        for (int j = 0; j < P; j++) pf[j] = m.sface[(size_t)j * N + n];
+#pragma unroll
+        for (int j = 0; j < P; j++) {
+            const int f = pf[j] >= 0 ? pf[j] : 0;
+            po[j] = m.owner[f];
+            pn[j] = m.neighbor[f];
+            pa[j] = m.area[f];
+        }
+    }
     a.u[n] -= a.DU[n] * a.gZ[n];
     a.v[n] -= a.DV[n] * a.gR[n];
     a.p[n] += a.alphaP * a.pp[n];
     const double rho = a.rho;
-    for (int j = 0; j < m.W; j++) {
-        const int f = m.sface[(size_t)j * N + n];
+#pragma unroll
+    for (int j = 0; j < (WC > 0 ? WC : 32); j++) {
+        if (WC == 0 && j >= m.W) break;
+        const int f = WC > 0 ? pf[j] : m.sface[(size_t)j * N + n];
         if (f < 0) break;
-        const int own = m.owner[f];
+        const int own = WC > 0 ? po[j] : m.owner[f];
         if (own != n) continue;
-        const int nb = m.neighbor[f];
-        const double area = m.area[f];
+        const int nb = WC > 0 ? pn[j] : m.neighbor[f];
+        const double area = WC > 0 ? pa[j] : m.area[f];
         if (area <= 1.0e-30) {
             a.mDot[f] = 0.0;
             continue;
@@ -804,6 +823,9 @@ __device__ __forceinline__ void blockReduce(double (&v)[kResQ], const int (&isMa
     }
 }
 
+// WC > 0: the slot count at compile time; the neighbour and face ids of
+// every slot are loaded first, then every value they point to.
+template <int WC>
 __global__ void __launch_bounds__(kThreads) k_residual(MeshDev m, const Ctl* ctl, const double* AF, const double* ACu,
                                                        const double* ACv, const double* bu, const double* bv,
                                                        const double* u, const double* v, const double* mDot,
@@ -822,19 +844,52 @@ __global__ void __launch_bounds__(kThreads) k_residual(MeshDev m, const Ctl* ctl
         double Axv = ACv[n] * v[n];
         const double su = Axu, sv = Axv;
         double imb = 0.0;
-        for (int j = 0; j < m.W; j++) {
-            const size_t s = (size_t)j * N + n;
-            const int nb = m.snb[s];
-            if (nb >= 0) {
-                const double a = AF[s];
-                Axu += a * u[nb];
-                Axv += a * v[nb];
+        if (WC > 0) {
+            constexpr int P = WC > 0 ? WC : 1;
+            int pb[P], pf[P], po[P], pn[P];
+            double pa[P], pu[P], pv[P], pm[P];
+#pragma unroll
+            for (int j = 0; j < P; j++) {
+                pb[j] = m.snb[(size_t)j * N + n];
+                pf[j] = m.sface[(size_t)j * N + n];
             }
-            const int f = m.sface[s];
-            if (f >= 0) {
-                const double md = mDot[f];
-                if (m.owner[f] == n) imb += md;
-                else if (m.neighbor[f] == n) imb -= md;
+#pragma unroll
+            for (int j = 0; j < P; j++) {
+                const int c = pb[j] >= 0 ? pb[j] : n;
+                const int f = pf[j] >= 0 ? pf[j] : 0;
+                pa[j] = AF[(size_t)j * N + n];
+                pu[j] = u[c];
+                pv[j] = v[c];
+                pm[j] = mDot[f];
+                po[j] = m.owner[f];
+                pn[j] = m.neighbor[f];
+            }
+#pragma unroll
+            for (int j = 0; j < P; j++) {
+                if (pb[j] >= 0) {
+                    Axu += pa[j] * pu[j];
+                    Axv += pa[j] * pv[j];
+                }
+                if (pf[j] >= 0) {
+                    if (po[j] == n) imb += pm[j];
+                    else if (pn[j] == n) imb -= pm[j];
+                }
+            }
+        } else {
+            for (int j = 0; j < m.W; j++) {
+                const size_t s = (size_t)j * N + n;
+                const int nb = m.snb[s];
+                if (nb >= 0) {
+                    const double a = AF[s];
+                    Axu += a * u[nb];
+                    Axv += a * v[nb];
+                }
+                const int f = m.sface[s];
+                if (f >= 0) {
+                    const double md = mDot[f];
+                    if (m.owner[f] == n) imb += md;
+                    else if (m.neighbor[f] == n) imb -= md;
+                }
             }
         }
         const double ru = fabs(bu[n] - Axu);
@@ -1153,7 +1208,9 @@ void launchCorrect(const MeshDev& m, const Ctl* ctl, const BCDev& bcP, double rh
                    const double* pp, const double* gZ, const double* gR, const double* DU, const double* DV, double* u,
                    double* v, double* p, double* mDot, cudaStream_t s) {
     CorrectArgs a{rho, alphaP, nonOrtho, pp, gZ, gR, DU, DV, u, v, p, mDot};
-    launchPDL(k_correct, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcP, a);
+    if (m.W == 4) launchPDL(k_correct<4>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcP, a);
+    else if (m.W == 3) launchPDL(k_correct<3>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcP, a);
+    else launchPDL(k_correct<0>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcP, a);
 }
 
 void launchResiduals(const MeshDev& m, const Ctl* ctl, const double* AF, const double* ACu, const double* ACv,
@@ -1162,7 +1219,11 @@ void launchResiduals(const MeshDev& m, const Ctl* ctl, const double* AF, const d
                      int* nBlocksOut, cudaStream_t s) {
     const int b = blocksFor(m.N);
     *nBlocksOut = b;
-    launchPDL(k_residual, dim3(b), dim3(kThreads), 0, s, m, ctl, AF, ACu, ACv, bu, bv, u, v, mDot, resU, resV, resC, scaleU, scaleV,
+    if (m.W == 4) launchPDL(k_residual<4>, dim3(b), dim3(kThreads), 0, s, m, ctl, AF, ACu, ACv, bu, bv, u, v, mDot, resU, resV, resC, scaleU, scaleV,
+                                      partial);
+    else if (m.W == 3) launchPDL(k_residual<3>, dim3(b), dim3(kThreads), 0, s, m, ctl, AF, ACu, ACv, bu, bv, u, v, mDot, resU, resV, resC, scaleU, scaleV,
+                                      partial);
+    else launchPDL(k_residual<0>, dim3(b), dim3(kThreads), 0, s, m, ctl, AF, ACu, ACv, bu, bv, u, v, mDot, resU, resV, resC, scaleU, scaleV,
                                       partial);
 }
 
