@@ -598,10 +598,6 @@ struct PressureArgs {
     float* AC32;
 };
 
-// WC > 0: the slot count at compile time; every slot's face id, owner,
-// neighbour, area and 1/d_PN are loaded before the per-face arithmetic (in
-// the reference's order), so the cell's face chains are in flight together.
-template <int WC>
 __global__ void __launch_bounds__(kThreads) k_pressure(MeshDev m, const Ctl* ctl, BCDev bcU, BCDev bcV, BCDev bcP,
                                                        PressureArgs a) {
     pdlEnter();
@@ -610,35 +606,18 @@ __global__ void __launch_bounds__(kThreads) k_pressure(MeshDev m, const Ctl* ctl
     if (n >= m.N) return;
     const int N = m.N;
     const double rho = a.rho;
-    constexpr int P = WC > 0 ? WC : 1;
-    int pf[P], po[P], pn[P];
-    double pa[P], pd[P];
-    if (WC > 0) {
-#pragma unroll
-        for (int j = 0; j < P; j++) pf[j] = m.sface[(size_t)j * N + n];
-#pragma unroll
-        for (int j = 0; j < P; j++) {
-            const int f = pf[j] >= 0 ? pf[j] : 0;
-            po[j] = m.owner[f];
-            pn[j] = m.neighbor[f];
-            pa[j] = m.area[f];
-            pd[j] = m.invDPN[f];
-        }
-    }
     double AC = 0.0;
-#pragma unroll
-    for (int j = 0; j < (WC > 0 ? WC : 32); j++) {
-        if (WC == 0 && j >= m.W) break;
+    for (int j = 0; j < m.W; j++) {
         const size_t s = (size_t)j * N + n;
-        const int f = WC > 0 ? pf[j] : m.sface[s];
+        const int f = m.sface[s];
         if (f < 0) break;
-        const int own = WC > 0 ? po[j] : m.owner[f], nb = WC > 0 ? pn[j] : m.neighbor[f];
-        const double area = WC > 0 ? pa[j] : m.area[f];
+        const int own = m.owner[f], nb = m.neighbor[f];
+        const double area = m.area[f];
         const double nz = m.nZ[f], nr = m.nR[f];
         const double Df = interpCorr(m, a.DU, a.DV, n, f, own, nb);
         // createPPCoeff (simple.cu:7-88)
         if (nb >= 0) {
-            const double K = rho * area * Df * (WC > 0 ? pd[j] : m.invDPN[f]);
+            const double K = rho * area * Df * m.invDPN[f];
             AC += K;
             a.AFpp[s] = 0.0 - K;
             if (a.AF32) a.AF32[s] = (float)(0.0 - K);
@@ -679,7 +658,7 @@ __global__ void __launch_bounds__(kThreads) k_pressure(MeshDev m, const Ctl* ctl
                 un = unLin - Df * (gc - gn);
             }
         } else {
-            const double gpn = (a.p[nb] - a.p[n]) * (WC > 0 ? pd[j] : m.invDPN[f]);
+            const double gpn = (a.p[nb] - a.p[n]) * m.invDPN[f];
             const double w = m.wP[f];
             const double gzf = w * a.gPZ[n] + (1.0 - w) * a.gPZ[nb];
             const double grf = w * a.gPR[n] + (1.0 - w) * a.gPR[nb];
@@ -1183,9 +1162,7 @@ void launchPressureSystem(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, co
                           const double* gPR, const double* DU, const double* DV, double* AFpp, double* ACpp,
                           double* invACpp, double* mDot, float* AF32, float* AC32, cudaStream_t s) {
     PressureArgs a{rho, u, v, p, gPZ, gPR, DU, DV, AFpp, ACpp, invACpp, mDot, AF32, AC32};
-    if (m.W == 4) launchPDL(k_pressure<4>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcU, bcV, bcP, a);
-    else if (m.W == 3) launchPDL(k_pressure<3>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcU, bcV, bcP, a);
-    else launchPDL(k_pressure<0>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcU, bcV, bcP, a);
+    launchPDL(k_pressure, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcU, bcV, bcP, a);
 }
 
 void launchPressureRhs(const MeshDev& m, const Ctl* ctl, double rho, const double* mDot, const double* DU,
