@@ -685,8 +685,8 @@ class Solver:
         return dict(applied=a.value, fallbacks=f.value, score_net=sn.value, score_vcycle=sv.value)
 
     def set_vcycle_kernel(self, mode):
-        """VCYCLE_RESIDENT (default): the coarser levels' V-cycle in one cooperative kernel;
-        VCYCLE_PER_PHASE: one launch per phase."""
+        """VCYCLE_PER_PHASE (default): one launch per phase; VCYCLE_RESIDENT: the coarser
+        levels' V-cycle in one cooperative kernel."""
         self._check(lib().axisim_set_vcycle_kernel(self.h, mode))
 
     def set_autotune(self, on=True):

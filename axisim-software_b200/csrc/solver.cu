@@ -1281,7 +1281,12 @@ private:
     ResidentArgsT<double>* rec64_ = nullptr;
     ResidentArgsT<float>* rec32_ = nullptr;
     double recBytes_ = 0.0;
-    int residentVcycle_ = 1;
+    int residentVcycle_ = 0;
+    // coarse levels up to this size fuse residual + restriction and
+    // prolongation + first post-sweep (beyond it the fused forms, one thread
+    // per row gathering its neighbours' corrections, run slower than two
+    // coalesced passes)
+    static constexpr int kFuseMaxCells = 65536;
     int barrierPhantom_ = 0;  // test hook: extra arrivals each grid barrier expects
     bool timedOut_ = false;   // the last run ended on a barrier that gave up
     template <class T>
@@ -1331,10 +1336,11 @@ private:
         smoothT<T>(lv, l, cmg_.linearPreSweep - (firstDone ? 1 : 0), cur, alt);
         LevelT<T>& F = lv[(size_t)l];
         LevelT<T>& C = lv[(size_t)l + 1];
-        // on a coarse level the restriction forms its members' residuals itself;
-        // the finest level (coalesced [W][N] rows) and the level above the tail
-        // (whose residual the tail reads) keep the separate residual pass
-        const bool gatherRes = F.sliceOff != nullptr && l + 1 != tailStart_;
+        // on a small coarse level the restriction forms its members' residuals
+        // itself (one launch instead of two where launches dominate); larger
+        // levels, the finest one (coalesced [W][N] rows) and the level above
+        // the tail (whose residual the tail reads) keep the separate pass
+        const bool gatherRes = F.sliceOff != nullptr && F.N <= kFuseMaxCells && l + 1 != tailStart_;
         if (!gatherRes) {
             T* x = cur[(size_t)l];
             emit<T>(kOpResidual, l, x, nullptr, 0, 0.0, 0, std::string("mg_residual") + tag,
@@ -1425,7 +1431,7 @@ private:
         // layout-generic one on coarse levels
         const bool fusedEll = post >= 1 && !blockSmoother && !F.sliceOff && F.c2c && (F.W == 3 || F.W == 4) &&
                               !recSlot<T>();
-        const bool fusedAny = post >= 1 && !blockSmoother && F.sliceOff && F.c2c;
+        const bool fusedAny = post >= 1 && !blockSmoother && F.sliceOff && F.c2c && F.N <= kFuseMaxCells;
         if (fusedAny) {
             T* x = cur[(size_t)l];
             T* xc = cur[(size_t)l + 1];

@@ -246,11 +246,13 @@ int axisim_set_pressure_solver(axisim_handle* h, int32_t mode, double relTol, do
 int axisim_pressure_stats(axisim_handle* h, int64_t* solves, int64_t* iterations);
 /* New (the reference launches every multigrid phase as its own kernel or
  * graph node, multigrid.cu:607-662): how the V-cycle below the finest level
- * runs. AXISIM_VCYCLE_RESIDENT (the default): one cooperative kernel, one CTA
- * per SM, runs every phase of the coarser levels in order with a grid-wide
- * barrier between phases (the same per-cell arithmetic, so the same results
- * bit for bit); a barrier that waits longer than a second ends the solve with
- * AXISIM_E_TIMEOUT. AXISIM_VCYCLE_PER_PHASE: one launch per phase. */
+ * runs. AXISIM_VCYCLE_PER_PHASE (the default): one launch per phase, chained
+ * by programmatic dependent launch inside the captured graph.
+ * AXISIM_VCYCLE_RESIDENT: one cooperative kernel, one CTA per SM, runs every
+ * phase of the coarser levels in order with a grid-wide barrier between
+ * phases (the same per-cell arithmetic, so the same results bit for bit; on a
+ * B200 it measured slower than the launches it replaces); a barrier that
+ * waits longer than a second ends the solve with AXISIM_E_TIMEOUT. */
 #define AXISIM_VCYCLE_PER_PHASE 0
 #define AXISIM_VCYCLE_RESIDENT 1
 int axisim_set_vcycle_kernel(axisim_handle* h, int32_t mode);

@@ -40,8 +40,8 @@ def test_fcg_runs_krylov_kernels_and_rejects_unknown_mode():
     gpu.solve()
     names = {k["name"] for k in gpu.profile(1)}
     assert {"fcg_init", "fcg_dots", "fcg_spmv", "fcg_update"} <= names
-    # the coarser levels' sweeps run inside the resident V-cycle kernel by default
-    assert any((n.startswith("mg_smooth") or n.startswith("mg_resident")) and n.endswith("32") for n in names)
+    # the coarser levels' sweeps: their own launches, or inside the resident kernel
+    assert any(n.startswith(("mg_smooth", "mg_prolong_smooth", "mg_resident")) and n.endswith("32") for n in names)
     assert "ir_update_pp" not in names
     st = abi.lib().axisim_set_pressure_solver(gpu.h, 7, 0.0, 1.0)
     assert st == abi.E_ARG

@@ -38,8 +38,8 @@ def test_mixed_path_runs_fp32_inner_kernels():
     gpu.solve()
     names = {k["name"] for k in gpu.profile(1)}
     assert {"jacobi_uv32", "ir_residual_uv", "ir_residual_pp", "ir_update_pp"} <= names
-    # the coarser levels' sweeps run inside the resident V-cycle kernel by default
-    assert any((n.startswith("mg_smooth") or n.startswith("mg_resident")) and n.endswith("32") for n in names)
+    # the coarser levels' sweeps: their own launches, or inside the resident kernel
+    assert any(n.startswith(("mg_smooth", "mg_prolong_smooth", "mg_resident")) and n.endswith("32") for n in names)
     assert "jacobi_uv" not in names
 
 
