@@ -416,32 +416,6 @@ PackedMesh buildTriangleMesh(const std::vector<double>& pz, const std::vector<do
     return m;
 }
 
-namespace {
-
-// fn(begin, end) over [0, n) split into contiguous ranges, one per host
-// thread (up to 16); small ranges run on the calling thread. Each index is
-// handled by exactly one call, so results do not depend on the split.
-template <class Fn>
-void parallelFor(int n, Fn&& fn) {
-    const unsigned hw = std::thread::hardware_concurrency();
-    const int nt = std::max(1, std::min({(int)(hw ? hw : 1), 16, n / 16384}));
-    if (nt <= 1) {
-        fn(0, n);
-        return;
-    }
-    std::vector<std::thread> pool;
-    pool.reserve((size_t)nt - 1);
-    const int chunk = (n + nt - 1) / nt;
-    for (int t = 1; t < nt; t++) {
-        const int b = t * chunk, e = std::min(n, b + chunk);
-        if (b < e) pool.emplace_back([&fn, b, e] { fn(b, e); });
-    }
-    fn(0, std::min(n, chunk));
-    for (std::thread& th : pool) th.join();
-}
-
-}  // namespace
-
 GridLevel finestLevel(int nCells, int nFaces, const int32_t* cfs, const int32_t* cfi, const int32_t* owner,
                       const int32_t* neighbor) {
     GridLevel g;

@@ -9,11 +9,35 @@
 // (manager/source/boundary_func.cpp:104-201, 333-378).
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace axisim {
+
+// fn(begin, end) over [0, n) split into contiguous ranges, one per host
+// thread (up to 16); small ranges run on the calling thread. Each index is
+// handled by exactly one call, so results do not depend on the split.
+template <class Fn>
+void parallelFor(int n, Fn&& fn) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nt = std::max(1, std::min({(int)(hw ? hw : 1), 16, n / 16384}));
+    if (nt <= 1) {
+        fn(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    pool.reserve((size_t)nt - 1);
+    const int chunk = (n + nt - 1) / nt;
+    for (int t = 1; t < nt; t++) {
+        const int b = t * chunk, e = std::min(n, b + chunk);
+        if (b < e) pool.emplace_back([&fn, b, e] { fn(b, e); });
+    }
+    fn(0, std::min(n, chunk));
+    for (std::thread& th : pool) th.join();
+}
 
 // Packed face-based mesh (FVMeshHostPacked, structs/solver_struct.h:400-429).
 struct PackedMesh {

@@ -1083,9 +1083,11 @@ private:
                 d.W = W;
                 d.totalSlots = off[(size_t)nS];
                 std::vector<int32_t> nb((size_t)std::max(d.totalSlots, 1), -1);
-                for (int c = 0; c < g.nCells; c++)
-                    for (int k = g.faceStart[(size_t)c], j = 0; k < g.faceStart[(size_t)c + 1]; k++, j++)
-                        nb[(size_t)pos(l, c, j)] = g.faceNeighbor[(size_t)k];
+                parallelFor(g.nCells, [&](int c0, int c1) {
+                    for (int c = c0; c < c1; c++)
+                        for (int k = g.faceStart[(size_t)c], j = 0; k < g.faceStart[(size_t)c + 1]; k++, j++)
+                            nb[(size_t)pos(l, c, j)] = g.faceNeighbor[(size_t)k];
+                });
                 d.sliceOff = mgArena_.upload(off.data(), off.size());
                 d.nb = mgArena_.upload(nb.data(), nb.size());
                 d.AF = mgArena_.alloc<double>(nb.size());
@@ -1116,29 +1118,44 @@ private:
                     if (f.cellToCoarse[(size_t)n] >= 0) mList[(size_t)fill[(size_t)f.cellToCoarse[(size_t)n]]++] = n;
             }
             std::vector<int32_t> coarsePos((size_t)std::max(c.nFaceRefs(), 1));
-            for (int cc = 0; cc < c.nCells; cc++)
-                for (int k = c.faceStart[(size_t)cc], j = 0; k < c.faceStart[(size_t)cc + 1]; k++, j++)
-                    coarsePos[(size_t)k] = pos(l, cc, j);
+            parallelFor(c.nCells, [&](int c0, int c1) {
+                for (int cc = c0; cc < c1; cc++)
+                    for (int k = c.faceStart[(size_t)cc], j = 0; k < c.faceStart[(size_t)cc + 1]; k++, j++)
+                        coarsePos[(size_t)k] = pos(l, cc, j);
+            });
+            // Each coarse slot is fed only by members of its own coarse cell, so
+            // the counts and lists are built per coarse cell in parallel; its
+            // members in ascending order keep every list in ascending fine order.
             std::vector<int32_t> gCount((size_t)cd.totalSlots + 1, 0);
             std::vector<uint32_t> mask((size_t)f.nCells, 0u);
-            for (int n = 0; n < f.nCells; n++)
-                for (int k = f.faceStart[(size_t)n], j = 0; k < f.faceStart[(size_t)n + 1]; k++, j++) {
-                    if (f.faceNeighbor[(size_t)k] < 0) continue;
-                    const int sI = f.fineSlotToCoarseSlot[(size_t)k];
-                    if (sI >= 0) gCount[(size_t)coarsePos[(size_t)sI] + 1]++;
-                    else mask[(size_t)n] |= (1u << j);
+            parallelFor(f.nCells, [&](int n0, int n1) {
+                for (int n = n0; n < n1; n++)
+                    for (int k = f.faceStart[(size_t)n], j = 0; k < f.faceStart[(size_t)n + 1]; k++, j++)
+                        if (f.faceNeighbor[(size_t)k] >= 0 && f.fineSlotToCoarseSlot[(size_t)k] < 0)
+                            mask[(size_t)n] |= (1u << j);
+            });
+            auto eachSource = [&](int cc, auto&& fn) {
+                for (int q = mStart[(size_t)cc]; q < mStart[(size_t)cc + 1]; q++) {
+                    const int n = mList[(size_t)q];
+                    for (int k = f.faceStart[(size_t)n], j = 0; k < f.faceStart[(size_t)n + 1]; k++, j++) {
+                        if (f.faceNeighbor[(size_t)k] < 0) continue;
+                        const int sI = f.fineSlotToCoarseSlot[(size_t)k];
+                        if (sI >= 0) fn(coarsePos[(size_t)sI], n, j);
+                    }
                 }
+            };
+            parallelFor(c.nCells, [&](int c0, int c1) {
+                for (int cc = c0; cc < c1; cc++) eachSource(cc, [&](int p, int, int) { gCount[(size_t)p + 1]++; });
+            });
             std::vector<int32_t> gStart(gCount.size(), 0);
             for (size_t i = 1; i < gCount.size(); i++) gStart[i] = gStart[i - 1] + gCount[i];
             std::vector<int32_t> gList((size_t)std::max(gStart.back(), 1));
             {
                 std::vector<int32_t> fill(gStart);
-                for (int n = 0; n < f.nCells; n++)
-                    for (int k = f.faceStart[(size_t)n], j = 0; k < f.faceStart[(size_t)n + 1]; k++, j++) {
-                        if (f.faceNeighbor[(size_t)k] < 0) continue;
-                        const int sI = f.fineSlotToCoarseSlot[(size_t)k];
-                        if (sI >= 0) gList[(size_t)fill[(size_t)coarsePos[(size_t)sI]]++] = pos(l - 1, n, j);
-                    }
+                parallelFor(c.nCells, [&](int c0, int c1) {
+                    for (int cc = c0; cc < c1; cc++)
+                        eachSource(cc, [&](int p, int n, int j) { gList[(size_t)fill[(size_t)p]++] = pos(l - 1, n, j); });
+                });
             }
             cd.mStart = mgArena_.upload(mStart.data(), mStart.size());
             cd.mList = mgArena_.upload(mList.data(), mList.size());
