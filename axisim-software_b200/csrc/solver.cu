@@ -383,20 +383,40 @@ public:
         for (const void* p : req)
             if (!p) throw StatusError(AXISIM_E_ARG, "mesh array is null");
         if (pm.cellFaceStart[0] != 0) throw StatusError(AXISIM_E_MESH, "cellFaceStart[0] must be 0");
-        int W = 0;
-        for (int c = 0; c < N; c++) {
-            const int d = pm.cellFaceStart[c + 1] - pm.cellFaceStart[c];
-            if (d < 0) throw StatusError(AXISIM_E_MESH, "cellFaceStart is not monotone");
-            W = std::max(W, d);
-        }
+        // range checks in parallel; each range reports its largest face count
+        // and a violation flag (1 order, 2 slot face id, 3 owner, 4 neighbour)
+        std::atomic<int> W{0}, bad{0};
+        auto note = [&](int code) {
+            int z = 0;
+            bad.compare_exchange_strong(z, code);
+        };
+        parallelFor(N, [&](int c0, int c1) {
+            int w = 0;
+            for (int c = c0; c < c1; c++) {
+                const int d = pm.cellFaceStart[c + 1] - pm.cellFaceStart[c];
+                if (d < 0) note(1);
+                w = std::max(w, d);
+            }
+            int cur = W.load();
+            while (w > cur && !W.compare_exchange_weak(cur, w)) {
+            }
+        });
+        if (bad == 1) throw StatusError(AXISIM_E_MESH, "cellFaceStart is not monotone");
         if (W > 32) throw StatusError(AXISIM_E_MESH, "a cell has more than 32 faces");
         const int S = pm.cellFaceStart[N];
-        for (int k = 0; k < S; k++)
-            if (pm.cellFaceIDs[k] < 0 || pm.cellFaceIDs[k] >= F) throw StatusError(AXISIM_E_MESH, "cellFaceIDs out of range");
-        for (int f = 0; f < F; f++) {
-            if (pm.faceOwner[f] < 0 || pm.faceOwner[f] >= N) throw StatusError(AXISIM_E_MESH, "faceOwner out of range");
-            if (pm.faceNeighbor[f] >= N) throw StatusError(AXISIM_E_MESH, "faceNeighbor out of range");
-        }
+        parallelFor(S, [&](int k0, int k1) {
+            for (int k = k0; k < k1; k++)
+                if (pm.cellFaceIDs[k] < 0 || pm.cellFaceIDs[k] >= F) note(2);
+        });
+        if (bad == 2) throw StatusError(AXISIM_E_MESH, "cellFaceIDs out of range");
+        parallelFor(F, [&](int f0, int f1) {
+            for (int f = f0; f < f1; f++) {
+                if (pm.faceOwner[f] < 0 || pm.faceOwner[f] >= N) note(3);
+                if (pm.faceNeighbor[f] >= N) note(4);
+            }
+        });
+        if (bad == 3) throw StatusError(AXISIM_E_MESH, "faceOwner out of range");
+        if (bad == 4) throw StatusError(AXISIM_E_MESH, "faceNeighbor out of range");
         destroyGraph();
         batchArena_.release();
         batch_ = BatchDev{};
