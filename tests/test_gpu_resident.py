@@ -76,6 +76,7 @@ def test_resident_barrier_gives_up_and_the_handle_recovers():
     case = cases.expansion(scale=1 / 8, max_iter=50, tol=1e-30)
     mesh = abi.multiblock(case.blocks)
     s = abi.Solver(mesh, case.bc_fields(), case.settings)
+    s.set_vcycle_kernel(abi.VCYCLE_RESIDENT)
     assert abi.lib().axisim_test_barrier_timeout(s.h, 1) == abi.OK
     t0 = time.perf_counter()
     r = s.solve(allow=(abi.E_TIMEOUT,))
@@ -89,6 +90,7 @@ def test_resident_barrier_gives_up_and_the_handle_recovers():
     r = s.solve()
     assert r["status"] == abi.OK and r["iterations"] == 5
     g = abi.Solver(mesh, case.bc_fields(), dict(case.settings, maxIter=5))
+    g.set_vcycle_kernel(abi.VCYCLE_RESIDENT)
     g.solve()
     for f in FIELDS:
         np.testing.assert_array_equal(s.get(f), g.get(f), err_msg=f)
