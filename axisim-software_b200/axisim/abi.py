@@ -44,6 +44,7 @@ EXPORTS = [
     "axisim_mg_levels_host", "axisim_mg_level_maps_host", "axisim_coloring_host",
     "axisim_set_autotune", "axisim_autotune_report", "axisim_setup_profile", "axisim_profile_levels",
     "axisim_mg_batch_levels_host", "axisim_set_vcycle_kernel", "axisim_test_barrier_timeout",
+    "axisim_set_momentum_sweeps", "axisim_sweep_tiles", "axisim_sweep_tiles_host",
 ]
 VAR_U, VAR_V, VAR_P, VAR_T, VAR_C = range(5)
 VAR_INDEX = {"u": VAR_U, "v": VAR_V, "p": VAR_P, "T": VAR_T, "C": VAR_C}
@@ -162,6 +163,11 @@ def lib():
             "axisim_set_pressure_solver": (C.c_int, [vp, C.c_int32, C.c_double, C.c_double]),
             "axisim_set_autotune": (C.c_int, [vp, C.c_int32]),
             "axisim_set_vcycle_kernel": (C.c_int, [vp, C.c_int32]),
+            "axisim_set_momentum_sweeps": (C.c_int, [vp, C.c_int32, C.c_int32]),
+            "axisim_sweep_tiles": (C.c_int, [vp, C.POINTER(C.c_int32)]),
+            "axisim_sweep_tiles_host": (C.c_int64, [C.POINTER(MeshPacked), C.c_int32, C.c_int32, C.c_int32,
+                                                    C.POINTER(C.c_int32), _i32p, _i32p, _i32p,
+                                                    C.POINTER(C.c_uint64), C.c_int64]),
             "axisim_test_barrier_timeout": (C.c_int, [vp, C.c_int32]),
             "axisim_autotune_report": (C.c_int, [vp, _i32p, _f64p, C.c_int32]),
             "axisim_pressure_stats": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
@@ -364,6 +370,31 @@ def mg_batch_levels_host(mesh, case_cell_start):
     if n < 0:
         raise AxisimError(-n, "mg_batch_levels_host failed")
     return cells[:n].copy(), term[:n].copy()
+
+
+def sweep_tiles_host(mesh, S, cap, tile_cells):
+    """The momentum sweep tiles (axisim_sweep_tiles_host): dict of tileStart,
+    layerEnd (n_tiles x (S + 1)), gid and lnb (n_local x 4 local neighbours,
+    -1 for none); n_tiles = 0 when no tiling fits."""
+    s, keep = mesh_struct(mesh)
+    f = lib().axisim_sweep_tiles_host
+    nt = C.c_int32()
+    total = int(f(C.byref(s), S, cap, tile_cells, C.byref(nt), None, None, None, None, 0))
+    if total < 0:
+        raise AxisimError(-total, "sweep_tiles_host failed")
+    n = nt.value
+    ts = np.zeros(n + 1, np.int32)
+    le = np.zeros(max(n, 1) * (S + 1), np.int32)
+    gid = np.zeros(max(total, 1), np.int32)
+    lnb = np.zeros(max(total, 1), np.uint64)
+    got = int(f(C.byref(s), S, cap, tile_cells, C.byref(nt), ts.ctypes.data_as(_i32p), le.ctypes.data_as(_i32p),
+                gid.ctypes.data_as(_i32p), lnb.ctypes.data_as(C.POINTER(C.c_uint64)), total))
+    if got != total:
+        raise AxisimError(E_MESH, "sweep_tiles_host changed between calls")
+    words = lnb[:total].view(np.uint16).reshape(total, 4).astype(np.int32)
+    words[words == 0xFFFF] = -1
+    return {"n_tiles": n, "tileStart": ts, "layerEnd": le[:n * (S + 1)].reshape(n, S + 1), "gid": gid[:total],
+            "lnb": words}
 
 
 def mg_level_maps_host(mesh, level):
@@ -683,6 +714,17 @@ class Solver:
         a, f, sn, sv = C.c_int64(), C.c_int64(), C.c_double(), C.c_double()
         self._check(lib().axisim_learned_stats(self.h, C.byref(a), C.byref(f), C.byref(sn), C.byref(sv)))
         return dict(applied=a.value, fallbacks=f.value, score_net=sn.value, score_vcycle=sv.value)
+
+    def set_momentum_sweeps(self, sweeps_per_launch, threads=0):
+        """Momentum Jacobi sweeps per launch (1 = one launch per sweep; default 4, run on
+        shared-memory tiles) and the CTA size of the tiled launches (0 = 1024)."""
+        self._check(lib().axisim_set_momentum_sweeps(self.h, sweeps_per_launch, threads))
+
+    def sweep_tiles(self):
+        """Tiles the momentum sweeps of the last captured solve ran on (0: one launch per sweep)."""
+        n = C.c_int32()
+        self._check(lib().axisim_sweep_tiles(self.h, C.byref(n)))
+        return n.value
 
     def set_vcycle_kernel(self, mode):
         """VCYCLE_PER_PHASE (default): one launch per phase; VCYCLE_RESIDENT: the coarser

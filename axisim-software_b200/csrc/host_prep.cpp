@@ -686,6 +686,205 @@ int pickBlock(const std::vector<int>& candidates, const std::vector<double>& tim
     return best;
 }
 
+namespace {
+
+uint32_t spreadBits16(uint32_t v) {
+    v &= 0xFFFFu;
+    v = (v | (v << 8)) & 0x00FF00FFu;
+    v = (v | (v << 4)) & 0x0F0F0F0Fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+// Open-addressing map from mesh cell to local index, cleared per tile by
+// forgetting only the slots it used.
+class LocalMap {
+public:
+    explicit LocalMap(int entries) {
+        uint32_t size = 1024;
+        while (size < 2u * (uint32_t)entries) size <<= 1;
+        key_.assign(size, -1);
+        val_.assign(size, -1);
+        mask_ = size - 1;
+    }
+    void clear() {
+        for (uint32_t i : used_) key_[i] = -1;
+        used_.clear();
+    }
+    bool insert(int32_t k) {  // true when k was not present
+        uint32_t i = slot(k);
+        if (key_[i] == k) return false;
+        key_[i] = k;
+        val_[i] = -1;
+        used_.push_back(i);
+        return true;
+    }
+    void set(int32_t k, int32_t v) { val_[slot(k)] = v; }
+    int32_t get(int32_t k) const {
+        const uint32_t i = slot(k);
+        return key_[i] == k ? val_[i] : -1;
+    }
+
+private:
+    uint32_t slot(int32_t k) const {
+        uint32_t i = ((uint32_t)k * 2654435761u) & mask_;
+        while (key_[i] != -1 && key_[i] != k) i = (i + 1) & mask_;
+        return i;
+    }
+    std::vector<int32_t> key_, val_;
+    std::vector<uint32_t> used_;
+    uint32_t mask_ = 0;
+};
+
+struct TileRun {
+    std::vector<int32_t> count, layerEnd, gid;
+    std::vector<uint64_t> lnb;
+};
+
+// The tiles of curve positions [a, b), appended to out; false when one cell
+// with its halo does not fit in cap local cells.
+bool buildTileRun(const int32_t* order, int a, int b, int N, int W, const int32_t* nb, int S, int cap, LocalMap& map,
+                  std::vector<int32_t>& cells, TileRun& out) {
+    cells.assign(order + a, order + b);
+    std::sort(cells.begin(), cells.end());
+    map.clear();
+    for (int32_t c : cells) map.insert(c);
+    std::vector<int32_t> layerEnd((size_t)S + 1);
+    layerEnd[0] = (int32_t)cells.size();
+    bool fits = (int)cells.size() <= cap;
+    size_t from = 0;
+    for (int k = 1; k <= S && fits; k++) {
+        const size_t to = cells.size();
+        for (size_t i = from; i < to && fits; i++)
+            for (int j = 0; j < W && fits; j++) {
+                const int32_t m = nb[(size_t)j * N + cells[i]];
+                if (m >= 0 && map.insert(m)) {
+                    cells.push_back(m);
+                    fits = (int)cells.size() <= cap;  // the map holds at most cap + 1 cells
+                }
+            }
+        std::sort(cells.begin() + (std::ptrdiff_t)to, cells.end());
+        from = to;
+        layerEnd[(size_t)k] = (int32_t)cells.size();
+    }
+    if (!fits) {
+        if (b - a <= 1) return false;
+        const int mid = a + (b - a) / 2;
+        return buildTileRun(order, a, mid, N, W, nb, S, cap, map, cells, out) &&
+               buildTileRun(order, mid, b, N, W, nb, S, cap, map, cells, out);
+    }
+    for (size_t i = 0; i < cells.size(); i++) map.set(cells[i], (int32_t)i);
+    const size_t inner = (size_t)layerEnd[(size_t)S - 1];
+    for (size_t i = 0; i < cells.size(); i++) {
+        uint64_t word = ~0ull;
+        if (i < inner)
+            for (int j = 0; j < W; j++) {
+                const int32_t m = nb[(size_t)j * N + cells[i]];
+                const uint64_t l = m >= 0 ? (uint64_t)(uint32_t)map.get(m) : 0xFFFFull;
+                word = (word & ~(0xFFFFull << (16 * j))) | (l << (16 * j));
+            }
+        out.lnb.push_back(word);
+    }
+    out.count.push_back((int32_t)cells.size());
+    out.layerEnd.insert(out.layerEnd.end(), layerEnd.begin(), layerEnd.end());
+    out.gid.insert(out.gid.end(), cells.begin(), cells.end());
+    return true;
+}
+
+}  // namespace
+
+std::vector<int32_t> slotNeighbours(int N, int W, const int32_t* cfs, const int32_t* cfi, const int32_t* owner,
+                                    const int32_t* neighbor) {
+    std::vector<int32_t> nb((size_t)W * (size_t)std::max(N, 0));
+    parallelFor(N, [&](int c0, int c1) {
+        for (int c = c0; c < c1; c++) {
+            const int k0 = cfs[c], deg = cfs[c + 1] - k0;
+            for (int j = 0; j < W; j++) {
+                int m = -1;
+                if (j < deg) {
+                    const int f = cfi[k0 + j];
+                    if (owner[f] == c) m = neighbor[f];
+                    else if (neighbor[f] == c) m = owner[f];
+                }
+                nb[(size_t)j * N + c] = m;
+            }
+        }
+    });
+    return nb;
+}
+
+SweepTiles buildSweepTiles(int N, int W, const int32_t* nb, const double* cz, const double* cr, int S, int cap,
+                           int tileCells, const int32_t* caseStart, int nCases) {
+    SweepTiles t;
+    t.S = S;
+    t.cap = cap;
+    t.tileStart.assign(1, 0);
+    if (N <= 0 || W < 1 || W > 4 || S < 1 || cap < 1 || cap >= 0xFFFF || tileCells < 1) return t;
+    double z0 = cz[0], z1 = cz[0], r0 = cr[0], r1 = cr[0];
+    for (int n = 1; n < N; n++) {
+        z0 = std::min(z0, cz[n]);
+        z1 = std::max(z1, cz[n]);
+        r0 = std::min(r0, cr[n]);
+        r1 = std::max(r1, cr[n]);
+    }
+    const double span = std::max(z1 - z0, r1 - r0);
+    const double sc = span > 0.0 ? 65535.0 / span : 0.0;
+    std::vector<uint32_t> key((size_t)N);
+    parallelFor(N, [&](int b, int e) {
+        for (int n = b; n < e; n++) {
+            const double qz = (cz[n] - z0) * sc, qr = (cr[n] - r0) * sc;
+            const uint32_t iz = qz >= 0.0 ? (uint32_t)std::min(qz, 65535.0) : 0u;
+            const uint32_t ir = qr >= 0.0 ? (uint32_t)std::min(qr, 65535.0) : 0u;
+            key[(size_t)n] = spreadBits16(iz) | (spreadBits16(ir) << 1);
+        }
+    });
+    // stable LSD radix sort of the cells by key, two 16-bit digits
+    std::vector<int32_t> order((size_t)N), tmp((size_t)N);
+    std::iota(order.begin(), order.end(), 0);
+    std::vector<int32_t> cnt(65537);
+    for (int shift = 0; shift < 32; shift += 16) {
+        std::fill(cnt.begin(), cnt.end(), 0);
+        for (int n = 0; n < N; n++) cnt[((key[(size_t)order[(size_t)n]] >> shift) & 0xFFFFu) + 1]++;
+        for (int d = 0; d < 65536; d++) cnt[(size_t)d + 1] += cnt[(size_t)d];
+        for (int n = 0; n < N; n++) {
+            const int32_t c = order[(size_t)n];
+            tmp[(size_t)cnt[(key[(size_t)c] >> shift) & 0xFFFFu]++] = c;
+        }
+        order.swap(tmp);
+    }
+    if (nCases > 1) {  // stable by case: the curve of case 0, then of case 1, ...
+        std::vector<int32_t> at((size_t)nCases + 1);
+        std::copy(caseStart, caseStart + nCases + 1, at.begin());
+        for (int n = 0; n < N; n++) {
+            const int32_t c = order[(size_t)n];
+            const int k = (int)(std::upper_bound(caseStart, caseStart + nCases + 1, c) - caseStart) - 1;
+            tmp[(size_t)at[(size_t)k]++] = c;
+        }
+        order.swap(tmp);
+    }
+    const int nRuns = (N + tileCells - 1) / tileCells;
+    std::vector<TileRun> runs((size_t)nRuns);
+    std::vector<char> ok((size_t)nRuns, 1);
+    parallelFor(nRuns, [&](int rb, int re) {
+        LocalMap map(cap + 1);
+        std::vector<int32_t> cells;
+        for (int r = rb; r < re; r++) {
+            const int a = r * tileCells, b = std::min(N, a + tileCells);
+            ok[(size_t)r] = buildTileRun(order.data(), a, b, N, W, nb, S, cap, map, cells, runs[(size_t)r]);
+        }
+    }, 4);
+    for (char o : ok)
+        if (!o) return t;
+    for (const TileRun& r : runs) {
+        for (int32_t c : r.count) t.tileStart.push_back(t.tileStart.back() + c);
+        t.layerEnd.insert(t.layerEnd.end(), r.layerEnd.begin(), r.layerEnd.end());
+        t.gid.insert(t.gid.end(), r.gid.begin(), r.gid.end());
+        t.lnb.insert(t.lnb.end(), r.lnb.begin(), r.lnb.end());
+    }
+    return t;
+}
+
 int greedyColoring(const GridLevel& g, std::vector<int32_t>& color) {
     const int N = g.nCells;
     color.assign((size_t)N, -1);

@@ -21,9 +21,9 @@ namespace axisim {
 // thread (up to 16); small ranges run on the calling thread. Each index is
 // handled by exactly one call, so results do not depend on the split.
 template <class Fn>
-void parallelFor(int n, Fn&& fn) {
+void parallelFor(int n, Fn&& fn, int grain = 16384) {
     const unsigned hw = std::thread::hardware_concurrency();
-    const int nt = std::max(1, std::min({(int)(hw ? hw : 1), 16, n / 16384}));
+    const int nt = std::max(1, std::min({(int)(hw ? hw : 1), 16, n / std::max(grain, 1)}));
     if (nt <= 1) {
         fn(0, n);
         return;
@@ -119,6 +119,36 @@ std::vector<GridLevel> buildHierarchy(GridLevel finest);
 // Every level of every case is then exactly its standalone level.
 std::vector<GridLevel> buildBatchHierarchy(const GridLevel& finest, const std::vector<int32_t>& caseStart,
                                            std::vector<std::vector<int32_t>>& terminal);
+
+// Tiles for running several momentum Jacobi sweeps (linear_solver.cu:9-33)
+// per launch out of shared memory. Cells are ordered along a Morton curve of
+// their centres (one scale for both axes) and cut into runs of `tileCells`
+// curve positions; a tile lists its own cells (layer 0) and then halo layers
+// 1..S, layer k holding the neighbours of layer k-1 not listed before it, each
+// layer in ascending cell order. Sweep s of a launch of s' <= S sweeps updates
+// layers 0..s'-s from the values of layers 0..s'-s+1, so layer 0 ends with
+// exactly the values of s' whole-mesh sweeps. A run whose cells and halo
+// exceed `cap` local cells is halved until it fits. nb is the slot
+// neighbour block [W][N] (-1 for a boundary or unused slot), W <= 4.
+struct SweepTiles {
+    int S = 0, cap = 0;
+    std::vector<int32_t> tileStart;  // nTiles + 1 offsets into gid / lnb
+    std::vector<int32_t> layerEnd;   // S + 1 per tile: local cells in layers 0..k
+    std::vector<int32_t> gid;        // the mesh cell of each local cell
+    std::vector<uint64_t> lnb;       // slot j's local neighbour in bits 16j..16j+15, 0xFFFF for none
+    int nTiles() const { return (int)tileStart.size() - 1; }
+};
+// The slot neighbour block [W][N] of a packed mesh as the device builds it
+// (slot j of cell n: the other cell of its j-th face, -1 for a boundary face
+// or j beyond the cell's face count).
+std::vector<int32_t> slotNeighbours(int nCells, int W, const int32_t* cellFaceStart, const int32_t* cellFaceIDs,
+                                    const int32_t* faceOwner, const int32_t* faceNeighbor);
+// With nCases > 0 the cells of case c are [caseStart[c], caseStart[c+1]) and
+// the curve runs case by case, so a tile mixes cases only where one ends.
+// Empty tiles (tileStart = {0}) when some cell with its S-layer halo alone
+// exceeds cap.
+SweepTiles buildSweepTiles(int nCells, int W, const int32_t* nb, const double* cz, const double* cr, int S, int cap,
+                           int tileCells, const int32_t* caseStart = nullptr, int nCases = 0);
 
 // buildMeshColoring (memory_manger.cpp:334-409): greedy colour per cell.
 int greedyColoring(const GridLevel& g, std::vector<int32_t>& color);

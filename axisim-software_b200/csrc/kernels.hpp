@@ -99,6 +99,21 @@ void launchPrecompute(const MeshDev& m, const int32_t* cfs, const int32_t* cfi, 
 void launchBuildEll(int N, int W, const int32_t* cfs, const int32_t* cfi, const int32_t* owner,
                     const int32_t* neighbor, int32_t* sface, int32_t* snb, cudaStream_t s);
 
+// Tiles of the momentum Jacobi sweeps run several per launch from shared
+// memory (SweepTiles in host_prep.hpp, kernel in sweep_tiles.cuh): one CTA of
+// `threads` per tile, cap = K threads local cells, K = kSweepK32 (FP32) or
+// kSweepK64 (FP64); lnb holds four 16-bit local neighbour indices per cell.
+struct SweepTilesDev {
+    int nTiles = 0, S = 0, cap = 0, threads = 0;
+    const int32_t* tileStart = nullptr;
+    const int32_t* layerEnd = nullptr;
+    const int32_t* gid = nullptr;
+    const uint2* lnb = nullptr;
+};
+constexpr int kSweepK32 = 4;
+constexpr int kSweepK64 = 2;
+constexpr int kMaxSweepsPerLaunch = 8;
+
 // ---- one SIMPLE iteration ----
 void launchIterBegin(Ctl* ctl, const volatile int* hostStop, cudaStream_t s);
 // gradients of up to five fields (u, v, p, T, C) with their boundary fields
@@ -109,6 +124,12 @@ void launchMomentum(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, const BC
 void launchJacobiUV(const MeshDev& m, const Ctl* ctl, const double* AF, const double* bu, const double* bv,
                     const double* invu, const double* invv, const double* xu, const double* xv, double* yu,
                     double* yv, cudaStream_t s);
+// `sweeps` (<= t.S) Jacobi sweeps of u and v from x to y on tiles (W 3 or 4)
+void launchJacobiUVTiles(const MeshDev& m, const Ctl* ctl, const SweepTilesDev& t, int sweeps, const double* AF,
+                         const double* bu, const double* bv, const double* invu, const double* invv,
+                         const double* xu, const double* xv, double* yu, double* yv, cudaStream_t s);
+// the shared-memory size of the FP64 tile kernels (before the first launch)
+cudaError_t allowJacobiUVTiles(int cap);
 void launchGaussSeidelUV(const MeshDev& m, const Ctl* ctl, const double* AF, const double* bu, const double* bv,
                          const double* invu, const double* invv, double* xu, double* xv, const int32_t* order,
                          int begin, int count, cudaStream_t s);
@@ -213,6 +234,10 @@ void launchIRResidualUV(const MeshDev& m, const Ctl* ctl, const double* AF, cons
 void launchJacobiUV32(const MeshDev& m, const Ctl* ctl, const float* AF32, const float* ru, const float* rv,
                       const float* iu32, const float* iv32, const float* du, const float* dv, float* du2, float* dv2,
                       cudaStream_t s);
+void launchJacobiUV32Tiles(const MeshDev& m, const Ctl* ctl, const SweepTilesDev& t, int sweeps, const float* AF32,
+                           const float* ru, const float* rv, const float* iu32, const float* iv32, const float* du,
+                           const float* dv, float* du2, float* dv2, cudaStream_t s);
+cudaError_t allowJacobiUV32Tiles(int cap);
 void launchIRUpdateUV(const Ctl* ctl, int N, double* u, double* v, const float* du, const float* dv, cudaStream_t s);
 
 // ---- flexible CG on the p' system, FP32 V-cycle preconditioner (krylov.cu) ----

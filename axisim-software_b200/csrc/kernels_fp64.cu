@@ -21,6 +21,7 @@
 
 #include "face.cuh"
 #include "kernels.hpp"
+#include "sweep_tiles.cuh"
 
 namespace axisim {
 
@@ -1149,6 +1150,14 @@ void launchJacobiUV(const MeshDev& m, const Ctl* ctl, const double* AF, const do
     else if (m.W == 3) launchPDL(k_jacobi_uv<3>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
     else launchPDL(k_jacobi_uv_wide, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
 }
+
+void launchJacobiUVTiles(const MeshDev& m, const Ctl* ctl, const SweepTilesDev& t, int sweeps, const double* AF,
+                         const double* bu, const double* bv, const double* invu, const double* invv,
+                         const double* xu, const double* xv, double* yu, double* yv, cudaStream_t s) {
+    launchJacobiUVTilesT<double, kSweepK64>(m, ctl, t, sweeps, AF, bu, bv, invu, invv, xu, xv, yu, yv, s);
+}
+
+cudaError_t allowJacobiUVTiles(int cap) { return allowJacobiUVTilesSmem<double, kSweepK64>(cap); }
 
 void launchGaussSeidelUV(const MeshDev& m, const Ctl* ctl, const double* AF, const double* bu, const double* bv,
                          const double* iu, const double* iv, double* xu, double* xv, const int32_t* order, int begin,

@@ -14,6 +14,7 @@
 #include <cmath>
 
 #include "kernels.hpp"
+#include "sweep_tiles.cuh"
 
 namespace axisim {
 
@@ -141,9 +142,9 @@ __global__ void __launch_bounds__(kThreads) k_jacobi_uv32(int N, int W, const in
         float vu = ru[n], vv = rv[n];
 #pragma unroll
         for (int j = 0; j < WC; j++)
-            if (k[j] >= 0) {
-                vu -= a[j] * gu[j];
-                vv -= a[j] * gv[j];
+            if (k[j] >= 0) {  // one rounding per slot, as the tile kernel (sweep_tiles.cuh)
+                vu = __fmaf_rn(-a[j], gu[j], vu);
+                vv = __fmaf_rn(-a[j], gv[j], vv);
             }
         const float au = iu[n], av = iv[n];
         yu[n] = (au != 0.f) ? vu * au : xu[n];
@@ -154,8 +155,8 @@ __global__ void __launch_bounds__(kThreads) k_jacobi_uv32(int N, int W, const in
             const size_t s = (size_t)j * N + n;
             const int k = snb[s];
             if (k >= 0) {
-                vu -= AF[s] * xu[k];
-                vv -= AF[s] * xv[k];
+                vu = __fmaf_rn(-AF[s], xu[k], vu);
+                vv = __fmaf_rn(-AF[s], xv[k], vv);
             }
         }
         const float au = iu[n], av = iv[n];
@@ -216,6 +217,14 @@ void launchJacobiUV32(const MeshDev& m, const Ctl* ctl, const float* AF32, const
         launchPDL(k_jacobi_uv32<0>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF32, ru, rv, iu32, iv32, du, dv,
                                                             du2, dv2);
 }
+
+void launchJacobiUV32Tiles(const MeshDev& m, const Ctl* ctl, const SweepTilesDev& t, int sweeps, const float* AF32,
+                           const float* ru, const float* rv, const float* iu32, const float* iv32, const float* du,
+                           const float* dv, float* du2, float* dv2, cudaStream_t s) {
+    launchJacobiUVTilesT<float, kSweepK32>(m, ctl, t, sweeps, AF32, ru, rv, iu32, iv32, du, dv, du2, dv2, s);
+}
+
+cudaError_t allowJacobiUV32Tiles(int cap) { return allowJacobiUVTilesSmem<float, kSweepK32>(cap); }
 
 void launchIRUpdateUV(const Ctl* ctl, int N, double* u, double* v, const float* du, const float* dv, cudaStream_t s) {
     launchPDL(k_ir_update_uv, dim3(blocksFor(N)), dim3(kThreads), 0, s, ctl, N, u, v, du, dv);

@@ -445,6 +445,9 @@ public:
         hCfi_.assign(pm.cellFaceIDs, pm.cellFaceIDs + S);
         hOwner_.assign(pm.faceOwner, pm.faceOwner + F);
         hNeighbor_.assign(pm.faceNeighbor, pm.faceNeighbor + F);
+        hCcZ_.assign(pm.cellCenterZ, pm.cellCenterZ + N);
+        hCcR_.assign(pm.cellCenterR, pm.cellCenterR + N);
+        dropSweepTiles();
         ph.reset(new PhaseTimer(*this, "mesh_upload"));
         Arena& A = meshArena_;
         MeshDev& m = mesh_;
@@ -529,6 +532,7 @@ public:
         destroyGraph();
         batchArena_.release();
         batch_ = BatchDev{};
+        dropSweepTiles();  // the tile curve runs case by case
         // the multigrid hierarchy depends on the case layout (one per case)
         if (haveHierarchy_ && (nCases > 0 || !termRanges_.empty())) {
             mixArena_.release();
@@ -787,7 +791,15 @@ private:
     bool haveMesh_ = false;
     int N_ = 0, F_ = 0, S_ = 0, W_ = 0;
     std::vector<int32_t> hCfs_, hCfi_, hOwner_, hNeighbor_;
+    std::vector<double> hCcZ_, hCcR_;  // cell centres: the tile curve of the momentum sweeps
     Arena meshArena_, mgArena_, bcArena_;
+    // momentum Jacobi sweeps per launch out of shared memory (1: one launch
+    // per sweep), CTA size of those launches, and the tiles they run on
+    int sweepsPerLaunch_ = 4;
+    int sweepThreads_ = 1024;
+    SweepTilesDev tiles_;
+    int tilesKey_ = 0;  // cap * 8 + S the tiles were built for, 0 = none
+    Arena tileArena_;
     MeshDev mesh_;
     double *u_ = nullptr, *v_ = nullptr, *p_ = nullptr, *pp_ = nullptr, *uT_ = nullptr, *vT_ = nullptr, *ppT_ = nullptr;
     double *DU_ = nullptr, *DV_ = nullptr, *gPZ_ = nullptr, *gPR_ = nullptr, *gUZ_ = nullptr, *gUR_ = nullptr;
@@ -1217,6 +1229,57 @@ private:
     bool fp32PressureCycle() const {
         return cs_.useMultigrid && (precision_ == AXISIM_PREC_MIXED || psolve_ == AXISIM_PSOLVE_FCG);
     }
+
+    void dropSweepTiles() {
+        tileArena_.release();
+        tiles_ = SweepTilesDev{};
+        tilesKey_ = 0;
+    }
+
+    // Tiles for several momentum sweeps per launch (SweepTiles), built for
+    // the precision of the sweeps: cap = K x CTA size local cells. Runs of the
+    // cell curve are sized so the tiles fill whole waves of resident CTAs;
+    // where no tiling fits (a cell whose halo alone exceeds cap) the sweeps
+    // stay one launch each.
+    void ensureSweepTiles() {
+        const bool fp32 = precision_ == AXISIM_PREC_MIXED && cs_.type != 1;
+        const int S = sweepsPerLaunch_;
+        if (S <= 1 || cs_.type == 1 || W_ < 3 || W_ > 4 || cs_.linearMaxIter < 2) {
+            dropSweepTiles();
+            return;
+        }
+        const int cap = (fp32 ? kSweepK32 : kSweepK64) * sweepThreads_;
+        const int key = cap * 8 + S;
+        if (tilesKey_ == key) return;
+        PhaseTimer ph(*this, "sweep_tiles");
+        dropSweepTiles();
+        const std::vector<int32_t> nb =
+            slotNeighbours(N_, W_, hCfs_.data(), hCfi_.data(), hOwner_.data(), hNeighbor_.data());
+        int sms = 148;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
+        const int slots = sms * std::max(1, 1024 / sweepThreads_);  // 64 registers a thread: 1024 threads per SM
+        const int l0max = std::max(32, (int)(cap / (1.0 + 0.1 * S)));
+        const long long per = (long long)slots * l0max;
+        const int waves = (int)std::max(1LL, ((long long)N_ + per - 1) / per);
+        const int tileCells = (int)(((long long)N_ + (long long)waves * slots - 1) / ((long long)waves * slots));
+        const int nCases = hCaseStart_.empty() ? 0 : (int)hCaseStart_.size() - 1;
+        SweepTiles t = buildSweepTiles(N_, W_, nb.data(), hCcZ_.data(), hCcR_.data(), S, cap, tileCells,
+                                       nCases ? hCaseStart_.data() : nullptr, nCases);
+        tilesKey_ = key;
+        if (t.nTiles() == 0) return;
+        CK(fp32 ? allowJacobiUV32Tiles(cap) : allowJacobiUVTiles(cap));
+        Arena& A = tileArena_;
+        tiles_.nTiles = t.nTiles();
+        tiles_.S = S;
+        tiles_.cap = cap;
+        tiles_.threads = sweepThreads_;
+        tiles_.tileStart = A.upload(t.tileStart.data(), t.tileStart.size());
+        tiles_.layerEnd = A.upload(t.layerEnd.data(), t.layerEnd.size());
+        tiles_.gid = A.upload(t.gid.data(), t.gid.size());
+        tiles_.lnb = reinterpret_cast<const uint2*>(A.upload(t.lnb.data(), t.lnb.size()));
+        tileLocal_ = (double)t.gid.size();
+    }
+    double tileLocal_ = 0.0;  // local cells of all tiles (layer 0 and halo)
 
     void ensureMixedBuffers() {
         if (precision_ != AXISIM_PREC_MIXED && !fp32PressureCycle()) return;
@@ -1787,21 +1850,45 @@ private:
                                dv32_[0], stream_);
             mark("ir_residual_uv", (double)N_ * (12.0 * W_ + 64.0 + 24.0));
             int c = 0;
-            for (int k = 1; k < iters; k++) {
-                launchJacobiUV32(mesh_, ctl_, AF32m_, ru32_, rv32_, iu32_, iv32_, du32_[c], dv32_[c], du32_[1 - c],
-                                 dv32_[1 - c], stream_);
-                mark("jacobi_uv32", (double)N_ * (8.0 * W_ + 32.0));
-                c = 1 - c;
+            const int rest = iters - 1;
+            if (tiles_.nTiles > 0 && rest > 1) {
+                // the remaining sweeps in launches of at most S, as even as possible
+                const int L = (rest + tiles_.S - 1) / tiles_.S;
+                for (int q = 0; q < L; q++) {
+                    const int k = rest / L + (q < rest % L ? 1 : 0);
+                    launchJacobiUV32Tiles(mesh_, ctl_, tiles_, k, AF32m_, ru32_, rv32_, iu32_, iv32_, du32_[c],
+                                          dv32_[c], du32_[1 - c], dv32_[1 - c], stream_);
+                    mark("jacobi_uv32_tiles", (double)N_ * (4.0 * W_ + 32.0));
+                    c = 1 - c;
+                }
+            } else {
+                for (int k = 1; k < iters; k++) {
+                    launchJacobiUV32(mesh_, ctl_, AF32m_, ru32_, rv32_, iu32_, iv32_, du32_[c], dv32_[c],
+                                     du32_[1 - c], dv32_[1 - c], stream_);
+                    mark("jacobi_uv32", (double)N_ * (8.0 * W_ + 32.0));
+                    c = 1 - c;
+                }
             }
             launchIRUpdateUV(ctl_, N_, u_, v_, du32_[c], dv32_[c], stream_);
             mark("ir_update_uv", 40.0 * N_);
         } else {
             double *lu = u_, *su = uT_, *lv = v_, *sv = vT_;
-            for (int k = 0; k < iters; k++) {
-                launchJacobiUV(mesh_, ctl_, AFm_, bu_, bv_, iu_, iv_, lu, lv, su, sv, stream_);
-                mark("jacobi_uv", (double)N_ * (12.0 * W_ + 64.0));
-                std::swap(lu, su);
-                std::swap(lv, sv);
+            if (tiles_.nTiles > 0 && iters > 1) {
+                const int L = (iters + tiles_.S - 1) / tiles_.S;
+                for (int q = 0; q < L; q++) {
+                    const int k = iters / L + (q < iters % L ? 1 : 0);
+                    launchJacobiUVTiles(mesh_, ctl_, tiles_, k, AFm_, bu_, bv_, iu_, iv_, lu, lv, su, sv, stream_);
+                    mark("jacobi_uv_tiles", (double)N_ * (8.0 * W_ + 64.0));
+                    std::swap(lu, su);
+                    std::swap(lv, sv);
+                }
+            } else {
+                for (int k = 0; k < iters; k++) {
+                    launchJacobiUV(mesh_, ctl_, AFm_, bu_, bv_, iu_, iv_, lu, lv, su, sv, stream_);
+                    mark("jacobi_uv", (double)N_ * (12.0 * W_ + 64.0));
+                    std::swap(lu, su);
+                    std::swap(lv, sv);
+                }
             }
             if (lu != u_) {
                 launchCopy(ctl_, u_, lu, N_, stream_);
@@ -2070,6 +2157,18 @@ private:
 
 public:
     void testBarrierTimeout(int on) { barrierPhantom_ = on ? 1 : 0; }
+    void setMomentumSweeps(int sweepsPerLaunch, int threads) {
+        if (sweepsPerLaunch < 1 || sweepsPerLaunch > kMaxSweepsPerLaunch)
+            throw StatusError(AXISIM_E_ARG, "sweeps per launch must be 1..8");
+        if (threads != 0 && threads != 256 && threads != 512 && threads != 1024)
+            throw StatusError(AXISIM_E_ARG, "sweep CTA size must be 256, 512 or 1024 (0: default)");
+        sweepsPerLaunch_ = sweepsPerLaunch;
+        sweepThreads_ = threads ? threads : 1024;
+        dropSweepTiles();
+        destroyGraph();
+    }
+    int tileCount() const { return tiles_.nTiles; }
+
     void setVcycleKernel(int mode) {
         if (mode != AXISIM_VCYCLE_PER_PHASE && mode != AXISIM_VCYCLE_RESIDENT)
             throw StatusError(AXISIM_E_ARG, "V-cycle kernel mode must be 0 (one launch per phase) or 1 (resident)");
@@ -2106,6 +2205,7 @@ private:
         ensureMixedBuffers();
         if (cs_.useMultigrid && psolve_ == AXISIM_PSOLVE_FCG) ensureNetStats();
         if (cs_.type == 1) ensureColoring();
+        ensureSweepTiles();
         if (autotune_ && cs_.useMultigrid) {  // launch shapes are fixed in the graph: tune first
             if (fp32PressureCycle()) {
                 if (!levels32_.empty() && levels32_[0].block == 0) tuneLevels(levels32_);
@@ -2648,6 +2748,24 @@ int axisim_set_vcycle_kernel(axisim_handle* h, int32_t mode) {
     });
 }
 
+int axisim_set_momentum_sweeps(axisim_handle* h, int32_t sweepsPerLaunch, int32_t threads) {
+    if (!h) return AXISIM_E_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    return guarded(h, [&] {
+        h->s->setMomentumSweeps(sweepsPerLaunch, threads);
+        return AXISIM_OK;
+    });
+}
+
+int axisim_sweep_tiles(axisim_handle* h, int32_t* nTiles) {
+    if (!h || !nTiles) return AXISIM_E_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    return guarded(h, [&] {
+        *nTiles = h->s->tileCount();
+        return AXISIM_OK;
+    });
+}
+
 int axisim_test_barrier_timeout(axisim_handle* h, int32_t on) {
     if (!h) return AXISIM_E_ARG;
     std::lock_guard<std::mutex> lk(h->mu);
@@ -2919,6 +3037,36 @@ int64_t axisim_mg_level_maps_host(const axisim_mesh_packed* mesh, int32_t level,
         if (coarseFaceStart) std::copy(c.faceStart.begin(), c.faceStart.end(), coarseFaceStart);
         if (coarseFaceNeighbor) std::copy(c.faceNeighbor.begin(), c.faceNeighbor.end(), coarseFaceNeighbor);
         return c.nFaceRefs();
+    } catch (...) {
+        return -AXISIM_E_MESH;
+    }
+}
+
+int64_t axisim_sweep_tiles_host(const axisim_mesh_packed* mesh, int32_t S, int32_t cap, int32_t tileCells,
+                                int32_t* nTiles, int32_t* tileStart, int32_t* layerEnd, int32_t* gid, uint64_t* lnb,
+                                int64_t capacity) {
+    if (!nTiles || S < 1 || S > axisim::kMaxSweepsPerLaunch || cap < 1 || cap >= 0xFFFF || tileCells < 1)
+        return -AXISIM_E_ARG;
+    if (!connectivityOk(mesh)) return -AXISIM_E_MESH;
+    const int N = mesh->nCells;
+    int W = 0;
+    for (int c = 0; c < N; c++) W = std::max(W, mesh->cellFaceStart[c + 1] - mesh->cellFaceStart[c]);
+    if (W < 1 || W > 4) return -AXISIM_E_MESH;
+    if (!mesh->cellCenterZ || !mesh->cellCenterR) return -AXISIM_E_ARG;
+    try {
+        const std::vector<int32_t> nb = axisim::slotNeighbours(N, W, mesh->cellFaceStart, mesh->cellFaceIDs,
+                                                               mesh->faceOwner, mesh->faceNeighbor);
+        const axisim::SweepTiles t =
+            axisim::buildSweepTiles(N, W, nb.data(), mesh->cellCenterZ, mesh->cellCenterR, S, cap, tileCells);
+        *nTiles = t.nTiles();
+        const int64_t local = (int64_t)t.gid.size();
+        if (tileStart && layerEnd && gid && lnb && capacity >= local) {
+            std::copy(t.tileStart.begin(), t.tileStart.end(), tileStart);
+            std::copy(t.layerEnd.begin(), t.layerEnd.end(), layerEnd);
+            std::copy(t.gid.begin(), t.gid.end(), gid);
+            std::copy(t.lnb.begin(), t.lnb.end(), lnb);
+        }
+        return local;
     } catch (...) {
         return -AXISIM_E_MESH;
     }

@@ -256,6 +256,21 @@ int axisim_pressure_stats(axisim_handle* h, int64_t* solves, int64_t* iterations
 #define AXISIM_VCYCLE_PER_PHASE 0
 #define AXISIM_VCYCLE_RESIDENT 1
 int axisim_set_vcycle_kernel(axisim_handle* h, int32_t mode);
+/* New (the reference launches one kernel per Jacobi sweep of each momentum
+ * component, linear_solver.cu:91-146): how many of the u/v momentum Jacobi
+ * sweeps one launch runs (1..8, default 4). Above 1 the cells are cut into
+ * tiles along a space-filling curve of their centres; a launch loads a
+ * tile's coefficients once, keeps the iterate of the tile and its halo in
+ * shared memory and repeats the sweep there, each sweep on a halo one layer
+ * thinner, so the tile's own cells end with the values of that many
+ * whole-mesh sweeps (the same arithmetic, so the same results bit for bit).
+ * threads is the CTA size of those launches (256, 512 or 1024; 0 = 1024).
+ * Meshes with more than four faces on a cell, and the Gauss-Seidel momentum
+ * solver, always run one launch per sweep. */
+int axisim_set_momentum_sweeps(axisim_handle* h, int32_t sweepsPerLaunch, int32_t threads);
+/* New: the number of tiles the sweeps of the last captured solve ran on (0 =
+ * one launch per sweep). */
+int axisim_sweep_tiles(axisim_handle* h, int32_t* nTiles);
 /* Test hook for the failure path above: on = 1 makes every grid-wide barrier
  * of the resident V-cycle expect one arrival that never comes, so its waits
  * run out (after one second), the solve returns AXISIM_E_TIMEOUT and the
@@ -405,6 +420,18 @@ int64_t axisim_mg_level_maps_host(const axisim_mesh_packed* mesh, int32_t level,
                                   int32_t* fineSlotToCoarseSlot, int32_t* coarseFaceStart,
                                   int32_t* coarseFaceNeighbor);
 int axisim_coloring_host(const axisim_mesh_packed* mesh, int32_t* colorOut, size_t n);
+/* New: the tiles of several momentum sweeps per launch (see
+ * axisim_set_momentum_sweeps) for a mesh of at most four faces per cell:
+ * S halo layers, at most cap local cells a tile (< 65535), runs of tileCells
+ * curve positions. Writes *nTiles and returns the total local cells (>= 0) or
+ * -status; when every array is given and capacity >= that total, also fills
+ * tileStart (nTiles + 1 offsets), layerEnd (S + 1 cumulative layer sizes per
+ * tile), gid (mesh cell of each local cell) and lnb (slot j's local neighbour
+ * in bits 16j..16j+15, 0xFFFF for none). nTiles = 0 when some cell with its
+ * halo exceeds cap. */
+int64_t axisim_sweep_tiles_host(const axisim_mesh_packed* mesh, int32_t S, int32_t cap, int32_t tileCells,
+                                int32_t* nTiles, int32_t* tileStart, int32_t* layerEnd, int32_t* gid, uint64_t* lnb,
+                                int64_t capacity);
 
 /* ---- measurement ---- */
 /* Per-kernel statistics of the profiled iterations: launches, summed CUDA-event

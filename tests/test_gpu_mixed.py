@@ -37,10 +37,11 @@ def test_mixed_path_runs_fp32_inner_kernels():
     gpu = abi.Solver(mesh, case.bc_fields(), case.settings, precision=abi.PREC_MIXED)
     gpu.solve()
     names = {k["name"] for k in gpu.profile(1)}
-    assert {"jacobi_uv32", "ir_residual_uv", "ir_residual_pp", "ir_update_pp"} <= names
+    assert {"ir_residual_uv", "ir_residual_pp", "ir_update_pp"} <= names
+    assert names & {"jacobi_uv32", "jacobi_uv32_tiles"}
     # the coarser levels' sweeps: their own launches, or inside the resident kernel
     assert any(n.startswith(("mg_smooth", "mg_prolong_smooth", "mg_resident")) and n.endswith("32") for n in names)
-    assert "jacobi_uv" not in names
+    assert not names & {"jacobi_uv", "jacobi_uv_tiles"}
 
 
 def test_mixed_few_iterations_close_to_fp64():
