@@ -1259,9 +1259,11 @@ private:
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
         const int slots = sms * std::max(1, 1024 / sweepThreads_);  // 64 registers a thread: 1024 threads per SM
         const int l0max = std::max(32, (int)(cap / (1.0 + 0.1 * S)));
+        // whole waves of tiles when that costs at most 15 % of the tile size
         const long long per = (long long)slots * l0max;
         const int waves = (int)std::max(1LL, ((long long)N_ + per - 1) / per);
-        const int tileCells = (int)(((long long)N_ + (long long)waves * slots - 1) / ((long long)waves * slots));
+        int tileCells = (int)(((long long)N_ + (long long)waves * slots - 1) / ((long long)waves * slots));
+        if (tileCells < l0max * 85 / 100) tileCells = l0max;
         const int nCases = hCaseStart_.empty() ? 0 : (int)hCaseStart_.size() - 1;
         SweepTiles t = buildSweepTiles(N_, W_, nb.data(), hCcZ_.data(), hCcR_.data(), S, cap, tileCells,
                                        nCases ? hCaseStart_.data() : nullptr, nCases);

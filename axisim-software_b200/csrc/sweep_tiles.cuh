@@ -8,7 +8,7 @@
 // kept by thread c % blockDim.x, register slot c / blockDim.x (< K): its slot
 // coefficients, right-hand sides, inverse diagonals and the local indices of
 // its neighbours are loaded once; the iterate of every local cell lives in
-// shared memory, two buffers of `cap` (u, v) pairs. A launch of s sweeps loads
+// shared memory, two buffers of `cap` (u, v) pairs and a zero entry. A launch of s sweeps loads
 // the iterate of layers 0..s, runs sweep k over layers 0..s-k and writes
 // layer 0 back: per launch each coefficient crosses HBM once instead of s
 // times, and the halo layers are the only cells loaded twice.
@@ -42,22 +42,34 @@ __global__ void __launch_bounds__(1024) k_jacobi_uv_tiles(const Ctl* ctl, SweepT
                                                           T* __restrict__ yv) {
     using V = typename SweepVec<T>::type;
     extern __shared__ __align__(16) unsigned char sweepSmem[];
+    // two buffers of cap + 1 (u, v) pairs; entry cap of each stays zero and
+    // stands in for every missing neighbour (its slot coefficient is zeroed,
+    // so the update subtracts +0 * +0 = +0, which leaves every value -- -0
+    // and NaN included -- exactly as skipping the slot does)
     V* X0 = reinterpret_cast<V*>(sweepSmem);
-    V* X1 = X0 + t.cap;
+    V* X1 = X0 + (t.cap + 1);
     pdlEnter();
     if (ctl->done) return;
     const int base = t.tileStart[blockIdx.x];
     const int* le = t.layerEnd + (size_t)blockIdx.x * (t.S + 1);
     const int nX = le[sweeps], nA = le[sweeps - 1], n0 = le[0];
+    const unsigned none = (unsigned)t.cap;
     T a[K][WC], cu[K], cv[K], du[K], dv[K];
-    uint2 lk[K];
+    unsigned nb[K][(WC + 1) / 2];  // two local neighbour indices per word, 16 bits each
+    if (threadIdx.x == 0) {
+        V z;
+        z.x = z.y = T(0);
+        X0[t.cap] = z;
+        X1[t.cap] = z;
+    }
 #pragma unroll
     for (int i = 0; i < K; i++) {
         const int c = threadIdx.x + i * blockDim.x;
-        lk[i] = make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
         cu[i] = cv[i] = du[i] = dv[i] = T(0);
 #pragma unroll
         for (int j = 0; j < WC; j++) a[i][j] = T(0);
+#pragma unroll
+        for (int h = 0; h < (WC + 1) / 2; h++) nb[i][h] = none | (none << 16);
         if (c < nX) {
             const int g = t.gid[base + c];
             V x;
@@ -65,9 +77,15 @@ __global__ void __launch_bounds__(1024) k_jacobi_uv_tiles(const Ctl* ctl, SweepT
             x.y = xv[g];
             X0[c] = x;
             if (c < nA) {
-                lk[i] = t.lnb[base + c];
+                const uint2 w = t.lnb[base + c];
 #pragma unroll
-                for (int j = 0; j < WC; j++) a[i][j] = AF[(size_t)j * N + g];
+                for (int j = 0; j < WC; j++) {
+                    const unsigned raw = ((j < 2 ? w.x : w.y) >> (16 * (j & 1))) & 0xFFFFu;
+                    const bool has = raw != 0xFFFFu;
+                    const unsigned l = has ? raw : none;
+                    nb[i][j / 2] = (j & 1) ? ((nb[i][j / 2] & 0xFFFFu) | (l << 16)) : ((nb[i][j / 2] & 0xFFFF0000u) | l);
+                    a[i][j] = has ? AF[(size_t)j * N + g] : T(0);
+                }
                 cu[i] = bu[g];
                 cv[i] = bv[g];
                 du[i] = iu[g];
@@ -84,22 +102,15 @@ __global__ void __launch_bounds__(1024) k_jacobi_uv_tiles(const Ctl* ctl, SweepT
         for (int i = 0; i < K; i++) {
             const int c = threadIdx.x + i * blockDim.x;
             if (c < n) {
-                int k[WC];
                 V g[WC];
 #pragma unroll
-                for (int j = 0; j < WC; j++) {
-                    const unsigned w = (j < 2) ? lk[i].x : lk[i].y;
-                    k[j] = (int)(short)(w >> (16 * (j & 1)));
-                }
-#pragma unroll
-                for (int j = 0; j < WC; j++) g[j] = src[k[j] >= 0 ? k[j] : c];
+                for (int j = 0; j < WC; j++) g[j] = src[(nb[i][j / 2] >> (16 * (j & 1))) & 0xFFFFu];
                 T vu = cu[i], vv = cv[i];
 #pragma unroll
-                for (int j = 0; j < WC; j++)
-                    if (k[j] >= 0) {
-                        vu = SweepVec<T>::sub(vu, a[i][j], g[j].x);
-                        vv = SweepVec<T>::sub(vv, a[i][j], g[j].y);
-                    }
+                for (int j = 0; j < WC; j++) {
+                    vu = SweepVec<T>::sub(vu, a[i][j], g[j].x);
+                    vv = SweepVec<T>::sub(vv, a[i][j], g[j].y);
+                }
                 const V own = src[c];
                 V y;
                 y.x = (du[i] != T(0)) ? vu * du[i] : own.x;
@@ -124,7 +135,7 @@ __global__ void __launch_bounds__(1024) k_jacobi_uv_tiles(const Ctl* ctl, SweepT
 
 template <class T, int K>
 cudaError_t allowJacobiUVTilesSmem(int cap) {
-    const int bytes = 2 * cap * (int)sizeof(typename SweepVec<T>::type);
+    const int bytes = 2 * (cap + 1) * (int)sizeof(typename SweepVec<T>::type);
     cudaError_t e = cudaFuncSetAttribute(k_jacobi_uv_tiles<T, 4, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_jacobi_uv_tiles<T, 3, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -135,7 +146,7 @@ template <class T, int K>
 void launchJacobiUVTilesT(const MeshDev& m, const Ctl* ctl, const SweepTilesDev& t, int sweeps, const T* AF,
                           const T* bu, const T* bv, const T* iu, const T* iv, const T* xu, const T* xv, T* yu, T* yv,
                           cudaStream_t s) {
-    const size_t smem = 2 * (size_t)t.cap * sizeof(typename SweepVec<T>::type);
+    const size_t smem = 2 * ((size_t)t.cap + 1) * sizeof(typename SweepVec<T>::type);
     if (m.W == 4)
         launchPDL(k_jacobi_uv_tiles<T, 4, K>, dim3(t.nTiles), dim3(t.threads), smem, s, ctl, t, sweeps, m.N, AF, bu,
                   bv, iu, iv, xu, xv, yu, yv);
