@@ -573,14 +573,19 @@ class Solver:
 
     FACE_FIELDS = frozenset(("mDot", "invDPN", "wP", "dPB", "length2D", "lsqWZ", "lsqWR", "cw", "ocrWall"))
 
-    def get(self, name):
+    def get(self, name, out=None):
+        """Field `name` copied into `out` (a float64 array of the field's size,
+        e.g. in pinned memory) or into a new array."""
         if name.startswith("AF_"):
             n = len(self.mesh["cellFaceIDs"])
         elif name in self.FACE_FIELDS:
             n = self.mesh["nFaces"]
         else:
             n = self.mesh["nCells"]
-        out = np.empty(n)
+        if out is None:
+            out = np.empty(n)
+        elif out.dtype != np.float64 or out.size < n or not out.flags.c_contiguous:
+            raise AxisimError(E_ARG, "out must be a contiguous float64 array of the field's size")
         k = lib().axisim_get_field(self.h, name.encode(), out.ctypes.data_as(_f64p), n)
         if k < 0:
             self._check(int(-k))
@@ -716,8 +721,8 @@ class Solver:
         return dict(applied=a.value, fallbacks=f.value, score_net=sn.value, score_vcycle=sv.value)
 
     def set_momentum_sweeps(self, sweeps_per_launch, threads=0):
-        """Momentum Jacobi sweeps per launch (1 = one launch per sweep; default 4, run on
-        shared-memory tiles) and the CTA size of the tiled launches (0 = 1024)."""
+        """Momentum Jacobi sweeps per launch (default 1 = one launch per sweep; above 1 run
+        on shared-memory tiles) and the CTA size of the tiled launches (0 = 1024)."""
         self._check(lib().axisim_set_momentum_sweeps(self.h, sweeps_per_launch, threads))
 
     def sweep_tiles(self):

@@ -697,42 +697,44 @@ uint32_t spreadBits16(uint32_t v) {
     return v;
 }
 
-// Open-addressing map from mesh cell to local index, cleared per tile by
-// forgetting only the slots it used.
+// Open-addressing map from mesh cell to local index (key and value side by
+// side, at most half full), cleared per tile by forgetting only the slots it
+// used.
 class LocalMap {
 public:
     explicit LocalMap(int entries) {
         uint32_t size = 1024;
         while (size < 2u * (uint32_t)entries) size <<= 1;
-        key_.assign(size, -1);
-        val_.assign(size, -1);
+        slots_.assign(size, Slot{-1, -1});
         mask_ = size - 1;
     }
     void clear() {
-        for (uint32_t i : used_) key_[i] = -1;
+        for (uint32_t i : used_) slots_[i].key = -1;
         used_.clear();
     }
     bool insert(int32_t k) {  // true when k was not present
-        uint32_t i = slot(k);
-        if (key_[i] == k) return false;
-        key_[i] = k;
-        val_[i] = -1;
+        const uint32_t i = slot(k);
+        if (slots_[i].key == k) return false;
+        slots_[i] = Slot{k, -1};
         used_.push_back(i);
         return true;
     }
-    void set(int32_t k, int32_t v) { val_[slot(k)] = v; }
+    void set(int32_t k, int32_t v) { slots_[slot(k)].val = v; }
     int32_t get(int32_t k) const {
-        const uint32_t i = slot(k);
-        return key_[i] == k ? val_[i] : -1;
+        const Slot& e = slots_[slot(k)];
+        return e.key == k ? e.val : -1;
     }
 
 private:
+    struct Slot {
+        int32_t key, val;
+    };
     uint32_t slot(int32_t k) const {
         uint32_t i = ((uint32_t)k * 2654435761u) & mask_;
-        while (key_[i] != -1 && key_[i] != k) i = (i + 1) & mask_;
+        while (slots_[i].key != -1 && slots_[i].key != k) i = (i + 1) & mask_;
         return i;
     }
-    std::vector<int32_t> key_, val_;
+    std::vector<Slot> slots_;
     std::vector<uint32_t> used_;
     uint32_t mask_ = 0;
 };
@@ -839,19 +841,49 @@ SweepTiles buildSweepTiles(int N, int W, const int32_t* nb, const double* cz, co
             key[(size_t)n] = spreadBits16(iz) | (spreadBits16(ir) << 1);
         }
     });
-    // stable LSD radix sort of the cells by key, two 16-bit digits
+    // cells by key: a counting sort on the top 16 bits (a 256 x 256 grid of
+    // the bounding square; per-thread counts, so each bucket keeps ascending
+    // cell order), then buckets of more than half a run by the whole key
+    const int refine = std::max(64, tileCells / 2);
     std::vector<int32_t> order((size_t)N), tmp((size_t)N);
-    std::iota(order.begin(), order.end(), 0);
-    std::vector<int32_t> cnt(65537);
-    for (int shift = 0; shift < 32; shift += 16) {
-        std::fill(cnt.begin(), cnt.end(), 0);
-        for (int n = 0; n < N; n++) cnt[((key[(size_t)order[(size_t)n]] >> shift) & 0xFFFFu) + 1]++;
-        for (int d = 0; d < 65536; d++) cnt[(size_t)d + 1] += cnt[(size_t)d];
-        for (int n = 0; n < N; n++) {
-            const int32_t c = order[(size_t)n];
-            tmp[(size_t)cnt[(key[(size_t)c] >> shift) & 0xFFFFu]++] = c;
-        }
-        order.swap(tmp);
+    {
+        const unsigned hw = std::thread::hardware_concurrency();
+        const int nt = std::max(1, std::min({(int)(hw ? hw : 1), 16, N / 16384}));
+        const int chunk = (N + nt - 1) / nt;
+        std::vector<int32_t> cnt((size_t)nt * 65536, 0);
+        parallelFor(nt, [&](int t0, int t1) {
+            for (int t = t0; t < t1; t++)
+                for (int n = t * chunk, e = std::min(N, n + chunk); n < e; n++)
+                    cnt[(size_t)t * 65536 + (key[(size_t)n] >> 16)]++;
+        }, 1);
+        // bucket starts, then each thread's first position in every bucket
+        // (threads in order within a bucket), in row passes over the counts
+        std::vector<int32_t> bucketStart(65537, 0), at(65536, 0);
+        for (int t = 0; t < nt; t++)
+            for (int d = 0; d < 65536; d++) at[(size_t)d] += cnt[(size_t)t * 65536 + d];
+        for (int d = 0; d < 65536; d++) bucketStart[(size_t)d + 1] = bucketStart[(size_t)d] + at[(size_t)d];
+        std::copy(bucketStart.begin(), bucketStart.end() - 1, at.begin());
+        for (int t = 0; t < nt; t++)
+            for (int d = 0; d < 65536; d++) {
+                const int32_t c = cnt[(size_t)t * 65536 + d];
+                cnt[(size_t)t * 65536 + d] = at[(size_t)d];
+                at[(size_t)d] += c;
+            }
+        parallelFor(nt, [&](int t0, int t1) {
+            for (int t = t0; t < t1; t++)
+                for (int n = t * chunk, e = std::min(N, n + chunk); n < e; n++)
+                    order[(size_t)cnt[(size_t)t * 65536 + (key[(size_t)n] >> 16)]++] = n;
+        }, 1);
+        parallelFor(65536, [&](int d0, int d1) {
+            for (int d = d0; d < d1; d++) {
+                int32_t* b = order.data() + bucketStart[(size_t)d];
+                int32_t* e = order.data() + bucketStart[(size_t)d + 1];
+                if (e - b > refine)
+                    std::sort(b, e, [&](int32_t x, int32_t y) {
+                        return key[(size_t)x] != key[(size_t)y] ? key[(size_t)x] < key[(size_t)y] : x < y;
+                    });
+            }
+        }, 4096);
     }
     if (nCases > 1) {  // stable by case: the curve of case 0, then of case 1, ...
         std::vector<int32_t> at((size_t)nCases + 1);
@@ -876,12 +908,31 @@ SweepTiles buildSweepTiles(int N, int W, const int32_t* nb, const double* cz, co
     }, 4);
     for (char o : ok)
         if (!o) return t;
-    for (const TileRun& r : runs) {
-        for (int32_t c : r.count) t.tileStart.push_back(t.tileStart.back() + c);
-        t.layerEnd.insert(t.layerEnd.end(), r.layerEnd.begin(), r.layerEnd.end());
-        t.gid.insert(t.gid.end(), r.gid.begin(), r.gid.end());
-        t.lnb.insert(t.lnb.end(), r.lnb.begin(), r.lnb.end());
+    // concatenate the runs in order, copies in parallel
+    std::vector<size_t> tileOff((size_t)nRuns + 1, 0), localOff((size_t)nRuns + 1, 0);
+    for (int r = 0; r < nRuns; r++) {
+        tileOff[(size_t)r + 1] = tileOff[(size_t)r] + runs[(size_t)r].count.size();
+        localOff[(size_t)r + 1] = localOff[(size_t)r] + runs[(size_t)r].gid.size();
     }
+    const size_t nT = tileOff[(size_t)nRuns], nL = localOff[(size_t)nRuns];
+    t.tileStart.resize(nT + 1);
+    t.layerEnd.resize(nT * ((size_t)S + 1));
+    t.gid.resize(nL);
+    t.lnb.resize(nL);
+    parallelFor(nRuns, [&](int r0, int r1) {
+        for (int r = r0; r < r1; r++) {
+            const TileRun& u = runs[(size_t)r];
+            int32_t at = (int32_t)localOff[(size_t)r];
+            for (size_t k = 0; k < u.count.size(); k++) {
+                t.tileStart[tileOff[(size_t)r] + k] = at;
+                at += u.count[k];
+            }
+            std::copy(u.layerEnd.begin(), u.layerEnd.end(), t.layerEnd.begin() + (std::ptrdiff_t)(tileOff[(size_t)r] * ((size_t)S + 1)));
+            std::copy(u.gid.begin(), u.gid.end(), t.gid.begin() + (std::ptrdiff_t)localOff[(size_t)r]);
+            std::copy(u.lnb.begin(), u.lnb.end(), t.lnb.begin() + (std::ptrdiff_t)localOff[(size_t)r]);
+        }
+    }, 4);
+    t.tileStart[nT] = (int32_t)nL;
     return t;
 }
 

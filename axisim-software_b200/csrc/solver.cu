@@ -795,7 +795,7 @@ private:
     Arena meshArena_, mgArena_, bcArena_;
     // momentum Jacobi sweeps per launch out of shared memory (1: one launch
     // per sweep), CTA size of those launches, and the tiles they run on
-    int sweepsPerLaunch_ = 4;
+    int sweepsPerLaunch_ = 1;
     int sweepThreads_ = 1024;
     SweepTilesDev tiles_;
     int tilesKey_ = 0;  // cap * 8 + S the tiles were built for, 0 = none

@@ -2,10 +2,10 @@
 
 The tile kernel repeats the per-sweep kernel's arithmetic on a tile and its
 halo, so a solve with S sweeps per launch must equal the solve with one launch
-per sweep bit for bit: FP64 (and so the oracle, which the FP64 parity tests
-check with the default of four sweeps per launch), the FP32 correction sweeps
-of mixed precision, every S from 2 to 8, every CTA size, the triangle mesh
-(three faces per cell) and a batch whose tile curve runs case by case.
+per sweep (the default) bit for bit: FP64 (and so the oracle), the FP32
+correction sweeps of mixed precision, every S from 2 to 8, every CTA size, the
+triangle mesh (three faces per cell) and a batch whose tile curve runs case by
+case.
 """
 import numpy as np
 import pytest
@@ -69,10 +69,14 @@ def test_tiled_sweeps_in_a_batch_equal_one_launch_per_sweep():
         np.testing.assert_array_equal(got[f], ref[f], err_msg=f)
 
 
-def test_default_is_four_sweeps_per_launch_and_gauss_seidel_keeps_its_launches():
+def test_launch_counts_and_gauss_seidel_keeps_its_launches():
     case = cases.expansion(scale=1 / 8, max_iter=2, tol=1e-30)
     mesh = abi.multiblock(case.blocks)
     s = abi.Solver(mesh, case.bc_fields(), case.settings)
+    s.solve()
+    assert s.sweep_tiles() == 0  # default: one launch per sweep
+    assert {k["name"]: k for k in s.profile(1)}["jacobi_uv"]["launches"] == 20
+    s.set_momentum_sweeps(4)
     s.solve()
     assert s.sweep_tiles() > 0
     prof = {k["name"]: k for k in s.profile(1)}
@@ -80,6 +84,7 @@ def test_default_is_four_sweeps_per_launch_and_gauss_seidel_keeps_its_launches()
     s.close()
     gs = dict(case.settings, linearType=1)
     g = abi.Solver(mesh, case.bc_fields(), gs)
+    g.set_momentum_sweeps(4)
     g.solve()
     assert g.sweep_tiles() == 0
     g.close()
