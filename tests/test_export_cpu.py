@@ -4,6 +4,7 @@ import json
 import os
 
 import numpy as np
+import pytest
 
 from axisim import cases, export, trimesh
 import oracle
@@ -99,3 +100,50 @@ def test_triangles_and_transient_frames(tmp_path):
     assert meta["frames"] == [{"file": "frame_0000.npy", "time": 0.001}, {"file": "frame_0001.npy", "time": 0.002}]
     assert "nr" not in meta and meta["structured"] is False
     assert os.path.getsize(tmp_path / "solution.npy") % 64 == (N * 6 * 8) % 64
+
+
+def test_reference_reader_record_on_the_pipe_export(tmp_path):
+    """The same export as tests/golden/make_npy_reader_golden.py, which ran the
+    reference's own reader (tools/validation.py load_solution / load_cells) and
+    Hagen-Poiseuille analysis (poiseuille_flow / poiseuille_report,
+    validation.py:180-274) on it and recorded what they returned and printed.
+    The folder is read back the way that reader reads it (meta.json columns
+    name the solution.npy columns; points[cells] gives the cell polygons) and
+    its analysis is repeated step by step against the record."""
+    import sys
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "npy_reader_pipe10x50_fd.json")))
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_npy_reader_golden as mk
+    cols, it, conv = mk.export_pipe(str(tmp_path))
+    assert it == g["oracle_iterations"] and conv == g["oracle_converged"]
+    meta = json.load(open(tmp_path / "meta.json"))
+    sol = np.load(tmp_path / "solution.npy")
+    col = {n: i for i, n in enumerate(meta["columns"])}
+    assert meta["columns"] == g["columns"] and col == g["col"] and list(sol.shape) == g["solution_shape"]
+    pts, cells = np.load(tmp_path / "points.npy"), np.load(tmp_path / "cells.npy")
+    verts = pts[cells]
+    assert [list(pts.shape), list(cells.shape), list(verts.shape)] == [g["points_shape"], g["cells_shape"],
+                                                                      g["verts_shape"]]
+    c = lambda n: sol[:, col[n]]  # noqa: E731
+    z, r, u, vol = c("z"), c("r"), c("Axial Velocity"), c("volume")
+    rho, mu = meta["fluid"]["rho"], meta["fluid"]["mu"]
+    R = pts[:, 1].max()
+    Umean = (u * vol).sum() / vol.sum()
+    Re = rho * Umean * 2.0 * R / mu
+    zDev = 2.0 * R * (0.619 ** 1.6 + (0.0567 * Re) ** 1.6) ** (1.0 / 1.6)
+    dev = z >= zDev
+    if not dev.any():
+        dev = np.ones(len(z), bool)
+    Umean = (u[dev] * vol[dev]).sum() / vol[dev].sum()
+    UmaxDp = -c("dP/dz")[dev].mean() * R * R / (4.0 * mu)
+    Umax = 2.0 * Umean
+    prof = Umax * (1.0 - r * r / (R * R))
+    want = g["poiseuille"]
+    got = {"R": R, "Umean": Umean, "Umax": Umax, "UmaxFlux": Umax, "UmaxDp": UmaxDp, "Re": Re, "zDev": zDev,
+           "u_sum": prof.sum()}
+    for k, v in got.items():
+        assert v == pytest.approx(want[k], rel=1e-12, abs=0), k
+    assert int(dev.sum()) == want["dev_cells"]
+    res = (u - prof)[dev] / Umax
+    assert f"L2   error        = {100.0 * np.sqrt((res ** 2).mean()):.4f} % of Umax" in g["report"]
+    assert f"Linf error        = {100.0 * np.abs(res).max():.4f} % of Umax" in g["report"]
