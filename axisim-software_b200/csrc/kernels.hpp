@@ -24,7 +24,7 @@ struct LevelT {
     T* b = nullptr;
     T* x = nullptr;
     T* xNew = nullptr;
-    T* res = nullptr;          // fine residual / Galerkin diagonal scratch (N)
+    T* res = nullptr;          // fine residual (N)
     int32_t* c2c = nullptr;    // fine -> coarse (null on the coarsest level)
     // restriction / Galerkin gathers, stored on the COARSE level:
     int32_t* mStart = nullptr;  // [N+1] members of each coarse cell

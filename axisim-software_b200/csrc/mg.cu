@@ -410,15 +410,13 @@ __global__ void __launch_bounds__(kThreads) k_mg_prolong(const Ctl* ctl, int N, 
     if (c >= 0) x[n] += scale * xc[c];  // a batch's terminal cells have no coarse parent
 }
 
-// Galerkin, step 1 (coalesced over fine cells): each row's contribution to
-// its coarse diagonal, AC plus the agglomerate-internal off-diagonals in slot
-// order (multigrid.cu:371-386).
+// Galerkin (multigrid.cu:350-389) as gathers, one launch per level: thread t
+// sums the fine slots feeding coarse slot t, and the first N threads also sum
+// their members' diagonal contributions, each member's AC plus its
+// agglomerate-internal off-diagonals in slot order (multigrid.cu:371-386).
+// Sums run in the fine type and are stored in the coarse type.
 template <class TF>
-__global__ void __launch_bounds__(kThreads) k_gal_diag(const Ctl* ctl, LevelT<TF> F) {
-    pdlEnter();
-    if (ctl->done || ctl->ppSkip) return;
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= F.N) return;
+__device__ __forceinline__ TF galDiag(const LevelT<TF>& F, int n) {
     TF diag = F.AC[n];
     uint32_t mask = F.internalMask[n];
     const Slots sl = slotsOf(F, n);
@@ -427,12 +425,9 @@ __global__ void __launch_bounds__(kThreads) k_gal_diag(const Ctl* ctl, LevelT<TF
         mask &= mask - 1;
         diag += F.AF[sl.base + j * sl.stride];
     }
-    F.res[n] = diag;
+    return diag;
 }
 
-// Galerkin, step 2: one thread per coarse slot sums its feeding fine slots;
-// the first N threads also sum their members' diagonal contributions. Sums
-// run in the fine type and are stored in the coarse type.
 template <class TF, class TC>
 __global__ void __launch_bounds__(kThreads) k_gal_coarse(const Ctl* ctl, LevelT<TF> F, LevelT<TC> C) {
     pdlEnter();
@@ -445,7 +440,7 @@ __global__ void __launch_bounds__(kThreads) k_gal_coarse(const Ctl* ctl, LevelT<
     }
     if (t < C.N) {
         TF ac = TF(0);
-        for (int q = C.mStart[t]; q < C.mStart[t + 1]; q++) ac += F.res[C.mList[q]];
+        for (int q = C.mStart[t]; q < C.mStart[t + 1]; q++) ac += galDiag(F, C.mList[q]);
         C.AC[t] = (TC)ac;
     }
 }
@@ -710,7 +705,6 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_resident(Ctl* ctl, const
 
 template <class TF, class TC>
 void launchGalerkin(const Ctl* ctl, const LevelT<TF>& fine, const LevelT<TC>& coarse, cudaStream_t s) {
-    launchPDL(k_gal_diag<TF>, dim3(blocksFor(fine.N)), dim3(kThreads), 0, s, ctl, fine);
     const int n = coarse.totalSlots > coarse.N ? coarse.totalSlots : coarse.N;
     launchPDL(k_gal_coarse<TF, TC>, dim3(blocksFor(n)), dim3(kThreads), 0, s, ctl, fine, coarse);
 }

@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--bullet-only", action="store_true", help="the 485k-cell unstructured bullet leg alone")
     ap.add_argument("--accuracy-only", action="store_true",
                     help="time to 1e-6 relative L2 of the converged FP64 fields on the workload (all arms)")
+    ap.add_argument("--momentum-sweeps", type=int, default=1,
+                    help="momentum Jacobi sweeps per launch (above 1: shared-memory tiles; the default 1 is the "
+                         "faster setting measured on a B200)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="mixed: FP32 inner solves inside FP64 refinement (the workload's setting); fp64: plain")
     return ap.parse_args()
@@ -286,6 +289,8 @@ def measure(abi, mesh, bcs, settings, args, local, dist, prec, sampler=None):
     s["maxIter"] = max(3, args.warmup)
     s["resTol"] = [0.0, 0.0, 0.0]
     solver = abi.Solver(mesh, bcs, s, device=local, precision=prec)
+    if args.momentum_sweeps != 1:
+        solver.set_momentum_sweeps(args.momentum_sweeps)
     solver.solve()                       # warm-up (+ capture of the iteration graph)
     solver.set_max_iter(args.steps, tol=0.0)
     barrier(dist)
@@ -619,12 +624,15 @@ def transient_leg(abi, local, scale=1.512, warm_steps=2, timed_steps=3, max_iter
     out["fcg_fp64"]["error_vs_fp64"] = err(f)
     out["learned_mixed_fcg"], f = arm(abi.PREC_MIXED, abi.PSOLVE_FCG, tol=chosen, cap=3000, learned=True)
     out["learned_mixed_fcg"]["error_vs_fp64"] = err(f)
+    out["plain_fp64"]["within_target"] = max(out["plain_fp64"]["error_vs_fp64"].values()) <= 1e-6
+    longer = out["plain_fp64_long"]
     for k in ("mixed_fcg", "fcg_fp64", "learned_mixed_fcg"):
         out[k]["within_target"] = max(out[k]["error_vs_fp64"].values()) <= 1e-6
-        # the reference method's time over this arm's; where the reference
-        # method misses the target the ratio is a lower bound on the speed-up
-        out[k]["plain_seconds_over_arm_seconds"] = out["plain_fp64"]["seconds"] / out[k]["seconds"]
-    out["plain_fp64"]["within_target"] = max(out["plain_fp64"]["error_vs_fp64"].values()) <= 1e-6
+        # the reference method's time (ten times the iteration cap) over this
+        # arm's; where the reference method still misses the target the ratio
+        # is a lower bound on the speed-up
+        out[k]["plain_seconds_over_arm_seconds"] = longer["seconds"] / out[k]["seconds"]
+        out[k]["plain_ratio_is_lower_bound"] = not longer["within_target"]
     return out
 
 
@@ -734,7 +742,8 @@ def summary(line):
             t[k] = {"s": _r(a["seconds"]), "steps_conv": a["steps_converged"],
                     "err": _r(max(a["error_vs_fp64"].values()), 2)}
             if "plain_seconds_over_arm_seconds" in a:
-                t[k]["plain_s_over_s"] = _r(a["plain_seconds_over_arm_seconds"], 3)
+                t[k]["plain_long_s_over_s"] = _r(a["plain_seconds_over_arm_seconds"], 3)
+                t[k]["lower_bound"] = a.get("plain_ratio_is_lower_bound", False)
             if "fallback_rate" in a:
                 t[k]["fallback_rate"] = _r(a["fallback_rate"], 3)
         t["step_tol"] = tr.get("mixed_fcg", {}).get("step_tol")
@@ -810,7 +819,9 @@ def run_b200(args):
         "vs_baseline": None, "dtype": "f64+f32" if prec == abi.PREC_MIXED else "f64", "data": "synthetic",
         "config": {"workload": case.name, "cells": N, "faces": mesh["nFaces"], "precision": args.precision,
                    "convection": "second-order upwind", "gradient": "least squares",
-                   "momentum_solver": "Jacobi x20 (u,v fused)", "pressure_solver": "agglomeration MG, 3 V-cycles",
+                   "momentum_solver": "Jacobi x20 (u,v fused)" + (
+                       ", %d sweeps per launch" % args.momentum_sweeps if args.momentum_sweeps != 1 else ""),
+                   "pressure_solver": "agglomeration MG, 3 V-cycles",
                    "parallelism": f"replicas{world}" if world > 1 else "single",
                    "l2": "inputs larger than L2 (mesh + fields ~%.0f MB per iteration)" % (
                        (mesh_bytes(mesh) + N * 8 * 40) / 1e6)},
