@@ -61,36 +61,12 @@ __device__ __forceinline__ Slots slotsOf(const LevelT<T>& L, int n) {
     return Slots{n, L.N, L.W};
 }
 
-// Weighted Jacobi row, jacobiRow (multigrid.cu:447-484).
-template <class T>
-__device__ __forceinline__ T jacobiRow(const LevelT<T>& L, int n, const T* xo, T w, T bn) {
-    const T ac = L.AC[n];
-    if (fabs(ac) < tiny<T>()) return xo[n];
-    T Ax = ac * xo[n];
-    const Slots sl = slotsOf(L, n);
-    for (int j = 0; j < sl.width; j++) {
-        const int p = sl.base + j * sl.stride;
-        const int k = L.nb[p];
-        if (k != -1) Ax += L.AF[p] * xo[k];
-    }
-    return xo[n] + w * (bn - Ax) / ac;
-}
-
-// residualRaw with sign (residuals.cuh:17-48)
-template <class T>
-__device__ __forceinline__ T residualRow(const LevelT<T>& L, int n, const T* x, T bn) {
-    T Ax = L.AC[n] * x[n];
-    const Slots sl = slotsOf(L, n);
-    for (int j = 0; j < sl.width; j++) {
-        const int p = sl.base + j * sl.stride;
-        const int k = L.nb[p];
-        if (k >= 0) Ax += L.AF[p] * x[k];
-    }
-    return bn - Ax;
-}
-
-// The same rows with every slot load issued before the neighbour gathers
-// (latency-bound single-CTA tail).
+// A row's A x in the reference's order (AC x_n first, then the slots in
+// order; jacobiTest: a slot counts when its neighbour is not -1, as jacobiRow
+// tests it, else when it is >= 0, as residualRaw does). Every slot's neighbour
+// and coefficient, and then every neighbour value, is loaded before the sum
+// starts, eight slots at a time, so a row waits for two or three load
+// latencies instead of one per slot; the arithmetic is unchanged.
 template <class T>
 __device__ __forceinline__ T axEager(const LevelT<T>& L, int n, const T* x, bool jacobiTest) {
     const Slots sl = slotsOf(L, n);
@@ -119,12 +95,24 @@ __device__ __forceinline__ T axEager(const LevelT<T>& L, int n, const T* x, bool
     return Ax;
 }
 
+// Weighted Jacobi row, jacobiRow (multigrid.cu:447-484).
 template <class T>
-__device__ __forceinline__ T jacobiRowT(const LevelT<T>& L, int n, const T* xo, T w, T bn) {
+__device__ __forceinline__ T jacobiRow(const LevelT<T>& L, int n, const T* xo, T w, T bn) {
     const T ac = L.AC[n];
     if (fabs(ac) < tiny<T>()) return xo[n];
     const T Ax = axEager(L, n, xo, true);
     return xo[n] + w * (bn - Ax) / ac;
+}
+
+// residualRaw with sign (residuals.cuh:17-48)
+template <class T>
+__device__ __forceinline__ T residualRow(const LevelT<T>& L, int n, const T* x, T bn) {
+    return bn - axEager(L, n, x, false);
+}
+
+template <class T>
+__device__ __forceinline__ T jacobiRowT(const LevelT<T>& L, int n, const T* xo, T w, T bn) {
+    return jacobiRow(L, n, xo, w, bn);
 }
 
 // Level 0 ([W][N] slots, W fixed at compile time): loads issued before gathers.
@@ -249,10 +237,26 @@ __device__ __forceinline__ void terminalBody(const LevelT<T>& L, T* x, T w, int 
             }
             T Ax = ac * xo[i];
             const Slots sl = slotsOf(L, n);
-            for (int j = 0; j < sl.width; j++) {
-                const int p = sl.base + j * sl.stride;
-                const int k = L.nb[p];
-                if (k != -1) Ax += L.AF[p] * xo[k - s0];
+            constexpr int kU = 8;
+            for (int j0 = 0; j0 < sl.width; j0 += kU) {  // loads first, sums in slot order
+                int k[kU];
+                T a[kU], g[kU];
+#pragma unroll
+                for (int j = 0; j < kU; j++) {
+                    if (j0 + j < sl.width) {
+                        const int p = sl.base + (j0 + j) * sl.stride;
+                        k[j] = __ldg(L.nb + p);
+                        a[j] = __ldg(L.AF + p);
+                    } else {
+                        k[j] = -1;
+                        a[j] = T(0);
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < kU; j++) g[j] = xo[k[j] >= 0 ? k[j] - s0 : i];
+#pragma unroll
+                for (int j = 0; j < kU; j++)
+                    if (k[j] != -1) Ax += a[j] * g[j];
             }
             xn[i] = xo[i] + w * (L.b[n] - Ax) / ac;
         }
@@ -326,9 +330,17 @@ template <class T>
 __device__ __forceinline__ void gatherResCell(int c, const LevelT<T>& F, const T* __restrict__ xf, const LevelT<T>& C,
                                               T* xCur, T* xAlt, int firstSweep, T w) {
     T sum = T(0);
-    for (int q = C.mStart[c]; q < C.mStart[c + 1]; q++) {
-        const int m = C.mList[q];
-        sum += residualRow(F, m, xf, F.b[m]);
+    const int q0 = C.mStart[c], q1 = C.mStart[c + 1];
+    for (int q = q0; q < q1; q += 2) {  // two members' rows at once, summed in member order
+        T r[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int m = (q + u < q1) ? C.mList[q + u] : -1;
+            r[u] = (m >= 0) ? residualRow(F, m, xf, F.b[m]) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++)
+            if (q + u < q1) sum += r[u];
     }
     gatherFinish(c, C, xCur, xAlt, firstSweep, w, sum);
 }
@@ -367,13 +379,32 @@ __device__ __forceinline__ T prolongSmoothRow(const LevelT<T>& L, int n, const T
     if (fabs(ac) < tiny<T>()) return xn;
     T Ax = ac * xn;
     const Slots sl = slotsOf(L, n);
-    for (int j = 0; j < sl.width; j++) {
-        const int p = sl.base + j * sl.stride;
-        const int k = L.nb[p];
-        if (k != -1) {
-            const int ck = L.c2c[k];
-            Ax += L.AF[p] * (ck >= 0 ? x[k] + scale * xc[ck] : x[k]);
+    constexpr int kU = 8;
+    for (int j0 = 0; j0 < sl.width; j0 += kU) {  // loads first, eight slots at a time; sums in slot order
+        int k[kU], ck[kU];
+        T a[kU], gx[kU], gc[kU];
+#pragma unroll
+        for (int j = 0; j < kU; j++) {
+            if (j0 + j < sl.width) {
+                const int p = sl.base + (j0 + j) * sl.stride;
+                k[j] = __ldg(L.nb + p);
+                a[j] = __ldg(L.AF + p);
+            } else {
+                k[j] = -1;
+                a[j] = T(0);
+            }
         }
+#pragma unroll
+        for (int j = 0; j < kU; j++) {
+            const int m = k[j] >= 0 ? k[j] : n;
+            ck[j] = L.c2c[m];
+            gx[j] = x[m];
+        }
+#pragma unroll
+        for (int j = 0; j < kU; j++) gc[j] = xc[ck[j] >= 0 ? ck[j] : 0];
+#pragma unroll
+        for (int j = 0; j < kU; j++)
+            if (k[j] != -1) Ax += a[j] * (ck[j] >= 0 ? gx[j] + scale * gc[j] : gx[j]);
     }
     return xn + w * (L.b[n] - Ax) / ac;
 }
@@ -418,12 +449,16 @@ __global__ void __launch_bounds__(kThreads) k_mg_prolong(const Ctl* ctl, int N, 
 template <class TF>
 __device__ __forceinline__ TF galDiag(const LevelT<TF>& F, int n) {
     TF diag = F.AC[n];
-    uint32_t mask = F.internalMask[n];
+    const uint32_t mask = F.internalMask[n];
     const Slots sl = slotsOf(F, n);
-    while (mask) {
-        const int j = __ffs(mask) - 1;
-        mask &= mask - 1;
-        diag += F.AF[sl.base + j * sl.stride];
+    constexpr int kU = 8;
+    for (int j0 = 0; j0 < sl.width; j0 += kU) {  // the slots' loads first, sums in slot order
+        TF a[kU];
+#pragma unroll
+        for (int j = 0; j < kU; j++) a[j] = (j0 + j < sl.width) ? __ldg(F.AF + sl.base + (j0 + j) * sl.stride) : TF(0);
+#pragma unroll
+        for (int j = 0; j < kU; j++)
+            if (j0 + j < 32 && ((mask >> (j0 + j)) & 1u)) diag += a[j];
     }
     return diag;
 }
@@ -440,7 +475,15 @@ __global__ void __launch_bounds__(kThreads) k_gal_coarse(const Ctl* ctl, LevelT<
     }
     if (t < C.N) {
         TF ac = TF(0);
-        for (int q = C.mStart[t]; q < C.mStart[t + 1]; q++) ac += galDiag(F, C.mList[q]);
+        const int q0 = C.mStart[t], q1 = C.mStart[t + 1];
+        for (int q = q0; q < q1; q += 4) {  // four members' contributions at once, summed in member order
+            TF d[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) d[u] = (q + u < q1) ? galDiag(F, C.mList[q + u]) : TF(0);
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (q + u < q1) ac += d[u];
+        }
         C.AC[t] = (TC)ac;
     }
 }
