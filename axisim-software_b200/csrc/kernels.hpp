@@ -180,6 +180,16 @@ void launchScalarResidual(const MeshDev& m, const Ctl* ctl, int ns, int first, c
 // Galerkin P^T A P from a fine level of type TF into a coarse level of type TC
 template <class TF, class TC>
 void launchGalerkin(const Ctl* ctl, const LevelT<TF>& fine, const LevelT<TC>& coarse, cudaStream_t s);
+// Galerkin of a chain of small levels (lv[i] -> lv[i+1], i < count - 1) in one
+// single-CTA launch, level by level: the coarse operators of the V-cycle
+// tail, each at most 1024 cells, without a launch per level.
+template <class T>
+struct GalChainArgsT {
+    int count = 0;
+    LevelT<T> lv[kMaxTail + 1];
+};
+template <class T>
+void launchGalerkinChain(const Ctl* ctl, const GalChainArgsT<T>& a, cudaStream_t s);
 template <class T>
 void launchMGSmooth(const Ctl* ctl, const LevelT<T>& L, const T* x, T* y, T w, cudaStream_t s);
 template <class T>

@@ -903,7 +903,8 @@ __global__ void __launch_bounds__(kThreads) k_iter_end(Ctl* ctl, const double* p
                                ctl->resNormS[0] == 2, 0, ctl->resNormS[1] == 2, 0};
         double acc[NQ];
         for (int q = 0; q < NQ; q++) acc[q] = isMax[q] ? -INFINITY : 0.0;
-        for (int i = threadIdx.x; i < nBlocks; i += blockDim.x) {
+#pragma unroll 4
+        for (int i = threadIdx.x; i < nBlocks; i += blockDim.x) {  // unrolled: the loads of four rows in flight
             for (int q = 0; q < kResQ; q++) acc[q] = combine(acc[q], partial[(size_t)i * kResQ + q], isMax[q]);
             if (partialS)
                 for (int q = 0; q < kResS; q++)

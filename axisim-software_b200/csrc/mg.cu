@@ -446,7 +446,7 @@ __global__ void __launch_bounds__(kThreads) k_mg_prolong(const Ctl* ctl, int N, 
 // their members' diagonal contributions, each member's AC plus its
 // agglomerate-internal off-diagonals in slot order (multigrid.cu:371-386).
 // Sums run in the fine type and are stored in the coarse type.
-template <class TF>
+template <class TF, bool NC = true>
 __device__ __forceinline__ TF galDiag(const LevelT<TF>& F, int n) {
     TF diag = F.AC[n];
     const uint32_t mask = F.internalMask[n];
@@ -455,7 +455,10 @@ __device__ __forceinline__ TF galDiag(const LevelT<TF>& F, int n) {
     for (int j0 = 0; j0 < sl.width; j0 += kU) {  // the slots' loads first, sums in slot order
         TF a[kU];
 #pragma unroll
-        for (int j = 0; j < kU; j++) a[j] = (j0 + j < sl.width) ? __ldg(F.AF + sl.base + (j0 + j) * sl.stride) : TF(0);
+        for (int j = 0; j < kU; j++) {
+            const TF* p = F.AF + sl.base + (j0 + j) * sl.stride;
+            a[j] = (j0 + j < sl.width) ? (NC ? __ldg(p) : *p) : TF(0);
+        }
 #pragma unroll
         for (int j = 0; j < kU; j++)
             if (j0 + j < 32 && ((mask >> (j0 + j)) & 1u)) diag += a[j];
@@ -463,11 +466,10 @@ __device__ __forceinline__ TF galDiag(const LevelT<TF>& F, int n) {
     return diag;
 }
 
-template <class TF, class TC>
-__global__ void __launch_bounds__(kThreads) k_gal_coarse(const Ctl* ctl, LevelT<TF> F, LevelT<TC> C) {
-    pdlEnter();
-    if (ctl->done || ctl->ppSkip) return;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+// NC: the fine level's coefficients were written by an earlier kernel, so
+// they may go through the read-only cache
+template <class TF, class TC, bool NC>
+__device__ __forceinline__ void galCoarseCell(const LevelT<TF>& F, const LevelT<TC>& C, int t) {
     if (t < C.totalSlots) {
         TF af = TF(0);
         for (int q = C.gStart[t]; q < C.gStart[t + 1]; q++) af += F.AF[C.gList[q]];
@@ -479,12 +481,35 @@ __global__ void __launch_bounds__(kThreads) k_gal_coarse(const Ctl* ctl, LevelT<
         for (int q = q0; q < q1; q += 4) {  // four members' contributions at once, summed in member order
             TF d[4];
 #pragma unroll
-            for (int u = 0; u < 4; u++) d[u] = (q + u < q1) ? galDiag(F, C.mList[q + u]) : TF(0);
+            for (int u = 0; u < 4; u++) d[u] = (q + u < q1) ? galDiag<TF, NC>(F, C.mList[q + u]) : TF(0);
 #pragma unroll
             for (int u = 0; u < 4; u++)
                 if (q + u < q1) ac += d[u];
         }
         C.AC[t] = (TC)ac;
+    }
+}
+
+template <class TF, class TC>
+__global__ void __launch_bounds__(kThreads) k_gal_coarse(const Ctl* ctl, LevelT<TF> F, LevelT<TC> C) {
+    pdlEnter();
+    if (ctl->done || ctl->ppSkip) return;
+    galCoarseCell<TF, TC, true>(F, C, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// The tail levels' Galerkin in one CTA: a coarse level's operator is read as
+// the next pair's fine level after the barrier (plain loads: it was written
+// in this launch).
+template <class T>
+__global__ void __launch_bounds__(kTailThreads) k_gal_chain(const Ctl* ctl, GalChainArgsT<T> a) {
+    pdlEnter();
+    if (ctl->done || ctl->ppSkip) return;
+    for (int i = 0; i + 1 < a.count; i++) {
+        const LevelT<T>& F = a.lv[i];
+        const LevelT<T>& C = a.lv[i + 1];
+        const int n = C.totalSlots > C.N ? C.totalSlots : C.N;
+        for (int t = threadIdx.x; t < n; t += blockDim.x) galCoarseCell<T, T, false>(F, C, t);
+        __syncthreads();
     }
 }
 
@@ -507,7 +532,7 @@ __device__ __forceinline__ void groupSync(int threads) {
     else asm volatile("bar.sync 1, %0;" ::"r"(threads) : "memory");
 }
 
-template <class T>
+template <class T, int RW>
 __device__ __forceinline__ void tailCoarsestGroup(const LevelT<T>& L, T*& xo, T*& xn, const T* b, T w, int sweeps,
                                                   int group);
 
@@ -519,7 +544,10 @@ template <class T>
 __device__ __forceinline__ void tailCoarsest(const LevelT<T>& L, T*& xo, T*& xn, const T* b, T w, int sweeps) {
     const int n = threadIdx.x;
     const int group = ((L.N + 31) / 32) * 32;  // threads of the warps holding rows (whole warps)
-    if (n < group) tailCoarsestGroup(L, xo, xn, b, w, sweeps, group);
+    if (n < group) {
+        if (L.W <= 8) tailCoarsestGroup<T, 8>(L, xo, xn, b, w, sweeps, group);
+        else tailCoarsestGroup<T, kRegW>(L, xo, xn, b, w, sweeps, group);
+    }
     else if (sweeps & 1) {  // the same buffer roles as the sweeping warps end with
         T* t = xo;
         xo = xn;
@@ -528,19 +556,22 @@ __device__ __forceinline__ void tailCoarsest(const LevelT<T>& L, T*& xo, T*& xn,
     __syncthreads();
 }
 
-template <class T>
+// RW register slots per row (the level's width at most). With eight, every
+// neighbour value of a sweep is read before the row's ordered sum; with
+// sixteen the reads stay inside the sum (the registers run out otherwise).
+template <class T, int RW>
 __device__ __forceinline__ void tailCoarsestGroup(const LevelT<T>& L, T*& xo, T*& xn, const T* b, T w, int sweeps,
                                                   int group) {
     const int n = threadIdx.x;
     const bool active = n < L.N;
-    T af[kRegW];
-    int nb[kRegW];
+    T af[RW];
+    int nb[RW];
     int width = 0;
     T ac = T(0), bn = T(0);
     if (active) {
         const Slots sl = slotsOf(L, n);
         width = sl.width;
-        for (int j = 0; j < kRegW; j++) {
+        for (int j = 0; j < RW; j++) {
             if (j < width) {
                 af[j] = L.AF[sl.base + j * sl.stride];
                 nb[j] = L.nb[sl.base + j * sl.stride];
@@ -559,9 +590,18 @@ __device__ __forceinline__ void tailCoarsestGroup(const LevelT<T>& L, T*& xo, T*
                 xn[n] = xo[n];
             } else {
                 T Ax = ac * xo[n];
+                if (RW <= 8) {
+                    T g[RW];
 #pragma unroll
-                for (int j = 0; j < kRegW; j++)
-                    if (j < width && nb[j] != -1) Ax += af[j] * xo[nb[j]];
+                    for (int j = 0; j < RW; j++) g[j] = xo[nb[j] >= 0 ? nb[j] : n];
+#pragma unroll
+                    for (int j = 0; j < RW; j++)
+                        if (j < width && nb[j] != -1) Ax += af[j] * g[j];
+                } else {
+#pragma unroll
+                    for (int j = 0; j < RW; j++)
+                        if (j < width && nb[j] != -1) Ax += af[j] * xo[nb[j]];
+                }
                 xn[n] = xo[n] + w * (bn - Ax) / ac;
             }
         }
@@ -753,6 +793,11 @@ void launchGalerkin(const Ctl* ctl, const LevelT<TF>& fine, const LevelT<TC>& co
 }
 
 template <class T>
+void launchGalerkinChain(const Ctl* ctl, const GalChainArgsT<T>& a, cudaStream_t s) {
+    launchPDL(k_gal_chain<T>, dim3(1), dim3(kTailThreads), 0, s, ctl, a);
+}
+
+template <class T>
 void launchMGSmooth(const Ctl* ctl, const LevelT<T>& L, const T* x, T* y, T w, cudaStream_t s) {
     const int t = tpb(L);
     if (!L.sliceOff && L.W == 4) launchPDL(k_mg_smooth_ell<T, 4>, dim3(blocksFor(L.N, t)), dim3(t), 0, s, ctl, L, x, y, w);
@@ -893,6 +938,8 @@ void launchMGTail(const Ctl* ctl, const TailArgsT<T>& a, cudaStream_t s) {
 template void launchGalerkin<double, double>(const Ctl*, const LevelT<double>&, const LevelT<double>&, cudaStream_t);
 template void launchGalerkin<double, float>(const Ctl*, const LevelT<double>&, const LevelT<float>&, cudaStream_t);
 template void launchGalerkin<float, float>(const Ctl*, const LevelT<float>&, const LevelT<float>&, cudaStream_t);
+template void launchGalerkinChain<double>(const Ctl*, const GalChainArgsT<double>&, cudaStream_t);
+template void launchGalerkinChain<float>(const Ctl*, const GalChainArgsT<float>&, cudaStream_t);
 #define AXISIM_MG_INSTANTIATE(T)                                                                               \
     template void launchMGSmooth<T>(const Ctl*, const LevelT<T>&, const T*, T*, T, cudaStream_t);               \
     template void launchMGSmoothBlock<T>(const Ctl*, const LevelT<T>&, T*, T, int, cudaStream_t);               \

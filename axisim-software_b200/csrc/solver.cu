@@ -1568,11 +1568,39 @@ private:
             launchGalerkin<double, float>(ctl_, levels_[0], levels32_[1], stream_);
             markL("mg_galerkin", 1, (double)levels_[0].N * (20.0 + 8.0 * levels_[0].W) + 12.0 * levels32_[1].totalSlots);
         }
-        for (int l = 2; l < L; l++) {
+        const int chain = galerkinChainStart(L);
+        for (int l = 2; l < chain; l++) {
             launchGalerkin<float, float>(ctl_, levels32_[(size_t)l - 1], levels32_[(size_t)l], stream_);
-            markL("mg_galerkin32", l, (double)levels32_[(size_t)l - 1].N * (12.0 + 4.0 * levels32_[(size_t)l - 1].W) +
-                                      8.0 * levels32_[(size_t)l].totalSlots);
+            markL("mg_galerkin32", l, galerkinBytes(levels32_[(size_t)l - 1], levels32_[(size_t)l]));
         }
+        if (chain < L) enqueueGalerkinChain<float>(levels32_, chain, "mg_galerkin32");
+    }
+
+    // The Galerkin steps into the tail levels (at most 1024 cells each) run in
+    // one single-CTA launch; returns the first coarse level of that chain (L:
+    // none). The chain starts at level 2 or deeper, so its first fine level is
+    // one of the cycle's own levels in either precision.
+    int galerkinChainStart(int L) const {
+        if (tailStart_ < 2 || L - tailStart_ + 1 > kMaxTail + 1) return L;
+        return tailStart_;
+    }
+    template <class T>
+    static double galerkinBytes(const LevelT<T>& f, const LevelT<T>& c) {
+        return (double)f.N * ((double)sizeof(T) * (1.0 + f.W) + 4.0) + (12.0 + sizeof(T)) * c.totalSlots +
+               (8.0 + sizeof(T)) * c.N;
+    }
+    template <class T>
+    void enqueueGalerkinChain(const std::vector<LevelT<T>>& lv, int chain, const char* name) {
+        GalChainArgsT<T> a;
+        const int L = (int)lv.size();
+        a.count = L - chain + 1;
+        double bytes = 0.0;
+        for (int i = 0; i < a.count; i++) {
+            a.lv[i] = lv[(size_t)chain - 1 + i];
+            if (i > 0) bytes += galerkinBytes(a.lv[i - 1], a.lv[i]);
+        }
+        launchGalerkinChain<T>(ctl_, a, stream_);
+        markL(name, chain, bytes);
     }
 
     void enqueueMultigridMixed() {
@@ -1715,13 +1743,14 @@ private:
             return;
         }
         const int L = (int)levels_.size();
-        for (int l = 1; l < L; l++) {
+        const int chain = galerkinChainStart(L);
+        for (int l = 1; l < chain; l++) {
             const LevelDev& f = levels_[(size_t)l - 1];
             const LevelDev& c = levels_[(size_t)l];
             launchGalerkin(ctl_, f, c, stream_);
-            markL("mg_galerkin", l, (double)f.N * (20.0 + 8.0 * std::max(1, f.W / 2)) + (double)c.totalSlots * 8.0 +
-                                    (double)c.N * 16.0);
+            markL("mg_galerkin", l, galerkinBytes(f, c));
         }
+        if (chain < L) enqueueGalerkinChain<double>(levels_, chain, "mg_galerkin");
         std::vector<double*> cur((size_t)L), alt((size_t)L);
         for (int l = 0; l < L; l++) {
             cur[(size_t)l] = levels_[(size_t)l].x;
