@@ -52,6 +52,35 @@ struct StatusError : std::runtime_error {
 // 256-byte aligned and zero-filled, out of a few large chunks (one cudaMalloc
 // and one memset per chunk instead of per buffer: set-up makes about a hundred
 // buffers per mesh).
+// Host arrays filled right after they are sized: no zero fill, and the copy
+// runs on all host threads (first touch of the pages included).
+template <class T>
+struct UninitAlloc : std::allocator<T> {
+    using std::allocator<T>::allocator;
+    template <class U>
+    struct rebind {
+        using other = UninitAlloc<U>;
+    };
+    template <class U>
+    void construct(U* p) noexcept {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+    }
+};
+using HostI32 = std::vector<int32_t, UninitAlloc<int32_t>>;
+
+template <class V, class T>
+void copyParallel(V& v, const T* src, size_t n) {
+    v.resize(n);
+    T* d = v.data();
+    axisim::parallelFor((int)std::min<size_t>(n, (size_t)INT32_MAX), [&](int b, int e) {
+        std::memcpy(d + b, src + b, (size_t)(e - b) * sizeof(T));
+    });
+}
+
 class Arena {
 public:
     ~Arena() { release(); }
@@ -72,6 +101,18 @@ public:
         void* p = static_cast<char*>(chunks_.back()) + used_;
         used_ += bytes;
         return static_cast<T*>(p);
+    }
+    // at least `bytes` of room for the next buffers in one chunk (one
+    // cudaMalloc for a set-up whose size is known instead of a chain of them)
+    void reserve(size_t bytes) {
+        bytes = (bytes + 255) & ~size_t(255);
+        if (!chunks_.empty() && used_ + bytes <= cap_) return;
+        void* p = nullptr;
+        CK(cudaMalloc(&p, bytes));
+        chunks_.push_back(p);
+        CK(cudaMemset(p, 0, bytes));
+        cap_ = bytes;
+        used_ = 0;
     }
     template <class T>
     T* upload(const T* h, size_t n) {
@@ -441,15 +482,18 @@ public:
         F_ = F;
         S_ = S;
         W_ = W;
-        hCfs_.assign(pm.cellFaceStart, pm.cellFaceStart + N + 1);
-        hCfi_.assign(pm.cellFaceIDs, pm.cellFaceIDs + S);
-        hOwner_.assign(pm.faceOwner, pm.faceOwner + F);
-        hNeighbor_.assign(pm.faceNeighbor, pm.faceNeighbor + F);
-        hCcZ_.assign(pm.cellCenterZ, pm.cellCenterZ + N);
-        hCcR_.assign(pm.cellCenterR, pm.cellCenterR + N);
+        copyParallel(hCfs_, pm.cellFaceStart, (size_t)N + 1);
+        copyParallel(hCfi_, pm.cellFaceIDs, (size_t)S);
+        copyParallel(hOwner_, pm.faceOwner, (size_t)F);
+        copyParallel(hNeighbor_, pm.faceNeighbor, (size_t)F);
         dropSweepTiles();
         ph.reset(new PhaseTimer(*this, "mesh_upload"));
         Arena& A = meshArena_;
+        // the mesh, its precomputed geometry and the fields below, in one
+        // chunk: 13 face arrays of 8 bytes and 3 of 4, 7 cell arrays of 8 and
+        // ~35 field and system arrays of 8, 4 [W][N] blocks of 8, the slot ids
+        A.reserve((size_t)F * (13 * 8 + 3 * 4 + 8) + (size_t)N * (7 * 8 + 4 + 35 * 8) +
+                  (size_t)W * N * (4 * 8 + 2 * 4) + (size_t)S * 4 + (size_t)64 * 256);
         MeshDev& m = mesh_;
         m.N = N;
         m.F = F;
@@ -790,8 +834,7 @@ private:
     // mesh
     bool haveMesh_ = false;
     int N_ = 0, F_ = 0, S_ = 0, W_ = 0;
-    std::vector<int32_t> hCfs_, hCfi_, hOwner_, hNeighbor_;
-    std::vector<double> hCcZ_, hCcR_;  // cell centres: the tile curve of the momentum sweeps
+    HostI32 hCfs_, hCfi_, hOwner_, hNeighbor_;
     Arena meshArena_, mgArena_, bcArena_;
     // momentum Jacobi sweeps per launch out of shared memory (1: one launch
     // per sweep), CTA size of those launches, and the tiles they run on
@@ -1265,7 +1308,10 @@ private:
         int tileCells = (int)(((long long)N_ + (long long)waves * slots - 1) / ((long long)waves * slots));
         if (tileCells < l0max * 85 / 100) tileCells = l0max;
         const int nCases = hCaseStart_.empty() ? 0 : (int)hCaseStart_.size() - 1;
-        SweepTiles t = buildSweepTiles(N_, W_, nb.data(), hCcZ_.data(), hCcR_.data(), S, cap, tileCells,
+        std::vector<double> cz((size_t)N_), cr((size_t)N_);  // the cell centres, for the tile curve
+        CK(cudaMemcpy(cz.data(), mesh_.ccZ, (size_t)N_ * sizeof(double), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(cr.data(), mesh_.ccR, (size_t)N_ * sizeof(double), cudaMemcpyDeviceToHost));
+        SweepTiles t = buildSweepTiles(N_, W_, nb.data(), cz.data(), cr.data(), S, cap, tileCells,
                                        nCases ? hCaseStart_.data() : nullptr, nCases);
         tilesKey_ = key;
         if (t.nTiles() == 0) return;
