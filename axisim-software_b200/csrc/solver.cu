@@ -167,6 +167,9 @@ public:
         if (ev1_) cudaEventDestroy(ev1_);
         if (stream_) cudaStreamDestroy(stream_);
         if (loopStream_) cudaStreamDestroy(loopStream_);
+        if (galStream_) cudaStreamDestroy(galStream_);
+        if (evFork_) cudaEventDestroy(evFork_);
+        if (evJoin_) cudaEventDestroy(evJoin_);
     }
 
     // Every entry point makes the handle's device current on the calling thread.
@@ -824,6 +827,13 @@ private:
 
     cudaStream_t stream_ = nullptr;
     cudaStream_t loopStream_ = nullptr;  // captures the body of the Krylov loop's WHILE node
+    // the coarse operators of the p' solve are built on a second stream of the
+    // captured graph, beside the right-hand side and the finest level's
+    // residual, and joined before the first restriction reads them
+    cudaStream_t galStream_ = nullptr;
+    cudaEvent_t evFork_ = nullptr, evJoin_ = nullptr;
+    bool galerkinForked_ = false;       // this solve's Galerkin is on galStream_
+    bool galerkinJoinPending_ = false;  // ... and stream_ has not waited for it yet
     volatile int* hostStop_ = nullptr;
     int* hostStopDev_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
@@ -1266,6 +1276,7 @@ private:
         }
     }
     int tailStart_ = -1;
+    bool galerkinThisSolve_ = true;  // false: the coarse operators of this p' solve are already built
 
     // FP32 p' hierarchy: used by the mixed-precision cycle and as the
     // preconditioner of the flexible CG solve in either precision
@@ -1494,6 +1505,7 @@ private:
             emit<T>(kOpResidual, l, x, nullptr, 0, 0.0, 0, std::string("mg_residual") + tag,
                     (double)F.N * ((4.0 + vb) * F.W + 4.0 * vb), [&] { launchMGResidual<T>(ctl_, F, x, stream_); });
         }
+        joinGalerkin();  // the coarse operators are read from here on
         if (l + 1 == tailStart_) {
             TailArgsT<T> a;
             a.first = l + 1;
@@ -1608,18 +1620,59 @@ private:
 
     // Mixed precision: every V-cycle is one refinement step on the FP64 system
     // (residual and update in FP64, the cycle for the correction in FP32).
-    void enqueueGalerkin32() {
+    void enqueueGalerkin64(cudaStream_t st) {
+        if (!galerkinThisSolve_) return;
+        const int L = (int)levels_.size();
+        const int chain = galerkinChainStart(L);
+        for (int l = 1; l < chain; l++) {
+            const LevelDev& f = levels_[(size_t)l - 1];
+            const LevelDev& c = levels_[(size_t)l];
+            launchGalerkin(ctl_, f, c, st);
+            markL("mg_galerkin", l, galerkinBytes(f, c));
+        }
+        if (chain < L) enqueueGalerkinChain<double>(levels_, chain, "mg_galerkin", st);
+    }
+
+    void enqueueGalerkin32(cudaStream_t st) {
+        if (!galerkinThisSolve_) return;
         const int L = (int)levels_.size();
         if (L > 1) {
-            launchGalerkin<double, float>(ctl_, levels_[0], levels32_[1], stream_);
+            launchGalerkin<double, float>(ctl_, levels_[0], levels32_[1], st);
             markL("mg_galerkin", 1, (double)levels_[0].N * (20.0 + 8.0 * levels_[0].W) + 12.0 * levels32_[1].totalSlots);
         }
         const int chain = galerkinChainStart(L);
         for (int l = 2; l < chain; l++) {
-            launchGalerkin<float, float>(ctl_, levels32_[(size_t)l - 1], levels32_[(size_t)l], stream_);
+            launchGalerkin<float, float>(ctl_, levels32_[(size_t)l - 1], levels32_[(size_t)l], st);
             markL("mg_galerkin32", l, galerkinBytes(levels32_[(size_t)l - 1], levels32_[(size_t)l]));
         }
-        if (chain < L) enqueueGalerkinChain<float>(levels32_, chain, "mg_galerkin32");
+        if (chain < L) enqueueGalerkinChain<float>(levels32_, chain, "mg_galerkin32", st);
+    }
+
+    // Forks this p' solve's Galerkin onto galStream_ (captured graph only: the
+    // per-kernel profile keeps one stream so every launch has its own events).
+    // The V-cycle joins it before its first restriction.
+    void forkGalerkin() {
+        const bool mixed = fp32PressureCycle();
+        if (profiling_ || !cs_.useMultigrid || psolve_ == AXISIM_PSOLVE_FCG || residentVcycle_ ||
+            levels_.size() < 2 || !galerkinThisSolve_)
+            return;
+        if (!galStream_) CK(cudaStreamCreateWithFlags(&galStream_, cudaStreamNonBlocking));
+        if (!evFork_) CK(cudaEventCreateWithFlags(&evFork_, cudaEventDisableTiming));
+        if (!evJoin_) CK(cudaEventCreateWithFlags(&evJoin_, cudaEventDisableTiming));
+        CK(cudaEventRecord(evFork_, stream_));
+        CK(cudaStreamWaitEvent(galStream_, evFork_, 0));
+        tNextLaunchPlain = true;  // its first kernel follows an event, not a kernel
+        if (mixed) enqueueGalerkin32(galStream_);
+        else enqueueGalerkin64(galStream_);
+        CK(cudaEventRecord(evJoin_, galStream_));
+        galerkinForked_ = true;
+        galerkinJoinPending_ = true;
+    }
+    void joinGalerkin() {
+        if (!galerkinJoinPending_) return;
+        CK(cudaStreamWaitEvent(stream_, evJoin_, 0));
+        galerkinJoinPending_ = false;
+        tNextLaunchPlain = true;  // the next kernel follows the join
     }
 
     // The Galerkin steps into the tail levels (at most 1024 cells each) run in
@@ -1636,7 +1689,7 @@ private:
                (8.0 + sizeof(T)) * c.N;
     }
     template <class T>
-    void enqueueGalerkinChain(const std::vector<LevelT<T>>& lv, int chain, const char* name) {
+    void enqueueGalerkinChain(const std::vector<LevelT<T>>& lv, int chain, const char* name, cudaStream_t st) {
         GalChainArgsT<T> a;
         const int L = (int)lv.size();
         a.count = L - chain + 1;
@@ -1645,12 +1698,12 @@ private:
             a.lv[i] = lv[(size_t)chain - 1 + i];
             if (i > 0) bytes += galerkinBytes(a.lv[i - 1], a.lv[i]);
         }
-        launchGalerkinChain<T>(ctl_, a, stream_);
+        launchGalerkinChain<T>(ctl_, a, st);
         markL(name, chain, bytes);
     }
 
     void enqueueMultigridMixed() {
-        enqueueGalerkin32();
+        if (!galerkinForked_) enqueueGalerkin32(stream_);
         const int L = (int)levels_.size();
         const bool coarsest0 = hier_[0].isCoarsest();
         const int first = coarsest0 ? cmg_.linearSweep : cmg_.linearPreSweep;
@@ -1677,7 +1730,7 @@ private:
     // buffers keep their parity), and the kernels of iterations past the
     // stopping point are never launched.
     void enqueuePressureFcg() {
-        enqueueGalerkin32();
+        enqueueGalerkin32(stream_);
         curProlong_ = prolongScale_;
         const bool firstSweep = (hier_[0].isCoarsest() ? cmg_.linearSweep : cmg_.linearPreSweep) >= 1;
         const int iters = cmg_.maxIter > 1 ? cmg_.maxIter : 1;
@@ -1789,14 +1842,7 @@ private:
             return;
         }
         const int L = (int)levels_.size();
-        const int chain = galerkinChainStart(L);
-        for (int l = 1; l < chain; l++) {
-            const LevelDev& f = levels_[(size_t)l - 1];
-            const LevelDev& c = levels_[(size_t)l];
-            launchGalerkin(ctl_, f, c, stream_);
-            markL("mg_galerkin", l, galerkinBytes(f, c));
-        }
-        if (chain < L) enqueueGalerkinChain<double>(levels_, chain, "mg_galerkin");
+        if (!galerkinForked_) enqueueGalerkin64(stream_);
         std::vector<double*> cur((size_t)L), alt((size_t)L);
         for (int l = 0; l < L; l++) {
             cur[(size_t)l] = levels_[(size_t)l].x;
@@ -1986,10 +2032,18 @@ private:
                 launchGradient(mesh_, ctl_, 1, phi, &bc_[3], gz, gr, grad, stream_);
                 mark("gradient_pp", gradBytes(1, grad));
             }
+            galerkinThisSolve_ = corr == 0;
+            forkGalerkin();
             launchPressureRhs(mesh_, ctl_, fluid_.rho, mDot_, DU_, DV_, gPZ_, gPR_, cross, corr == 0, bpp_, pp_, stream_);
             mark("pp_rhs", 16.0 * F_ + (4.0 * W_ + 16.0) * N_);
+            // the non-orthogonal corrector's pass solves the same p' operator
+            // with a new right-hand side: its coarse operators are the ones
+            // the first pass built
             if (cs_.useMultigrid) enqueueMultigrid();
             else enqueueLinear(pp_, ppT_, AFpp_, bpp_, ipp_);
+            joinGalerkin();  // (a V-cycle joins it before its first restriction)
+            galerkinForked_ = false;
+            galerkinThisSolve_ = true;
         }
         if (harvestEvery_ > 0 && samples_) {
             launchHarvest(ctl_, N_, harvestEvery_, sampleCap_, bpp_, pp_, ACpp_, AFpp_, mesh_.snb, W_,
