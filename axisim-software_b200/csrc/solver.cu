@@ -169,7 +169,7 @@ public:
         if (loopStream_) cudaStreamDestroy(loopStream_);
         if (galStream_) cudaStreamDestroy(galStream_);
         if (evFork_) cudaEventDestroy(evFork_);
-        if (evJoin_) cudaEventDestroy(evJoin_);
+        for (cudaEvent_t e : evGal_) cudaEventDestroy(e);
     }
 
     // Every entry point makes the handle's device current on the calling thread.
@@ -831,9 +831,11 @@ private:
     // captured graph, beside the right-hand side and the finest level's
     // residual, and joined before the first restriction reads them
     cudaStream_t galStream_ = nullptr;
-    cudaEvent_t evFork_ = nullptr, evJoin_ = nullptr;
-    bool galerkinForked_ = false;       // this solve's Galerkin is on galStream_
-    bool galerkinJoinPending_ = false;  // ... and stream_ has not waited for it yet
+    cudaEvent_t evFork_ = nullptr;
+    std::vector<cudaEvent_t> evGal_;  // recorded after each coarse level's operator is built
+    std::vector<int> galEvOf_;        // level -> the event that covers it (the chain covers several)
+    bool galerkinForked_ = false;     // this solve's Galerkin is on galStream_
+    int galJoined_ = 0;               // stream_ has waited for the operators of levels 1..galJoined_
     volatile int* hostStop_ = nullptr;
     int* hostStopDev_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
@@ -1505,7 +1507,9 @@ private:
             emit<T>(kOpResidual, l, x, nullptr, 0, 0.0, 0, std::string("mg_residual") + tag,
                     (double)F.N * ((4.0 + vb) * F.W + 4.0 * vb), [&] { launchMGResidual<T>(ctl_, F, x, stream_); });
         }
-        joinGalerkin();  // the coarse operators are read from here on
+        // level l + 1's operator is read from here on; the tail reads every
+        // level below it as well
+        joinGalerkin(l + 1 == tailStart_ ? L - 1 : l + 1);
         if (l + 1 == tailStart_) {
             TailArgsT<T> a;
             a.first = l + 1;
@@ -1618,8 +1622,13 @@ private:
         }
     }
 
-    // Mixed precision: every V-cycle is one refinement step on the FP64 system
-    // (residual and update in FP64, the cycle for the correction in FP32).
+    // After level l's operator on galStream_: the event the V-cycle waits for.
+    void galerkinBuilt(cudaStream_t st, int l, int last) {
+        if (st != galStream_ || !galerkinForked_) return;
+        CK(cudaEventRecord(evGal_[(size_t)l], st));
+        for (int k = l; k <= last; k++) galEvOf_[(size_t)k] = l;
+    }
+
     void enqueueGalerkin64(cudaStream_t st) {
         if (!galerkinThisSolve_) return;
         const int L = (int)levels_.size();
@@ -1629,8 +1638,12 @@ private:
             const LevelDev& c = levels_[(size_t)l];
             launchGalerkin(ctl_, f, c, st);
             markL("mg_galerkin", l, galerkinBytes(f, c));
+            galerkinBuilt(st, l, l);
         }
-        if (chain < L) enqueueGalerkinChain<double>(levels_, chain, "mg_galerkin", st);
+        if (chain < L) {
+            enqueueGalerkinChain<double>(levels_, chain, "mg_galerkin", st);
+            galerkinBuilt(st, chain, L - 1);
+        }
     }
 
     void enqueueGalerkin32(cudaStream_t st) {
@@ -1639,18 +1652,24 @@ private:
         if (L > 1) {
             launchGalerkin<double, float>(ctl_, levels_[0], levels32_[1], st);
             markL("mg_galerkin", 1, (double)levels_[0].N * (20.0 + 8.0 * levels_[0].W) + 12.0 * levels32_[1].totalSlots);
+            galerkinBuilt(st, 1, 1);
         }
         const int chain = galerkinChainStart(L);
         for (int l = 2; l < chain; l++) {
             launchGalerkin<float, float>(ctl_, levels32_[(size_t)l - 1], levels32_[(size_t)l], st);
             markL("mg_galerkin32", l, galerkinBytes(levels32_[(size_t)l - 1], levels32_[(size_t)l]));
+            galerkinBuilt(st, l, l);
         }
-        if (chain < L) enqueueGalerkinChain<float>(levels32_, chain, "mg_galerkin32", st);
+        if (chain < L) {
+            enqueueGalerkinChain<float>(levels32_, chain, "mg_galerkin32", st);
+            galerkinBuilt(st, chain, L - 1);
+        }
     }
 
     // Forks this p' solve's Galerkin onto galStream_ (captured graph only: the
     // per-kernel profile keeps one stream so every launch has its own events).
-    // The V-cycle joins it before its first restriction.
+    // The V-cycle waits for level l's operator just before it first restricts
+    // into level l, so the finer levels' phases overlap the coarser builds.
     void forkGalerkin() {
         const bool mixed = fp32PressureCycle();
         if (profiling_ || !cs_.useMultigrid || psolve_ == AXISIM_PSOLVE_FCG || residentVcycle_ ||
@@ -1658,20 +1677,32 @@ private:
             return;
         if (!galStream_) CK(cudaStreamCreateWithFlags(&galStream_, cudaStreamNonBlocking));
         if (!evFork_) CK(cudaEventCreateWithFlags(&evFork_, cudaEventDisableTiming));
-        if (!evJoin_) CK(cudaEventCreateWithFlags(&evJoin_, cudaEventDisableTiming));
+        const size_t L = levels_.size();
+        while (evGal_.size() < L) {
+            cudaEvent_t e = nullptr;
+            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            evGal_.push_back(e);
+        }
+        galEvOf_.assign(L, -1);
         CK(cudaEventRecord(evFork_, stream_));
         CK(cudaStreamWaitEvent(galStream_, evFork_, 0));
         tNextLaunchPlain = true;  // its first kernel follows an event, not a kernel
+        galerkinForked_ = true;
+        galJoined_ = 0;
         if (mixed) enqueueGalerkin32(galStream_);
         else enqueueGalerkin64(galStream_);
-        CK(cudaEventRecord(evJoin_, galStream_));
-        galerkinForked_ = true;
-        galerkinJoinPending_ = true;
     }
-    void joinGalerkin() {
-        if (!galerkinJoinPending_) return;
-        CK(cudaStreamWaitEvent(stream_, evJoin_, 0));
-        galerkinJoinPending_ = false;
+    // stream_ waits for the operators of levels up to l (no-op unless forked)
+    void joinGalerkin(int l) {
+        if (!galerkinForked_) return;
+        l = std::min(l, (int)galEvOf_.size() - 1);
+        if (l <= galJoined_) return;
+        const int e = galEvOf_[(size_t)l];
+        if (e < 0) return;
+        CK(cudaStreamWaitEvent(stream_, evGal_[(size_t)e], 0));
+        int covered = l;  // the event also covers the levels its launch built
+        while (covered + 1 < (int)galEvOf_.size() && galEvOf_[(size_t)covered + 1] == e) covered++;
+        galJoined_ = covered;
         tNextLaunchPlain = true;  // the next kernel follows the join
     }
 
@@ -1702,6 +1733,8 @@ private:
         markL(name, chain, bytes);
     }
 
+    // Mixed precision: every V-cycle is one refinement step on the FP64 system
+    // (residual and update in FP64, the cycle for the correction in FP32).
     void enqueueMultigridMixed() {
         if (!galerkinForked_) enqueueGalerkin32(stream_);
         const int L = (int)levels_.size();
@@ -2041,7 +2074,7 @@ private:
             // the first pass built
             if (cs_.useMultigrid) enqueueMultigrid();
             else enqueueLinear(pp_, ppT_, AFpp_, bpp_, ipp_);
-            joinGalerkin();  // (a V-cycle joins it before its first restriction)
+            joinGalerkin((int)levels_.size() - 1);  // whatever the solve did not wait for
             galerkinForked_ = false;
             galerkinThisSolve_ = true;
         }
