@@ -44,7 +44,7 @@ EXPORTS = [
     "axisim_mg_levels_host", "axisim_mg_level_maps_host", "axisim_coloring_host",
     "axisim_set_autotune", "axisim_autotune_report", "axisim_setup_profile", "axisim_profile_levels",
     "axisim_mg_batch_levels_host", "axisim_set_vcycle_kernel", "axisim_test_barrier_timeout",
-    "axisim_set_momentum_sweeps", "axisim_sweep_tiles", "axisim_sweep_tiles_host",
+    "axisim_set_momentum_sweeps", "axisim_sweep_tiles", "axisim_sweep_tiles_host", "axisim_mesh_segments",
 ]
 VAR_U, VAR_V, VAR_P, VAR_T, VAR_C = range(5)
 VAR_INDEX = {"u": VAR_U, "v": VAR_V, "p": VAR_P, "T": VAR_T, "C": VAR_C}
@@ -215,6 +215,7 @@ def lib():
             "axisim_coloring_host": (C.c_int, [C.POINTER(MeshPacked), _i32p, C.c_size_t]),
             "axisim_profile_iteration": (C.c_int, [vp, C.c_int32, C.POINTER(KernelStat), C.c_int32, _i32p]),
             "axisim_setup_profile": (C.c_int, [vp, C.POINTER(KernelStat), C.c_int32, _i32p, C.c_int32]),
+            "axisim_mesh_segments": (C.c_int, [vp, _i32p, _i32p, _i32p, _i32p]),
             "axisim_profile_levels": (C.c_int, [vp, C.c_int32, C.POINTER(KernelStat), C.c_int32, _i32p]),
             "axisim_set_batch": (C.c_int, [vp, C.c_int32, _i32p]),
             "axisim_batch_status": (C.c_int, [vp, _i32p, _f64p, C.c_int32]),
@@ -762,6 +763,15 @@ class Solver:
 
     def request_stop(self):
         return lib().axisim_request_stop(self.h)
+
+    def mesh_segments(self):
+        """The mesh's 32-cell segments as set_mesh classified them: dict of
+        segments, offset_segments (slot neighbours at fixed offsets),
+        face_segments (also affine faces) and in_use (the tables are used)."""
+        v = [C.c_int32(0) for _ in range(4)]
+        self._check(lib().axisim_mesh_segments(self.h, *(C.byref(x) for x in v)))
+        return dict(segments=v[0].value, offset_segments=v[1].value, face_segments=v[2].value,
+                    in_use=bool(v[3].value))
 
     def mg_levels(self):
         cells = np.zeros(64, np.int32)

@@ -82,7 +82,75 @@ struct MeshDev {
     const double* lsqIRR = nullptr;
     const int32_t* sface = nullptr;  // [W][N]
     const int32_t* snb = nullptr;    // [W][N]
+    const int4* sseg = nullptr;      // [(N + 31) / 32] slot offsets by segment (segNeighbours); null: none
+    const int4* ssegF = nullptr;     // [(N + 31) / 32] face of each slot at the segment's first cell (slotFaces)
+    const int* ssegM = nullptr;      // [(N + 31) / 32] face strides and owner sides (slotFaces); < 0: none
 };
+
+// Slot neighbours by 32-cell segment. Where all 32 cells n = 32s .. 32s + 31
+// of a segment have every slot's neighbour at the same offset,
+// snb[j][n] = n + d_j (the interior of a structured block), sseg[s] holds
+// d_0 .. d_3 and the sweeps form the neighbours without reading snb; every
+// other segment (a boundary, a block seam, a partial last segment, an
+// irregular numbering) holds kSegIrregular in .x and its cells read snb. A
+// warp is one segment, so its lanes take the same branch and the segment's
+// entry is one broadcast load. The neighbours, and so every result, are the
+// same either way.
+constexpr int kSegIrregular = (int)0x80000000;
+
+template <int WC>
+__device__ __forceinline__ void segNeighbours(const int4* __restrict__ seg, const int32_t* __restrict__ snb, int N,
+                                              int n, int (&k)[WC]) {
+    static_assert(WC >= 1 && WC <= 4, "segment offsets cover four slots");
+    int4 d = make_int4(kSegIrregular, 0, 0, 0);
+    if (seg) d = __ldg(seg + (n >> 5));
+    if (d.x != kSegIrregular) {
+        const int dd[4] = {d.x, d.y, d.z, d.w};
+#pragma unroll
+        for (int j = 0; j < WC; j++) k[j] = n + dd[j];
+    } else {
+#pragma unroll
+        for (int j = 0; j < WC; j++) k[j] = snb[(size_t)j * N + n];
+    }
+}
+
+// The face, owner and neighbour of each of a cell's WC slots. Where the
+// cell's segment numbers its faces affinely (ssegM[s] >= 0; on the
+// structured blocks every segment with slot offsets does): slot j's face is
+// ssegF[s].j + t_j (n - 32s) with stride t_j = 1 or 2 (bit j of ssegM[s]), and
+// the cell is that face's owner throughout the segment (bit 4 + j) or its
+// neighbour, the other cell being n + d_j. Elsewhere from sface, owner and
+// neighbor; a slot beyond the cell's faces gets face -1, and the owner and
+// neighbour read for it (face 0's) are never used. Either way the values are
+// those the face arrays hold.
+template <int WC>
+__device__ __forceinline__ void slotFaces(const MeshDev& m, int n, int (&f)[WC], int (&own)[WC], int (&nb)[WC]) {
+    static_assert(WC >= 1 && WC <= 4, "segment faces cover four slots");
+    const int s = n >> 5;
+    const int meta = m.ssegM ? __ldg(m.ssegM + s) : -1;
+    if (meta >= 0) {
+        const int4 d = __ldg(m.sseg + s);
+        const int4 b = __ldg(m.ssegF + s);
+        const int r = n & 31;
+        const int dd[4] = {d.x, d.y, d.z, d.w}, bb[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int j = 0; j < WC; j++) {
+            f[j] = bb[j] + (((meta >> j) & 1) ? 2 * r : r);
+            const bool o = (meta >> (4 + j)) & 1;
+            own[j] = o ? n : n + dd[j];
+            nb[j] = o ? n + dd[j] : n;
+        }
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < WC; j++) f[j] = m.sface[(size_t)j * m.N + n];
+#pragma unroll
+    for (int j = 0; j < WC; j++) {
+        const int g = f[j] >= 0 ? f[j] : 0;
+        own[j] = m.owner[g];
+        nb[j] = m.neighbor[g];
+    }
+}
 
 struct BCDev {
     int nGroups = 0;

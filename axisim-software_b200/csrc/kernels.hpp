@@ -19,6 +19,7 @@ struct LevelT {
     int totalSlots = 0;
     const int32_t* sliceOff = nullptr;  // null: [W][N] layout
     int32_t* nb = nullptr;
+    const int4* seg = nullptr;  // finest level: the mesh's segment offsets (segNeighbours); null elsewhere
     T* AF = nullptr;
     T* AC = nullptr;
     T* b = nullptr;
@@ -98,6 +99,9 @@ void launchPrecompute(const MeshDev& m, const int32_t* cfs, const int32_t* cfi, 
                       cudaStream_t s);
 void launchBuildEll(int N, int W, const int32_t* cfs, const int32_t* cfi, const int32_t* owner,
                     const int32_t* neighbor, int32_t* sface, int32_t* snb, cudaStream_t s);
+// the segment tables of segNeighbours and slotFaces; adds the segments without
+// slot offsets to nIrregular[0], those without affine faces to nIrregular[1]
+void launchBuildSegments(const MeshDev& m, int4* seg, int4* segF, int* segM, int* nIrregular, cudaStream_t s);
 
 // Tiles of the momentum Jacobi sweeps run several per launch from shared
 // memory (SweepTiles in host_prep.hpp, kernel in sweep_tiles.cuh): one CTA of
@@ -212,10 +216,11 @@ template <class T>
 void launchMGProlongSmoothAny(const Ctl* ctl, const LevelT<T>& fine, const T* xFine, const T* xCoarse, T* y, T w,
                               T scale, cudaStream_t s);
 // prolongation fused into the first post-smoothing sweep (ELL levels with
-// W = 3 or 4): y = smooth(x + s P e); returns false when not applicable
+// W = 3 or 4): y = smooth(x + s P e), and upd[n] += (double)y[n] when upd is
+// given; returns false when not applicable
 template <class T>
 bool launchMGProlongSmooth(const Ctl* ctl, const LevelT<T>& fine, const T* xFine, const T* xCoarse, T* y, T w,
-                           T scale, cudaStream_t s);
+                           T scale, cudaStream_t s, double* upd = nullptr);
 // the coarsest-level solve of each terminal case of a level: `sweeps` Jacobi
 // sweeps from zero, one CTA per case, written to x (cells of other cases untouched)
 template <class T>

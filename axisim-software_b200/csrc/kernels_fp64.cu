@@ -132,6 +132,55 @@ __global__ void k_build_ell(int N, int W, const int32_t* cfs, const int32_t* cfi
     }
 }
 
+// The segment tables of segNeighbours and slotFaces (device.cuh), one thread
+// per 32-cell segment; the segments without slot offsets are counted in
+// nIrregular[0], those without affine faces in nIrregular[1].
+__global__ void k_build_seg(int N, int W, const int32_t* __restrict__ snb, const int32_t* __restrict__ sface,
+                            const int32_t* __restrict__ owner, const int32_t* __restrict__ neighbor,
+                            int4* __restrict__ seg, int4* __restrict__ segF, int* __restrict__ segM,
+                            int* nIrregular) {
+    pdlEnter();
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= (N + 31) / 32) return;
+    const int a = 32 * s;
+    int d[4] = {0, 0, 0, 0};
+    bool ok = a + 32 <= N && W >= 1 && W <= 4;
+    for (int j = 0; ok && j < W; j++) {
+        d[j] = snb[(size_t)j * N + a] - a;
+        for (int c = a; c < a + 32; c++) {
+            const int k = snb[(size_t)j * N + c];
+            if (k < 0 || k - c != d[j]) {
+                ok = false;
+                break;
+            }
+        }
+    }
+    int meta = ok ? 0 : -1;
+    int fb[4] = {0, 0, 0, 0};
+    for (int j = 0; meta >= 0 && j < W; j++) {
+        const int f0 = sface[(size_t)j * N + a], t = sface[(size_t)j * N + a + 1] - f0;
+        const bool o = f0 >= 0 && owner[f0] == a;
+        bool aff = f0 >= 0 && (t == 1 || t == 2);
+        for (int c = a; aff && c < a + 32; c++) {
+            const int f = sface[(size_t)j * N + c];
+            aff = f == f0 + t * (c - a) && (o ? (owner[f] == c && neighbor[f] == c + d[j])
+                                              : (owner[f] == c + d[j] && neighbor[f] == c));
+        }
+        if (!aff) {
+            meta = -1;
+        } else {
+            fb[j] = f0;
+            meta |= (t == 2 ? 1 : 0) << j;
+            meta |= (o ? 1 : 0) << (4 + j);
+        }
+    }
+    seg[s] = ok ? make_int4(d[0], d[1], d[2], d[3]) : make_int4(kSegIrregular, 0, 0, 0);
+    segF[s] = make_int4(fb[0], fb[1], fb[2], fb[3]);
+    segM[s] = meta;
+    if (!ok) atomicAdd(nIrregular, 1);
+    if (meta < 0) atomicAdd(nIrregular + 1, 1);
+}
+
 // ---------------- iteration control ----------------
 __global__ void k_iter_begin(Ctl* ctl, const volatile int* hostStop) {
     pdlEnter();
@@ -159,11 +208,13 @@ struct GradArgs {
     double* gR[5];
 };
 
-// Bounded to 4 resident CTAs per SM up to two fields (64 registers, no
-// spills); three to five fields keep 3 (85 registers: the four face chains
-// of the least-squares loop are loaded ahead, in registers).
+// Bounded to 4 resident CTAs per SM for one field (64 registers, no spills);
+// two to five fields keep 3 (85 registers: the four face chains of the
+// least-squares loop and their other-cell values are loaded ahead, in
+// registers, with a few spills from three fields up, which measured faster
+// than 2 CTAs per SM without spills).
 template <int NF>
-__global__ void __launch_bounds__(kThreads, NF <= 2 ? 4 : 3) k_gradient(MeshDev m, const Ctl* ctl, GradArgs a,
+__global__ void __launch_bounds__(kThreads, NF == 1 ? 4 : 3) k_gradient(MeshDev m, const Ctl* ctl, GradArgs a,
                                                                        int scheme) {
     pdlEnter();
     if (ctl && ctl->done) return;
@@ -221,12 +272,13 @@ __global__ void __launch_bounds__(kThreads, NF <= 2 ? 4 : 3) k_gradient(MeshDev 
             bz[q] = br[q] = 0.0;
             phiP[q] = a.phi[q][n];
         }
-        auto face = [&](int f, int own, int nb, double wz, double wr) {
+        // pre: the other cell's values of the NF fields, loaded ahead (null: load here)
+        auto face = [&](int f, int own, int nb, double wz, double wr, const double* pre) {
             for (int q = 0; q < NF; q++) {
                 double dphi;
                 if (nb >= 0) {
                     const bool isOwner = (own == n);
-                    const double phiNb = a.phi[q][isOwner ? nb : own];
+                    const double phiNb = pre ? pre[q] : a.phi[q][isOwner ? nb : own];
                     dphi = isOwner ? (phiNb - phiP[q]) : (phiP[q] - phiNb);
                 } else {
                     dphi = boundaryFaceValue(m, f, a.bc[q], phiP[q]) - phiP[q];
@@ -239,15 +291,43 @@ __global__ void __launch_bounds__(kThreads, NF <= 2 ? 4 : 3) k_gradient(MeshDev 
         // loaded before any arithmetic, so those chains are in flight together
         int pf[4], po[4], pn[4];
         double pz[4], pr[4];
+        if (m.W == 4) {
+            slotFaces<4>(m, n, pf, po, pn);
+        } else if (m.W == 3) {
+            int f3[3], o3[3], n3[3];
+            slotFaces<3>(m, n, f3, o3, n3);
 #pragma unroll
-        for (int j = 0; j < 4; j++) pf[j] = j < m.W ? m.sface[(size_t)j * N + n] : -1;
+            for (int j = 0; j < 3; j++) {
+                pf[j] = f3[j];
+                po[j] = o3[j];
+                pn[j] = n3[j];
+            }
+            pf[3] = -1;
+            po[3] = pn[3] = -1;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) pf[j] = j < m.W ? m.sface[(size_t)j * N + n] : -1;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int f = pf[j] >= 0 ? pf[j] : 0;
+                po[j] = m.owner[f];
+                pn[j] = m.neighbor[f];
+            }
+        }
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const int f = pf[j] >= 0 ? pf[j] : 0;
-            po[j] = m.owner[f];
-            pn[j] = m.neighbor[f];
             pz[j] = m.lsqWZ[f];
             pr[j] = m.lsqWR[f];
+        }
+        // and so are those slots' other-cell values of every field (a boundary
+        // or missing slot loads the cell's own values and does not use them)
+        double pv[4][NF];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int o = (pf[j] >= 0 && pn[j] >= 0) ? (po[j] == n ? pn[j] : po[j]) : n;
+#pragma unroll
+            for (int q = 0; q < NF; q++) pv[j][q] = a.phi[q][o];
         }
         bool more = true;
 #pragma unroll
@@ -256,12 +336,12 @@ __global__ void __launch_bounds__(kThreads, NF <= 2 ? 4 : 3) k_gradient(MeshDev 
                 more = false;
                 break;
             }
-            face(pf[j], po[j], pn[j], pz[j], pr[j]);
+            face(pf[j], po[j], pn[j], pz[j], pr[j], pv[j]);
         }
         for (int j = 4; more && j < m.W; j++) {
             const int f = m.sface[(size_t)j * N + n];
             if (f < 0) break;
-            face(f, m.owner[f], m.neighbor[f], m.lsqWZ[f], m.lsqWR[f]);
+            face(f, m.owner[f], m.neighbor[f], m.lsqWZ[f], m.lsqWR[f], nullptr);
         }
         const double izz = m.lsqIZZ[n], izr = m.lsqIZR[n], irr = m.lsqIRR[n];
         for (int q = 0; q < NF; q++) {
@@ -335,13 +415,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_momentum(MeshDev m, const Ctl* 
     int pf[P], po[P], pn[P];
     double pa[P], pd[P], pm[P];
     if (WC > 0) {
-#pragma unroll
-        for (int j = 0; j < P; j++) pf[j] = m.sface[(size_t)j * N + n];
+        slotFaces<P>(m, n, pf, po, pn);
 #pragma unroll
         for (int j = 0; j < P; j++) {
             const int f = pf[j] >= 0 ? pf[j] : 0;
-            po[j] = m.owner[f];
-            pn[j] = m.neighbor[f];
             pa[j] = m.area[f];
             pd[j] = m.invDPN[f];
             pm[j] = a.conv ? a.mDot[f] : 0.0;
@@ -451,6 +528,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_momentum(MeshDev m, const Ctl* 
 // ---------------- momentum sweeps (linear_solver.cu:9-72) ----------------
 template <int WC>
 __global__ void __launch_bounds__(kThreads) k_jacobi_uv(int N, int W, const int32_t* __restrict__ snb,
+                                                        const int4* __restrict__ seg,
                                                         const Ctl* ctl, const double* __restrict__ AF,
                                                         const double* __restrict__ bu, const double* __restrict__ bv,
                                                         const double* __restrict__ iu, const double* __restrict__ iv,
@@ -464,12 +542,9 @@ __global__ void __launch_bounds__(kThreads) k_jacobi_uv(int N, int W, const int3
     // the neighbour test); a boundary slot reads its own cell and is skipped.
     int nbs[WC];
     double af[WC];
+    segNeighbours<WC>(seg, snb, N, n, nbs);
 #pragma unroll
-    for (int j = 0; j < WC; j++) {
-        const size_t s = (size_t)j * N + n;
-        nbs[j] = snb[s];
-        af[j] = AF[s];
-    }
+    for (int j = 0; j < WC; j++) af[j] = AF[(size_t)j * N + n];
     double gu[WC], gv[WC];
 #pragma unroll
     for (int j = 0; j < WC; j++) {
@@ -599,6 +674,9 @@ struct PressureArgs {
     float* AC32;
 };
 
+// WC > 0: the mesh's slot count; every slot's face, owner and neighbour come
+// first (slotFaces), the per-face work then runs in slot order as for WC = 0.
+template <int WC>
 __global__ void __launch_bounds__(kThreads) k_pressure(MeshDev m, const Ctl* ctl, BCDev bcU, BCDev bcV, BCDev bcP,
                                                        PressureArgs a) {
     pdlEnter();
@@ -607,12 +685,17 @@ __global__ void __launch_bounds__(kThreads) k_pressure(MeshDev m, const Ctl* ctl
     if (n >= m.N) return;
     const int N = m.N;
     const double rho = a.rho;
+    constexpr int P = WC > 0 ? WC : 1;
+    int pf[P], po[P], pn[P];
+    if (WC > 0) slotFaces<P>(m, n, pf, po, pn);
     double AC = 0.0;
-    for (int j = 0; j < m.W; j++) {
+#pragma unroll
+    for (int j = 0; j < (WC > 0 ? WC : 32); j++) {
+        if (WC == 0 && j >= m.W) break;
         const size_t s = (size_t)j * N + n;
-        const int f = m.sface[s];
+        const int f = WC > 0 ? pf[j] : m.sface[s];
         if (f < 0) break;
-        const int own = m.owner[f], nb = m.neighbor[f];
+        const int own = WC > 0 ? po[j] : m.owner[f], nb = WC > 0 ? pn[j] : m.neighbor[f];
         const double area = m.area[f];
         const double nz = m.nZ[f], nr = m.nR[f];
         const double Df = interpCorr(m, a.DU, a.DV, n, f, own, nb);
@@ -674,6 +757,7 @@ __global__ void __launch_bounds__(kThreads) k_pressure(MeshDev m, const Ctl* ctl
 }
 
 // createPPRhs (simple.cu:90-142) + the p' reset before the corrector loop
+template <int WC>
 __global__ void __launch_bounds__(kThreads) k_pp_rhs(MeshDev m, const Ctl* ctl, double rho, const double* mDot,
                                                      const double* DU, const double* DV, const double* gZ,
                                                      const double* gR, int cross, int zeroPP, double* bpp,
@@ -683,11 +767,16 @@ __global__ void __launch_bounds__(kThreads) k_pp_rhs(MeshDev m, const Ctl* ctl, 
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m.N) return;
     const int N = m.N;
+    constexpr int P = WC > 0 ? WC : 1;
+    int pf[P], po[P], pn[P];
+    if (WC > 0) slotFaces<P>(m, n, pf, po, pn);
     double imb = 0.0, crossSum = 0.0;
-    for (int j = 0; j < m.W; j++) {
-        const int f = m.sface[(size_t)j * N + n];
+#pragma unroll
+    for (int j = 0; j < (WC > 0 ? WC : 32); j++) {
+        if (WC == 0 && j >= m.W) break;
+        const int f = WC > 0 ? pf[j] : m.sface[(size_t)j * N + n];
         if (f < 0) break;
-        const int own = m.owner[f], nb = m.neighbor[f];
+        const int own = WC > 0 ? po[j] : m.owner[f], nb = WC > 0 ? pn[j] : m.neighbor[f];
         const double md = mDot[f];
         if (own == n) imb += md;
         else if (nb == n) imb -= md;
@@ -729,15 +818,9 @@ __global__ void __launch_bounds__(kThreads) k_correct(MeshDev m, const Ctl* ctl,
     int pf[P], po[P], pn[P];
     double pa[P];
     if (WC > 0) {
+        slotFaces<P>(m, n, pf, po, pn);
 #pragma unroll
-        for (int j = 0; j < P; j++) pf[j] = m.sface[(size_t)j * N + n];
-#pragma unroll
-        for (int j = 0; j < P; j++) {
-            const int f = pf[j] >= 0 ? pf[j] : 0;
-            po[j] = m.owner[f];
-            pn[j] = m.neighbor[f];
-            pa[j] = m.area[f];
-        }
+        for (int j = 0; j < P; j++) pa[j] = m.area[pf[j] >= 0 ? pf[j] : 0];
     }
     a.u[n] -= a.DU[n] * a.gZ[n];
     a.v[n] -= a.DV[n] * a.gR[n];
@@ -828,11 +911,8 @@ __global__ void __launch_bounds__(kThreads) k_residual(MeshDev m, const Ctl* ctl
             constexpr int P = WC > 0 ? WC : 1;
             int pb[P], pf[P], po[P], pn[P];
             double pa[P], pu[P], pv[P], pm[P];
-#pragma unroll
-            for (int j = 0; j < P; j++) {
-                pb[j] = m.snb[(size_t)j * N + n];
-                pf[j] = m.sface[(size_t)j * N + n];
-            }
+            segNeighbours<P>(m.sseg, m.snb, N, n, pb);
+            slotFaces<P>(m, n, pf, po, pn);
 #pragma unroll
             for (int j = 0; j < P; j++) {
                 const int c = pb[j] >= 0 ? pb[j] : n;
@@ -841,8 +921,6 @@ __global__ void __launch_bounds__(kThreads) k_residual(MeshDev m, const Ctl* ctl
                 pu[j] = u[c];
                 pv[j] = v[c];
                 pm[j] = mDot[f];
-                po[j] = m.owner[f];
-                pn[j] = m.neighbor[f];
             }
 #pragma unroll
             for (int j = 0; j < P; j++) {
@@ -1116,6 +1194,11 @@ void launchBuildEll(int N, int W, const int32_t* cfs, const int32_t* cfi, const 
     launchPDL(k_build_ell, dim3(blocksFor(N)), dim3(kThreads), 0, s, N, W, cfs, cfi, owner, neighbor, sface, snb);
 }
 
+void launchBuildSegments(const MeshDev& m, int4* seg, int4* segF, int* segM, int* nIrregular, cudaStream_t s) {
+    launchPDL(k_build_seg, dim3(blocksFor((m.N + 31) / 32)), dim3(kThreads), 0, s, m.N, m.W, m.snb, m.sface, m.owner,
+              m.neighbor, seg, segF, segM, nIrregular);
+}
+
 void launchIterBegin(Ctl* ctl, const volatile int* hostStop, cudaStream_t s) {
     launchPDL(k_iter_begin, dim3(1), dim3(1), 0, s, ctl, hostStop);
 }
@@ -1147,8 +1230,8 @@ void launchMomentum(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, const BC
 void launchJacobiUV(const MeshDev& m, const Ctl* ctl, const double* AF, const double* bu, const double* bv,
                     const double* iu, const double* iv, const double* xu, const double* xv, double* yu, double* yv,
                     cudaStream_t s) {
-    if (m.W == 4) launchPDL(k_jacobi_uv<4>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
-    else if (m.W == 3) launchPDL(k_jacobi_uv<3>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
+    if (m.W == 4) launchPDL(k_jacobi_uv<4>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, m.sseg, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
+    else if (m.W == 3) launchPDL(k_jacobi_uv<3>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, m.sseg, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
     else launchPDL(k_jacobi_uv_wide, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF, bu, bv, iu, iv, xu, xv, yu, yv);
 }
 
@@ -1172,13 +1255,20 @@ void launchPressureSystem(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, co
                           const double* gPR, const double* DU, const double* DV, double* AFpp, double* ACpp,
                           double* invACpp, double* mDot, float* AF32, float* AC32, cudaStream_t s) {
     PressureArgs a{rho, u, v, p, gPZ, gPR, DU, DV, AFpp, ACpp, invACpp, mDot, AF32, AC32};
-    launchPDL(k_pressure, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcU, bcV, bcP, a);
+    if (m.W == 4) launchPDL(k_pressure<4>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcU, bcV, bcP, a);
+    else if (m.W == 3) launchPDL(k_pressure<3>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcU, bcV, bcP, a);
+    else launchPDL(k_pressure<0>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcU, bcV, bcP, a);
 }
 
 void launchPressureRhs(const MeshDev& m, const Ctl* ctl, double rho, const double* mDot, const double* DU,
                        const double* DV, const double* gZ, const double* gR, int cross, int zeroPP, double* bpp,
                        double* pp, cudaStream_t s) {
-    launchPDL(k_pp_rhs, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, rho, mDot, DU, DV, gZ, gR, cross, zeroPP, bpp, pp);
+    if (m.W == 4)
+        launchPDL(k_pp_rhs<4>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, rho, mDot, DU, DV, gZ, gR, cross, zeroPP, bpp, pp);
+    else if (m.W == 3)
+        launchPDL(k_pp_rhs<3>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, rho, mDot, DU, DV, gZ, gR, cross, zeroPP, bpp, pp);
+    else
+        launchPDL(k_pp_rhs<0>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, rho, mDot, DU, DV, gZ, gR, cross, zeroPP, bpp, pp);
 }
 
 void launchJacobi1(const MeshDev& m, const Ctl* ctl, const double* AF, const double* b, const double* inv,

@@ -30,13 +30,12 @@ __global__ void __launch_bounds__(kThreads) k_ir_residual_pp(const Ctl* ctl, Lev
     if (ctl->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= L.N) return;
+    int k[WC];
+    segNeighbours<WC>(L.seg, L.nb, L.N, n, k);
     double Ax = L.AC[n] * L.x[n];
 #pragma unroll
-    for (int j = 0; j < WC; j++) {
-        const size_t s = (size_t)j * L.N + n;
-        const int k = L.nb[s];
-        if (k >= 0) Ax += L.AF[s] * L.x[k];
-    }
+    for (int j = 0; j < WC; j++)
+        if (k[j] >= 0) Ax += L.AF[(size_t)j * L.N + n] * L.x[k[j]];
     const double r = L.b[n] - Ax;
     r32[n] = (float)r;
     if (firstSweep) {
@@ -76,6 +75,7 @@ __global__ void __launch_bounds__(kThreads) k_ir_update(const Ctl* ctl, int N, d
 
 template <int WC>
 __global__ void __launch_bounds__(kThreads) k_ir_residual_uv(int N, int W, const int32_t* __restrict__ snb,
+                                                             const int4* __restrict__ seg,
                                                              const Ctl* ctl, const double* __restrict__ AF,
                                                              const double* __restrict__ ACu,
                                                              const double* __restrict__ ACv,
@@ -91,17 +91,26 @@ __global__ void __launch_bounds__(kThreads) k_ir_residual_uv(int N, int W, const
     if (ctl->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
-    const int nw = WC > 0 ? WC : W;
     double Au = ACu[n] * u[n], Av = ACv[n] * v[n];
+    if (WC > 0) {
+        int k[WC > 0 ? WC : 1];
+        segNeighbours<(WC > 0 ? WC : 1)>(seg, snb, N, n, k);
 #pragma unroll
-    for (int j = 0; j < (WC > 0 ? WC : 32); j++) {
-        if (j >= nw) break;
-        const size_t s = (size_t)j * N + n;
-        const int k = snb[s];
-        if (k >= 0) {
-            const double a = AF[s];
-            Au += a * u[k];
-            Av += a * v[k];
+        for (int j = 0; j < WC; j++)
+            if (k[j] >= 0) {
+                const double a = AF[(size_t)j * N + n];
+                Au += a * u[k[j]];
+                Av += a * v[k[j]];
+            }
+    } else {
+        for (int j = 0; j < W; j++) {
+            const size_t s = (size_t)j * N + n;
+            const int k = snb[s];
+            if (k >= 0) {
+                const double a = AF[s];
+                Au += a * u[k];
+                Av += a * v[k];
+            }
         }
     }
     const float r_u = (float)(bu[n] - Au), r_v = (float)(bv[n] - Av);
@@ -115,6 +124,7 @@ __global__ void __launch_bounds__(kThreads) k_ir_residual_uv(int N, int W, const
 
 template <int WC>
 __global__ void __launch_bounds__(kThreads) k_jacobi_uv32(int N, int W, const int32_t* __restrict__ snb,
+                                                          const int4* __restrict__ seg,
                                                           const Ctl* ctl, const float* __restrict__ AF,
                                                           const float* __restrict__ ru, const float* __restrict__ rv,
                                                           const float* __restrict__ iu, const float* __restrict__ iv,
@@ -127,12 +137,9 @@ __global__ void __launch_bounds__(kThreads) k_jacobi_uv32(int N, int W, const in
     if (WC > 0) {
         int k[WC > 0 ? WC : 1];
         float a[WC > 0 ? WC : 1], gu[WC > 0 ? WC : 1], gv[WC > 0 ? WC : 1];
+        segNeighbours<(WC > 0 ? WC : 1)>(seg, snb, N, n, k);
 #pragma unroll
-        for (int j = 0; j < WC; j++) {
-            const size_t s = (size_t)j * N + n;
-            k[j] = snb[s];
-            a[j] = AF[s];
-        }
+        for (int j = 0; j < WC; j++) a[j] = AF[(size_t)j * N + n];
 #pragma unroll
         for (int j = 0; j < WC; j++) {
             const int c = k[j] >= 0 ? k[j] : n;
@@ -194,13 +201,13 @@ void launchIRResidualUV(const MeshDev& m, const Ctl* ctl, const double* AF, cons
                         const double* bu, const double* bv, const double* u, const double* v, const float* iu32,
                         const float* iv32, float* ru, float* rv, float* du, float* dv, cudaStream_t s) {
     if (m.W == 4)
-        launchPDL(k_ir_residual_uv<4>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF, ACu, ACv, bu, bv, u, v, iu32,
+        launchPDL(k_ir_residual_uv<4>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, m.sseg, ctl, AF, ACu, ACv, bu, bv, u, v, iu32,
                                                                iv32, ru, rv, du, dv);
     else if (m.W == 3)
-        launchPDL(k_ir_residual_uv<3>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF, ACu, ACv, bu, bv, u, v, iu32,
+        launchPDL(k_ir_residual_uv<3>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, m.sseg, ctl, AF, ACu, ACv, bu, bv, u, v, iu32,
                                                                iv32, ru, rv, du, dv);
     else
-        launchPDL(k_ir_residual_uv<0>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF, ACu, ACv, bu, bv, u, v, iu32,
+        launchPDL(k_ir_residual_uv<0>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, m.sseg, ctl, AF, ACu, ACv, bu, bv, u, v, iu32,
                                                                iv32, ru, rv, du, dv);
 }
 
@@ -208,13 +215,13 @@ void launchJacobiUV32(const MeshDev& m, const Ctl* ctl, const float* AF32, const
                       const float* iu32, const float* iv32, const float* du, const float* dv, float* du2, float* dv2,
                       cudaStream_t s) {
     if (m.W == 4)
-        launchPDL(k_jacobi_uv32<4>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF32, ru, rv, iu32, iv32, du, dv,
+        launchPDL(k_jacobi_uv32<4>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, m.sseg, ctl, AF32, ru, rv, iu32, iv32, du, dv,
                                                             du2, dv2);
     else if (m.W == 3)
-        launchPDL(k_jacobi_uv32<3>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF32, ru, rv, iu32, iv32, du, dv,
+        launchPDL(k_jacobi_uv32<3>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, m.sseg, ctl, AF32, ru, rv, iu32, iv32, du, dv,
                                                             du2, dv2);
     else
-        launchPDL(k_jacobi_uv32<0>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, ctl, AF32, ru, rv, iu32, iv32, du, dv,
+        launchPDL(k_jacobi_uv32<0>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m.N, m.W, m.snb, m.sseg, ctl, AF32, ru, rv, iu32, iv32, du, dv,
                                                             du2, dv2);
 }
 

@@ -120,11 +120,9 @@ template <class T, int WC>
 __device__ __forceinline__ T ellAx(const LevelT<T>& L, int n, const T* x, bool jacobiTest) {
     int k[WC];
     T a[WC], g[WC];
+    segNeighbours<WC>(L.seg, L.nb, L.N, n, k);
 #pragma unroll
-    for (int j = 0; j < WC; j++) {
-        k[j] = L.nb[(size_t)j * L.N + n];
-        a[j] = L.AF[(size_t)j * L.N + n];
-    }
+    for (int j = 0; j < WC; j++) a[j] = L.AF[(size_t)j * L.N + n];
 #pragma unroll
     for (int j = 0; j < WC; j++) g[j] = x[k[j] >= 0 ? k[j] : n];
     T Ax = L.AC[n] * x[n];
@@ -155,11 +153,14 @@ __global__ void __launch_bounds__(kThreads) k_mg_smooth_ell(const Ctl* ctl, Leve
 // y = x' + w (b - A x') / A_C, with the expressions and their order of the
 // separate prolongation and sweep kernels, so the result is the same bit for
 // bit; x' itself is never stored (one pass over x instead of three).
+// With upd (the mixed cycle's last finest-level pass), the FP64 iterate the
+// cycle corrects is updated in the same pass, upd[n] += (double)y[n], the
+// arithmetic of the separate refinement update.
 template <class T, int WC>
 __global__ void __launch_bounds__(kThreads) k_mg_prolong_smooth_ell(const Ctl* ctl, LevelT<T> L,
                                                                     const T* __restrict__ x,
                                                                     const T* __restrict__ xc, T* __restrict__ y,
-                                                                    T w, T scale) {
+                                                                    T w, T scale, double* __restrict__ upd) {
     pdlEnter();
     if (ctl->done || ctl->ppSkip) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -169,15 +170,14 @@ __global__ void __launch_bounds__(kThreads) k_mg_prolong_smooth_ell(const Ctl* c
     const T ac = L.AC[n];
     if (fabs(ac) < tiny<T>()) {
         y[n] = xn;
+        if (upd) upd[n] += (double)xn;
         return;
     }
     int k[WC];
     T a[WC], g[WC];
+    segNeighbours<WC>(L.seg, L.nb, L.N, n, k);
 #pragma unroll
-    for (int j = 0; j < WC; j++) {
-        k[j] = L.nb[(size_t)j * L.N + n];
-        a[j] = L.AF[(size_t)j * L.N + n];
-    }
+    for (int j = 0; j < WC; j++) a[j] = L.AF[(size_t)j * L.N + n];
 #pragma unroll
     for (int j = 0; j < WC; j++) {
         const int m = k[j] >= 0 ? k[j] : n;
@@ -187,7 +187,9 @@ __global__ void __launch_bounds__(kThreads) k_mg_prolong_smooth_ell(const Ctl* c
 #pragma unroll
     for (int j = 0; j < WC; j++)
         if (k[j] != -1) Ax += a[j] * g[j];
-    y[n] = xn + w * (L.b[n] - Ax) / ac;
+    const T yn = xn + w * (L.b[n] - Ax) / ac;
+    y[n] = yn;
+    if (upd) upd[n] += (double)yn;
 }
 
 template <class T, int WC>
@@ -356,14 +358,41 @@ __device__ __forceinline__ void gatherFinish(int c, const LevelT<T>& C, T* xCur,
     xAlt[c] = (fabs(ac) < tiny<T>()) ? T(0) : T(0) + w * (sum - ac * T(0)) / ac;
 }
 
+// The restriction with residual, four lanes per coarse cell (aggregates hold
+// four members almost everywhere): lane u of the cell's group forms the
+// residual row of member q0 + 4k + u in round k, so the members' load chains
+// run side by side instead of one after another. Every lane of the group then
+// adds the four residuals in ascending member order to its own running sum,
+// the order of gatherResCell, so the sum is the same bit for bit, and the
+// group's first lane finishes the cell. Rounds are warp-uniform so every lane
+// takes part in every shuffle. (The plain restriction of a stored residual
+// keeps one thread per coarse cell: its two loads per member pipeline well.)
 template <class T>
-__global__ void __launch_bounds__(kThreads) k_mg_gather_res(const Ctl* ctl, LevelT<T> F, const T* __restrict__ xf,
-                                                            LevelT<T> C, T* xCur, T* xAlt, int firstSweep, T w) {
+__global__ void __launch_bounds__(kThreads) k_mg_gather_res4(const Ctl* ctl, LevelT<T> F, const T* __restrict__ xf,
+                                                             LevelT<T> C, T* xCur, T* xAlt, int firstSweep, T w) {
     pdlEnter();
     if (ctl->done || ctl->ppSkip) return;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= C.N) return;
-    gatherResCell(c, F, xf, C, xCur, xAlt, firstSweep, w);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = t >> 2, u = t & 3;
+    const bool live = c < C.N;
+    const int q0 = live ? C.mStart[c] : 0;
+    const int q1 = live ? C.mStart[c + 1] : 0;
+    const int rounds = __reduce_max_sync(0xFFFFFFFFu, (q1 - q0 + 3) >> 2);
+    T sum = T(0);
+    for (int k = 0; k < rounds; k++) {
+        const int q = q0 + 4 * k + u;
+        T r = T(0);
+        if (q < q1) {
+            const int m = C.mList[q];
+            r = residualRow(F, m, xf, F.b[m]);
+        }
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const T rv = __shfl_sync(0xFFFFFFFFu, r, v, 4);
+            if (q0 + 4 * k + v < q1) sum += rv;
+        }
+    }
+    if (live && u == 0) gatherFinish(c, C, xCur, xAlt, firstSweep, w, sum);
 }
 
 // Prolongation fused into the first post-smoothing sweep on any level layout:
@@ -828,15 +857,16 @@ template <class T>
 void launchMGGather(const Ctl* ctl, const LevelT<T>& fine, const LevelT<T>& coarse, T* xCur, T* xAlt, int firstSweep,
                     T w, cudaStream_t s) {
     const int t = tpb(coarse);
-    launchPDL(k_mg_gather<T>, dim3(blocksFor(coarse.N, t)), dim3(t), 0, s, ctl, fine.res, coarse, xCur, xAlt, firstSweep, w);
+    launchPDL(k_mg_gather<T>, dim3(blocksFor(coarse.N, t)), dim3(t), 0, s, ctl, fine.res, coarse, xCur, xAlt,
+              firstSweep, w);
 }
 
 template <class T>
 void launchMGGatherRes(const Ctl* ctl, const LevelT<T>& fine, const T* xFine, const LevelT<T>& coarse, T* xCur,
                        T* xAlt, int firstSweep, T w, cudaStream_t s) {
-    const int t = tpb(coarse);
-    launchPDL(k_mg_gather_res<T>, dim3(blocksFor(coarse.N, t)), dim3(t), 0, s, ctl, fine, xFine, coarse, xCur, xAlt,
-              firstSweep, w);
+    const int t = tpb(coarse);  // a multiple of 32: a cell's four lanes share a warp
+    launchPDL(k_mg_gather_res4<T>, dim3(blocksFor(4LL * coarse.N, t)), dim3(t), 0, s, ctl, fine, xFine, coarse, xCur,
+              xAlt, firstSweep, w);
 }
 
 template <class T>
@@ -856,15 +886,15 @@ void launchMGProlong(const Ctl* ctl, const LevelT<T>& fine, T* xFine, const T* x
 
 template <class T>
 bool launchMGProlongSmooth(const Ctl* ctl, const LevelT<T>& fine, const T* xFine, const T* xCoarse, T* y, T w,
-                           T scale, cudaStream_t s) {
+                           T scale, cudaStream_t s, double* upd) {
     if (fine.sliceOff || !fine.c2c) return false;
     const int t = tpb(fine);
     if (fine.W == 4)
         launchPDL(k_mg_prolong_smooth_ell<T, 4>, dim3(blocksFor(fine.N, t)), dim3(t), 0, s, ctl, fine, xFine,
-                  xCoarse, y, w, scale);
+                  xCoarse, y, w, scale, upd);
     else if (fine.W == 3)
         launchPDL(k_mg_prolong_smooth_ell<T, 3>, dim3(blocksFor(fine.N, t)), dim3(t), 0, s, ctl, fine, xFine,
-                  xCoarse, y, w, scale);
+                  xCoarse, y, w, scale, upd);
     else
         return false;
     return true;
@@ -946,7 +976,8 @@ template void launchGalerkinChain<float>(const Ctl*, const GalChainArgsT<float>&
     template void launchMGResidual<T>(const Ctl*, const LevelT<T>&, const T*, cudaStream_t);                    \
     template void launchMGGather<T>(const Ctl*, const LevelT<T>&, const LevelT<T>&, T*, T*, int, T, cudaStream_t); \
     template void launchMGProlong<T>(const Ctl*, const LevelT<T>&, T*, const T*, T, cudaStream_t);                 \
-    template bool launchMGProlongSmooth<T>(const Ctl*, const LevelT<T>&, const T*, const T*, T*, T, T, cudaStream_t); \
+    template bool launchMGProlongSmooth<T>(const Ctl*, const LevelT<T>&, const T*, const T*, T*, T, T, cudaStream_t, \
+                                           double*);                                                             \
     template void launchMGTerminal<T>(const Ctl*, const LevelT<T>&, T*, T, int, cudaStream_t);                  \
     template bool launchMGResident<T>(Ctl*, const ResidentArgsT<T>&, cudaStream_t);                              \
     template void launchMGGatherRes<T>(const Ctl*, const LevelT<T>&, const T*, const LevelT<T>&, T*, T*, int, T,     \

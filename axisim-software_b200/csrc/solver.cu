@@ -159,6 +159,7 @@ public:
         destroyGraph();
         if (stream_) cudaStreamSynchronize(stream_);
         meshArena_.release();
+        segArena_.release();
         mgArena_.release();
         bcArena_.release();
         if (hostStop_) cudaFreeHost((void*)hostStop_);
@@ -480,6 +481,7 @@ public:
         colorN_ = 0;
         releaseScalarBuffers();
         meshArena_.release();
+        segArena_.release();
         meshType_ = AXISIM_MESH_UNSTRUCTURED;
         N_ = N;
         F_ = F;
@@ -533,8 +535,36 @@ public:
         ph.reset(new PhaseTimer(*this, "mesh_precompute_ell"));
         launchPrecompute(m, dCfs, dCfi, tz, tr, stream_);
         launchBuildEll(N, W, dCfs, dCfi, m.owner, m.neighbor, sface, snb, stream_);
+        segCounts_[0] = segCounts_[1] = (N + 31) / 32;
+        nSeg_ = (N + 31) / 32;
+        m.sseg = nullptr;
+        m.ssegF = nullptr;
+        m.ssegM = nullptr;
+        if (W == 3 || W == 4) {
+            Arena& B = segArena_;
+            B.reserve((size_t)nSeg_ * (16 + 16 + 4) + 3 * 256);
+            int4* seg = B.alloc<int4>((size_t)nSeg_);
+            int4* segF = B.alloc<int4>((size_t)nSeg_);
+            int* segM = B.alloc<int>((size_t)nSeg_ + 2);
+            int* nIrr = segM + nSeg_;  // [0] without slot offsets, [1] without affine faces
+            CK(cudaMemsetAsync(nIrr, 0, 2 * sizeof(int), stream_));
+            launchBuildSegments(m, seg, segF, segM, nIrr, stream_);
+            CK(cudaMemcpyAsync(segCounts_, nIrr, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+            m.sseg = seg;
+            m.ssegF = segF;
+            m.ssegM = segM;
+        }
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(stream_));
+        segIrregular_ = m.sseg ? segCounts_[0] : nSeg_;
+        if (m.sseg && 2 * segIrregular_ > nSeg_) {
+            // mostly irregular numbering (unstructured cells): the segment test
+            // would only put a load ahead of every slot neighbour read
+            m.sseg = nullptr;
+            m.ssegF = nullptr;
+            m.ssegM = nullptr;
+            segArena_.release();
+        }
         ph.reset(new PhaseTimer(*this, "fields_alloc"));
         // fields and coefficient systems (allocateSimple / allocateCoefficients)
         const size_t WN = (size_t)W * N;
@@ -846,8 +876,11 @@ private:
     // mesh
     bool haveMesh_ = false;
     int N_ = 0, F_ = 0, S_ = 0, W_ = 0;
+    int nSeg_ = 0, segIrregular_ = 0;  // 32-cell segments of the mesh; those without shared slot offsets
+    int segCounts_[2] = {0, 0};        // segments without slot offsets, without affine faces
     HostI32 hCfs_, hCfi_, hOwner_, hNeighbor_;
     Arena meshArena_, mgArena_, bcArena_;
+    Arena segArena_;  // the mesh's segment tables, kept only when the kernels use them
     // momentum Jacobi sweeps per launch out of shared memory (1: one launch
     // per sweep), CTA size of those launches, and the tiles they run on
     int sweepsPerLaunch_ = 1;
@@ -962,6 +995,15 @@ private:
     }
 
 public:
+    // The 32-cell segment tables of the mesh (segNeighbours / slotFaces).
+    void meshSegments(int32_t* nSeg, int32_t* nOffsets, int32_t* nFaces, int32_t* inUse) const {
+        if (!haveMesh_) throw StatusError(AXISIM_E_STATE, "no mesh");
+        if (nSeg) *nSeg = nSeg_;
+        if (nOffsets) *nOffsets = nSeg_ - segCounts_[0];
+        if (nFaces) *nFaces = nSeg_ - segCounts_[1];
+        if (inUse) *inUse = mesh_.sseg ? 1 : 0;
+    }
+
     int setupProfile(axisim_kernel_stat* out, int maxOut, int reset) {
         const int n = (int)phases_.size();
         for (int i = 0; i < n && i < maxOut; i++) {
@@ -1150,6 +1192,7 @@ private:
                 d.W = W_;
                 d.totalSlots = W_ * N_;
                 d.nb = const_cast<int32_t*>(mesh_.snb);
+                d.seg = mesh_.sseg;
                 d.AF = AFpp_;
                 d.AC = ACpp_;
                 d.b = bpp_;
@@ -1279,6 +1322,8 @@ private:
     }
     int tailStart_ = -1;
     bool galerkinThisSolve_ = true;  // false: the coarse operators of this p' solve are already built
+    double* irUpdate_ = nullptr;     // set during a mixed refinement cycle: the FP64 iterate it corrects
+    bool irUpdated_ = false;         // the cycle's last finest-level pass applied the correction
 
     // FP32 p' hierarchy: used by the mixed-precision cycle and as the
     // preconditioner of the flexible CG solve in either precision
@@ -1384,6 +1429,7 @@ private:
             f.totalSlots = d.totalSlots;
             f.sliceOff = d.sliceOff;
             f.nb = d.nb;
+            f.seg = d.seg;
             f.c2c = d.c2c;
             f.mStart = d.mStart;
             f.mList = d.mList;
@@ -1430,7 +1476,7 @@ private:
             T* x = cur[(size_t)l];
             T* y = alt[(size_t)l];
             emit<T>(kOpSmooth, l, x, y, 0, 0.0, 0, std::string(l == 0 ? "mg_smooth_l0" : "mg_smooth") + tag,
-                    (double)L.N * ((4.0 + sizeof(T)) * L.W + 4.0 * sizeof(T)),
+                    (double)L.N * ((double)sizeof(T) * L.W + 4.0 * sizeof(T)) + slotIndexBytes(L),
                     [&] { launchMGSmooth<T>(ctl_, L, x, y, w, stream_); });
             std::swap(cur[(size_t)l], alt[(size_t)l]);
         }
@@ -1505,7 +1551,8 @@ private:
         if (!gatherRes) {
             T* x = cur[(size_t)l];
             emit<T>(kOpResidual, l, x, nullptr, 0, 0.0, 0, std::string("mg_residual") + tag,
-                    (double)F.N * ((4.0 + vb) * F.W + 4.0 * vb), [&] { launchMGResidual<T>(ctl_, F, x, stream_); });
+                    (double)F.N * (vb * F.W + 4.0 * vb) + slotIndexBytes(F),
+                    [&] { launchMGResidual<T>(ctl_, F, x, stream_); });
         }
         // level l + 1's operator is read from here on; the tail reads every
         // level below it as well
@@ -1602,14 +1649,17 @@ private:
             T* y = alt[(size_t)l];
             const T sc = (T)curProlong_;
             emit<T>(kOpProlongSmooth, l, x, xc, 0, (double)sc, 0, std::string("mg_prolong_smooth") + tag,
-                    (double)F.N * ((4.0 + vb) * F.W + 4.0 + 4.0 * vb) + vb * C.N,
+                    (double)F.N * (vb * F.W + 4.0 + 4.0 * vb) + slotIndexBytes(F) + vb * C.N,
                     [&] { launchMGProlongSmoothAny<T>(ctl_, F, x, xc, y, w, sc, stream_); }, y);
             std::swap(cur[(size_t)l], alt[(size_t)l]);
             smoothT<T>(lv, l, post - 1, cur, alt);
         } else if (fusedEll && launchMGProlongSmooth<T>(ctl_, F, cur[(size_t)l], cur[(size_t)l + 1], alt[(size_t)l], w,
-                                                        (T)curProlong_, stream_)) {
-            markL(std::string("mg_prolong_smooth") + tag, l,
-                 (double)F.N * ((4.0 + vb) * F.W + 4.0 + 4.0 * vb) + vb * C.N);
+                                                        (T)curProlong_, stream_,
+                                                        (l == 0 && post == 1) ? irUpdate_ : nullptr)) {
+            const bool ir = l == 0 && post == 1 && irUpdate_;
+            markL(std::string(ir ? "mg_prolong_smooth_ir" : "mg_prolong_smooth") + tag, l,
+                 (double)F.N * (vb * F.W + 4.0 + 4.0 * vb + (ir ? 16.0 : 0.0)) + slotIndexBytes(F) + vb * C.N);
+            if (ir) irUpdated_ = true;
             std::swap(cur[(size_t)l], alt[(size_t)l]);
             smoothT<T>(lv, l, post - 1, cur, alt);
         } else {
@@ -1714,6 +1764,17 @@ private:
         if (tailStart_ < 2 || L - tailStart_ + 1 > kMaxTail + 1) return L;
         return tailStart_;
     }
+    // Neighbour-index bytes one pass over the mesh's slots reads: the segment
+    // offsets plus the slot neighbours of the irregular segments where the
+    // mesh has segment offsets, else the whole [W][N] block.
+    double meshSlotIndexBytes() const {
+        if (!mesh_.sseg) return 4.0 * W_ * N_;
+        return 16.0 * nSeg_ + 4.0 * W_ * 32.0 * segIrregular_;
+    }
+    template <class T>
+    double slotIndexBytes(const LevelT<T>& L) const {
+        return L.seg ? meshSlotIndexBytes() : 4.0 * L.W * L.N;
+    }
     template <class T>
     static double galerkinBytes(const LevelT<T>& f, const LevelT<T>& c) {
         return (double)f.N * ((double)sizeof(T) * (1.0 + f.W) + 4.0) + (12.0 + sizeof(T)) * c.totalSlots +
@@ -1749,10 +1810,17 @@ private:
                 alt[(size_t)l] = levels32_[(size_t)l].xNew;
             }
             launchIRResidualPP(ctl_, levels_[0], r32pp_, cur[0], cmg_.weight, firstSweep ? 1 : 0, stream_);
-            mark("ir_residual_pp", (double)N_ * (12.0 * W_ + 32.0 + 8.0));
+            mark("ir_residual_pp", (double)N_ * (8.0 * W_ + 32.0 + 8.0) + slotIndexBytes(levels_[0]));
+            // the cycle's last finest-level pass, when it is the fused
+            // prolongation and sweep, also adds the correction to p'
+            irUpdate_ = pp_;
+            irUpdated_ = false;
             vcycleT<float>(levels32_, 0, cur, alt, firstSweep);
-            launchIRUpdatePP(ctl_, N_, pp_, cur[0], stream_);
-            mark("ir_update_pp", 20.0 * N_);
+            irUpdate_ = nullptr;
+            if (!irUpdated_) {
+                launchIRUpdatePP(ctl_, N_, pp_, cur[0], stream_);
+                mark("ir_update_pp", 20.0 * N_);
+            }
         }
     }
 
@@ -2004,7 +2072,7 @@ private:
             // correction form: FP64 residual, FP32 Jacobi sweeps on the correction, FP64 update
             launchIRResidualUV(mesh_, ctl_, AFm_, ACu_, ACv_, bu_, bv_, u_, v_, iu32_, iv32_, ru32_, rv32_, du32_[0],
                                dv32_[0], stream_);
-            mark("ir_residual_uv", (double)N_ * (12.0 * W_ + 64.0 + 24.0));
+            mark("ir_residual_uv", (double)N_ * (8.0 * W_ + 64.0 + 24.0) + meshSlotIndexBytes());
             int c = 0;
             const int rest = iters - 1;
             if (tiles_.nTiles > 0 && rest > 1) {
@@ -2021,7 +2089,7 @@ private:
                 for (int k = 1; k < iters; k++) {
                     launchJacobiUV32(mesh_, ctl_, AF32m_, ru32_, rv32_, iu32_, iv32_, du32_[c], dv32_[c],
                                      du32_[1 - c], dv32_[1 - c], stream_);
-                    mark("jacobi_uv32", (double)N_ * (8.0 * W_ + 32.0));
+                    mark("jacobi_uv32", (double)N_ * (4.0 * W_ + 32.0) + meshSlotIndexBytes());
                     c = 1 - c;
                 }
             }
@@ -2041,7 +2109,7 @@ private:
             } else {
                 for (int k = 0; k < iters; k++) {
                     launchJacobiUV(mesh_, ctl_, AFm_, bu_, bv_, iu_, iv_, lu, lv, su, sv, stream_);
-                    mark("jacobi_uv", (double)N_ * (12.0 * W_ + 64.0));
+                    mark("jacobi_uv", (double)N_ * (8.0 * W_ + 64.0) + meshSlotIndexBytes());
                     std::swap(lu, su);
                     std::swap(lv, sv);
                 }
@@ -3281,6 +3349,16 @@ int axisim_setup_profile(axisim_handle* h, axisim_kernel_stat* out, int32_t maxO
         if (!out || maxOut < 1) throw StatusError(AXISIM_E_ARG, "bad setup profile arguments");
         const int n = h->s->setupProfile(out, maxOut, reset);
         if (nOut) *nOut = n;
+        return AXISIM_OK;
+    });
+}
+
+int axisim_mesh_segments(axisim_handle* h, int32_t* nSegments, int32_t* nOffsetSegments, int32_t* nFaceSegments,
+                         int32_t* inUse) {
+    if (!h) return AXISIM_E_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    return guarded(h, [&] {
+        h->s->meshSegments(nSegments, nOffsetSegments, nFaceSegments, inUse);
         return AXISIM_OK;
     });
 }

@@ -465,6 +465,17 @@ int axisim_profile_levels(axisim_handle* h, int32_t iterations, axisim_kernel_st
  * entry reuses axisim_kernel_stat: `launches` counts the stage's calls, `ms`
  * is their total, `bytes` is 0. reset != 0 clears the record after reading. */
 int axisim_setup_profile(axisim_handle* h, axisim_kernel_stat* out, int32_t maxOut, int32_t* nOut, int32_t reset);
+/* New; no counterpart in the reference. The mesh's 32-cell segments (cells
+ * 32s .. 32s + 31) as set_mesh classified them for the kernels on its slots:
+ * nOffsetSegments have every slot's neighbour at one offset from the cell for
+ * all 32 cells (no boundary slot), so the sweeps form the neighbour indices
+ * instead of loading them; nFaceSegments of those also number each slot's face
+ * affinely (stride 1 or 2) with the cell on the same side of it, so the
+ * assembly kernels form the face, owner and neighbour too. inUse is 0 when the
+ * tables are not used: a mesh with more than four faces per cell, or with
+ * fewer than half its segments regular. Any argument may be NULL. */
+int axisim_mesh_segments(axisim_handle* h, int32_t* nSegments, int32_t* nOffsetSegments, int32_t* nFaceSegments,
+                         int32_t* inUse);
 
 /* New; no counterpart in the reference. The SIMPLE residuals of caller-owned
  * device arrays, computed with the same arithmetic as a solve's residual step
