@@ -425,6 +425,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_momentum(MeshDev m, const Ctl* 
         }
     }
     double ACu = 0.0, ACv = 0.0, bu = 0.0, bv = 0.0, netF = 0.0;
+    // WC > 0: the slots' coefficients are stored after the loop, so no store
+    // sits between one slot's loads and the next's
+    double afv[P];
+    bool wr[P];
+#pragma unroll
+    for (int j = 0; j < P; j++) wr[j] = false;
 #pragma unroll
     for (int j = 0; j < (WC > 0 ? WC : 32); j++) {
         if (WC == 0 && j >= m.W) break;
@@ -464,14 +470,33 @@ __global__ void __launch_bounds__(kThreads, 4) k_momentum(MeshDev m, const Ctl* 
                     bv -= F * (hoV - udV);
                 }
             }
-            a.AF[s] = af;
-            if (a.AF32) a.AF32[s] = (float)af;
+            if (WC > 0) {
+                afv[j] = af;
+                wr[j] = true;
+            } else {
+                a.AF[s] = af;
+                if (a.AF32) a.AF32[s] = (float)af;
+            }
         } else {
-            a.AF[s] = 0.0;
-            if (a.AF32) a.AF32[s] = 0.f;
+            if (WC > 0) {
+                afv[j] = 0.0;
+                wr[j] = true;
+            } else {
+                a.AF[s] = 0.0;
+                if (a.AF32) a.AF32[s] = 0.f;
+            }
             momentumBoundary(m, n, f, area, F, a.mu, bcU, ACu, bu);
             momentumBoundary(m, n, f, area, F, a.mu, bcV, ACv, bv);
         }
+    }
+    if (WC > 0) {
+#pragma unroll
+        for (int j = 0; j < P; j++)
+            if (wr[j]) {
+                const size_t s = (size_t)j * N + n;
+                a.AF[s] = afv[j];
+                if (a.AF32) a.AF32[s] = (float)afv[j];
+            }
     }
     if (a.conv) {
         ACu -= netF;
