@@ -127,10 +127,17 @@ template <int WC>
 __device__ __forceinline__ void slotFaces(const MeshDev& m, int n, int (&f)[WC], int (&own)[WC], int (&nb)[WC]) {
     static_assert(WC >= 1 && WC <= 4, "segment faces cover four slots");
     const int s = n >> 5;
-    const int meta = m.ssegM ? __ldg(m.ssegM + s) : -1;
+    // the segment's three entries are loaded together (the tables exist as a
+    // set), so the test below does not put a second load round trip ahead of
+    // the face numbers
+    int meta = -1;
+    int4 d = make_int4(0, 0, 0, 0), b = make_int4(0, 0, 0, 0);
+    if (m.ssegM) {
+        meta = __ldg(m.ssegM + s);
+        d = __ldg(m.sseg + s);
+        b = __ldg(m.ssegF + s);
+    }
     if (meta >= 0) {
-        const int4 d = __ldg(m.sseg + s);
-        const int4 b = __ldg(m.ssegF + s);
         const int r = n & 31;
         const int dd[4] = {d.x, d.y, d.z, d.w}, bb[4] = {b.x, b.y, b.z, b.w};
 #pragma unroll
