@@ -782,7 +782,10 @@ __global__ void __launch_bounds__(kThreads) k_pressure(MeshDev m, const Ctl* ctl
 }
 
 // createPPRhs (simple.cu:90-142) + the p' reset before the corrector loop
-template <int WC>
+// NO: the cross-diffusion (non-orthogonal) term off (0) or on (1) at compile
+// time, or read from the arguments (2); the fixed forms leave the other
+// branch's registers out (32 instead of 60 registers on quads without it).
+template <int WC, int NO>
 __global__ void __launch_bounds__(kThreads) k_pp_rhs(MeshDev m, const Ctl* ctl, double rho, const double* mDot,
                                                      const double* DU, const double* DV, const double* gZ,
                                                      const double* gR, int cross, int zeroPP, double* bpp,
@@ -805,7 +808,7 @@ __global__ void __launch_bounds__(kThreads) k_pp_rhs(MeshDev m, const Ctl* ctl, 
         const double md = mDot[f];
         if (own == n) imb += md;
         else if (nb == n) imb -= md;
-        if (cross) {
+        if (NO == 2 ? cross != 0 : NO == 1) {
             const double Df = interpCorr(m, DU, DV, n, f, own, nb);
             crossSum += nonOrthoFlux(m, n, f, own, nb, gZ, gR, rho * Df);
         }
@@ -832,7 +835,7 @@ struct CorrectArgs {
 
 // WC > 0: the slot count at compile time; every slot's face id, owner,
 // neighbour and area are loaded before the first store.
-template <int WC>
+template <int WC, int NO>  // NO as k_pp_rhs's, for the non-orthogonal flux correction
 __global__ void __launch_bounds__(kThreads) k_correct(MeshDev m, const Ctl* ctl, BCDev bcP, CorrectArgs a) {
     pdlEnter();
     if (ctl->done) return;
@@ -868,7 +871,7 @@ __global__ void __launch_bounds__(kThreads) k_correct(MeshDev m, const Ctl* ctl,
         if (nb >= 0) {
             double md = a.mDot[f];
             md -= rho * area * Df * (a.pp[nb] - a.pp[n]) * m.invDPN[f];
-            if (a.nonOrtho) md -= nonOrthoFlux(m, n, f, own, nb, a.gZ, a.gR, rho * Df);
+            if (NO == 2 ? a.nonOrtho != 0 : NO == 1) md -= nonOrthoFlux(m, n, f, own, nb, a.gZ, a.gR, rho * Df);
             a.mDot[f] = md;
             continue;
         }
@@ -1289,11 +1292,17 @@ void launchPressureRhs(const MeshDev& m, const Ctl* ctl, double rho, const doubl
                        const double* DV, const double* gZ, const double* gR, int cross, int zeroPP, double* bpp,
                        double* pp, cudaStream_t s) {
     if (m.W == 4)
-        launchPDL(k_pp_rhs<4>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, rho, mDot, DU, DV, gZ, gR, cross, zeroPP, bpp, pp);
+        cross ? launchPDL(k_pp_rhs<4, 1>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, rho, mDot, DU, DV, gZ, gR, cross,
+                          zeroPP, bpp, pp)
+              : launchPDL(k_pp_rhs<4, 0>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, rho, mDot, DU, DV, gZ, gR, cross,
+                          zeroPP, bpp, pp);
     else if (m.W == 3)
-        launchPDL(k_pp_rhs<3>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, rho, mDot, DU, DV, gZ, gR, cross, zeroPP, bpp, pp);
+        cross ? launchPDL(k_pp_rhs<3, 1>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, rho, mDot, DU, DV, gZ, gR, cross,
+                          zeroPP, bpp, pp)
+              : launchPDL(k_pp_rhs<3, 0>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, rho, mDot, DU, DV, gZ, gR, cross,
+                          zeroPP, bpp, pp);
     else
-        launchPDL(k_pp_rhs<0>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, rho, mDot, DU, DV, gZ, gR, cross, zeroPP, bpp, pp);
+        launchPDL(k_pp_rhs<0, 2>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, rho, mDot, DU, DV, gZ, gR, cross, zeroPP, bpp, pp);
 }
 
 void launchJacobi1(const MeshDev& m, const Ctl* ctl, const double* AF, const double* b, const double* inv,
@@ -1310,9 +1319,12 @@ void launchCorrect(const MeshDev& m, const Ctl* ctl, const BCDev& bcP, double rh
                    const double* pp, const double* gZ, const double* gR, const double* DU, const double* DV, double* u,
                    double* v, double* p, double* mDot, cudaStream_t s) {
     CorrectArgs a{rho, alphaP, nonOrtho, pp, gZ, gR, DU, DV, u, v, p, mDot};
-    if (m.W == 4) launchPDL(k_correct<4>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcP, a);
-    else if (m.W == 3) launchPDL(k_correct<3>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcP, a);
-    else launchPDL(k_correct<0>, dim3(blocksFor(m.N)), dim3(kThreads), 0, s, m, ctl, bcP, a);
+    const dim3 g(blocksFor(m.N)), t(kThreads);
+    if (m.W == 4 && nonOrtho) launchPDL(k_correct<4, 1>, g, t, 0, s, m, ctl, bcP, a);
+    else if (m.W == 4) launchPDL(k_correct<4, 0>, g, t, 0, s, m, ctl, bcP, a);
+    else if (m.W == 3 && nonOrtho) launchPDL(k_correct<3, 1>, g, t, 0, s, m, ctl, bcP, a);
+    else if (m.W == 3) launchPDL(k_correct<3, 0>, g, t, 0, s, m, ctl, bcP, a);
+    else launchPDL(k_correct<0, 2>, g, t, 0, s, m, ctl, bcP, a);
 }
 
 void launchResiduals(const MeshDev& m, const Ctl* ctl, const double* AF, const double* ACu, const double* ACv,
