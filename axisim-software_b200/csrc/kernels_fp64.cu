@@ -213,7 +213,9 @@ struct GradArgs {
 // least-squares loop and their other-cell values are loaded ahead, in
 // registers, with a few spills from three fields up, which measured faster
 // than 2 CTAs per SM without spills).
-template <int NF>
+// SCH: the scheme at compile time (0 Green-Gauss, 1 least squares) so the
+// other scheme's registers stay out, or 2 to read it from `scheme`.
+template <int NF, int SCH>
 __global__ void __launch_bounds__(kThreads, NF == 1 ? 4 : 3) k_gradient(MeshDev m, const Ctl* ctl, GradArgs a,
                                                                        int scheme) {
     pdlEnter();
@@ -221,7 +223,7 @@ __global__ void __launch_bounds__(kThreads, NF == 1 ? 4 : 3) k_gradient(MeshDev 
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m.N) return;
     const int N = m.N;
-    if (scheme == 0) {
+    if (SCH == 2 ? scheme == 0 : SCH == 0) {
         double gz[NF], gr[NF], axisPhi[NF];
         double clZ = 0.0, clR = 0.0;
         bool hasAxis = false;
@@ -266,7 +268,7 @@ __global__ void __launch_bounds__(kThreads, NF == 1 ? 4 : 3) k_gradient(MeshDev 
             a.gZ[q][n] = gz[q] * inv;
             a.gR[q][n] = gr[q] * inv;
         }
-    } else if (scheme == 1) {
+    } else if (SCH == 2 ? scheme == 1 : SCH == 1) {
         double bz[NF], br[NF], phiP[NF];
         for (int q = 0; q < NF; q++) {
             bz[q] = br[q] = 0.0;
@@ -1241,11 +1243,16 @@ void launchGradient(const MeshDev& m, const Ctl* ctl, int nFields, const double*
         a.gR[q] = gR[q];
     }
     const int b = blocksFor(m.N);
-    if (nFields == 1) launchPDL(k_gradient<1>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme);
-    else if (nFields == 2) launchPDL(k_gradient<2>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme);
-    else if (nFields == 3) launchPDL(k_gradient<3>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme);
-    else if (nFields == 4) launchPDL(k_gradient<4>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme);
-    else launchPDL(k_gradient<5>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme);
+#define AXISIM_GRAD(NF)                                                                                         \
+    (scheme == 1   ? launchPDL(k_gradient<NF, 1>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme)                 \
+     : scheme == 0 ? launchPDL(k_gradient<NF, 0>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme)                 \
+                   : launchPDL(k_gradient<NF, 2>, dim3(b), dim3(kThreads), 0, s, m, ctl, a, scheme))
+    if (nFields == 1) AXISIM_GRAD(1);
+    else if (nFields == 2) AXISIM_GRAD(2);
+    else if (nFields == 3) AXISIM_GRAD(3);
+    else if (nFields == 4) AXISIM_GRAD(4);
+    else AXISIM_GRAD(5);
+#undef AXISIM_GRAD
 }
 
 void launchMomentum(const MeshDev& m, const Ctl* ctl, const BCDev& bcU, const BCDev& bcV, const MomentumArgs& a,
