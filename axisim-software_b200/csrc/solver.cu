@@ -1771,6 +1771,15 @@ private:
         if (!mesh_.sseg) return 4.0 * W_ * N_;
         return 16.0 * nSeg_ + 4.0 * W_ * 32.0 * segIrregular_;
     }
+    // Face-id, owner and neighbour bytes an assembly pass (momentum, pressure,
+    // p' right-hand side, correction, residual, least-squares gradient) does
+    // not read where the segment tables give them (slotFaces): the slot's face
+    // id and its half of the face's owner and neighbour, for every slot of the
+    // segments with affine faces, less the tables' 36 bytes per segment.
+    double faceIndexSaving() const {
+        if (!mesh_.ssegM) return 0.0;
+        return 8.0 * W_ * 32.0 * (nSeg_ - segCounts_[1]) - 36.0 * nSeg_;
+    }
     template <class T>
     double slotIndexBytes(const LevelT<T>& L) const {
         return L.seg ? meshSlotIndexBytes() : 4.0 * L.W * L.N;
@@ -2038,7 +2047,7 @@ private:
                         phi[nf] = sb_[q].phi; bc[nf] = bcS_[q]; gz[nf] = sb_[q].gZ; gr[nf] = sb_[q].gR; nf++;
                     }
             launchGradient(mesh_, ctl_, nf, phi, bc, gz, gr, grad, stream_);
-            mark("gradient", gradBytes(nf, grad));
+            mark("gradient", gradBytes(nf, grad) - (grad == 1 ? faceIndexSaving() : 0.0));
         }
         MomentumArgs a{};
         a.mDot = mDot_; a.u = u_; a.v = v_; a.gUZ = gUZ_; a.gUR = gUR_; a.gVZ = gVZ_; a.gVR = gVR_;
@@ -2055,7 +2064,7 @@ private:
             double face = 32.0 + (scheme == 1 ? 8.0 : scheme == 2 ? 16.0 : 0.0);
             double cell = 4.0 * W_ + 16.0 + 16.0 + 16.0 + 8.0 * W_ + 64.0 + (scheme == 2 ? 40.0 : 0.0);
             if (cs_.transient) cell += 32.0;
-            mark("momentum", face * F_ + cell * N_);
+            mark("momentum", face * F_ + cell * N_ - faceIndexSaving());
         }
         // momentum solves (LinearSolver::run for u then v; fused, identical arithmetic)
         const int iters = cs_.linearMaxIter;
@@ -2123,7 +2132,7 @@ private:
         const bool mixedPP = fp32PressureCycle();
         launchPressureSystem(mesh_, ctl_, bc_[0], bc_[1], bc_[2], fluid_.rho, u_, v_, p_, gPZ_, gPR_, DU_, DV_, AFpp_,
                              ACpp_, ipp_, mDot_, mixedPP ? AF32pp_ : nullptr, mixedPP ? AC32pp_ : nullptr, stream_);
-        mark("pressure_rhiechow", 56.0 * F_ + (12.0 * W_ + 72.0) * N_);
+        mark("pressure_rhiechow", 56.0 * F_ + (12.0 * W_ + 72.0) * N_ - faceIndexSaving());
         for (int corr = 0; corr <= nonOrtho; corr++) {
             const int cross = corr > 0;
             if (cross) {
@@ -2131,12 +2140,12 @@ private:
                 double* gz[1] = {gPZ_};
                 double* gr[1] = {gPR_};
                 launchGradient(mesh_, ctl_, 1, phi, &bc_[3], gz, gr, grad, stream_);
-                mark("gradient_pp", gradBytes(1, grad));
+                mark("gradient_pp", gradBytes(1, grad) - (grad == 1 ? faceIndexSaving() : 0.0));
             }
             galerkinThisSolve_ = corr == 0;
             forkGalerkin();
             launchPressureRhs(mesh_, ctl_, fluid_.rho, mDot_, DU_, DV_, gPZ_, gPR_, cross, corr == 0, bpp_, pp_, stream_);
-            mark("pp_rhs", 16.0 * F_ + (4.0 * W_ + 16.0) * N_);
+            mark("pp_rhs", 16.0 * F_ + (4.0 * W_ + 16.0) * N_ - faceIndexSaving());
             // the non-orthogonal corrector's pass solves the same p' operator
             // with a new right-hand side: its coarse operators are the ones
             // the first pass built
@@ -2157,11 +2166,11 @@ private:
             double* gz[1] = {gPZ_};
             double* gr[1] = {gPR_};
             launchGradient(mesh_, ctl_, 1, phi, &bc_[3], gz, gr, grad, stream_);
-            mark("gradient_pp", gradBytes(1, grad));
+            mark("gradient_pp", gradBytes(1, grad) - (grad == 1 ? faceIndexSaving() : 0.0));
         }
         launchCorrect(mesh_, ctl_, bc_[2], fluid_.rho, alphaP_, nonOrtho, pp_, gPZ_, gPR_, DU_, DV_, u_, v_, p_, mDot_,
                       stream_);
-        mark("correct_massflux", 64.0 * F_ + (88.0 + 4.0 * W_) * N_);
+        mark("correct_massflux", 64.0 * F_ + (88.0 + 4.0 * W_) * N_ - faceIndexSaving());
         // energy and concentration (solver.cpp:1218-1238): both assembled in one
         // pass (each system depends only on its own field, mDot and the mesh),
         // then each solved with the momentum linear solver
@@ -2214,7 +2223,8 @@ private:
         }
         launchResiduals(mesh_, ctl_, AFm_, ACu_, ACv_, bu_, bv_, u_, v_, mDot_, resU_, resV_, resC_, scU_, scV_,
                         partial_, &residualBlocks_, stream_);
-        mark("residual", 16.0 * F_ + (16.0 * W_ + 88.0) * N_);
+        mark("residual", 16.0 * F_ + (12.0 * W_ + 88.0) * N_ + meshSlotIndexBytes() - 16.0 * nSeg_ * (mesh_.sseg ? 1 : 0) -
+                             faceIndexSaving());
         const bool monitorS = (solveS_[0] && sres_[0].enabled) || (solveS_[1] && sres_[1].enabled);
         if (monitorS) {
             const double* AF[2];
